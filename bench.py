@@ -1,0 +1,482 @@
+#!/usr/bin/env python
+"""Throughput of the plain WCSPH step: particle-steps/s at 1M particles.
+
+Workload (default ``tank_1m``): 1,048,576 fp32 particles as a 128x128x64
+jittered lattice block (spacing 0.005 m, jitter +-0.1 spacing, seed rule of
+ModelBuilder.add_particle_grid) in the corner of a 2x1x1 m tank, initial
+velocities N(0, 0.01 m/s) per component (numpy default_rng(2)), h = 2 x
+spacing, rho0 = 1000, Tait gamma = 7, c0 = 20 m/s, XSPH 0.01, gravity -9.81,
+dt = 5e-5 s. Synthetic data, generated on the host like the reference's
+builder.
+
+One step = one SolverSPH.step (grid build, density/EOS pass,
+force/XSPH/integrate pass), replayed from a CUDA graph captured per step.
+Between timed steps L2 is flushed by writing a 256 MiB buffer (outside the
+timed intervals); each step is timed on the device with CUDA events recorded
+inside the graph, which also split it into build / density / force phases.
+
+Multi-GPU: the step does not shard (a single scene); ``--gpus N`` runs N
+independent replicas, one per rank, timed as the max over ranks.
+
+``--impl reference`` times the CPU restatement of the path (the oracle,
+OpenMP on all host cores) on the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+if str(REPO) not in sys.path:
+    sys.path.insert(0, str(REPO))
+
+METRIC = "particle-steps/s"
+B_ALG_STEP = 64  # algorithmic HBM bytes per particle-step (read x,v 24 + write x,v 24 + density 8 + cell key 8)
+# algorithmic bytes per particle of each single-kernel pass (unique data it must move)
+B_ALG_DENSITY = 12 + 8  # read x; write (m/rho, p/rho^2)
+B_ALG_FORCE = 24 + 8 + 24  # read x, v; read density scratch; write x, v
+
+WORKLOADS = {
+    "tank_1m": dict(shape=(128, 128, 64), spacing=0.005, box=(2.0, 1.0, 1.0), dt=5e-5, vel_std=0.01,
+                    desc="1,048,576 particles, 128x128x64 block at 0.005 m in a 2x1x1 m tank"),
+    "tank_2m": dict(shape=(128, 128, 128), spacing=0.005, box=(2.0, 1.0, 1.0), dt=5e-5, vel_std=0.01,
+                    desc="2,097,152 particles, 128^3 block at 0.005 m in a 2x1x1 m tank"),
+    "dam_break_32k": dict(shape=(32, 32, 32), spacing=0.01, box=(1.0, 1.0, 1.0), dt=1e-4, vel_std=0.0,
+                          desc="32,768 particles, 32^3 block at 0.01 m in a 1 m box"),
+}
+
+
+def make_scene(name: str, device: str):
+    import torch
+
+    import newton_sph_dev_b200 as nsph
+    from newton_sph_dev_b200.solvers import SolverSPH
+
+    w = WORKLOADS[name]
+    s = w["spacing"]
+    b = nsph.ModelBuilder()
+    b.add_particle_grid(pos=(s / 2, s / 2, s / 2), rot=(0, 0, 0, 1), vel=(0, 0, 0), dim_x=w["shape"][0],
+                        dim_y=w["shape"][1], dim_z=w["shape"][2], cell_x=s, cell_y=s, cell_z=s,
+                        mass=1000.0 * s**3, jitter=0.2 * s)
+    model = b.finalize(device)
+    if w["vel_std"] > 0:
+        rng = np.random.default_rng(seed=2)
+        v = rng.normal(0.0, w["vel_std"], (model.particle_count, 3)).astype(np.float32)
+        model.particle_qd.copy_(torch.from_numpy(v))
+    cfg = SolverSPH.Config(smoothing_length=2 * s, rest_density=1000.0, sound_speed=20.0, eos_gamma=7, xsph=0.01,
+                           box_lo=(0.0, 0.0, 0.0), box_hi=w["box"])
+    return model, cfg, w
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu_index = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu_index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas; timing = max over ranks)
+# ---------------------------------------------------------------------------
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def max_over_ranks(value: float, device=None) -> float:
+    """Max of a per-rank float over all ranks (identity without a process group)."""
+    import torch
+    import torch.distributed as dist
+
+    if not (dist.is_available() and dist.is_initialized()):
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(device=None):
+    import torch.distributed as dist
+
+    if dist.is_available() and dist.is_initialized():
+        if device is not None and device.type == "cuda":
+            dist.barrier(device_ids=[device.index])
+        else:
+            dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (oracle restatement, all host threads)
+# ---------------------------------------------------------------------------
+def cpu_oracle_rate(model_cpu, cfg, w, budget_s: float, max_steps: int, sample_shape=None):
+    """particle-steps/s of the oracle's fp32 step on the host cores."""
+    from oracle import oracle as O
+
+    O.build()
+    x = model_cpu.particle_q.numpy()
+    v = model_cpu.particle_qd.numpy()
+    args = dict(mass=model_cpu.particle_mass.numpy(), inv_mass=model_cpu.particle_inv_mass.numpy(),
+                flags=model_cpu.particle_flags.numpy(), world=model_cpu.particle_world.numpy(),
+                gravity=model_cpu.gravity.numpy())
+    consts = cfg.constants(w["dt"], model_cpu.particle_max_velocity)
+    dims = cfg.resolved_grid_dims()
+    f = np.zeros_like(x)
+    steps = 0
+    t0 = time.perf_counter()
+    while True:
+        r = O.sph_step(consts, dims, x, v, args["mass"], args["inv_mass"], args["flags"], args["world"],
+                       args["gravity"], f_ext=f, v_out_init=v, precision="f32")
+        x, v = r["x"], r["v"]
+        steps += 1
+        el = time.perf_counter() - t0
+        if steps >= max_steps or el >= budget_s:
+            break
+    return x.shape[0] * steps / el, steps, el, O.get_threads()
+
+
+def run_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    import torch  # noqa: F401
+
+    name = args.workload
+    model, cfg, w = make_scene(name, "cpu")
+    n = model.particle_count
+    from oracle import oracle as O
+
+    O.build()
+    # one untimed probe step sizes the sample so the whole run stays within a few minutes
+    rate_probe, _, el, threads = cpu_oracle_rate(model, cfg, w, budget_s=0.0, max_steps=1)
+    per_step = n / rate_probe
+    total_steps = args.steps + args.warmup
+    budget = 150.0
+    sample_n = n
+    sub = None
+    if per_step * total_steps > budget:
+        frac = budget / (per_step * total_steps)
+        # cubic sub-block of the lattice with the same spacing
+        k = max(8, int(round(min(w["shape"]) * frac ** (1 / 3))))
+        sub = (min(k, w["shape"][0]), min(k, w["shape"][1]), min(k, w["shape"][2]))
+        wsub = dict(w, shape=sub)
+        WORKLOADS["_sample"] = wsub
+        model, cfg, w = make_scene("_sample", "cpu")
+        sample_n = model.particle_count
+    from oracle import oracle as O2
+
+    x = model.particle_q.numpy()
+    v = model.particle_qd.numpy()
+    consts = cfg.constants(w["dt"], model.particle_max_velocity)
+    dims = cfg.resolved_grid_dims()
+    a = dict(mass=model.particle_mass.numpy(), inv_mass=model.particle_inv_mass.numpy(),
+             flags=model.particle_flags.numpy(), world=model.particle_world.numpy(), gravity=model.gravity.numpy())
+    f = np.zeros_like(x)
+
+    def step(x, v):
+        r = O2.sph_step(consts, dims, x, v, a["mass"], a["inv_mass"], a["flags"], a["world"], a["gravity"], f_ext=f,
+                        v_out_init=v, precision="f32")
+        return r["x"], r["v"]
+
+    for _ in range(args.warmup):
+        x, v = step(x, v)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        x, v = step(x, v)
+    el = time.perf_counter() - t0
+    value = sample_n * args.steps / el
+    sample = (f"{args.steps} steps of the {sample_n}-particle "
+              + (f"{sub[0]}x{sub[1]}x{sub[2]} sub-block of the workload (same spacing and physics)" if sub
+                 else "full workload"))
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": METRIC,
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": name, "particles": n, "desc": WORKLOADS[name]["desc"]},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def load_traffic(kernel: str):
+    p = REPO / "profiles" / "ncu_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return d.get(kernel, {}).get("traffic_bytes_per_launch")
+    except (ValueError, OSError):
+        return None
+
+
+def load_peak():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except (ValueError, KeyError, OSError):
+            pass
+    return 6650.0, "fallback"
+
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = dist_env()
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", device_id=device, timeout=timedelta(seconds=120))
+
+    from newton_sph_dev_b200.solvers import SolverSPH
+
+    model, cfg, w = make_scene(args.workload, str(device))
+    n = model.particle_count
+    solver = SolverSPH(model, cfg)
+    dt = w["dt"]
+    s0, s1 = model.state(), model.state()
+    stream = torch.cuda.current_stream(device)
+
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    ev = {k: torch.cuda.Event(enable_timing=True, external=True) for k in ("start", "build", "density", "end")}
+    solver.set_phase_events(ev["build"], ev["density"])
+
+    def step(a, b):
+        # record on the current stream: the capture stream inside torch.cuda.graph
+        ev["start"].record()
+        solver.step(a, b, None, None, dt)
+        ev["end"].record()
+
+    # warm-up (eager), then capture one graph per ping-pong direction
+    for i in range(max(args.warmup, 3)):
+        step(s0, s1) if i % 2 == 0 else step(s1, s0)
+    torch.cuda.synchronize()
+    launches_per_step = solver.last_launches
+    use_graph = not args.no_graph
+    graphs = None
+    if use_graph:
+        try:
+            ga, gb = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+            with torch.cuda.graph(ga):
+                step(s0, s1)
+            with torch.cuda.graph(gb):
+                step(s1, s0)
+            graphs = (ga, gb)
+            for g in graphs:  # one replay each to validate event timing through graphs
+                g.replay()
+                ev["end"].synchronize()
+                ev["start"].elapsed_time(ev["end"])
+        except Exception as exc:  # timing events through graphs unavailable: fall back to eager steps
+            print(f"[bench] graph capture unavailable ({exc}); timing eager steps", file=sys.stderr)
+            graphs = None
+            use_graph = False
+            torch.cuda.synchronize()
+
+    phase = {"build": 0.0, "density": 0.0, "force": 0.0}
+    total_ms = 0.0
+    barrier(device)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            if graphs is not None:
+                graphs[i % 2].replay()
+            else:
+                step(s0, s1) if i % 2 == 0 else step(s1, s0)
+            ev["end"].synchronize()
+            t_build = ev["start"].elapsed_time(ev["build"])
+            t_dens = ev["build"].elapsed_time(ev["density"])
+            t_force = ev["density"].elapsed_time(ev["end"])
+            phase["build"] += t_build
+            phase["density"] += t_dens
+            phase["force"] += t_force
+            total_ms += ev["start"].elapsed_time(ev["end"])
+    torch.cuda.synchronize()
+    barrier(device)
+    total_ms_max = max_over_ranks(total_ms, device)
+    status = solver.status()
+
+    value = world * n * args.steps / (total_ms_max * 1e-3)
+    ms_per_step = total_ms_max / args.steps
+
+    # ---- end to end through the public API with host buffers ----
+    e2e_steps = min(args.steps, 100)
+    hx = model.particle_q.cpu().pin_memory()
+    hv = model.particle_qd.cpu().pin_memory()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    solver.set_phase_events(None, None)
+    e2e_ms = 0.0
+    barrier(device)
+    torch.cuda.synchronize()
+    for _ in range(e2e_steps):
+        e0.record(stream)
+        s0.particle_q.copy_(hx, non_blocking=True)
+        s0.particle_qd.copy_(hv, non_blocking=True)
+        solver.step(s0, s1, None, None, dt)
+        hx.copy_(s1.particle_q, non_blocking=True)
+        hv.copy_(s1.particle_qd, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+    barrier(device)
+    e2e_ms_max = max_over_ranks(e2e_ms, device)
+    e2e_value = world * n * e2e_steps / (e2e_ms_max * 1e-3)
+    state_bytes = n * 3 * 4 * 2
+
+    # ---- roofline of the dominant single-kernel pass ----
+    peak, peak_kind = load_peak()
+    dom = "force" if phase["force"] >= phase["density"] else "density"
+    b_alg = (B_ALG_FORCE if dom == "force" else B_ALG_DENSITY) * n
+    t_launch = phase[dom] / args.steps * 1e-3
+    achieved = b_alg / t_launch / 1e9
+    kname = "k_force" if dom == "force" else "k_density"
+    traffic = load_traffic(kname)
+    roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                "alg_bytes_per_launch": b_alg}
+    step_achieved = B_ALG_STEP * n / (ms_per_step * 1e-3) / 1e9
+    roofline_step = {"bound": "hbm", "achieved": step_achieved, "peak": peak, "unit": "GB/s",
+                     "frac": step_achieved / peak, "alg_bytes_per_particle_step": B_ALG_STEP}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        model_cpu, cfg_cpu, w_cpu = make_scene(args.workload, "cpu")
+        rate, steps_done, el, threads = cpu_oracle_rate(model_cpu, cfg_cpu, w_cpu, budget_s=15.0, max_steps=40)
+        cpu = {"value": rate, "unit": METRIC, "cores": threads, "kind": "port",
+               "sample": f"{steps_done} full steps of the {n}-particle workload in {el:.1f} s (fp32 oracle, OpenMP)"}
+
+    if rank == 0:
+        clocks = clk.summary()
+        line = {
+            "metric": METRIC,
+            "value": value,
+            "unit": METRIC,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_per_step,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {
+                "workload": args.workload,
+                "particles": n,
+                "desc": w["desc"],
+                "grid_dims": list(solver.grid_dims),
+                "graph": use_graph,
+                "l2": "flushed (256 MiB write) before every timed step, outside the timed interval",
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            },
+            "phase_ms_per_step": {k: v / args.steps for k, v in phase.items()},
+            "roofline": roofline,
+            "roofline_step": roofline_step,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": state_bytes,
+                    "d2h_bytes_per_step": state_bytes, "steps": e2e_steps},
+            "gpu_launches": launches_per_step * args.steps,
+            "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+            "status": status,
+        }
+        print(json.dumps(line), flush=True)
+    if graphs is not None:
+        del graphs
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=[k for k in WORKLOADS if not k.startswith("_")], default="tank_1m")
+    ap.add_argument("--no-graph", action="store_true", help="time eager steps instead of graph replays")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_gpu(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

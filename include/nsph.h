@@ -1,0 +1,212 @@
+/*
+ * nsph.h — C ABI of libnsph.so, the sm_100a implementation of Newton's
+ * particle-fluid hot path (hash-grid neighbour search + WCSPH step).
+ *
+ * Every entry point takes plain pointers and sizes. Pointers named *device*
+ * below are CUDA device pointers (e.g. torch.Tensor.data_ptr() of a CUDA
+ * tensor). `stream` is a cudaStream_t passed as void* (0 = legacy default
+ * stream). Every entry point returns an int status (NSPH_OK == 0); no C++
+ * exception crosses this boundary and no kernel traps. The message of the last
+ * failure on the calling host thread is returned by nsph_last_error().
+ *
+ * Entry points that enqueue work are stream-ordered and perform no host
+ * synchronisation and no device allocation, so they can be captured into a
+ * CUDA graph (the Newton contract exercised by
+ * newton/tests/test_runtime_gravity.py:141-210). Allocation happens only in
+ * the *_create / *_reserve calls.
+ *
+ * Reference interfaces replaced (paths inside the Newton source tree):
+ *   - wp.HashGrid (external warp-lang 1.14.0.dev20260511), constructed at
+ *     newton/_src/sim/builder.py:9853, reserved at
+ *     newton/_src/solvers/xpbd/solver_xpbd.py:139, built at
+ *     newton/_src/solvers/xpbd/solver_xpbd.py:315-319, queried from kernels at
+ *     newton/_src/solvers/semi_implicit/kernels_contact.py:54,68,71.
+ *   - the integrate_particles kernel, newton/_src/solvers/solver.py:10-47,
+ *     launched by SolverBase.integrate_particles, solver.py:266-299.
+ *   - SolverBase.step, newton/_src/solvers/solver.py:301-316, for the new
+ *     WCSPH solver (the reference has no SPH solver; the step follows the
+ *     neighbour-gather structure of kernels_contact.py:35-84).
+ */
+#ifndef NSPH_H
+#define NSPH_H
+
+#if defined(__GNUC__)
+#define NSPH_API __attribute__((visibility("default")))
+#else
+#define NSPH_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define NSPH_OK                 0
+#define NSPH_ERR_INVALID_ARG    1   /* bad pointer, size or parameter           */
+#define NSPH_ERR_CAPACITY       2   /* more points than reserved                 */
+#define NSPH_ERR_CUDA           3   /* a CUDA runtime call failed                */
+#define NSPH_ERR_NOT_BUILT      4   /* query before the first build              */
+#define NSPH_ERR_OUT_OF_MEMORY  5   /* allocation in *_create / *_reserve failed */
+
+/* ---- device-side status word bits (nsph_sph_status) -------------------- */
+#define NSPH_STATUS_NONFINITE_INPUT   1u  /* a position was NaN/Inf at the build     */
+#define NSPH_STATUS_NONFINITE_OUTPUT  2u  /* a new position/velocity was NaN/Inf     */
+#define NSPH_STATUS_ZERO_DENSITY      4u  /* an active particle had density <= 0     */
+
+/* Particle flag bit, newton/_src/geometry/flags.py:8-14 (ParticleFlags.ACTIVE). */
+#define NSPH_PARTICLE_ACTIVE 1
+
+NSPH_API int         nsph_version(void);
+NSPH_API const char* nsph_status_string(int status);
+/* Message of the last failed call on this host thread ("" if none). */
+NSPH_API const char* nsph_last_error(void);
+
+/* ======================================================================== *
+ *  HashGrid — replaces wp.HashGrid(dim_x, dim_y, dim_z)                    *
+ *  (builder.py:9853; reserve solver_xpbd.py:139; build solver_xpbd.py:319) *
+ *                                                                          *
+ *  Semantics (Warp's public HashGrid behaviour):                           *
+ *   cell_width = radius, inv = 1.0f / radius (fp32)                        *
+ *   virtual cell c_a = int(p_a * inv)  (truncation toward zero, saturating,*
+ *                                      NaN -> 0)                           *
+ *   physical  k_a = max(c_a + 2^20, 0) % dim_a                             *
+ *   cell id   = k_z*dim_x*dim_y + k_y*dim_x + k_x                          *
+ *   points are stably sorted by cell id; cell_starts/cell_ends hold the    *
+ *   [start,end) range of each cell in sorted order, 0/0 for empty cells.   *
+ * ======================================================================== */
+typedef struct nsph_grid nsph_grid;
+
+/* HashGrid(dim_x, dim_y, dim_z) on CUDA device `device`. dim_x*dim_y*dim_z
+ * must be <= 2^28. */
+NSPH_API int nsph_grid_create(int dim_x, int dim_y, int dim_z, int device, nsph_grid** out);
+NSPH_API int nsph_grid_destroy(nsph_grid* grid);
+/* HashGrid.reserve(num_points): size the point buffers (allocates). */
+NSPH_API int nsph_grid_reserve(nsph_grid* grid, int num_points);
+/* HashGrid.build(points, radius). points: device, num_points x 3 float32
+ * (AoS vec3). Requires num_points <= reserved capacity (no allocation). */
+NSPH_API int nsph_grid_build(nsph_grid* grid, const float* points, int num_points, float radius, void* stream);
+
+/* Device pointers of the last build: sorted cell ids (num_points), sorted
+ * point ids (num_points; hash_grid_point_id(grid, tid) == point_ids[tid]),
+ * cell_starts and cell_ends (dim_x*dim_y*dim_z each). Any out pointer may be
+ * NULL. */
+typedef struct nsph_grid_view {
+    const int* point_cells;
+    const int* point_ids;
+    const int* cell_starts;
+    const int* cell_ends;
+    int   num_points;
+    int   dim_x, dim_y, dim_z;
+    float cell_width;
+    float cell_width_inv;
+    int   built;
+} nsph_grid_view;
+NSPH_API int nsph_grid_get_view(const nsph_grid* grid, nsph_grid_view* view);
+
+/* Batched hash_grid_query(grid, pos, radius) + hash_grid_query_next:
+ * enumerate, for each of num_queries positions (device, num_queries x 3
+ * float32), the candidate point ids in Warp's iteration order (cells x
+ * fastest, then y, then z; within a cell in sorted order; no distance test).
+ * Two calls: with out_ids == NULL it writes counts[q]; with out_ids != NULL
+ * it writes the candidates of query q at out_ids[offsets[q] ...]. */
+NSPH_API int nsph_grid_query(const nsph_grid* grid, const float* queries, int num_queries, float radius,
+                    int* counts, const long long* offsets, int* out_ids, void* stream);
+
+/* ======================================================================== *
+ *  integrate_particles — replaces newton/_src/solvers/solver.py:10-47      *
+ *  v1 = v0 + (f*w + g[max(world,0)]*(w>0))*dt; |v1| clamped to v_max;     *
+ *  x1 = x0 + v1*dt; inactive particles: x1 = x0 and v_new not written.     *
+ *  x, v, f, x_new, v_new: device num x 3 float32; inv_mass: float32[n];    *
+ *  flags, world: int32[n]; gravity: device world_count x 3 float32.        *
+ * ======================================================================== */
+NSPH_API int nsph_integrate_particles(const float* x, const float* v, const float* f, const float* inv_mass,
+                             const int* flags, const int* world, const float* gravity, int world_count,
+                             int num, float dt, float v_max, float* x_new, float* v_new, void* stream);
+
+/* ======================================================================== *
+ *  WCSPH solver — the SolverSPH.step hot path                             *
+ * ======================================================================== */
+
+/* Scalar parameters of one step, precomputed on the host in fp32 so that the
+ * device and the fp32 oracle use bit-identical constants. */
+typedef struct nsph_sph_params {
+    float h;           /* kernel support radius (neighbour radius)          */
+    float h2;          /* h*h rounded to fp32: neighbour test r2 < h2       */
+    float inv_h;       /* 1/h                                               */
+    float cell_width;  /* grid cell width (== h by default)                 */
+    float cell_inv;    /* 1.0f / cell_width (fp32)                          */
+    float sigma;       /* 8/(pi h^3): 3-D cubic-spline normalisation        */
+    float dsigma;      /* sigma/h: factor of dW/dr                          */
+    float c_near;      /* 6 sigma/h^2: (dW/dr)/r = c_near (3q-2), q <= 1/2  */
+    float c_far;       /* -6 sigma/h:  (dW/dr)/r = c_far (1-q)^2 / r, q > 1/2 */
+    float rho0;        /* rest density                                       */
+    float inv_rho0;
+    float eos_b;       /* Tait stiffness B = rho0 c0^2 / gamma              */
+    int   eos_gamma;   /* Tait exponent (integer, 7)                        */
+    int   clamp_pressure; /* 1: p = max(p, 0)                               */
+    float xsph_eps;    /* XSPH velocity-smoothing coefficient               */
+    float v_max;       /* Model.particle_max_velocity                        */
+    float dt;
+    int   use_box;     /* 1: clamp positions to [box_lo, box_hi]            */
+    float box_lo[3];
+    float box_hi[3];
+} nsph_sph_params;
+
+typedef struct nsph_sph nsph_sph;
+
+/* Create a solver context on `device` for up to `capacity` particles, with
+ * a neighbour grid of grid_dims[0..2] cells (HashGrid semantics above).
+ * Allocates all scratch (sort buffers, cell tables, sorted mirrors). */
+NSPH_API int nsph_sph_create(int device, int capacity, const int grid_dims[3], nsph_sph** out);
+NSPH_API int nsph_sph_destroy(nsph_sph* solver);
+
+/* One WCSPH step, state_in -> state_out (SolverBase.step, solver.py:301-316).
+ *   x_in, v_in:   device n x 3 float32 (State.particle_q / particle_qd)
+ *   f_ext:        device n x 3 float32 external forces (State.particle_f) or NULL
+ *   mass, inv_mass: device float32[n]; flags, world: device int32[n]
+ *   gravity:      device world_count x 3 float32 (Model.gravity), read on the device
+ *   x_out, v_out: device n x 3 float32 (must not alias x_in / v_in)
+ *   rho_out, p_out: device float32[n] or NULL (density / pressure of the step)
+ *   a_out:        device n x 3 float32 or NULL (SPH acceleration, no gravity)
+ * Kernels (stream-ordered, no allocation, no host sync):
+ *   grid build (hash + LSD radix sort + cell ranges + sorted gather),
+ *   density/EOS pass, force/XSPH/integrate pass. */
+NSPH_API int nsph_sph_step(nsph_sph* solver, const nsph_sph_params* params, int n,
+                  const float* x_in, const float* v_in, const float* f_ext,
+                  const float* mass, const float* inv_mass, const int* flags, const int* world,
+                  const float* gravity, int world_count,
+                  float* x_out, float* v_out, float* rho_out, float* p_out, float* a_out,
+                  void* stream);
+
+/* Neighbour lists of the last step's build, in original particle order: for
+ * each particle i the ids j (self included) of active particles visited by
+ * hash_grid_query(x_i, h) with fp32 r2 = fma(dz,dz,fma(dy,dy,dx*dx)) < h2,
+ * in Warp's iteration order. Inactive particles have none. Two calls as in
+ * nsph_grid_query (counts first, then ids at offsets). */
+NSPH_API int nsph_sph_neighbors(const nsph_sph* solver, const nsph_sph_params* params,
+                       int* counts, const long long* offsets, int* out_ids, void* stream);
+
+/* The solver's grid of the last step (sorted cell ids, permutation, ranges). */
+NSPH_API int nsph_sph_get_grid_view(const nsph_sph* solver, nsph_grid_view* view);
+
+/* Optional timing marks: when set, every later step records `after_build`
+ * (after the grid build and sorted gather) and `after_density` (after the
+ * density pass) on its stream with cudaEventRecordExternal, so the events
+ * also become record nodes of a captured CUDA graph. Events are cudaEvent_t
+ * created with timing enabled; NULL clears. */
+NSPH_API int nsph_sph_set_phase_events(nsph_sph* solver, void* after_build, void* after_density);
+
+/* Number of kernels the last nsph_sph_step launched. */
+NSPH_API int nsph_sph_last_launches(const nsph_sph* solver);
+
+/* Device-side status word (NSPH_STATUS_* bits), OR-accumulated by the step
+ * kernels. Reading copies 4 bytes to the host and synchronises the stream;
+ * reset clears it (stream-ordered). */
+NSPH_API int nsph_sph_status(nsph_sph* solver, unsigned int* status, void* stream);
+NSPH_API int nsph_sph_reset_status(nsph_sph* solver, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NSPH_H */

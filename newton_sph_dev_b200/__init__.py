@@ -1,0 +1,22 @@
+"""newton_sph_dev_b200 — Newton's particle-fluid hot path on B200 (sm_100a).
+
+Drop-in for the particle part of NVIDIA Newton's API:
+
+- ``ModelBuilder`` / ``Model`` / ``State`` / ``Control`` (torch tensors),
+- ``HashGrid`` (the ``wp.HashGrid`` build/query semantics),
+- ``solvers.SolverBase`` (``integrate_particles``) and ``solvers.SolverSPH``
+  (weakly-compressible SPH: hash-grid neighbour search, density/EOS,
+  pressure + XSPH forces, integration).
+
+All compute runs in libnsph.so (hand-written CUDA for sm_100a, C ABI in
+include/nsph.h); there is no CPU fallback.
+"""
+
+from . import solvers
+from .geometry import ParticleFlags
+from .hashgrid import HashGrid
+from .sim import Control, Model, ModelBuilder, State
+
+__version__ = "0.1.0"
+
+__all__ = ["Control", "HashGrid", "Model", "ModelBuilder", "ParticleFlags", "State", "solvers"]

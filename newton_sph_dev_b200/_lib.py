@@ -1,0 +1,176 @@
+"""ctypes binding of libnsph.so (the C ABI declared in include/nsph.h).
+
+The library is the only compute path: there is no CPU fallback. Loading fails
+loudly when the shared object is missing, and every entry point's status is
+turned into a Python exception by :func:`check`.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+_LIB_PATH = Path(__file__).resolve().parent / "libnsph.so"
+
+NSPH_OK = 0
+NSPH_ERR_INVALID_ARG = 1
+NSPH_ERR_CAPACITY = 2
+NSPH_ERR_CUDA = 3
+NSPH_ERR_NOT_BUILT = 4
+NSPH_ERR_OUT_OF_MEMORY = 5
+
+NSPH_STATUS_NONFINITE_INPUT = 1
+NSPH_STATUS_NONFINITE_OUTPUT = 2
+NSPH_STATUS_ZERO_DENSITY = 4
+
+c_int_p = ctypes.POINTER(ctypes.c_int)
+c_float_p = ctypes.POINTER(ctypes.c_float)
+c_void_p = ctypes.c_void_p
+
+
+class NsphGridView(ctypes.Structure):
+    _fields_ = [
+        ("point_cells", c_void_p),
+        ("point_ids", c_void_p),
+        ("cell_starts", c_void_p),
+        ("cell_ends", c_void_p),
+        ("num_points", ctypes.c_int),
+        ("dim_x", ctypes.c_int),
+        ("dim_y", ctypes.c_int),
+        ("dim_z", ctypes.c_int),
+        ("cell_width", ctypes.c_float),
+        ("cell_width_inv", ctypes.c_float),
+        ("built", ctypes.c_int),
+    ]
+
+
+class NsphSphParams(ctypes.Structure):
+    _fields_ = [
+        ("h", ctypes.c_float),
+        ("h2", ctypes.c_float),
+        ("inv_h", ctypes.c_float),
+        ("cell_width", ctypes.c_float),
+        ("cell_inv", ctypes.c_float),
+        ("sigma", ctypes.c_float),
+        ("dsigma", ctypes.c_float),
+        ("c_near", ctypes.c_float),
+        ("c_far", ctypes.c_float),
+        ("rho0", ctypes.c_float),
+        ("inv_rho0", ctypes.c_float),
+        ("eos_b", ctypes.c_float),
+        ("eos_gamma", ctypes.c_int),
+        ("clamp_pressure", ctypes.c_int),
+        ("xsph_eps", ctypes.c_float),
+        ("v_max", ctypes.c_float),
+        ("dt", ctypes.c_float),
+        ("use_box", ctypes.c_int),
+        ("box_lo", ctypes.c_float * 3),
+        ("box_hi", ctypes.c_float * 3),
+    ]
+
+
+# (name, restype, argtypes) of every exported entry point, in header order.
+SIGNATURES = [
+    ("nsph_version", ctypes.c_int, []),
+    ("nsph_status_string", ctypes.c_char_p, [ctypes.c_int]),
+    ("nsph_last_error", ctypes.c_char_p, []),
+    ("nsph_grid_create", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(c_void_p)]),
+    ("nsph_grid_destroy", ctypes.c_int, [c_void_p]),
+    ("nsph_grid_reserve", ctypes.c_int, [c_void_p, ctypes.c_int]),
+    ("nsph_grid_build", ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_float, c_void_p]),
+    ("nsph_grid_get_view", ctypes.c_int, [c_void_p, ctypes.POINTER(NsphGridView)]),
+    ("nsph_grid_query", ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_float, c_void_p, c_void_p, c_void_p, c_void_p]),
+    (
+        "nsph_integrate_particles",
+        ctypes.c_int,
+        [c_void_p] * 7 + [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, c_void_p, c_void_p, c_void_p],
+    ),
+    ("nsph_sph_create", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int * 3), ctypes.POINTER(c_void_p)]),
+    ("nsph_sph_destroy", ctypes.c_int, [c_void_p]),
+    (
+        "nsph_sph_step",
+        ctypes.c_int,
+        [c_void_p, ctypes.POINTER(NsphSphParams), ctypes.c_int]
+        + [c_void_p] * 8
+        + [ctypes.c_int]
+        + [c_void_p] * 5
+        + [c_void_p],
+    ),
+    ("nsph_sph_neighbors", ctypes.c_int, [c_void_p, ctypes.POINTER(NsphSphParams), c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("nsph_sph_get_grid_view", ctypes.c_int, [c_void_p, ctypes.POINTER(NsphGridView)]),
+    ("nsph_sph_set_phase_events", ctypes.c_int, [c_void_p, c_void_p, c_void_p]),
+    ("nsph_sph_last_launches", ctypes.c_int, [c_void_p]),
+    ("nsph_sph_status", ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_uint), c_void_p]),
+    ("nsph_sph_reset_status", ctypes.c_int, [c_void_p, c_void_p]),
+]
+
+_lib: ctypes.CDLL | None = None
+
+
+class NsphError(RuntimeError):
+    """A libnsph entry point returned a non-zero status."""
+
+    def __init__(self, status: int, where: str, message: str):
+        self.status = status
+        super().__init__(f"{where} failed with status {status}: {message}")
+
+
+def lib_path() -> Path:
+    return _LIB_PATH
+
+
+def load() -> ctypes.CDLL:
+    """Load libnsph.so (once) and declare the C signatures.
+
+    Raises:
+        RuntimeError: the library has not been built (``__graft_entry__.build()``
+            or ``python -m newton_sph_dev_b200._build``).
+    """
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not _LIB_PATH.exists():
+        raise RuntimeError(
+            f"{_LIB_PATH} is missing: build the CUDA library first "
+            "(python -m newton_sph_dev_b200._build). There is no CPU fallback."
+        )
+    # the torch runtime must own the primary context before our statically
+    # linked runtime touches it; importing torch first guarantees that order
+    import torch  # noqa: F401
+
+    lib = ctypes.CDLL(os.fspath(_LIB_PATH))
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    msg = load().nsph_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(status: int, where: str) -> None:
+    """Raise the Newton-style exception for a non-zero status."""
+    if status == NSPH_OK:
+        return
+    msg = last_error()
+    if status in (NSPH_ERR_INVALID_ARG, NSPH_ERR_CAPACITY):
+        raise ValueError(f"{where}: {msg}")
+    raise NsphError(status, where, msg)
+
+
+def ptr(t) -> int | None:
+    """Raw device pointer of a tensor (None for None)."""
+    if t is None:
+        return None
+    return t.data_ptr()
+
+
+def stream_handle(device) -> int:
+    import torch
+
+    return torch.cuda.current_stream(device).cuda_stream

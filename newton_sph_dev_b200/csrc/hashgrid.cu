@@ -1,0 +1,543 @@
+// hashgrid.cu — HashGrid build (hash + stable LSD radix sort + cell ranges)
+// and the batched Warp-order query.
+//
+// Replaces wp.HashGrid (external warp-lang 1.14.0.dev20260511), constructed
+// at newton/_src/sim/builder.py:9853, reserved at
+// newton/_src/solvers/xpbd/solver_xpbd.py:139 and built at
+// solver_xpbd.py:315-319; its device query is used at
+// newton/_src/solvers/semi_implicit/kernels_contact.py:54,68,71.
+//
+// Build pipeline (all stream-ordered, no allocation, no host sync):
+//   k_hash_hist   original order: cell id per point + digit-0 tile histograms;
+//                 also clears the cell ranges the previous build wrote.
+//   per 8-bit digit pass: [k_upsweep] -> k_scan -> k_downsweep
+//                 stable multi-split per 4096-key tile (warp match_any ranks,
+//                 shared-memory staging for coalesced scatter). The last pass
+//                 writes point_cells / point_ids and, in SPH mode, gathers the
+//                 sorted float4 mirrors of position and velocity.
+//   k_ranges      cell_starts / cell_ends from the sorted cell ids.
+#include <algorithm>
+#include <cstdio>
+
+#include "nsph_internal.cuh"
+
+namespace nsph {
+
+namespace {
+
+__device__ __forceinline__ unsigned lanemask_lt()
+{
+    unsigned m;
+    asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// --------------------------------------------------------------------------
+// k_hash_hist: keys/vals in original order + histogram of digit 0 per tile.
+// Also clears the previous build's occupied cells (their first sorted entry
+// resets start/end to 0), so no full memset of the cell tables is needed.
+// --------------------------------------------------------------------------
+__global__ void __launch_bounds__(kSortThreads) k_hash_hist(
+    const float* __restrict__ points, int n, float inv, int dx, int dy, int dz, int* __restrict__ keys,
+    int* __restrict__ vals, unsigned* __restrict__ hist, int ntiles, int digit_mask,
+    const int* __restrict__ prev_cells, int prev_n, int* __restrict__ starts, int* __restrict__ ends,
+    unsigned* __restrict__ status)
+{
+    __shared__ unsigned wh[kSortThreads / 32][kRadix];
+    const int warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < (kSortThreads / 32) * kRadix; i += kSortThreads) (&wh[0][0])[i] = 0u;
+    __syncthreads();
+
+    const int base = blockIdx.x * kSortTile;
+    bool bad = false;
+#pragma unroll 4
+    for (int it = 0; it < kSortItems; ++it) {
+        const int idx = base + it * kSortThreads + threadIdx.x;
+        if (idx < prev_n) {
+            const int c = prev_cells[idx];
+            if (idx == 0 || prev_cells[idx - 1] != c) {
+                starts[c] = 0;
+                ends[c] = 0;
+            }
+        }
+        if (idx < n) {
+            const float x = points[3 * (size_t)idx + 0];
+            const float y = points[3 * (size_t)idx + 1];
+            const float z = points[3 * (size_t)idx + 2];
+            bad |= !(isfinite(x) && isfinite(y) && isfinite(z));
+            const int key = point_cell(x, y, z, inv, dx, dy, dz);
+            keys[idx] = key;
+            vals[idx] = idx;
+            atomicAdd(&wh[warp][key & digit_mask], 1u);
+        }
+    }
+    if (bad && status) atomicOr(status, (unsigned)NSPH_STATUS_NONFINITE_INPUT);
+    __syncthreads();
+    if (blockIdx.x < ntiles) {
+        for (int d = threadIdx.x; d < kRadix; d += kSortThreads) {
+            unsigned s = 0;
+#pragma unroll
+            for (int w = 0; w < kSortThreads / 32; ++w) s += wh[w][d];
+            hist[(size_t)d * ntiles + blockIdx.x] = s;
+        }
+    }
+}
+
+// Histogram of one digit per tile (passes after the first).
+__global__ void __launch_bounds__(kSortThreads) k_upsweep(const int* __restrict__ keys, int n, int shift,
+                                                          int digit_mask, unsigned* __restrict__ hist,
+                                                          int ntiles)
+{
+    __shared__ unsigned wh[kSortThreads / 32][kRadix];
+    const int warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < (kSortThreads / 32) * kRadix; i += kSortThreads) (&wh[0][0])[i] = 0u;
+    __syncthreads();
+    const int base = blockIdx.x * kSortTile;
+#pragma unroll 4
+    for (int it = 0; it < kSortItems; ++it) {
+        const int idx = base + it * kSortThreads + threadIdx.x;
+        if (idx < n) atomicAdd(&wh[warp][(keys[idx] >> shift) & digit_mask], 1u);
+    }
+    __syncthreads();
+    for (int d = threadIdx.x; d < kRadix; d += kSortThreads) {
+        unsigned s = 0;
+#pragma unroll
+        for (int w = 0; w < kSortThreads / 32; ++w) s += wh[w][d];
+        hist[(size_t)d * ntiles + blockIdx.x] = s;
+    }
+}
+
+// Exclusive scan of the digit-major histogram table (kRadix * ntiles
+// entries) in one CTA of 1024 threads: entry [d][t] becomes the global
+// output offset of digit d's keys from tile t.
+constexpr int kScanThreads = 1024;
+__global__ void __launch_bounds__(kScanThreads) k_scan(unsigned* __restrict__ hist, int total)
+{
+    __shared__ unsigned warp_sums[kScanThreads / 32];
+    const int per = (total + kScanThreads - 1) / kScanThreads;
+    const int begin = min(total, threadIdx.x * per);
+    const int end = min(total, begin + per);
+    unsigned local = 0;
+    for (int i = begin; i < end; ++i) local += hist[i];
+    // block-wide exclusive scan of `local`
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned s = warp_sums[lane];
+        unsigned si = s;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned t = __shfl_up_sync(0xffffffffu, si, o);
+            if (lane >= o) si += t;
+        }
+        warp_sums[lane] = si - s;
+    }
+    __syncthreads();
+    unsigned run = warp_sums[warp] + incl - local;
+    for (int i = begin; i < end; ++i) {
+        const unsigned c = hist[i];
+        hist[i] = run;
+        run += c;
+    }
+}
+
+// --------------------------------------------------------------------------
+// k_downsweep: stable scatter of one digit pass.
+// Warp w owns tile elements [w*512, w*512+512) in 16 rounds of 32; within a
+// round lanes with equal digits are ranked by __match_any_sync, and a
+// per-warp counter carries ranks across rounds, so the order inside a tile
+// is exactly the input order per digit. Keys are staged in shared memory in
+// tile-sorted order and written out in runs (coalesced).
+// --------------------------------------------------------------------------
+constexpr int kWarps = kSortThreads / 32;
+constexpr int kPerWarp = kSortTile / kWarps;  // 512
+
+struct DownsweepSmem {
+    unsigned warp_cnt[kWarps][kRadix];
+    unsigned tile_off[kRadix];
+    unsigned glob_off[kRadix];
+    int keys[kSortTile];
+    int vals[kSortTile];
+};
+
+template <bool kGather>
+__global__ void __launch_bounds__(kSortThreads) k_downsweep(const int* __restrict__ keys_in,
+                                                            const int* __restrict__ vals_in,
+                                                            int* __restrict__ keys_out, int* __restrict__ vals_out,
+                                                            int n, int shift, int digit_mask,
+                                                            const unsigned* __restrict__ hist, int ntiles,
+                                                            GatherArgs gather)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    DownsweepSmem& sm = *reinterpret_cast<DownsweepSmem*>(smem_raw);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < kWarps * kRadix; i += kSortThreads) (&sm.warp_cnt[0][0])[i] = 0u;
+    __syncthreads();
+
+    const int tile_base = blockIdx.x * kSortTile;
+    const int tile_n = min(kSortTile, n - tile_base);
+    int key[kSortItems], val[kSortItems];
+    unsigned rank[kSortItems];
+    const unsigned lt = lanemask_lt();
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const int local = warp * kPerWarp + r * 32 + lane;
+        const bool valid = local < tile_n;
+        key[r] = valid ? keys_in[tile_base + local] : 0;
+        val[r] = valid ? vals_in[tile_base + local] : 0;
+        const int d = valid ? ((key[r] >> shift) & digit_mask) : kRadix;  // kRadix: sentinel group
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const unsigned before = __popc(peers & lt);
+        unsigned base = 0;
+        if (valid) base = sm.warp_cnt[warp][d];
+        __syncwarp();
+        if (valid && before == 0) sm.warp_cnt[warp][d] = base + __popc(peers);
+        __syncwarp();
+        rank[r] = base + before;
+    }
+    __syncthreads();
+    // per digit: exclusive prefix over warps, digit totals of this tile
+    unsigned total = 0;
+    if (threadIdx.x < kRadix) {
+        const int d = threadIdx.x;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const unsigned c = sm.warp_cnt[w][d];
+            sm.warp_cnt[w][d] = total;
+            total += c;
+        }
+        sm.glob_off[d] = hist[(size_t)d * ntiles + blockIdx.x];
+    }
+    // exclusive scan of digit totals (kRadix == kSortThreads == 256)
+    {
+        __shared__ unsigned ws[kWarps];
+        unsigned incl = total;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
+        }
+        if (lane == 31) ws[warp] = incl;
+        __syncthreads();
+        unsigned wbase = 0;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) wbase += (w < warp) ? ws[w] : 0u;
+        if (threadIdx.x < kRadix) sm.tile_off[threadIdx.x] = wbase + incl - total;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kSortItems; ++r) {
+        const int local = warp * kPerWarp + r * 32 + lane;
+        if (local < tile_n) {
+            const int d = (key[r] >> shift) & digit_mask;
+            const unsigned pos = sm.tile_off[d] + sm.warp_cnt[warp][d] + rank[r];
+            sm.keys[pos] = key[r];
+            sm.vals[pos] = val[r];
+        }
+    }
+    __syncthreads();
+    for (int p = threadIdx.x; p < tile_n; p += kSortThreads) {
+        const int k = sm.keys[p];
+        const int v = sm.vals[p];
+        const int d = (k >> shift) & digit_mask;
+        const unsigned g = sm.glob_off[d] + (unsigned)p - sm.tile_off[d];
+        keys_out[g] = k;
+        vals_out[g] = v;
+        if constexpr (kGather) {
+            const size_t i = (size_t)v;
+            const float x = gather.x[3 * i + 0], y = gather.x[3 * i + 1], z = gather.x[3 * i + 2];
+            const float vx = gather.v[3 * i + 0], vy = gather.v[3 * i + 1], vz = gather.v[3 * i + 2];
+            const int fl = gather.flags[i];
+            const bool active = (fl & NSPH_PARTICLE_ACTIVE) != 0;
+            const float m = gather.mass[i];
+            const float w = gather.inv_mass[i];
+            int gw = gather.world ? gather.world[i] : 0;
+            gw = gw < 0 ? 0 : (gw >= gather.world_count ? gather.world_count - 1 : gw);
+            const int attr = (active ? kAttrActive : 0) | (w > 0.f ? kAttrDynamic : 0) | (gw << kAttrGravShift);
+            gather.xs[g] = make_float4(x, y, z, active ? m : 0.f);
+            gather.vs[g] = make_float4(vx, vy, vz, __int_as_float(attr));
+        }
+    }
+}
+
+// Cell [start, end) ranges from sorted cell ids (Warp's compute_cell_offsets
+// semantics; cells not written keep the 0/0 of an empty cell).
+__global__ void k_ranges(const int* __restrict__ cells, int n, int* __restrict__ starts, int* __restrict__ ends)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int c = cells[k];
+    if (k == 0 || cells[k - 1] != c) starts[c] = k;
+    if (k == n - 1 || cells[k + 1] != c) ends[c] = k + 1;
+}
+
+// Batched Warp-order query: counts, or ids at offsets.
+__global__ void k_query(GridDev g, const float* __restrict__ q, int nq, float radius, int* __restrict__ counts,
+                        const long long* __restrict__ offsets, int* __restrict__ out)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nq) return;
+    const float px = q[3 * (size_t)t], py = q[3 * (size_t)t + 1], pz = q[3 * (size_t)t + 2];
+    if (out) {
+        long long o = offsets[t];
+        for_each_candidate(g, px, py, pz, radius, [&](int k) { out[o++] = g.ids[k]; });
+    } else {
+        int c = 0;
+        for_each_candidate(g, px, py, pz, radius, [&](int) { ++c; });
+        counts[t] = c;
+    }
+}
+
+inline int ntiles_of(int n) { return (n + kSortTile - 1) / kSortTile; }
+
+}  // namespace
+
+// --------------------------------------------------------------------------
+// host side
+// --------------------------------------------------------------------------
+int grid_init(Grid& g, int dx, int dy, int dz, int device)
+{
+    if (dx <= 0 || dy <= 0 || dz <= 0) return fail(NSPH_ERR_INVALID_ARG, "grid dims must be positive");
+    const long long nc = (long long)dx * dy * dz;
+    if (nc > (1LL << 28)) return fail(NSPH_ERR_INVALID_ARG, "grid has more than 2^28 cells");
+    g.device = device;
+    g.dx = dx;
+    g.dy = dy;
+    g.dz = dz;
+    g.ncells = nc;
+    int bits = 1;
+    while ((1LL << bits) < nc) ++bits;
+    g.key_bits = bits;
+    DeviceGuard guard(device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    NSPH_CUDA_TRY(cudaMalloc(&g.cell_starts, sizeof(int) * nc));
+    NSPH_CUDA_TRY(cudaMalloc(&g.cell_ends, sizeof(int) * nc));
+    NSPH_CUDA_TRY(cudaMemset(g.cell_starts, 0, sizeof(int) * nc));
+    NSPH_CUDA_TRY(cudaMemset(g.cell_ends, 0, sizeof(int) * nc));
+    // load every kernel now, so that a later stream capture never triggers
+    // lazy module loading
+    cudaFuncAttributes fa;
+    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_hash_hist));
+    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_upsweep));
+    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_scan));
+    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_downsweep<false>));
+    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_downsweep<true>));
+    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_ranges));
+    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_query));
+    NSPH_CUDA_TRY(cudaFuncSetAttribute(k_downsweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sizeof(DownsweepSmem)));
+    NSPH_CUDA_TRY(cudaFuncSetAttribute(k_downsweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)sizeof(DownsweepSmem)));
+    NSPH_CUDA_TRY(cudaDeviceSynchronize());
+    return NSPH_OK;
+}
+
+int grid_reserve(Grid& g, int capacity)
+{
+    if (capacity < 0) return fail(NSPH_ERR_INVALID_ARG, "negative capacity");
+    if (capacity <= g.capacity) return NSPH_OK;
+    DeviceGuard guard(g.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    // a grown reservation drops the previous build (the Warp contract)
+    if (g.built && g.num_points > 0) {
+        NSPH_CUDA_TRY(cudaDeviceSynchronize());
+        NSPH_CUDA_TRY(cudaMemset(g.cell_starts, 0, sizeof(int) * g.ncells));
+        NSPH_CUDA_TRY(cudaMemset(g.cell_ends, 0, sizeof(int) * g.ncells));
+    }
+    g.built = 0;
+    g.num_points = 0;
+    int* bufs[6] = {g.keys_a, g.vals_a, g.keys_b, g.vals_b, g.point_cells, g.point_ids};
+    for (int* b : bufs) cudaFree(b);
+    cudaFree(g.hist);
+    g.keys_a = g.vals_a = g.keys_b = g.vals_b = g.point_cells = g.point_ids = nullptr;
+    g.hist = nullptr;
+    g.capacity = 0;
+    const size_t sz = sizeof(int) * (size_t)capacity;
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = cudaMalloc(&g.keys_a, sz);
+    if (e == cudaSuccess) e = cudaMalloc(&g.vals_a, sz);
+    if (e == cudaSuccess) e = cudaMalloc(&g.keys_b, sz);
+    if (e == cudaSuccess) e = cudaMalloc(&g.vals_b, sz);
+    if (e == cudaSuccess) e = cudaMalloc(&g.point_cells, sz);
+    if (e == cudaSuccess) e = cudaMalloc(&g.point_ids, sz);
+    if (e == cudaSuccess) e = cudaMalloc(&g.hist, sizeof(unsigned) * kRadix * (size_t)std::max(1, ntiles_of(capacity)));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(NSPH_ERR_OUT_OF_MEMORY, std::string("reserve: ") + cudaGetErrorString(e));
+    }
+    g.capacity = capacity;
+    return NSPH_OK;
+}
+
+void grid_free(Grid& g)
+{
+    DeviceGuard guard(g.device);
+    int* bufs[8] = {g.keys_a, g.vals_a, g.keys_b, g.vals_b, g.point_cells, g.point_ids, g.cell_starts, g.cell_ends};
+    for (int* b : bufs) cudaFree(b);
+    cudaFree(g.hist);
+    g = Grid();
+}
+
+int grid_build(Grid& g, const float* points, int n, float cell_width, float cell_inv, const GatherArgs* gather,
+               unsigned int* status, cudaStream_t stream, int* launches)
+{
+    int local_launches = 0;
+    int& nl = launches ? *launches : local_launches;
+    if (n < 0) return fail(NSPH_ERR_INVALID_ARG, "negative point count");
+    if (n > g.capacity) return fail(NSPH_ERR_CAPACITY, "build: more points than reserved");
+    if (n > 0 && !points) return fail(NSPH_ERR_INVALID_ARG, "build: null points");
+    const int prev_n = g.built ? g.num_points : 0;
+    const int ntiles = ntiles_of(n);
+    const int launch_tiles = std::max(ntiles, ntiles_of(prev_n));
+    const int passes = (g.key_bits + kRadixBits - 1) / kRadixBits;
+    auto mask_of = [&](int p) {
+        const int bits = std::min(kRadixBits, g.key_bits - p * kRadixBits);
+        return (1 << bits) - 1;
+    };
+    if (launch_tiles > 0) {
+        k_hash_hist<<<launch_tiles, kSortThreads, 0, stream>>>(points, n, cell_inv, g.dx, g.dy, g.dz, g.keys_a,
+                                                               g.vals_a, g.hist, ntiles, mask_of(0),
+                                                               g.point_cells, prev_n, g.cell_starts, g.cell_ends,
+                                                               status);
+        NSPH_LAUNCH_CHECK("k_hash_hist");
+        ++nl;
+    }
+    if (n > 0) {
+        const int* kin = g.keys_a;
+        const int* vin = g.vals_a;
+        for (int p = 0; p < passes; ++p) {
+            const bool last = (p == passes - 1);
+            int* kout = last ? g.point_cells : ((p & 1) ? g.keys_a : g.keys_b);
+            int* vout = last ? g.point_ids : ((p & 1) ? g.vals_a : g.vals_b);
+            const int shift = p * kRadixBits;
+            if (p > 0) {
+                k_upsweep<<<ntiles, kSortThreads, 0, stream>>>(kin, n, shift, mask_of(p), g.hist, ntiles);
+                NSPH_LAUNCH_CHECK("k_upsweep");
+                ++nl;
+            }
+            k_scan<<<1, kScanThreads, 0, stream>>>(g.hist, kRadix * ntiles);
+            NSPH_LAUNCH_CHECK("k_scan");
+            ++nl;
+            GatherArgs ga{};
+            if (last && gather) {
+                ga = *gather;
+                k_downsweep<true><<<ntiles, kSortThreads, sizeof(DownsweepSmem), stream>>>(
+                    kin, vin, kout, vout, n, shift, mask_of(p), g.hist, ntiles, ga);
+            } else {
+                k_downsweep<false><<<ntiles, kSortThreads, sizeof(DownsweepSmem), stream>>>(
+                    kin, vin, kout, vout, n, shift, mask_of(p), g.hist, ntiles, ga);
+            }
+            NSPH_LAUNCH_CHECK("k_downsweep");
+            ++nl;
+            kin = kout;
+            vin = vout;
+        }
+        k_ranges<<<(n + 255) / 256, 256, 0, stream>>>(g.point_cells, n, g.cell_starts, g.cell_ends);
+        NSPH_LAUNCH_CHECK("k_ranges");
+        ++nl;
+    }
+    g.num_points = n;
+    g.cell_width = cell_width;
+    g.cell_inv = cell_inv;
+    g.built = 1;
+    return NSPH_OK;
+}
+
+}  // namespace nsph
+
+// ==========================================================================
+// C ABI: HashGrid
+// ==========================================================================
+struct nsph_grid {
+    nsph::Grid g;
+};
+
+using namespace nsph;
+
+extern "C" int nsph_grid_create(int dim_x, int dim_y, int dim_z, int device, nsph_grid** out)
+{
+    clear_error();
+    if (!out) return fail(NSPH_ERR_INVALID_ARG, "null out pointer");
+    *out = nullptr;
+    nsph_grid* h = new (std::nothrow) nsph_grid();
+    if (!h) return fail(NSPH_ERR_OUT_OF_MEMORY, "host allocation failed");
+    const int st = grid_init(h->g, dim_x, dim_y, dim_z, device);
+    if (st != NSPH_OK) {
+        grid_free(h->g);
+        delete h;
+        return st;
+    }
+    *out = h;
+    return NSPH_OK;
+}
+
+extern "C" int nsph_grid_destroy(nsph_grid* grid)
+{
+    clear_error();
+    if (!grid) return NSPH_OK;
+    grid_free(grid->g);
+    delete grid;
+    return NSPH_OK;
+}
+
+extern "C" int nsph_grid_reserve(nsph_grid* grid, int num_points)
+{
+    clear_error();
+    if (!grid) return fail(NSPH_ERR_INVALID_ARG, "null grid");
+    return grid_reserve(grid->g, num_points);
+}
+
+extern "C" int nsph_grid_build(nsph_grid* grid, const float* points, int num_points, float radius, void* stream)
+{
+    clear_error();
+    if (!grid) return fail(NSPH_ERR_INVALID_ARG, "null grid");
+    if (!(radius > 0.f) || !isfinite(radius)) return fail(NSPH_ERR_INVALID_ARG, "radius must be positive and finite");
+    DeviceGuard guard(grid->g.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    const float inv = 1.0f / radius;
+    return grid_build(grid->g, points, num_points, radius, inv, nullptr, nullptr, (cudaStream_t)stream);
+}
+
+extern "C" int nsph_grid_get_view(const nsph_grid* grid, nsph_grid_view* view)
+{
+    clear_error();
+    if (!grid || !view) return fail(NSPH_ERR_INVALID_ARG, "null argument");
+    const Grid& g = grid->g;
+    view->point_cells = g.point_cells;
+    view->point_ids = g.point_ids;
+    view->cell_starts = g.cell_starts;
+    view->cell_ends = g.cell_ends;
+    view->num_points = g.num_points;
+    view->dim_x = g.dx;
+    view->dim_y = g.dy;
+    view->dim_z = g.dz;
+    view->cell_width = g.cell_width;
+    view->cell_width_inv = g.cell_inv;
+    view->built = g.built;
+    return NSPH_OK;
+}
+
+extern "C" int nsph_grid_query(const nsph_grid* grid, const float* queries, int num_queries, float radius,
+                               int* counts, const long long* offsets, int* out_ids, void* stream)
+{
+    clear_error();
+    if (!grid) return fail(NSPH_ERR_INVALID_ARG, "null grid");
+    if (!grid->g.built) return fail(NSPH_ERR_NOT_BUILT, "query before build");
+    if (num_queries < 0) return fail(NSPH_ERR_INVALID_ARG, "negative query count");
+    if (num_queries == 0) return NSPH_OK;
+    if (!queries) return fail(NSPH_ERR_INVALID_ARG, "null queries");
+    if (out_ids ? !offsets : !counts) return fail(NSPH_ERR_INVALID_ARG, "counts (count call) or offsets (fill call) required");
+    DeviceGuard guard(grid->g.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    k_query<<<(num_queries + 127) / 128, 128, 0, (cudaStream_t)stream>>>(grid->g.view(), queries, num_queries,
+                                                                         radius, counts, offsets, out_ids);
+    NSPH_LAUNCH_CHECK("k_query");
+    return NSPH_OK;
+}

@@ -1,0 +1,198 @@
+// nsph_internal.cuh — shared device helpers and host plumbing of libnsph.so.
+//
+// Hash-grid semantics follow Warp's public HashGrid behaviour (the grid used by
+// newton/_src/solvers/semi_implicit/kernels_contact.py:54-71 and
+// newton/_src/solvers/xpbd/solver_xpbd.py:315-319): truncating cell
+// coordinates, a 2^20 origin offset, modulo dims, x-fastest query order.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "nsph.h"
+
+namespace nsph {
+
+// ---------------------------------------------------------------------------
+// error reporting (thread-local last message; no exception crosses the ABI)
+// ---------------------------------------------------------------------------
+void set_error(const std::string& msg);
+void clear_error();
+int fail(int status, const std::string& msg);
+int cuda_fail(cudaError_t err, const char* what);
+
+#define NSPH_CUDA_TRY(expr)                                   \
+    do {                                                      \
+        cudaError_t err__ = (expr);                           \
+        if (err__ != cudaSuccess) return ::nsph::cuda_fail(err__, #expr); \
+    } while (0)
+
+#define NSPH_LAUNCH_CHECK(what)                                       \
+    do {                                                              \
+        cudaError_t err__ = cudaGetLastError();                       \
+        if (err__ != cudaSuccess) return ::nsph::cuda_fail(err__, what); \
+    } while (0)
+
+// Makes `device` current for the lifetime of the guard and restores the
+// caller's device afterwards.
+struct DeviceGuard {
+    int prev = -1;
+    bool ok = false;
+    explicit DeviceGuard(int device)
+    {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        ok = (prev == device) || (cudaSetDevice(device) == cudaSuccess);
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+// ---------------------------------------------------------------------------
+// grid arithmetic (device side)
+// ---------------------------------------------------------------------------
+constexpr long long kOrigin = 1LL << 20;
+
+// float -> int like Warp's int(): truncation toward zero. cvt.rzi.s32.f32
+// saturates out-of-range values and maps NaN to 0.
+__device__ __forceinline__ int trunc_sat(float v) { return __float2int_rz(v); }
+
+__device__ __forceinline__ int phys_axis(long long c, int dim)
+{
+    long long v = c + kOrigin;
+    v = v < 0 ? 0 : v;
+    return (int)(v % dim);
+}
+
+// Per-axis query bounds, Warp: start = int((p-r)*inv), end = min(int((p+r)*inv),
+// start + dim - 1); the start cell is always visited. Rounded exactly as
+// written (no contraction).
+__device__ __forceinline__ void query_bounds(float p, float r, float inv, int dim, long long& s, long long& e)
+{
+    const long long a = trunc_sat(__fmul_rn(__fsub_rn(p, r), inv));
+    long long b = trunc_sat(__fmul_rn(__fadd_rn(p, r), inv));
+    const long long lim = a + dim - 1;
+    b = b > lim ? lim : b;
+    b = b < a ? a : b;
+    s = a;
+    e = b;
+}
+
+__device__ __forceinline__ int point_cell(float x, float y, float z, float inv, int dx, int dy, int dz)
+{
+    const int cx = phys_axis(trunc_sat(__fmul_rn(x, inv)), dx);
+    const int cy = phys_axis(trunc_sat(__fmul_rn(y, inv)), dy);
+    const int cz = phys_axis(trunc_sat(__fmul_rn(z, inv)), dz);
+    return cz * (dx * dy) + cy * dx + cx;
+}
+
+// Read-only view of a built grid as the kernels see it.
+struct GridDev {
+    int dx, dy, dz;
+    float inv;
+    const int* __restrict__ starts;
+    const int* __restrict__ ends;
+    const int* __restrict__ ids;  // sorted position -> original index
+};
+
+// Visit, in Warp's order, every sorted position k of the cells overlapping the
+// query box of (px,py,pz) +- r. Consecutive non-empty cells whose ranges abut
+// in sorted order are merged into one contiguous run, so the candidate
+// sequence is exactly Warp's while the loop restarts less often.
+template <class F>
+__device__ __forceinline__ void for_each_candidate(const GridDev& g, float px, float py, float pz, float r, F&& f)
+{
+    long long xs, xe, ys, ye, zs, ze;
+    query_bounds(px, r, g.inv, g.dx, xs, xe);
+    query_bounds(py, r, g.inv, g.dy, ys, ye);
+    query_bounds(pz, r, g.inv, g.dz, zs, ze);
+    int lo = 0, hi = 0;
+    for (long long z = zs; z <= ze; ++z) {
+        const int cz = phys_axis(z, g.dz);
+        for (long long y = ys; y <= ye; ++y) {
+            const int rowbase = cz * (g.dx * g.dy) + phys_axis(y, g.dy) * g.dx;
+            for (long long x = xs; x <= xe; ++x) {
+                const int c = rowbase + phys_axis(x, g.dx);
+                const int s = __ldg(g.starts + c);
+                const int e = __ldg(g.ends + c);
+                if (e > s) {
+                    if (s == hi && hi > lo) {
+                        hi = e;
+                    } else {
+                        for (int k = lo; k < hi; ++k) f(k);
+                        lo = s;
+                        hi = e;
+                    }
+                }
+            }
+        }
+    }
+    for (int k = lo; k < hi; ++k) f(k);
+}
+
+// ---------------------------------------------------------------------------
+// grid object (shared by the HashGrid API and the SPH solver)
+// ---------------------------------------------------------------------------
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per CTA
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+
+struct Grid {
+    int device = 0;
+    int dx = 0, dy = 0, dz = 0;
+    long long ncells = 0;
+    int key_bits = 0;
+    int capacity = 0;
+    int num_points = 0;   // points of the last build
+    int built = 0;
+    float cell_width = 0.f;
+    float cell_inv = 0.f;
+    // sort buffers (capacity each)
+    int* keys_a = nullptr;
+    int* vals_a = nullptr;
+    int* keys_b = nullptr;
+    int* vals_b = nullptr;
+    int* point_cells = nullptr;  // sorted cell ids of the last build
+    int* point_ids = nullptr;    // sorted original ids of the last build
+    unsigned int* hist = nullptr;  // kRadix * ntiles(capacity)
+    // cell tables (ncells each)
+    int* cell_starts = nullptr;
+    int* cell_ends = nullptr;
+
+    GridDev view() const { return GridDev{dx, dy, dz, cell_inv, cell_starts, cell_ends, point_ids}; }
+};
+
+// Gather performed by the last radix pass (SPH mode): writes the sorted
+// mirrors xs = (x, y, z, m_eff) and vs = (vx, vy, vz, attr bits).
+struct GatherArgs {
+    const float* x;
+    const float* v;
+    const float* mass;
+    const float* inv_mass;
+    const int* flags;
+    const int* world;
+    int world_count;
+    float4* xs;
+    float4* vs;
+};
+
+// attr bits stored in vs.w
+constexpr int kAttrActive = 1;
+constexpr int kAttrDynamic = 2;
+constexpr int kAttrGravShift = 2;
+
+int grid_init(Grid& g, int dx, int dy, int dz, int device);
+int grid_reserve(Grid& g, int capacity);
+void grid_free(Grid& g);
+// Build over `points` (n x 3 AoS float). gather may be null. status may be
+// null. launches (may be null) is incremented per kernel launched.
+int grid_build(Grid& g, const float* points, int n, float cell_width, float cell_inv, const GatherArgs* gather,
+               unsigned int* status, cudaStream_t stream, int* launches = nullptr);
+
+}  // namespace nsph

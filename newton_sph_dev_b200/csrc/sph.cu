@@ -1,0 +1,443 @@
+// sph.cu — the WCSPH step: grid build on x_n, density/EOS pass, then the
+// pressure + XSPH + integrate pass that writes x_{n+1}, v_{n+1}.
+//
+// The reference has no SPH solver (its particle hot path is the HashGrid
+// gather of newton/_src/solvers/semi_implicit/kernels_contact.py:35-84 plus
+// integrate_particles, newton/_src/solvers/solver.py:10-47); the step keeps
+// that structure and replaces the contact law with published WCSPH math:
+//   W      cubic spline with support h (Monaghan 1992), sigma = 8/(pi h^3)
+//   rho_i  = sum_j m_j W_ij (self included)
+//   p_i    = B((rho_i/rho0)^gamma - 1) clamped at 0 (Tait EOS)
+//   a_i    = -sum_{j!=i} m_j (p_i/rho_i^2 + p_j/rho_j^2) grad W_ij
+//   dv_i   = eps sum_{j!=i} (m_j/rho_j)(v_j - v_i) W_ij (XSPH on v_n)
+// and integrates with integrate_particles' semantics (gravity and forces
+// only for inv_mass > 0, |v| clamp, inactive particles keep x and v).
+//
+// Layout in HBM (sorted by cell, written by the last radix pass):
+//   xs[k]  float4 (x, y, z, m_eff)   m_eff = 0 for inactive particles
+//   vs[k]  float4 (vx, vy, vz, attr) attr = active | dynamic<<1 | gravity<<2
+//   aux[k] float2 (m/rho, p/rho^2)   written by the density pass
+//   rp[k]  float2 (rho, p)           written by the density pass
+// Outputs are scattered back to original particle order through point_ids.
+#include <cmath>
+
+#include "nsph_internal.cuh"
+
+namespace nsph {
+namespace {
+
+constexpr int kSphThreads = 256;
+
+// the neighbour test shared with the oracle (no contraction beyond the two
+// explicit FMAs): r2 = fma(dz, dz, fma(dy, dy, dx*dx))
+__device__ __forceinline__ float dist2(float4 a, float4 b, float& dx, float& dy, float& dz)
+{
+    dx = __fsub_rn(a.x, b.x);
+    dy = __fsub_rn(a.y, b.y);
+    dz = __fsub_rn(a.z, b.z);
+    return __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+}
+
+// Every fp32 operation below is written with an explicit rounding intrinsic
+// (no compiler contraction), in the same order as the fp32 oracle, and each
+// particle's neighbours are summed in the grid's query order, so the device
+// reproduces the fp32 restatement's sums.
+
+// W(q) = sigma * {fma((6q)q, q-1, 1) for q <= 1/2; ((2t)t)t with t = 1-q for q < 1}
+__device__ __forceinline__ float kernel_w(float q, const nsph_sph_params& p)
+{
+    const float t = __fsub_rn(1.f, q);
+    const float nearv = __fmaf_rn(__fmul_rn(__fmul_rn(6.f, q), q), __fsub_rn(q, 1.f), 1.f);
+    const float farv = __fmul_rn(__fmul_rn(__fmul_rn(2.f, t), t), t);
+    return __fmul_rn(p.sigma, q <= 0.5f ? nearv : (q < 1.f ? farv : 0.f));
+}
+
+// (dW/dr)/r = {c_near * fma(3, q, -2) for q <= 1/2; ((c_far t) t)(1/r) for q < 1}
+__device__ __forceinline__ float kernel_f(float q, float inv_r, const nsph_sph_params& p)
+{
+    const float t = __fsub_rn(1.f, q);
+    const float nearv = __fmul_rn(p.c_near, __fmaf_rn(3.f, q, -2.f));
+    const float farv = __fmul_rn(__fmul_rn(__fmul_rn(p.c_far, t), t), inv_r);
+    return q <= 0.5f ? nearv : (q < 1.f ? farv : 0.f);
+}
+
+__device__ __forceinline__ float eos(float rho, const nsph_sph_params& p)
+{
+    const float ratio = __fmul_rn(rho, p.inv_rho0);
+    float pw = 1.f;
+    for (int k = 0; k < p.eos_gamma; ++k) pw = __fmul_rn(pw, ratio);
+    float pr = __fmul_rn(p.eos_b, __fsub_rn(pw, 1.f));
+    if (p.clamp_pressure && pr < 0.f) pr = 0.f;
+    return pr;
+}
+
+// ---- pass 1: density + EOS --------------------------------------------------
+__global__ void __launch_bounds__(kSphThreads) k_density(GridDev g, const float4* __restrict__ xs,
+                                                         const float4* __restrict__ vs, int n,
+                                                         nsph_sph_params p, float2* __restrict__ aux,
+                                                         float2* __restrict__ rp, unsigned* __restrict__ status)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float4 xi = xs[k];
+    const int attr = __float_as_int(vs[k].w);
+    if (!(attr & kAttrActive)) {
+        aux[k] = make_float2(0.f, 0.f);
+        rp[k] = make_float2(0.f, 0.f);
+        return;
+    }
+    float rho = 0.f;
+    for_each_candidate(g, xi.x, xi.y, xi.z, p.h, [&](int j) {
+        const float4 xj = __ldg(xs + j);
+        float dx, dy, dz;
+        const float r2 = dist2(xi, xj, dx, dy, dz);
+        if (r2 < p.h2) rho = __fmaf_rn(xj.w, kernel_w(__fmul_rn(__fsqrt_rn(r2), p.inv_h), p), rho);
+    });
+    float pr = 0.f, mor = 0.f, pr2 = 0.f;
+    if (rho > 0.f) {
+        pr = eos(rho, p);
+        mor = __fdiv_rn(xi.w, rho);
+        pr2 = __fdiv_rn(pr, __fmul_rn(rho, rho));
+    } else if (status) {
+        atomicOr(status, (unsigned)NSPH_STATUS_ZERO_DENSITY);
+    }
+    aux[k] = make_float2(mor, pr2);
+    rp[k] = make_float2(rho, pr);
+}
+
+// ---- pass 2: pressure force + XSPH + integrate --------------------------------
+__global__ void __launch_bounds__(kSphThreads) k_force(GridDev g, const float4* __restrict__ xs,
+                                                       const float4* __restrict__ vs,
+                                                       const float2* __restrict__ aux,
+                                                       const float2* __restrict__ rp, int n, nsph_sph_params p,
+                                                       const float* __restrict__ f_ext,
+                                                       const float* __restrict__ inv_mass,
+                                                       const float* __restrict__ gravity, float* __restrict__ x_out,
+                                                       float* __restrict__ v_out, float* __restrict__ rho_out,
+                                                       float* __restrict__ p_out, float* __restrict__ a_out,
+                                                       unsigned* __restrict__ status)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float4 xi = xs[k];
+    const float4 vi = vs[k];
+    const int attr = __float_as_int(vi.w);
+    const size_t i = (size_t)g.ids[k];
+    if (rho_out || p_out) {
+        const float2 r = rp[k];
+        if (rho_out) rho_out[i] = r.x;
+        if (p_out) p_out[i] = r.y;
+    }
+    if (!(attr & kAttrActive)) {
+        x_out[3 * i + 0] = xi.x;
+        x_out[3 * i + 1] = xi.y;
+        x_out[3 * i + 2] = xi.z;
+        if (a_out) a_out[3 * i + 0] = a_out[3 * i + 1] = a_out[3 * i + 2] = 0.f;
+        return;
+    }
+    const float pr2_i = aux[k].y;
+    float ax = 0.f, ay = 0.f, az = 0.f;
+    float dvx = 0.f, dvy = 0.f, dvz = 0.f;
+    for_each_candidate(g, xi.x, xi.y, xi.z, p.h, [&](int j) {
+        const float4 xj = __ldg(xs + j);
+        float dx, dy, dz;
+        const float r2 = dist2(xi, xj, dx, dy, dz);
+        if (r2 < p.h2 && j != k) {
+            const float4 vj = __ldg(vs + j);
+            if (__float_as_int(vj.w) & kAttrActive) {
+                const float2 aj = __ldg(aux + j);
+                const float r = __fsqrt_rn(r2);
+                const float q = __fmul_rn(r, p.inv_h);
+                const float w = kernel_w(q, p);
+                if (r2 > 0.f) {
+                    const float f = kernel_f(q, __frcp_rn(r), p);
+                    const float s = __fmul_rn(__fmul_rn(xj.w, __fadd_rn(pr2_i, aj.y)), f);
+                    ax = __fmaf_rn(-s, dx, ax);
+                    ay = __fmaf_rn(-s, dy, ay);
+                    az = __fmaf_rn(-s, dz, az);
+                }
+                const float c = __fmul_rn(aj.x, w);
+                dvx = __fmaf_rn(c, __fsub_rn(vj.x, vi.x), dvx);
+                dvy = __fmaf_rn(c, __fsub_rn(vj.y, vi.y), dvy);
+                dvz = __fmaf_rn(c, __fsub_rn(vj.z, vi.z), dvz);
+            }
+        }
+    });
+    if (a_out) {
+        a_out[3 * i + 0] = ax;
+        a_out[3 * i + 1] = ay;
+        a_out[3 * i + 2] = az;
+    }
+    float v1x = vi.x, v1y = vi.y, v1z = vi.z;
+    const bool dynamic = (attr & kAttrDynamic) != 0;
+    if (dynamic) {
+        const int gw = attr >> kAttrGravShift;
+        float fx = 0.f, fy = 0.f, fz = 0.f;
+        if (f_ext) {
+            const float w = inv_mass[i];
+            fx = __fmul_rn(f_ext[3 * i + 0], w);
+            fy = __fmul_rn(f_ext[3 * i + 1], w);
+            fz = __fmul_rn(f_ext[3 * i + 2], w);
+        }
+        const float gx = gravity[3 * gw + 0], gy = gravity[3 * gw + 1], gz = gravity[3 * gw + 2];
+        // v1 = fma(eps, dv, fma((a + f w) + g, dt, v0))
+        v1x = __fmaf_rn(p.xsph_eps, dvx, __fmaf_rn(__fadd_rn(__fadd_rn(ax, fx), gx), p.dt, vi.x));
+        v1y = __fmaf_rn(p.xsph_eps, dvy, __fmaf_rn(__fadd_rn(__fadd_rn(ay, fy), gy), p.dt, vi.y));
+        v1z = __fmaf_rn(p.xsph_eps, dvz, __fmaf_rn(__fadd_rn(__fadd_rn(az, fz), gz), p.dt, vi.z));
+    }
+    const float vm = __fsqrt_rn(__fmaf_rn(v1z, v1z, __fmaf_rn(v1y, v1y, __fmul_rn(v1x, v1x))));
+    if (vm > p.v_max) {
+        const float s = __fdiv_rn(p.v_max, vm);
+        v1x = __fmul_rn(v1x, s);
+        v1y = __fmul_rn(v1y, s);
+        v1z = __fmul_rn(v1z, s);
+    }
+    float x1x = __fmaf_rn(v1x, p.dt, xi.x), x1y = __fmaf_rn(v1y, p.dt, xi.y), x1z = __fmaf_rn(v1z, p.dt, xi.z);
+    if (dynamic && p.use_box) {
+        if (x1x < p.box_lo[0]) { x1x = p.box_lo[0]; v1x = fmaxf(v1x, 0.f); }
+        if (x1x > p.box_hi[0]) { x1x = p.box_hi[0]; v1x = fminf(v1x, 0.f); }
+        if (x1y < p.box_lo[1]) { x1y = p.box_lo[1]; v1y = fmaxf(v1y, 0.f); }
+        if (x1y > p.box_hi[1]) { x1y = p.box_hi[1]; v1y = fminf(v1y, 0.f); }
+        if (x1z < p.box_lo[2]) { x1z = p.box_lo[2]; v1z = fmaxf(v1z, 0.f); }
+        if (x1z > p.box_hi[2]) { x1z = p.box_hi[2]; v1z = fminf(v1z, 0.f); }
+    }
+    if (status && !(isfinite(x1x) && isfinite(x1y) && isfinite(x1z) && isfinite(v1x) && isfinite(v1y) &&
+                    isfinite(v1z)))
+        atomicOr(status, (unsigned)NSPH_STATUS_NONFINITE_OUTPUT);
+    x_out[3 * i + 0] = x1x;
+    x_out[3 * i + 1] = x1y;
+    x_out[3 * i + 2] = x1z;
+    v_out[3 * i + 0] = v1x;
+    v_out[3 * i + 1] = v1y;
+    v_out[3 * i + 2] = v1z;
+}
+
+// ---- neighbour lists of the last build (parity export) ----------------------
+__global__ void k_neighbors(GridDev g, const float4* __restrict__ xs, const float4* __restrict__ vs, int n,
+                            nsph_sph_params p, int* __restrict__ counts, const long long* __restrict__ offsets,
+                            int* __restrict__ out)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = g.ids[k];
+    const float4 xi = xs[k];
+    const bool active = (__float_as_int(vs[k].w) & kAttrActive) != 0;
+    long long o = out ? offsets[i] : 0;
+    int c = 0;
+    if (active) {
+        for_each_candidate(g, xi.x, xi.y, xi.z, p.h, [&](int j) {
+            const float4 xj = xs[j];
+            float dx, dy, dz;
+            if (dist2(xi, xj, dx, dy, dz) < p.h2 && (__float_as_int(vs[j].w) & kAttrActive)) {
+                if (out) out[o++] = g.ids[j];
+                ++c;
+            }
+        });
+    }
+    if (!out) counts[i] = c;
+}
+
+}  // namespace
+}  // namespace nsph
+
+// ==========================================================================
+// C ABI: solver context
+// ==========================================================================
+using namespace nsph;
+
+struct nsph_sph {
+    Grid grid;
+    int capacity = 0;
+    float4* xs = nullptr;
+    float4* vs = nullptr;
+    float2* aux = nullptr;
+    float2* rp = nullptr;
+    unsigned* status = nullptr;
+    int last_n = 0;
+    int last_launches = 0;
+    cudaEvent_t ev_after_build = nullptr;
+    cudaEvent_t ev_after_density = nullptr;
+};
+
+static void sph_free(nsph_sph* s)
+{
+    DeviceGuard guard(s->grid.device);
+    cudaFree(s->xs);
+    cudaFree(s->vs);
+    cudaFree(s->aux);
+    cudaFree(s->rp);
+    cudaFree(s->status);
+    grid_free(s->grid);
+}
+
+extern "C" int nsph_sph_create(int device, int capacity, const int grid_dims[3], nsph_sph** out)
+{
+    clear_error();
+    if (!out || !grid_dims) return fail(NSPH_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    if (capacity < 0) return fail(NSPH_ERR_INVALID_ARG, "negative capacity");
+    nsph_sph* s = new (std::nothrow) nsph_sph();
+    if (!s) return fail(NSPH_ERR_OUT_OF_MEMORY, "host allocation failed");
+    int st = grid_init(s->grid, grid_dims[0], grid_dims[1], grid_dims[2], device);
+    if (st == NSPH_OK) st = grid_reserve(s->grid, capacity);
+    if (st == NSPH_OK) {
+        DeviceGuard guard(device);
+        const size_t c = (size_t)(capacity > 0 ? capacity : 1);
+        cudaError_t e = cudaMalloc(&s->xs, sizeof(float4) * c);
+        if (e == cudaSuccess) e = cudaMalloc(&s->vs, sizeof(float4) * c);
+        if (e == cudaSuccess) e = cudaMalloc(&s->aux, sizeof(float2) * c);
+        if (e == cudaSuccess) e = cudaMalloc(&s->rp, sizeof(float2) * c);
+        if (e == cudaSuccess) e = cudaMalloc(&s->status, sizeof(unsigned));
+        if (e == cudaSuccess) e = cudaMemset(s->status, 0, sizeof(unsigned));
+        cudaFuncAttributes fa;
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_density);
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_force);
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_neighbors);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            st = fail(NSPH_ERR_OUT_OF_MEMORY, std::string("solver allocation: ") + cudaGetErrorString(e));
+        }
+    }
+    if (st != NSPH_OK) {
+        sph_free(s);
+        delete s;
+        return st;
+    }
+    s->capacity = capacity;
+    *out = s;
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_destroy(nsph_sph* solver)
+{
+    clear_error();
+    if (!solver) return NSPH_OK;
+    sph_free(solver);
+    delete solver;
+    return NSPH_OK;
+}
+
+static int check_params(const nsph_sph_params* p)
+{
+    if (!p) return fail(NSPH_ERR_INVALID_ARG, "null params");
+    if (!(p->h > 0.f) || !(p->h2 > 0.f) || !(p->cell_inv > 0.f) || !isfinite(p->h) || !isfinite(p->cell_inv))
+        return fail(NSPH_ERR_INVALID_ARG, "h and cell width must be positive and finite");
+    if (p->eos_gamma < 0 || p->eos_gamma > 16) return fail(NSPH_ERR_INVALID_ARG, "eos_gamma out of [0, 16]");
+    if (!(p->rho0 > 0.f)) return fail(NSPH_ERR_INVALID_ARG, "rho0 must be positive");
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_step(nsph_sph* s, const nsph_sph_params* p, int n, const float* x_in, const float* v_in,
+                             const float* f_ext, const float* mass, const float* inv_mass, const int* flags,
+                             const int* world, const float* gravity, int world_count, float* x_out,
+                             float* v_out, float* rho_out, float* p_out, float* a_out, void* stream)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    int st = check_params(p);
+    if (st != NSPH_OK) return st;
+    if (n < 0) return fail(NSPH_ERR_INVALID_ARG, "negative particle count");
+    if (n > s->capacity) return fail(NSPH_ERR_CAPACITY, "more particles than the solver was created for");
+    if (world_count < 1 || !gravity) return fail(NSPH_ERR_INVALID_ARG, "gravity needs world_count >= 1");
+    if (n > 0 && (!x_in || !v_in || !mass || !inv_mass || !flags || !x_out || !v_out))
+        return fail(NSPH_ERR_INVALID_ARG, "null state or model array");
+    if (n > 0 && (x_out == x_in || v_out == v_in))
+        return fail(NSPH_ERR_INVALID_ARG, "state_out must not alias state_in");
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    cudaStream_t cs = (cudaStream_t)stream;
+    GatherArgs ga{x_in, v_in, mass, inv_mass, flags, world, world_count, s->xs, s->vs};
+    int launches = 0;
+    st = grid_build(s->grid, x_in, n, p->cell_width, p->cell_inv, &ga, s->status, cs, &launches);
+    if (st != NSPH_OK) return st;
+    s->last_n = n;
+    if (s->ev_after_build) NSPH_CUDA_TRY(cudaEventRecordWithFlags(s->ev_after_build, cs, cudaEventRecordExternal));
+    if (n > 0) {
+        const GridDev g = s->grid.view();
+        const int blocks = (n + kSphThreads - 1) / kSphThreads;
+        k_density<<<blocks, kSphThreads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->status);
+        NSPH_LAUNCH_CHECK("k_density");
+        ++launches;
+        if (s->ev_after_density)
+            NSPH_CUDA_TRY(cudaEventRecordWithFlags(s->ev_after_density, cs, cudaEventRecordExternal));
+        k_force<<<blocks, kSphThreads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, f_ext, inv_mass, gravity,
+                                                x_out, v_out, rho_out, p_out, a_out, s->status);
+        NSPH_LAUNCH_CHECK("k_force");
+        ++launches;
+    } else if (s->ev_after_density) {
+        NSPH_CUDA_TRY(cudaEventRecordWithFlags(s->ev_after_density, cs, cudaEventRecordExternal));
+    }
+    s->last_launches = launches;
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_neighbors(const nsph_sph* s, const nsph_sph_params* p, int* counts,
+                                  const long long* offsets, int* out_ids, void* stream)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    int st = check_params(p);
+    if (st != NSPH_OK) return st;
+    if (!s->grid.built) return fail(NSPH_ERR_NOT_BUILT, "no step has run yet");
+    if (out_ids ? !offsets : !counts) return fail(NSPH_ERR_INVALID_ARG, "counts (count call) or offsets (fill call) required");
+    const int n = s->last_n;
+    if (n == 0) return NSPH_OK;
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    k_neighbors<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(s->grid.view(), s->xs, s->vs, n, *p, counts,
+                                                                   offsets, out_ids);
+    NSPH_LAUNCH_CHECK("k_neighbors");
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_get_grid_view(const nsph_sph* s, nsph_grid_view* view)
+{
+    clear_error();
+    if (!s || !view) return fail(NSPH_ERR_INVALID_ARG, "null argument");
+    const Grid& g = s->grid;
+    view->point_cells = g.point_cells;
+    view->point_ids = g.point_ids;
+    view->cell_starts = g.cell_starts;
+    view->cell_ends = g.cell_ends;
+    view->num_points = g.num_points;
+    view->dim_x = g.dx;
+    view->dim_y = g.dy;
+    view->dim_z = g.dz;
+    view->cell_width = g.cell_width;
+    view->cell_width_inv = g.cell_inv;
+    view->built = g.built;
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_set_phase_events(nsph_sph* s, void* after_build, void* after_density)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    s->ev_after_build = (cudaEvent_t)after_build;
+    s->ev_after_density = (cudaEvent_t)after_density;
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_last_launches(const nsph_sph* s) { return s ? s->last_launches : 0; }
+
+extern "C" int nsph_sph_status(nsph_sph* s, unsigned int* status, void* stream)
+{
+    clear_error();
+    if (!s || !status) return fail(NSPH_ERR_INVALID_ARG, "null argument");
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    NSPH_CUDA_TRY(cudaMemcpyAsync(status, s->status, sizeof(unsigned), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    NSPH_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_reset_status(nsph_sph* s, void* stream)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    NSPH_CUDA_TRY(cudaMemsetAsync(s->status, 0, sizeof(unsigned), (cudaStream_t)stream));
+    return NSPH_OK;
+}

@@ -1,0 +1,366 @@
+"""SolverSPH: weakly-compressible SPH behind Newton's solver interface.
+
+The reference (NVIDIA Newton) has no SPH solver. This solver keeps its
+interface — ``SolverBase.step(state_in, state_out, control, contacts, dt)``
+(newton/_src/solvers/solver.py:301-316), ``notify_model_changed``
+(:318-345), ``register_custom_attributes`` (:358-366), a nested ``Config``
+like ``SolverImplicitMPM.Config`` (solver_implicit_mpm.py:643) — and the
+structure of its particle hot path: a HashGrid build on the particle
+positions (solver_xpbd.py:315-319), per-particle neighbour gathers through
+the grid (kernels_contact.py:35-84) and integrate_particles semantics
+(solver.py:10-47).
+
+One step = one ``nsph_sph_step`` call into libnsph.so: grid build (hash +
+LSD radix sort + cell ranges + sorted gather), density/EOS pass,
+pressure/XSPH/integrate pass. Stream-ordered on the current torch stream,
+no allocation and no host sync, so a step (or a loop of steps) can be
+captured with ``torch.cuda.graph``. Gravity is read from ``model.gravity``
+on the device, so ``model.set_gravity`` reaches replayed graphs; scalar
+parameters (dt, h, ...) are kernel arguments and are frozen into a captured
+graph, as they are in Warp.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from .. import _lib
+from ..sim import Model, ModelBuilder, State
+from ..sim.control import Control
+from .flags import SolverNotifyFlags
+from .solver import SolverBase, _require_cuda
+
+F32 = np.float32
+
+
+def _next_pow2(v: int) -> int:
+    p = 1
+    while p < v:
+        p <<= 1
+    return p
+
+
+def _trunc(v: float) -> int:
+    return int(math.trunc(v)) if math.isfinite(v) else 0
+
+
+@dataclass
+class SPHConfig:
+    """Parameters of :class:`SolverSPH`.
+
+    Attributes:
+        smoothing_length: kernel support radius h [m] (the neighbour radius;
+            the cubic spline vanishes at r = h). With h = 2 x spacing a
+            particle has about 33 neighbours.
+        rest_density: rho0 [kg/m^3].
+        sound_speed: c0 [m/s] of the Tait equation of state.
+        eos_gamma: Tait exponent (integer).
+        xsph: XSPH velocity-smoothing coefficient epsilon.
+        clamp_pressure: clamp negative pressure to 0 (no tensile suction at
+            free surfaces and walls).
+        box_lo, box_hi: axis-aligned domain [m]; dynamic particles are
+            clamped to it and lose the velocity component into the wall.
+            None disables the box.
+        cell_width: grid cell width [m]; defaults to h.
+        grid_dims: cells per axis of the neighbour grid; by default the
+            smallest powers of two that cover the box plus one guard cell on
+            each side (so no two box cells alias), else 128^3.
+        apply_particle_f: add ``state_in.particle_f * inv_mass`` (external
+            forces) to the acceleration, as integrate_particles does.
+    """
+
+    smoothing_length: float = 0.02
+    rest_density: float = 1000.0
+    sound_speed: float = 20.0
+    eos_gamma: int = 7
+    xsph: float = 0.01
+    clamp_pressure: bool = True
+    box_lo: tuple[float, float, float] | None = None
+    box_hi: tuple[float, float, float] | None = None
+    cell_width: float | None = None
+    grid_dims: tuple[int, int, int] | None = None
+    apply_particle_f: bool = True
+
+    # ---- derived constants ------------------------------------------
+    def constants(self, dt: float, v_max: float) -> dict:
+        """fp32 constants handed to the device (and to the fp32 oracle), plus
+        their fp64 counterparts for the fp64 oracle. The fp64 values start
+        from the fp32-rounded h so both describe the same kernel support."""
+        h32 = F32(self.smoothing_length)
+        cw32 = F32(self.cell_width if self.cell_width is not None else self.smoothing_length)
+        h = float(h32)
+        sigma = 8.0 / (math.pi * h**3)
+        b = self.rest_density * self.sound_speed**2 / self.eos_gamma if self.eos_gamma > 0 else 0.0
+        use_box = self.box_lo is not None and self.box_hi is not None
+        lo = tuple(float(F32(v)) for v in (self.box_lo if use_box else (0.0, 0.0, 0.0)))
+        hi = tuple(float(F32(v)) for v in (self.box_hi if use_box else (0.0, 0.0, 0.0)))
+        f32 = {
+            "h": h32,
+            "h2": F32(h32 * h32),
+            "inv_h": F32(F32(1.0) / h32),
+            "cell_width": cw32,
+            "cell_inv": F32(F32(1.0) / cw32),
+            "sigma": F32(sigma),
+            "dsigma": F32(sigma / h),
+            "c_near": F32(6.0 * sigma / (h * h)),
+            "c_far": F32(-6.0 * sigma / h),
+            "rho0": F32(self.rest_density),
+            "inv_rho0": F32(1.0 / self.rest_density),
+            "eos_b": F32(b),
+            "eos_gamma": int(self.eos_gamma),
+            "clamp_pressure": int(bool(self.clamp_pressure)),
+            "xsph_eps": F32(self.xsph),
+            "v_max": F32(v_max),
+            "dt": F32(dt),
+            "use_box": int(use_box),
+            "box_lo": tuple(F32(v) for v in lo),
+            "box_hi": tuple(F32(v) for v in hi),
+        }
+        f64 = {
+            "h": h,
+            "inv_h": 1.0 / h,
+            "sigma": sigma,
+            "dsigma": sigma / h,
+            "c_near": 6.0 * sigma / (h * h),
+            "c_far": -6.0 * sigma / h,
+            "rho0": float(self.rest_density),
+            "inv_rho0": 1.0 / self.rest_density,
+            "eos_b": b,
+            "xsph_eps": float(self.xsph),
+            "v_max": float(v_max),
+            "dt": float(dt),
+            "box_lo": lo,
+            "box_hi": hi,
+            "eos_gamma": int(self.eos_gamma),
+            "clamp_pressure": int(bool(self.clamp_pressure)),
+            "use_box": int(use_box),
+        }
+        return {"f32": f32, "f64": f64}
+
+    def resolved_grid_dims(self) -> tuple[int, int, int]:
+        if self.grid_dims is not None:
+            return tuple(int(d) for d in self.grid_dims)
+        if self.box_lo is None or self.box_hi is None:
+            return (128, 128, 128)
+        inv = float(F32(1.0) / F32(self.cell_width if self.cell_width is not None else self.smoothing_length))
+        dims = []
+        for a in range(3):
+            lo = _trunc(float(F32(F32(self.box_lo[a]) * F32(inv))))
+            hi = _trunc(float(F32(F32(self.box_hi[a]) * F32(inv))))
+            dims.append(min(2048, _next_pow2(max(4, hi - lo + 3))))
+        while dims[0] * dims[1] * dims[2] > (1 << 26):
+            k = int(np.argmax(dims))
+            dims[k] //= 2
+        return tuple(dims)
+
+    def params(self, dt: float, v_max: float) -> _lib.NsphSphParams:
+        c = self.constants(dt, v_max)["f32"]
+        p = _lib.NsphSphParams()
+        for name, _ in _lib.NsphSphParams._fields_:
+            val = c[name]
+            if name in ("box_lo", "box_hi"):
+                getattr(p, name)[:] = [float(v) for v in val]
+            elif isinstance(val, int):
+                setattr(p, name, val)
+            else:
+                setattr(p, name, float(val))
+        return p
+
+
+class SolverSPH(SolverBase):
+    """WCSPH particle-fluid solver on one CUDA device.
+
+    Example::
+
+        builder = ModelBuilder()
+        SolverSPH.register_custom_attributes(builder)   # optional sph.density/pressure
+        builder.add_particle_grid(...)
+        model = builder.finalize("cuda:0")
+        solver = SolverSPH(model, SolverSPH.Config(smoothing_length=0.02, box_lo=(0,0,0), box_hi=(1,1,1)))
+        s0, s1 = model.state(), model.state()
+        solver.step(s0, s1, model.control(), None, 1e-4)
+    """
+
+    Config = SPHConfig
+
+    def __init__(self, model: Model, config: SPHConfig | None = None):
+        super().__init__(model)
+        self.config = config if config is not None else SPHConfig()
+        if self.config.smoothing_length <= 0.0:
+            raise ValueError("smoothing_length must be positive")
+        if model.device.type != "cuda":
+            raise RuntimeError("SolverSPH runs on CUDA only (there is no CPU fallback)")
+        self._lib = _lib.load()
+        self.grid_dims = self.config.resolved_grid_dims()
+        self._handle = ctypes.c_void_p()
+        dims = (ctypes.c_int * 3)(*self.grid_dims)
+        _lib.check(
+            self._lib.nsph_sph_create(model.device.index or 0, int(model.particle_count), ctypes.byref(dims),
+                                      ctypes.byref(self._handle)),
+            "SolverSPH()",
+        )
+        self._params = self.config.params(0.0, model.particle_max_velocity)
+        self._dt = None
+
+    def __del__(self):
+        h = getattr(self, "_handle", None)
+        if h is not None and h.value:
+            self._lib.nsph_sph_destroy(h)
+            self._handle = None
+
+    # ------------------------------------------------------------------
+    def params_for(self, dt: float) -> _lib.NsphSphParams:
+        """The fp32 parameter block of a step with time step dt."""
+        if self._dt != dt:
+            self._params.dt = float(F32(dt))
+            self._dt = dt
+        return self._params
+
+    def step(self, state_in: State, state_out: State, control: Control | None, contacts, dt: float) -> None:
+        """Advance one WCSPH step from state_in to state_out.
+
+        Args:
+            state_in: positions/velocities at time t (and external forces in
+                ``particle_f`` when ``config.apply_particle_f``).
+            state_out: receives positions/velocities at t + dt; when the model
+                registered the ``sph`` state attributes, also the density and
+                pressure of the step (``state_out.sph.density`` / ``.pressure``).
+                Must not share arrays with state_in.
+            control: unused (a particle fluid has no control inputs); None is
+                accepted as in the reference.
+            contacts: must be None: particle-shape contacts are not part of
+                this solver (the box boundary is handled in the kernel).
+            dt: time step [s].
+        """
+        if contacts is not None:
+            raise ValueError("SolverSPH does not consume Contacts; pass contacts=None")
+        model = self.model
+        n = model.particle_count
+        if n == 0:
+            return
+        for name, t in (("state_in.particle_q", state_in.particle_q), ("state_in.particle_qd", state_in.particle_qd),
+                        ("state_out.particle_q", state_out.particle_q),
+                        ("state_out.particle_qd", state_out.particle_qd)):
+            _require_cuda(t, name)
+            if t.dtype != torch.float32 or tuple(t.shape) != (n, 3) or not t.is_contiguous():
+                raise ValueError(f"{name} must be a contiguous ({n}, 3) float32 tensor")
+        f_ext = state_in.particle_f if (self.config.apply_particle_f and state_in.particle_f is not None) else None
+        ns = getattr(state_out, "sph", None)
+        rho = getattr(ns, "density", None) if ns is not None else None
+        prs = getattr(ns, "pressure", None) if ns is not None else None
+        acc = getattr(ns, "acceleration", None) if ns is not None else None
+        p = self.params_for(dt)
+        st = self._lib.nsph_sph_step(
+            self._handle,
+            ctypes.byref(p),
+            n,
+            state_in.particle_q.data_ptr(),
+            state_in.particle_qd.data_ptr(),
+            _lib.ptr(f_ext),
+            model.particle_mass.data_ptr(),
+            model.particle_inv_mass.data_ptr(),
+            model.particle_flags.data_ptr(),
+            model.particle_world.data_ptr(),
+            model.gravity.data_ptr(),
+            int(model.gravity.shape[0]),
+            state_out.particle_q.data_ptr(),
+            state_out.particle_qd.data_ptr(),
+            _lib.ptr(rho),
+            _lib.ptr(prs),
+            _lib.ptr(acc),
+            _lib.stream_handle(model.device),
+        )
+        _lib.check(st, "SolverSPH.step")
+
+    def notify_model_changed(self, flags: int) -> None:
+        """MODEL_PROPERTIES re-reads particle_max_velocity; gravity needs no
+        action (read on the device every step)."""
+        if flags & SolverNotifyFlags.MODEL_PROPERTIES:
+            self._params = self.config.params(0.0 if self._dt is None else self._dt,
+                                              self.model.particle_max_velocity)
+
+    @classmethod
+    def register_custom_attributes(cls, builder: ModelBuilder) -> None:
+        """Declare the per-particle state outputs ``sph:density`` and
+        ``sph:pressure`` (float32), following the solver-namespace pattern of
+        SolverImplicitMPM.register_custom_attributes."""
+        for name in ("density", "pressure"):
+            builder.add_custom_attribute(
+                ModelBuilder.CustomAttribute(name, frequency=Model.AttributeFrequency.PARTICLE,
+                                             assignment=Model.AttributeAssignment.STATE, dtype=torch.float32,
+                                             default=0.0, namespace="sph")
+            )
+
+    # ---- inspection of the last step -----------------------------------
+    def neighbors(self) -> tuple[torch.Tensor, torch.Tensor]:
+        """Neighbour lists of the last step's positions, original order:
+        ids[offsets[i]:offsets[i+1]] are the active particles within h of
+        particle i (self included), in the grid query order.
+
+        Returns:
+            (offsets int64 (N+1,), ids int32)
+        """
+        n = self.model.particle_count
+        dev = self.model.device
+        counts = torch.zeros(n, dtype=torch.int32, device=dev)
+        stream = _lib.stream_handle(dev)
+        p = self._params
+        _lib.check(self._lib.nsph_sph_neighbors(self._handle, ctypes.byref(p), counts.data_ptr(), None, None, stream),
+                   "SolverSPH.neighbors")
+        offsets = torch.zeros(n + 1, dtype=torch.int64, device=dev)
+        offsets[1:] = torch.cumsum(counts.to(torch.int64), 0)
+        total = int(offsets[-1].item())
+        ids = torch.empty(max(total, 1), dtype=torch.int32, device=dev)
+        _lib.check(self._lib.nsph_sph_neighbors(self._handle, ctypes.byref(p), None, offsets.data_ptr(),
+                                                ids.data_ptr(), stream), "SolverSPH.neighbors")
+        return offsets, ids[:total]
+
+    def grid_arrays(self) -> dict[str, torch.Tensor]:
+        """Copies of the last step's grid: sorted cell ids, sorted point ids
+        (the permutation), cell_starts and cell_ends."""
+        from ..hashgrid import _view_int
+
+        v = _lib.NsphGridView()
+        _lib.check(self._lib.nsph_sph_get_grid_view(self._handle, ctypes.byref(v)), "SolverSPH.grid_arrays")
+        dev = self.model.device
+        nc = v.dim_x * v.dim_y * v.dim_z
+        return {
+            "point_cells": _view_int(v.point_cells, v.num_points, dev).clone(),
+            "point_ids": _view_int(v.point_ids, v.num_points, dev).clone(),
+            "cell_starts": _view_int(v.cell_starts, nc, dev).clone(),
+            "cell_ends": _view_int(v.cell_ends, nc, dev).clone(),
+        }
+
+    def set_phase_events(self, after_build=None, after_density=None) -> None:
+        """Record `after_build` / `after_density` (torch.cuda.Event with
+        enable_timing=True) inside every later step, between the grid build,
+        the density pass and the force pass. Recorded as external events, so
+        they also time the phases of a step replayed from a CUDA graph."""
+        eb = after_build.cuda_event if after_build is not None else None
+        ed = after_density.cuda_event if after_density is not None else None
+        _lib.check(self._lib.nsph_sph_set_phase_events(self._handle, eb, ed), "SolverSPH.set_phase_events")
+
+    @property
+    def last_launches(self) -> int:
+        """Kernels launched by the last step."""
+        return int(self._lib.nsph_sph_last_launches(self._handle))
+
+    def status(self) -> int:
+        """Device status word (NSPH_STATUS_* bits) accumulated since the last
+        reset; synchronises the current stream."""
+        s = ctypes.c_uint(0)
+        _lib.check(self._lib.nsph_sph_status(self._handle, ctypes.byref(s), _lib.stream_handle(self.model.device)),
+                   "SolverSPH.status")
+        return int(s.value)
+
+    def reset_status(self) -> None:
+        _lib.check(self._lib.nsph_sph_reset_status(self._handle, _lib.stream_handle(self.model.device)),
+                   "SolverSPH.reset_status")
+
+
+__all__ = ["SPHConfig", "SolverSPH"]

@@ -1,0 +1,388 @@
+"""CPU oracle for the particle-fluid hot path — ctypes wrapper of liboracle.so
+plus pure-Python restatements for small cases.
+
+TEST INFRASTRUCTURE ONLY. This module is the checker: only the tests, the
+smoke check (``__graft_entry__.smoke``) and the benchmark's CPU-baseline leg
+may import it, and never as the thing measured or shipped.
+
+What it restates (reference paths inside the Newton source tree):
+  - Warp HashGrid build/query (external warp-lang 1.14.0.dev20260511; call
+    sites newton/_src/sim/builder.py:9853,
+    newton/_src/solvers/xpbd/solver_xpbd.py:139,315-319,
+    newton/_src/solvers/semi_implicit/kernels_contact.py:54,68,71);
+  - integrate_particles, newton/_src/solvers/solver.py:10-47;
+  - the lattice generator ModelBuilder.add_particle_grid,
+    newton/_src/sim/builder.py:8085-8096 (``lattice_py``);
+  - the WCSPH step (published methods; the reference has no SPH).
+
+Parity status: UNPINNED against the reference itself — the reference ships
+no golden vectors for HashGrid or particle dynamics, cannot run here (no
+warp-lang) and has no SPH. The oracle is pinned by analytic known answers and
+brute-force restatements instead (tests/test_oracle.py).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+ORACLE_DIR = Path(__file__).resolve().parent
+LIB_PATH = ORACLE_DIR / "liboracle.so"
+
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(dtype=np.int64, flags="C_CONTIGUOUS")
+
+
+class SphParams32(ctypes.Structure):
+    """Layout of nsph_sph_params (include/nsph.h)."""
+
+    _fields_ = [
+        ("h", ctypes.c_float),
+        ("h2", ctypes.c_float),
+        ("inv_h", ctypes.c_float),
+        ("cell_width", ctypes.c_float),
+        ("cell_inv", ctypes.c_float),
+        ("sigma", ctypes.c_float),
+        ("dsigma", ctypes.c_float),
+        ("c_near", ctypes.c_float),
+        ("c_far", ctypes.c_float),
+        ("rho0", ctypes.c_float),
+        ("inv_rho0", ctypes.c_float),
+        ("eos_b", ctypes.c_float),
+        ("eos_gamma", ctypes.c_int),
+        ("clamp_pressure", ctypes.c_int),
+        ("xsph_eps", ctypes.c_float),
+        ("v_max", ctypes.c_float),
+        ("dt", ctypes.c_float),
+        ("use_box", ctypes.c_int),
+        ("box_lo", ctypes.c_float * 3),
+        ("box_hi", ctypes.c_float * 3),
+    ]
+
+
+class Phys64(ctypes.Structure):
+    """Layout of oracle_phys_f64 (oracle/nsph_oracle.h)."""
+
+    _fields_ = [
+        ("h", ctypes.c_double),
+        ("inv_h", ctypes.c_double),
+        ("sigma", ctypes.c_double),
+        ("dsigma", ctypes.c_double),
+        ("rho0", ctypes.c_double),
+        ("inv_rho0", ctypes.c_double),
+        ("eos_b", ctypes.c_double),
+        ("xsph_eps", ctypes.c_double),
+        ("v_max", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("c_near", ctypes.c_double),
+        ("c_far", ctypes.c_double),
+        ("box_lo", ctypes.c_double * 3),
+        ("box_hi", ctypes.c_double * 3),
+        ("eos_gamma", ctypes.c_int),
+        ("clamp_pressure", ctypes.c_int),
+        ("use_box", ctypes.c_int),
+    ]
+
+
+def build(force: bool = False) -> Path:
+    """Compile liboracle.so with the Makefile beside this file."""
+    srcs = list(ORACLE_DIR.glob("*.c")) + list(ORACLE_DIR.glob("*.h")) + [ORACLE_DIR / "Makefile"]
+    if not force and LIB_PATH.exists() and all(s.stat().st_mtime <= LIB_PATH.stat().st_mtime for s in srcs):
+        return LIB_PATH
+    res = subprocess.run(["make", "-B" if force else "-s", "-C", str(ORACLE_DIR)], capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{res.stdout}\n{res.stderr}")
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        build()
+    L = ctypes.CDLL(str(LIB_PATH))
+    L.oracle_trunc_sat.restype = ctypes.c_int
+    L.oracle_trunc_sat.argtypes = [ctypes.c_float]
+    L.oracle_grid_index.restype = ctypes.c_int
+    L.oracle_grid_index.argtypes = [ctypes.c_int] * 6
+    L.oracle_grid_build.restype = ctypes.c_int
+    L.oracle_grid_build.argtypes = [_f32p, ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    _i32p, _i32p, _i32p, _i32p]
+    L.oracle_grid_query.restype = ctypes.c_longlong
+    L.oracle_grid_query.argtypes = [_i32p, _i32p, _i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                                    _f32p, ctypes.c_float, ctypes.c_void_p, ctypes.c_longlong]
+    L.oracle_sph_neighbors.restype = ctypes.c_int
+    L.oracle_sph_neighbors.argtypes = [ctypes.POINTER(SphParams32), ctypes.c_int, _f32p, _i32p, _i32p, _i32p,
+                                       ctypes.c_void_p, ctypes.c_void_p]
+    L.oracle_sph_step_f32.restype = ctypes.c_int
+    L.oracle_sph_step_f32.argtypes = [ctypes.POINTER(SphParams32), _i32p, ctypes.c_int] + [ctypes.c_void_p] * 7 + \
+        [_f32p, ctypes.c_int] + [ctypes.c_void_p] * 6
+    L.oracle_sph_step_f64.restype = ctypes.c_int
+    L.oracle_sph_step_f64.argtypes = [ctypes.POINTER(SphParams32), ctypes.POINTER(Phys64), _i32p, ctypes.c_int] + \
+        [ctypes.c_void_p] * 7 + [_f32p, ctypes.c_int] + [ctypes.c_void_p] * 6
+    L.oracle_integrate_particles_f32.restype = None
+    L.oracle_integrate_particles_f32.argtypes = [_f32p, _f32p, _f32p, _f32p, _i32p, _i32p, _f32p, ctypes.c_int,
+                                                 ctypes.c_int, ctypes.c_float, ctypes.c_float, _f32p, _f32p]
+    L.oracle_integrate_particles_f64.restype = None
+    L.oracle_integrate_particles_f64.argtypes = [_f32p, _f32p, _f32p, _f32p, _i32p, _i32p, _f32p, ctypes.c_int,
+                                                 ctypes.c_int, ctypes.c_double, ctypes.c_double, _f64p, _f64p]
+    L.oracle_set_threads.restype = None
+    L.oracle_set_threads.argtypes = [ctypes.c_int]
+    L.oracle_get_threads.restype = ctypes.c_int
+    L.oracle_get_threads.argtypes = []
+    _lib = L
+    return L
+
+
+def set_threads(n: int) -> None:
+    lib().oracle_set_threads(int(n))
+
+
+def get_threads() -> int:
+    return int(lib().oracle_get_threads())
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+# ---------------------------------------------------------------------------
+# parameter blocks from the constants dict of SPHConfig.constants()
+# ---------------------------------------------------------------------------
+def params32(c32: dict) -> SphParams32:
+    p = SphParams32()
+    for name, _ in SphParams32._fields_:
+        v = c32[name]
+        if name in ("box_lo", "box_hi"):
+            getattr(p, name)[:] = [float(x) for x in v]
+        elif isinstance(v, int):
+            setattr(p, name, v)
+        else:
+            setattr(p, name, float(v))
+    return p
+
+
+def phys64(c64: dict) -> Phys64:
+    p = Phys64()
+    for name, _ in Phys64._fields_:
+        v = c64[name]
+        if name in ("box_lo", "box_hi"):
+            getattr(p, name)[:] = [float(x) for x in v]
+        elif isinstance(v, int):
+            setattr(p, name, v)
+        else:
+            setattr(p, name, float(v))
+    return p
+
+
+# ---------------------------------------------------------------------------
+# HashGrid
+# ---------------------------------------------------------------------------
+def grid_build(points: np.ndarray, radius: float, dims: tuple[int, int, int]) -> dict[str, np.ndarray]:
+    """HashGrid.build restated: sorted cell ids, sorted point ids, ranges."""
+    pts = _f32(points).reshape(-1, 3)
+    n = pts.shape[0]
+    nc = dims[0] * dims[1] * dims[2]
+    out = {
+        "point_cells": np.zeros(n, np.int32),
+        "point_ids": np.zeros(n, np.int32),
+        "cell_starts": np.zeros(nc, np.int32),
+        "cell_ends": np.zeros(nc, np.int32),
+    }
+    st = lib().oracle_grid_build(pts.reshape(-1) if n else np.zeros(3, np.float32), n, float(np.float32(radius)),
+                                 *dims, out["point_cells"] if n else np.zeros(1, np.int32),
+                                 out["point_ids"] if n else np.zeros(1, np.int32), out["cell_starts"],
+                                 out["cell_ends"])
+    if st != 0:
+        raise RuntimeError(f"oracle_grid_build status {st}")
+    return out
+
+
+def grid_query(grid: dict, dims, cell_inv: float, pos, radius: float) -> np.ndarray:
+    """hash_grid_query + query_next restated: candidates in Warp order."""
+    pos = _f32(pos).reshape(3)
+    L = lib()
+    n = L.oracle_grid_query(grid["point_ids"], grid["cell_starts"], grid["cell_ends"], *dims, float(cell_inv), pos,
+                            float(radius), None, 0)
+    out = np.zeros(max(n, 1), np.int32)
+    L.oracle_grid_query(grid["point_ids"], grid["cell_starts"], grid["cell_ends"], *dims, float(cell_inv), pos,
+                        float(radius), _p(out), n)
+    return out[:n]
+
+
+# ---------------------------------------------------------------------------
+# SPH
+# ---------------------------------------------------------------------------
+def sph_neighbors(c32: dict, dims, x: np.ndarray, flags: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """Neighbour lists (offsets int64 (N+1,), ids int32) in original order."""
+    x = _f32(x)
+    flags = _i32(flags)
+    n = x.shape[0]
+    p = params32(c32)
+    dims_a = _i32(dims)
+    counts = np.zeros(max(n, 1), np.int32)
+    L = lib()
+    st = L.oracle_sph_neighbors(ctypes.byref(p), n, x.reshape(-1), flags, dims_a, counts, None, None)
+    if st != 0:
+        raise RuntimeError(f"oracle_sph_neighbors status {st}")
+    offsets = np.zeros(n + 1, np.int64)
+    offsets[1:] = np.cumsum(counts[:n])
+    ids = np.zeros(max(int(offsets[-1]), 1), np.int32)
+    st = L.oracle_sph_neighbors(ctypes.byref(p), n, x.reshape(-1), flags, dims_a, counts, _p(offsets), _p(ids))
+    if st != 0:
+        raise RuntimeError(f"oracle_sph_neighbors status {st}")
+    return offsets, ids[: offsets[-1]]
+
+
+def sph_step(consts: dict, dims, x, v, mass, inv_mass, flags, world, gravity, f_ext=None, v_out_init=None,
+             precision: str = "f64") -> dict[str, np.ndarray]:
+    """One WCSPH step on the CPU (fp32 mirror or fp64 truth).
+
+    Returns dict with x, v, rho, p, a (SPH acceleration) and a_scale
+    (sum of the magnitudes of the acceleration's summands)."""
+    x = _f32(x)
+    v = _f32(v)
+    n = x.shape[0]
+    dt = np.float64 if precision == "f64" else np.float32
+    out = {
+        "x": np.zeros((n, 3), dt),
+        "v": np.array(v_out_init if v_out_init is not None else np.zeros((n, 3)), dtype=dt),
+        "rho": np.zeros(n, dt),
+        "p": np.zeros(n, dt),
+        "a": np.zeros((n, 3), dt),
+        "a_scale": np.zeros(n, dt),
+    }
+    gravity = _f32(gravity).reshape(-1, 3)
+    args = [
+        _p(x), _p(v), _p(_f32(f_ext) if f_ext is not None else None), _p(_f32(mass)), _p(_f32(inv_mass)),
+        _p(_i32(flags)), _p(_i32(world)),
+        gravity.reshape(-1), gravity.shape[0],
+        _p(out["x"]), _p(out["v"]), _p(out["rho"]), _p(out["p"]), _p(out["a"]), _p(out["a_scale"]),
+    ]
+    # keep converted temporaries alive for the call
+    keep = [x, v]
+    p32 = params32(consts["f32"])
+    if precision == "f64":
+        ph = phys64(consts["f64"])
+        st = lib().oracle_sph_step_f64(ctypes.byref(p32), ctypes.byref(ph), _i32(dims), n, *args)
+    else:
+        st = lib().oracle_sph_step_f32(ctypes.byref(p32), _i32(dims), n, *args)
+    del keep
+    if st != 0:
+        raise RuntimeError(f"oracle sph step status {st}")
+    return out
+
+
+def integrate_particles(x, v, f, inv_mass, flags, world, gravity, dt, v_max, x_new, v_new, precision="f32"):
+    """integrate_particles (solver.py:10-47); x_new / v_new updated in place."""
+    gravity = _f32(gravity).reshape(-1)
+    args = [_f32(x).reshape(-1), _f32(v).reshape(-1), _f32(f).reshape(-1), _f32(inv_mass), _i32(flags), _i32(world),
+            gravity, gravity.size // 3, _f32(x).shape[0], dt, v_max]
+    if precision == "f64":
+        lib().oracle_integrate_particles_f64(*args, x_new.reshape(-1), v_new.reshape(-1))
+    else:
+        lib().oracle_integrate_particles_f32(*args, x_new.reshape(-1), v_new.reshape(-1))
+
+
+# ---------------------------------------------------------------------------
+# pure-Python restatements (small cases; checks of the C oracle)
+# ---------------------------------------------------------------------------
+def trunc_sat_py(v: np.float32) -> int:
+    v = float(v)
+    if math.isnan(v):
+        return 0
+    if v >= 2147483648.0:
+        return 2**31 - 1
+    if v <= -2147483648.0:
+        return -(2**31)
+    return int(math.trunc(v))
+
+
+def cell_of_py(p, inv: np.float32, dims) -> int:
+    """Warp hash_grid_index of point p (fp32 products)."""
+    c = []
+    for a in range(3):
+        vc = trunc_sat_py(np.float32(np.float32(p[a]) * inv)) + (1 << 20)
+        c.append(max(vc, 0) % dims[a])
+    return c[2] * dims[0] * dims[1] + c[1] * dims[0] + c[0]
+
+
+def grid_build_py(points, radius, dims):
+    """HashGrid.build with Python sorting (stable sort by cell id)."""
+    inv = np.float32(1.0) / np.float32(radius)
+    keys = [cell_of_py(p, inv, dims) for p in np.asarray(points, np.float32)]
+    order = sorted(range(len(keys)), key=lambda i: keys[i])  # Python's sort is stable
+    nc = dims[0] * dims[1] * dims[2]
+    starts = np.zeros(nc, np.int32)
+    ends = np.zeros(nc, np.int32)
+    cells = [keys[i] for i in order]
+    for k, c in enumerate(cells):
+        if k == 0 or cells[k - 1] != c:
+            starts[c] = k
+        if k == len(cells) - 1 or cells[k + 1] != c:
+            ends[c] = k + 1
+    return {"point_cells": np.array(cells, np.int32), "point_ids": np.array(order, np.int32),
+            "cell_starts": starts, "cell_ends": ends}
+
+
+def neighbors_brute_py(x, h2: np.float32, flags):
+    """All j with fp32 r2 = fma(dz,dz,fma(dy,dy,dx*dx)) < h2 (O(N^2), as a set
+    per particle): the grid-free definition of the neighbour set."""
+    x = np.asarray(x, np.float32)
+    n = len(x)
+    d = x[:, None, :] - x[None, :, :]
+    # numpy has no fma; emulate exactly through float64 (exact products of
+    # fp32 values, one rounding per fma)
+    dx, dy, dz = (d[..., k].astype(np.float64) for k in range(3))
+    t = (dx * dx).astype(np.float32).astype(np.float64)
+    t = (dy * dy + t).astype(np.float32).astype(np.float64)
+    r2 = (dz * dz + t).astype(np.float32)
+    act = (np.asarray(flags) & 1) != 0
+    out = []
+    for i in range(n):
+        out.append(set(np.nonzero((r2[i] < h2) & act)[0].tolist()) if act[i] else set())
+    return out
+
+
+def lattice_py(pos, vel, dim_x, dim_y, dim_z, cell_x, cell_y, cell_z, jitter, seed_base=0):
+    """add_particle_grid's positions (builder.py:8085-8096) with explicit
+    loops: index = iy*(dim_x*dim_z) + ix*dim_z + iz, identity rotation, then
+    jitter from default_rng(42 + seed_base) over the (N, 3) array."""
+    pts = []
+    for iy in range(dim_y):
+        for ix in range(dim_x):
+            for iz in range(dim_z):
+                pts.append([ix * cell_x + pos[0], iy * cell_y + pos[1], iz * cell_z + pos[2]])
+    pts = np.array(pts, dtype=np.float64)
+    rng = np.random.default_rng(42 + seed_base)
+    pts += (rng.random(pts.shape) - 0.5) * jitter
+    return pts
+
+
+def cubic_spline_py(r: float, h: float) -> float:
+    """W(r) of the 3-D cubic spline with support h (Monaghan 1992)."""
+    q = r / h
+    s = 8.0 / (math.pi * h**3)
+    if q <= 0.5:
+        return s * (6.0 * (q**3 - q**2) + 1.0)
+    if q < 1.0:
+        return s * 2.0 * (1.0 - q) ** 3
+    return 0.0
