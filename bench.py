@@ -311,14 +311,12 @@ def run_gpu(args):
     stream = torch.cuda.current_stream(device)
 
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
-    ev = {k: torch.cuda.Event(enable_timing=True, external=True) for k in ("start", "build", "density", "end")}
-    solver.set_phase_events(ev["build"], ev["density"])
+    # the library records start / built / density / end events inside every
+    # step (as external event nodes when captured), on the launching stream
+    solver.enable_phase_timing(True)
 
     def step(a, b):
-        # record on the current stream: the capture stream inside torch.cuda.graph
-        ev["start"].record()
         solver.step(a, b, None, None, dt)
-        ev["end"].record()
 
     # warm-up (eager), then capture one graph per ping-pong direction
     for i in range(max(args.warmup, 3)):
@@ -337,8 +335,7 @@ def run_gpu(args):
             graphs = (ga, gb)
             for g in graphs:  # one replay each to validate event timing through graphs
                 g.replay()
-                ev["end"].synchronize()
-                ev["start"].elapsed_time(ev["end"])
+                solver.phase_times()
         except Exception as exc:  # timing events through graphs unavailable: fall back to eager steps
             print(f"[bench] graph capture unavailable ({exc}); timing eager steps", file=sys.stderr)
             graphs = None
@@ -356,14 +353,11 @@ def run_gpu(args):
                 graphs[i % 2].replay()
             else:
                 step(s0, s1) if i % 2 == 0 else step(s1, s0)
-            ev["end"].synchronize()
-            t_build = ev["start"].elapsed_time(ev["build"])
-            t_dens = ev["build"].elapsed_time(ev["density"])
-            t_force = ev["density"].elapsed_time(ev["end"])
+            t_build, t_dens, t_force = solver.phase_times()
             phase["build"] += t_build
             phase["density"] += t_dens
             phase["force"] += t_force
-            total_ms += ev["start"].elapsed_time(ev["end"])
+            total_ms += t_build + t_dens + t_force
     torch.cuda.synchronize()
     barrier(device)
     total_ms_max = max_over_ranks(total_ms, device)
@@ -378,7 +372,6 @@ def run_gpu(args):
     hv = model.particle_qd.cpu().pin_memory()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    solver.set_phase_events(None, None)
     e2e_ms = 0.0
     barrier(device)
     torch.cuda.synchronize()

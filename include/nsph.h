@@ -189,12 +189,14 @@ NSPH_API int nsph_sph_neighbors(const nsph_sph* solver, const nsph_sph_params* p
 /* The solver's grid of the last step (sorted cell ids, permutation, ranges). */
 NSPH_API int nsph_sph_get_grid_view(const nsph_sph* solver, nsph_grid_view* view);
 
-/* Optional timing marks: when set, every later step records `after_build`
- * (after the grid build and sorted gather) and `after_density` (after the
- * density pass) on its stream with cudaEventRecordExternal, so the events
- * also become record nodes of a captured CUDA graph. Events are cudaEvent_t
- * created with timing enabled; NULL clears. */
-NSPH_API int nsph_sph_set_phase_events(nsph_sph* solver, void* after_build, void* after_density);
+/* Phase timing. When enabled, every later step records four CUDA events on
+ * its stream (start, after the grid build and sorted gather, after the
+ * density pass, end) with cudaEventRecordExternal, so they also become event
+ * record nodes of a captured CUDA graph. nsph_sph_phase_times waits for the
+ * end event of the last executed step (eager or replayed) and returns its
+ * build / density / force durations in ms. Enable/disable outside capture. */
+NSPH_API int nsph_sph_enable_phase_timing(nsph_sph* solver, int enable);
+NSPH_API int nsph_sph_phase_times(nsph_sph* solver, float ms_out[3]);
 
 /* Number of kernels the last nsph_sph_step launched. */
 NSPH_API int nsph_sph_last_launches(const nsph_sph* solver);

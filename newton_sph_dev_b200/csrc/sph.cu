@@ -255,13 +255,17 @@ struct nsph_sph {
     unsigned* status = nullptr;
     int last_n = 0;
     int last_launches = 0;
-    cudaEvent_t ev_after_build = nullptr;
-    cudaEvent_t ev_after_density = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // start, built, density, end
 };
 
 static void sph_free(nsph_sph* s)
 {
     DeviceGuard guard(s->grid.device);
+    for (cudaEvent_t& e : s->ev)
+        if (e) {
+            cudaEventDestroy(e);
+            e = nullptr;
+        }
     cudaFree(s->xs);
     cudaFree(s->vs);
     cudaFree(s->aux);
@@ -349,25 +353,26 @@ extern "C" int nsph_sph_step(nsph_sph* s, const nsph_sph_params* p, int n, const
     cudaStream_t cs = (cudaStream_t)stream;
     GatherArgs ga{x_in, v_in, mass, inv_mass, flags, world, world_count, s->xs, s->vs};
     int launches = 0;
+    if (s->ev[0]) NSPH_CUDA_TRY(cudaEventRecordWithFlags(s->ev[0], cs, cudaEventRecordExternal));
     st = grid_build(s->grid, x_in, n, p->cell_width, p->cell_inv, &ga, s->status, cs, &launches);
     if (st != NSPH_OK) return st;
     s->last_n = n;
-    if (s->ev_after_build) NSPH_CUDA_TRY(cudaEventRecordWithFlags(s->ev_after_build, cs, cudaEventRecordExternal));
+    if (s->ev[1]) NSPH_CUDA_TRY(cudaEventRecordWithFlags(s->ev[1], cs, cudaEventRecordExternal));
     if (n > 0) {
         const GridDev g = s->grid.view();
         const int blocks = (n + kSphThreads - 1) / kSphThreads;
         k_density<<<blocks, kSphThreads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->status);
         NSPH_LAUNCH_CHECK("k_density");
         ++launches;
-        if (s->ev_after_density)
-            NSPH_CUDA_TRY(cudaEventRecordWithFlags(s->ev_after_density, cs, cudaEventRecordExternal));
+        if (s->ev[2]) NSPH_CUDA_TRY(cudaEventRecordWithFlags(s->ev[2], cs, cudaEventRecordExternal));
         k_force<<<blocks, kSphThreads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, f_ext, inv_mass, gravity,
                                                 x_out, v_out, rho_out, p_out, a_out, s->status);
         NSPH_LAUNCH_CHECK("k_force");
         ++launches;
-    } else if (s->ev_after_density) {
-        NSPH_CUDA_TRY(cudaEventRecordWithFlags(s->ev_after_density, cs, cudaEventRecordExternal));
+    } else if (s->ev[2]) {
+        NSPH_CUDA_TRY(cudaEventRecordWithFlags(s->ev[2], cs, cudaEventRecordExternal));
     }
+    if (s->ev[3]) NSPH_CUDA_TRY(cudaEventRecordWithFlags(s->ev[3], cs, cudaEventRecordExternal));
     s->last_launches = launches;
     return NSPH_OK;
 }
@@ -410,12 +415,31 @@ extern "C" int nsph_sph_get_grid_view(const nsph_sph* s, nsph_grid_view* view)
     return NSPH_OK;
 }
 
-extern "C" int nsph_sph_set_phase_events(nsph_sph* s, void* after_build, void* after_density)
+extern "C" int nsph_sph_enable_phase_timing(nsph_sph* s, int enable)
 {
     clear_error();
     if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
-    s->ev_after_build = (cudaEvent_t)after_build;
-    s->ev_after_density = (cudaEvent_t)after_density;
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    for (cudaEvent_t& e : s->ev) {
+        if (enable && !e) NSPH_CUDA_TRY(cudaEventCreate(&e));
+        if (!enable && e) {
+            NSPH_CUDA_TRY(cudaEventDestroy(e));
+            e = nullptr;
+        }
+    }
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_phase_times(nsph_sph* s, float ms_out[3])
+{
+    clear_error();
+    if (!s || !ms_out) return fail(NSPH_ERR_INVALID_ARG, "null argument");
+    if (!s->ev[0]) return fail(NSPH_ERR_INVALID_ARG, "phase timing is not enabled");
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    NSPH_CUDA_TRY(cudaEventSynchronize(s->ev[3]));
+    for (int k = 0; k < 3; ++k) NSPH_CUDA_TRY(cudaEventElapsedTime(ms_out + k, s->ev[k], s->ev[k + 1]));
     return NSPH_OK;
 }
 

@@ -93,7 +93,7 @@ class ModelBuilder:
             shape = {"q": (0, 3), "qd": (0, 3)}.get(key, (0,))
             dtype = {"flags": np.int32, "world": np.int32}.get(key, np.float64)
             return np.zeros(shape, dtype=dtype)
-        return np.concatenate([c[key] for c in self._chunks], axis=0)
+        return np.ascontiguousarray(np.concatenate([c[key] for c in self._chunks], axis=0))
 
     @property
     def particle_q(self) -> np.ndarray:
@@ -162,8 +162,8 @@ class ModelBuilder:
             return
         self._chunks.append(
             {
-                "q": np.asarray(q, dtype=np.float64).reshape(n, 3),
-                "qd": np.asarray(qd, dtype=np.float64).reshape(n, 3),
+                "q": np.ascontiguousarray(np.asarray(q, dtype=np.float64).reshape(n, 3)),
+                "qd": np.ascontiguousarray(np.asarray(qd, dtype=np.float64).reshape(n, 3)),
                 "mass": np.asarray(mass, dtype=np.float64).reshape(n),
                 "radius": np.asarray(radius, dtype=np.float64).reshape(n),
                 "flags": np.asarray(flags, dtype=np.int64).astype(np.int32).reshape(n),
@@ -240,8 +240,8 @@ class ModelBuilder:
         m.world_count = self.world_count
         m.up_axis = self.up_axis
         n = self._count
-        q = self.particle_q.astype(np.float32)
-        qd = self.particle_qd.astype(np.float32)
+        q = np.ascontiguousarray(self.particle_q, dtype=np.float32)
+        qd = np.ascontiguousarray(self.particle_qd, dtype=np.float32)
         ms = self.particle_mass.astype(np.float32)
         inv = np.divide(1.0, ms, out=np.zeros_like(ms), where=ms != 0.0).astype(np.float32)
         radius = self.particle_radius.astype(np.float32)

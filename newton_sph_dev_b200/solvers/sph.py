@@ -336,14 +336,19 @@ class SolverSPH(SolverBase):
             "cell_ends": _view_int(v.cell_ends, nc, dev).clone(),
         }
 
-    def set_phase_events(self, after_build=None, after_density=None) -> None:
-        """Record `after_build` / `after_density` (torch.cuda.Event with
-        enable_timing=True) inside every later step, between the grid build,
-        the density pass and the force pass. Recorded as external events, so
-        they also time the phases of a step replayed from a CUDA graph."""
-        eb = after_build.cuda_event if after_build is not None else None
-        ed = after_density.cuda_event if after_density is not None else None
-        _lib.check(self._lib.nsph_sph_set_phase_events(self._handle, eb, ed), "SolverSPH.set_phase_events")
+    def enable_phase_timing(self, enable: bool = True) -> None:
+        """Record CUDA events around the build, density and force phases of
+        every later step (also inside captured CUDA graphs). Call outside a
+        capture."""
+        _lib.check(self._lib.nsph_sph_enable_phase_timing(self._handle, int(bool(enable))),
+                   "SolverSPH.enable_phase_timing")
+
+    def phase_times(self) -> tuple[float, float, float]:
+        """(build, density, force) milliseconds of the last executed step;
+        waits for that step to finish."""
+        ms = (ctypes.c_float * 3)()
+        _lib.check(self._lib.nsph_sph_phase_times(self._handle, ctypes.byref(ms)), "SolverSPH.phase_times")
+        return float(ms[0]), float(ms[1]), float(ms[2])
 
     @property
     def last_launches(self) -> int:
