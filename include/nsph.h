@@ -88,13 +88,15 @@ NSPH_API int nsph_grid_build(nsph_grid* grid, const float* points, int num_point
 
 /* Device pointers of the last build: sorted cell ids (num_points), sorted
  * point ids (num_points; hash_grid_point_id(grid, tid) == point_ids[tid]),
- * cell_starts and cell_ends (dim_x*dim_y*dim_z each). Any out pointer may be
- * NULL. */
+ * and the cell table: the start and end of cell c are
+ * cell_starts[c * cell_stride] and cell_ends[c * cell_stride]
+ * (dim_x*dim_y*dim_z cells; the two live interleaved in one table). */
 typedef struct nsph_grid_view {
     const int* point_cells;
     const int* point_ids;
     const int* cell_starts;
     const int* cell_ends;
+    int   cell_stride;
     int   num_points;
     int   dim_x, dim_y, dim_z;
     float cell_width;

@@ -35,6 +35,7 @@ class NsphGridView(ctypes.Structure):
         ("point_ids", c_void_p),
         ("cell_starts", c_void_p),
         ("cell_ends", c_void_p),
+        ("cell_stride", ctypes.c_int),
         ("num_points", ctypes.c_int),
         ("dim_x", ctypes.c_int),
         ("dim_y", ctypes.c_int),

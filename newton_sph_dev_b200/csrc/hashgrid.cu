@@ -10,7 +10,7 @@
 // Build pipeline (all stream-ordered, no allocation, no host sync):
 //   k_hash_hist   original order: cell id per point + digit-0 tile histograms;
 //                 also clears the cell ranges the previous build wrote.
-//   per 8-bit digit pass: [k_upsweep] -> k_scan -> k_downsweep
+//   per 8-bit digit pass: [k_upsweep] -> k_scan_rows -> k_downsweep
 //                 stable multi-split per 4096-key tile (warp match_any ranks,
 //                 shared-memory staging for coalesced scatter). The last pass
 //                 writes point_cells / point_ids and, in SPH mode, gathers the
@@ -40,8 +40,7 @@ __device__ __forceinline__ unsigned lanemask_lt()
 __global__ void __launch_bounds__(kSortThreads) k_hash_hist(
     const float* __restrict__ points, int n, float inv, int dx, int dy, int dz, int* __restrict__ keys,
     int* __restrict__ vals, unsigned* __restrict__ hist, int ntiles, int digit_mask,
-    const int* __restrict__ prev_cells, int prev_n, int* __restrict__ starts, int* __restrict__ ends,
-    unsigned* __restrict__ status)
+    const int* __restrict__ prev_cells, int prev_n, int2* __restrict__ ranges, unsigned* __restrict__ status)
 {
     __shared__ unsigned wh[kSortThreads / 32][kRadix];
     const int warp = threadIdx.x >> 5;
@@ -55,10 +54,7 @@ __global__ void __launch_bounds__(kSortThreads) k_hash_hist(
         const int idx = base + it * kSortThreads + threadIdx.x;
         if (idx < prev_n) {
             const int c = prev_cells[idx];
-            if (idx == 0 || prev_cells[idx - 1] != c) {
-                starts[c] = 0;
-                ends[c] = 0;
-            }
+            if (idx == 0 || prev_cells[idx - 1] != c) ranges[c] = make_int2(0, 0);
         }
         if (idx < n) {
             const float x = points[3 * (size_t)idx + 0];
@@ -107,45 +103,48 @@ __global__ void __launch_bounds__(kSortThreads) k_upsweep(const int* __restrict_
     }
 }
 
-// Exclusive scan of the digit-major histogram table (kRadix * ntiles
-// entries) in one CTA of 1024 threads: entry [d][t] becomes the global
-// output offset of digit d's keys from tile t.
-constexpr int kScanThreads = 1024;
-__global__ void __launch_bounds__(kScanThreads) k_scan(unsigned* __restrict__ hist, int total)
+// Row scan of the digit-major histogram table: CTA d turns hist[d][0..ntiles)
+// into exclusive offsets within digit d and writes the digit's total to
+// digit_tot[d]. The downsweep adds the exclusive scan of the digit totals.
+constexpr int kScanThreads = 256;
+__device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned& total, unsigned* ws)
 {
-    __shared__ unsigned warp_sums[kScanThreads / 32];
-    const int per = (total + kScanThreads - 1) / kScanThreads;
-    const int begin = min(total, threadIdx.x * per);
-    const int end = min(total, begin + per);
-    unsigned local = 0;
-    for (int i = begin; i < end; ++i) local += hist[i];
-    // block-wide exclusive scan of `local`
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned incl = local;
+    unsigned incl = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += t;
     }
-    if (lane == 31) warp_sums[warp] = incl;
+    if (lane == 31) ws[warp] = incl;
     __syncthreads();
-    if (warp == 0) {
-        unsigned s = warp_sums[lane];
-        unsigned si = s;
+    unsigned base = 0, tot = 0;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned t = __shfl_up_sync(0xffffffffu, si, o);
-            if (lane >= o) si += t;
-        }
-        warp_sums[lane] = si - s;
+    for (int w = 0; w < kScanThreads / 32; ++w) {
+        const unsigned x = ws[w];
+        base += (w < warp) ? x : 0u;
+        tot += x;
     }
-    __syncthreads();
-    unsigned run = warp_sums[warp] + incl - local;
-    for (int i = begin; i < end; ++i) {
-        const unsigned c = hist[i];
-        hist[i] = run;
-        run += c;
+    __syncthreads();  // ws reusable after return
+    total = tot;
+    return base + incl - v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_rows(unsigned* __restrict__ hist, int ntiles,
+                                                            unsigned* __restrict__ digit_tot)
+{
+    __shared__ unsigned ws[kScanThreads / 32];
+    unsigned* row = hist + (size_t)blockIdx.x * ntiles;
+    unsigned carry = 0;
+    for (int base = 0; base < ntiles; base += kScanThreads) {
+        const int i = base + threadIdx.x;
+        const unsigned v = i < ntiles ? row[i] : 0u;
+        unsigned tot;
+        const unsigned ex = block_exclusive_scan(v, tot, ws);
+        if (i < ntiles) row[i] = carry + ex;
+        carry += tot;
     }
+    if (threadIdx.x == 0) digit_tot[blockIdx.x] = carry;
 }
 
 // --------------------------------------------------------------------------
@@ -173,6 +172,7 @@ __global__ void __launch_bounds__(kSortThreads) k_downsweep(const int* __restric
                                                             int* __restrict__ keys_out, int* __restrict__ vals_out,
                                                             int n, int shift, int digit_mask,
                                                             const unsigned* __restrict__ hist, int ntiles,
+                                                            const unsigned* __restrict__ digit_tot,
                                                             GatherArgs gather)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -203,34 +203,23 @@ __global__ void __launch_bounds__(kSortThreads) k_downsweep(const int* __restric
         rank[r] = base + before;
     }
     __syncthreads();
-    // per digit: exclusive prefix over warps, digit totals of this tile
+    // per digit (thread d): exclusive prefix over warps and this tile's total
+    const int d = threadIdx.x;  // kRadix == kSortThreads
     unsigned total = 0;
-    if (threadIdx.x < kRadix) {
-        const int d = threadIdx.x;
 #pragma unroll
-        for (int w = 0; w < kWarps; ++w) {
-            const unsigned c = sm.warp_cnt[w][d];
-            sm.warp_cnt[w][d] = total;
-            total += c;
-        }
-        sm.glob_off[d] = hist[(size_t)d * ntiles + blockIdx.x];
+    for (int w = 0; w < kWarps; ++w) {
+        const unsigned c = sm.warp_cnt[w][d];
+        sm.warp_cnt[w][d] = total;
+        total += c;
     }
-    // exclusive scan of digit totals (kRadix == kSortThreads == 256)
-    {
-        __shared__ unsigned ws[kWarps];
-        unsigned incl = total;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-        }
-        if (lane == 31) ws[warp] = incl;
-        __syncthreads();
-        unsigned wbase = 0;
-#pragma unroll
-        for (int w = 0; w < kWarps; ++w) wbase += (w < warp) ? ws[w] : 0u;
-        if (threadIdx.x < kRadix) sm.tile_off[threadIdx.x] = wbase + incl - total;
-    }
+    __shared__ unsigned ws[kWarps];
+    unsigned dummy;
+    // global offset of digit d from this tile: digits before d (all tiles) +
+    // digit d in the tiles before this one
+    const unsigned dbase = block_exclusive_scan(digit_tot[d], dummy, ws);
+    sm.glob_off[d] = dbase + hist[(size_t)d * ntiles + blockIdx.x];
+    // exclusive scan of this tile's digit totals
+    sm.tile_off[d] = block_exclusive_scan(total, dummy, ws);
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
@@ -268,14 +257,15 @@ __global__ void __launch_bounds__(kSortThreads) k_downsweep(const int* __restric
 }
 
 // Cell [start, end) ranges from sorted cell ids (Warp's compute_cell_offsets
-// semantics; cells not written keep the 0/0 of an empty cell).
-__global__ void k_ranges(const int* __restrict__ cells, int n, int* __restrict__ starts, int* __restrict__ ends)
+// semantics; cells not written keep the {0,0} of an empty cell).
+__global__ void k_ranges(const int* __restrict__ cells, int n, int2* __restrict__ ranges)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const int c = cells[k];
-    if (k == 0 || cells[k - 1] != c) starts[c] = k;
-    if (k == n - 1 || cells[k + 1] != c) ends[c] = k + 1;
+    int* r = reinterpret_cast<int*>(ranges + c);
+    if (k == 0 || cells[k - 1] != c) r[0] = k;
+    if (k == n - 1 || cells[k + 1] != c) r[1] = k + 1;
 }
 
 // Batched Warp-order query: counts, or ids at offsets.
@@ -317,16 +307,14 @@ int grid_init(Grid& g, int dx, int dy, int dz, int device)
     g.key_bits = bits;
     DeviceGuard guard(device);
     if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
-    NSPH_CUDA_TRY(cudaMalloc(&g.cell_starts, sizeof(int) * nc));
-    NSPH_CUDA_TRY(cudaMalloc(&g.cell_ends, sizeof(int) * nc));
-    NSPH_CUDA_TRY(cudaMemset(g.cell_starts, 0, sizeof(int) * nc));
-    NSPH_CUDA_TRY(cudaMemset(g.cell_ends, 0, sizeof(int) * nc));
+    NSPH_CUDA_TRY(cudaMalloc(&g.cell_ranges, sizeof(int2) * nc));
+    NSPH_CUDA_TRY(cudaMemset(g.cell_ranges, 0, sizeof(int2) * nc));
     // load every kernel now, so that a later stream capture never triggers
     // lazy module loading
     cudaFuncAttributes fa;
     NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_hash_hist));
     NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_upsweep));
-    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_scan));
+    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_scan_rows));
     NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_downsweep<false>));
     NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_downsweep<true>));
     NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_ranges));
@@ -348,8 +336,7 @@ int grid_reserve(Grid& g, int capacity)
     // a grown reservation drops the previous build (the Warp contract)
     if (g.built && g.num_points > 0) {
         NSPH_CUDA_TRY(cudaDeviceSynchronize());
-        NSPH_CUDA_TRY(cudaMemset(g.cell_starts, 0, sizeof(int) * g.ncells));
-        NSPH_CUDA_TRY(cudaMemset(g.cell_ends, 0, sizeof(int) * g.ncells));
+        NSPH_CUDA_TRY(cudaMemset(g.cell_ranges, 0, sizeof(int2) * g.ncells));
     }
     g.built = 0;
     g.num_points = 0;
@@ -367,7 +354,9 @@ int grid_reserve(Grid& g, int capacity)
     if (e == cudaSuccess) e = cudaMalloc(&g.vals_b, sz);
     if (e == cudaSuccess) e = cudaMalloc(&g.point_cells, sz);
     if (e == cudaSuccess) e = cudaMalloc(&g.point_ids, sz);
-    if (e == cudaSuccess) e = cudaMalloc(&g.hist, sizeof(unsigned) * kRadix * (size_t)std::max(1, ntiles_of(capacity)));
+    // per-tile digit histograms plus kRadix digit totals
+    if (e == cudaSuccess)
+        e = cudaMalloc(&g.hist, sizeof(unsigned) * kRadix * ((size_t)std::max(1, ntiles_of(capacity)) + 1));
     if (e != cudaSuccess) {
         cudaGetLastError();
         return fail(NSPH_ERR_OUT_OF_MEMORY, std::string("reserve: ") + cudaGetErrorString(e));
@@ -379,9 +368,10 @@ int grid_reserve(Grid& g, int capacity)
 void grid_free(Grid& g)
 {
     DeviceGuard guard(g.device);
-    int* bufs[8] = {g.keys_a, g.vals_a, g.keys_b, g.vals_b, g.point_cells, g.point_ids, g.cell_starts, g.cell_ends};
+    int* bufs[6] = {g.keys_a, g.vals_a, g.keys_b, g.vals_b, g.point_cells, g.point_ids};
     for (int* b : bufs) cudaFree(b);
     cudaFree(g.hist);
+    cudaFree(g.cell_ranges);
     g = Grid();
 }
 
@@ -404,8 +394,7 @@ int grid_build(Grid& g, const float* points, int n, float cell_width, float cell
     if (launch_tiles > 0) {
         k_hash_hist<<<launch_tiles, kSortThreads, 0, stream>>>(points, n, cell_inv, g.dx, g.dy, g.dz, g.keys_a,
                                                                g.vals_a, g.hist, ntiles, mask_of(0),
-                                                               g.point_cells, prev_n, g.cell_starts, g.cell_ends,
-                                                               status);
+                                                               g.point_cells, prev_n, g.cell_ranges, status);
         NSPH_LAUNCH_CHECK("k_hash_hist");
         ++nl;
     }
@@ -422,24 +411,25 @@ int grid_build(Grid& g, const float* points, int n, float cell_width, float cell
                 NSPH_LAUNCH_CHECK("k_upsweep");
                 ++nl;
             }
-            k_scan<<<1, kScanThreads, 0, stream>>>(g.hist, kRadix * ntiles);
-            NSPH_LAUNCH_CHECK("k_scan");
+            unsigned* digit_tot = g.hist + (size_t)kRadix * ntiles_of(g.capacity);
+            k_scan_rows<<<kRadix, kScanThreads, 0, stream>>>(g.hist, ntiles, digit_tot);
+            NSPH_LAUNCH_CHECK("k_scan_rows");
             ++nl;
             GatherArgs ga{};
             if (last && gather) {
                 ga = *gather;
                 k_downsweep<true><<<ntiles, kSortThreads, sizeof(DownsweepSmem), stream>>>(
-                    kin, vin, kout, vout, n, shift, mask_of(p), g.hist, ntiles, ga);
+                    kin, vin, kout, vout, n, shift, mask_of(p), g.hist, ntiles, digit_tot, ga);
             } else {
                 k_downsweep<false><<<ntiles, kSortThreads, sizeof(DownsweepSmem), stream>>>(
-                    kin, vin, kout, vout, n, shift, mask_of(p), g.hist, ntiles, ga);
+                    kin, vin, kout, vout, n, shift, mask_of(p), g.hist, ntiles, digit_tot, ga);
             }
             NSPH_LAUNCH_CHECK("k_downsweep");
             ++nl;
             kin = kout;
             vin = vout;
         }
-        k_ranges<<<(n + 255) / 256, 256, 0, stream>>>(g.point_cells, n, g.cell_starts, g.cell_ends);
+        k_ranges<<<(n + 255) / 256, 256, 0, stream>>>(g.point_cells, n, g.cell_ranges);
         NSPH_LAUNCH_CHECK("k_ranges");
         ++nl;
     }
@@ -512,8 +502,9 @@ extern "C" int nsph_grid_get_view(const nsph_grid* grid, nsph_grid_view* view)
     const Grid& g = grid->g;
     view->point_cells = g.point_cells;
     view->point_ids = g.point_ids;
-    view->cell_starts = g.cell_starts;
-    view->cell_ends = g.cell_ends;
+    view->cell_starts = reinterpret_cast<const int*>(g.cell_ranges);
+    view->cell_ends = reinterpret_cast<const int*>(g.cell_ranges) + 1;
+    view->cell_stride = 2;
     view->num_points = g.num_points;
     view->dim_x = g.dx;
     view->dim_y = g.dy;

@@ -94,15 +94,20 @@ __device__ __forceinline__ int point_cell(float x, float y, float z, float inv, 
 struct GridDev {
     int dx, dy, dz;
     float inv;
-    const int* __restrict__ starts;
-    const int* __restrict__ ends;
-    const int* __restrict__ ids;  // sorted position -> original index
+    const int2* __restrict__ ranges;  // per cell {start, end} in sorted order, {0,0} if empty
+    const int* __restrict__ ids;      // sorted position -> original index
 };
 
 // Visit, in Warp's order, every sorted position k of the cells overlapping the
 // query box of (px,py,pz) +- r. Consecutive non-empty cells whose ranges abut
 // in sorted order are merged into one contiguous run, so the candidate
 // sequence is exactly Warp's while the loop restarts less often.
+//
+// Fast path (every visited virtual cell c has 0 <= c + 2^20 < 2^31, i.e. no
+// clamping): the physical coordinate of the first cell per axis is computed
+// once with a 32-bit modulo and the next ones by an increment that wraps at
+// dim, which is what (c + 2^20) mod dim does for consecutive c. Otherwise each
+// cell is mapped with the general formula.
 template <class F>
 __device__ __forceinline__ void for_each_candidate(const GridDev& g, float px, float py, float pz, float r, F&& f)
 {
@@ -111,23 +116,45 @@ __device__ __forceinline__ void for_each_candidate(const GridDev& g, float px, f
     query_bounds(py, r, g.inv, g.dy, ys, ye);
     query_bounds(pz, r, g.inv, g.dz, zs, ze);
     int lo = 0, hi = 0;
-    for (long long z = zs; z <= ze; ++z) {
-        const int cz = phys_axis(z, g.dz);
-        for (long long y = ys; y <= ye; ++y) {
-            const int rowbase = cz * (g.dx * g.dy) + phys_axis(y, g.dy) * g.dx;
-            for (long long x = xs; x <= xe; ++x) {
-                const int c = rowbase + phys_axis(x, g.dx);
-                const int s = __ldg(g.starts + c);
-                const int e = __ldg(g.ends + c);
-                if (e > s) {
-                    if (s == hi && hi > lo) {
-                        hi = e;
-                    } else {
-                        for (int k = lo; k < hi; ++k) f(k);
-                        lo = s;
-                        hi = e;
-                    }
+    auto visit = [&](int c) {
+        const int2 se = __ldg(g.ranges + c);
+        if (se.y > se.x) {
+            if (se.x == hi && hi > lo) {
+                hi = se.y;
+            } else {
+                for (int k = lo; k < hi; ++k) f(k);
+                lo = se.x;
+                hi = se.y;
+            }
+        }
+    };
+    const long long kMax = 0x7fffffffLL - kOrigin;
+    const bool fast = xs >= -kOrigin && ys >= -kOrigin && zs >= -kOrigin && xe < kMax && ye < kMax && ze < kMax;
+    if (fast) {
+        const int nx = (int)(xe - xs) + 1, ny = (int)(ye - ys) + 1, nz = (int)(ze - zs) + 1;
+        const int cx0 = (int)((unsigned)(xs + kOrigin) % (unsigned)g.dx);
+        int cy0 = (int)((unsigned)(ys + kOrigin) % (unsigned)g.dy);
+        int cz = (int)((unsigned)(zs + kOrigin) % (unsigned)g.dz);
+        const int dxy = g.dx * g.dy;
+        for (int iz = 0; iz < nz; ++iz) {
+            int cy = cy0;
+            for (int iy = 0; iy < ny; ++iy) {
+                const int rowbase = cz * dxy + cy * g.dx;
+                int cx = cx0;
+                for (int ix = 0; ix < nx; ++ix) {
+                    visit(rowbase + cx);
+                    cx = (cx + 1 == g.dx) ? 0 : cx + 1;
                 }
+                cy = (cy + 1 == g.dy) ? 0 : cy + 1;
+            }
+            cz = (cz + 1 == g.dz) ? 0 : cz + 1;
+        }
+    } else {
+        for (long long z = zs; z <= ze; ++z) {
+            const int cz = phys_axis(z, g.dz);
+            for (long long y = ys; y <= ye; ++y) {
+                const int rowbase = cz * (g.dx * g.dy) + phys_axis(y, g.dy) * g.dx;
+                for (long long x = xs; x <= xe; ++x) visit(rowbase + phys_axis(x, g.dx));
             }
         }
     }
@@ -161,11 +188,10 @@ struct Grid {
     int* point_cells = nullptr;  // sorted cell ids of the last build
     int* point_ids = nullptr;    // sorted original ids of the last build
     unsigned int* hist = nullptr;  // kRadix * ntiles(capacity)
-    // cell tables (ncells each)
-    int* cell_starts = nullptr;
-    int* cell_ends = nullptr;
+    // cell table (ncells entries of {start, end})
+    int2* cell_ranges = nullptr;
 
-    GridDev view() const { return GridDev{dx, dy, dz, cell_inv, cell_starts, cell_ends, point_ids}; }
+    GridDev view() const { return GridDev{dx, dy, dz, cell_inv, cell_ranges, point_ids}; }
 };
 
 // Gather performed by the last radix pass (SPH mode): writes the sorted

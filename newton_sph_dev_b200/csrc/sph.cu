@@ -258,6 +258,17 @@ struct nsph_sph {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // start, built, density, end
 };
 
+// Record a timing event: as an external event node while the stream is being
+// captured (so a replayed graph records it), as a plain record otherwise.
+static cudaError_t record_mark(cudaEvent_t ev, cudaStream_t stream)
+{
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(stream, &cap);
+    if (e != cudaSuccess) return e;
+    return cap == cudaStreamCaptureStatusActive ? cudaEventRecordWithFlags(ev, stream, cudaEventRecordExternal)
+                                                : cudaEventRecord(ev, stream);
+}
+
 static void sph_free(nsph_sph* s)
 {
     DeviceGuard guard(s->grid.device);
@@ -353,26 +364,26 @@ extern "C" int nsph_sph_step(nsph_sph* s, const nsph_sph_params* p, int n, const
     cudaStream_t cs = (cudaStream_t)stream;
     GatherArgs ga{x_in, v_in, mass, inv_mass, flags, world, world_count, s->xs, s->vs};
     int launches = 0;
-    if (s->ev[0]) NSPH_CUDA_TRY(cudaEventRecordWithFlags(s->ev[0], cs, cudaEventRecordExternal));
+    if (s->ev[0]) NSPH_CUDA_TRY(record_mark(s->ev[0], cs));
     st = grid_build(s->grid, x_in, n, p->cell_width, p->cell_inv, &ga, s->status, cs, &launches);
     if (st != NSPH_OK) return st;
     s->last_n = n;
-    if (s->ev[1]) NSPH_CUDA_TRY(cudaEventRecordWithFlags(s->ev[1], cs, cudaEventRecordExternal));
+    if (s->ev[1]) NSPH_CUDA_TRY(record_mark(s->ev[1], cs));
     if (n > 0) {
         const GridDev g = s->grid.view();
         const int blocks = (n + kSphThreads - 1) / kSphThreads;
         k_density<<<blocks, kSphThreads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->status);
         NSPH_LAUNCH_CHECK("k_density");
         ++launches;
-        if (s->ev[2]) NSPH_CUDA_TRY(cudaEventRecordWithFlags(s->ev[2], cs, cudaEventRecordExternal));
+        if (s->ev[2]) NSPH_CUDA_TRY(record_mark(s->ev[2], cs));
         k_force<<<blocks, kSphThreads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, f_ext, inv_mass, gravity,
                                                 x_out, v_out, rho_out, p_out, a_out, s->status);
         NSPH_LAUNCH_CHECK("k_force");
         ++launches;
     } else if (s->ev[2]) {
-        NSPH_CUDA_TRY(cudaEventRecordWithFlags(s->ev[2], cs, cudaEventRecordExternal));
+        NSPH_CUDA_TRY(record_mark(s->ev[2], cs));
     }
-    if (s->ev[3]) NSPH_CUDA_TRY(cudaEventRecordWithFlags(s->ev[3], cs, cudaEventRecordExternal));
+    if (s->ev[3]) NSPH_CUDA_TRY(record_mark(s->ev[3], cs));
     s->last_launches = launches;
     return NSPH_OK;
 }
@@ -403,8 +414,9 @@ extern "C" int nsph_sph_get_grid_view(const nsph_sph* s, nsph_grid_view* view)
     const Grid& g = s->grid;
     view->point_cells = g.point_cells;
     view->point_ids = g.point_ids;
-    view->cell_starts = g.cell_starts;
-    view->cell_ends = g.cell_ends;
+    view->cell_starts = reinterpret_cast<const int*>(g.cell_ranges);
+    view->cell_ends = reinterpret_cast<const int*>(g.cell_ranges) + 1;
+    view->cell_stride = 2;
     view->num_points = g.num_points;
     view->dim_x = g.dx;
     view->dim_y = g.dy;

@@ -33,10 +33,12 @@ class _DeviceArray:
         self._device = device
 
 
-def _view_int(ptr: int | None, n: int, device: torch.device) -> torch.Tensor:
+def _view_int(ptr: int | None, n: int, device: torch.device, stride: int = 1) -> torch.Tensor:
+    """int32 view of n library-owned elements spaced `stride` apart."""
     if not ptr or n == 0:
         return torch.zeros(0, dtype=torch.int32, device=device)
-    return torch.as_tensor(_DeviceArray(ptr, n, device), device=device)
+    flat = torch.as_tensor(_DeviceArray(ptr, (n - 1) * stride + 1, device), device=device)
+    return flat[::stride] if stride != 1 else flat
 
 
 class HashGrid:
@@ -115,13 +117,15 @@ class HashGrid:
 
     @property
     def cell_starts(self) -> torch.Tensor:
+        """First sorted position of each cell (0 for empty cells)."""
         v = self._view()
-        return _view_int(v.cell_starts, self.dim_x * self.dim_y * self.dim_z, self.device)
+        return _view_int(v.cell_starts, self.dim_x * self.dim_y * self.dim_z, self.device, v.cell_stride)
 
     @property
     def cell_ends(self) -> torch.Tensor:
+        """One past the last sorted position of each cell (0 for empty cells)."""
         v = self._view()
-        return _view_int(v.cell_ends, self.dim_x * self.dim_y * self.dim_z, self.device)
+        return _view_int(v.cell_ends, self.dim_x * self.dim_y * self.dim_z, self.device, v.cell_stride)
 
     def query(self, points: torch.Tensor, radius: float) -> tuple[torch.Tensor, torch.Tensor]:
         """Candidates of hash_grid_query(points[q], radius) for every q, in

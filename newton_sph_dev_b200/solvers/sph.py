@@ -332,8 +332,8 @@ class SolverSPH(SolverBase):
         return {
             "point_cells": _view_int(v.point_cells, v.num_points, dev).clone(),
             "point_ids": _view_int(v.point_ids, v.num_points, dev).clone(),
-            "cell_starts": _view_int(v.cell_starts, nc, dev).clone(),
-            "cell_ends": _view_int(v.cell_ends, nc, dev).clone(),
+            "cell_starts": _view_int(v.cell_starts, nc, dev, v.cell_stride).clone(),
+            "cell_ends": _view_int(v.cell_ends, nc, dev, v.cell_stride).clone(),
         }
 
     def enable_phase_timing(self, enable: bool = True) -> None:
