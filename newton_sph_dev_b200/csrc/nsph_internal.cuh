@@ -98,18 +98,18 @@ struct GridDev {
     const int* __restrict__ ids;      // sorted position -> original index
 };
 
-// Visit, in Warp's order, every sorted position k of the cells overlapping the
-// query box of (px,py,pz) +- r. Consecutive non-empty cells whose ranges abut
-// in sorted order are merged into one contiguous run, so the candidate
-// sequence is exactly Warp's while the loop restarts less often.
+// Visit, in Warp's order, the sorted positions of the cells overlapping the
+// query box of (px,py,pz) +- r, as contiguous runs [lo, hi): consecutive
+// non-empty cells whose ranges abut in sorted order are merged into one run,
+// so the candidate sequence is exactly Warp's while loops restart less often.
 //
 // Fast path (every visited virtual cell c has 0 <= c + 2^20 < 2^31, i.e. no
 // clamping): the physical coordinate of the first cell per axis is computed
 // once with a 32-bit modulo and the next ones by an increment that wraps at
 // dim, which is what (c + 2^20) mod dim does for consecutive c. Otherwise each
 // cell is mapped with the general formula.
-template <class F>
-__device__ __forceinline__ void for_each_candidate(const GridDev& g, float px, float py, float pz, float r, F&& f)
+template <class R>
+__device__ __forceinline__ void for_each_run(const GridDev& g, float px, float py, float pz, float r, R&& run)
 {
     long long xs, xe, ys, ye, zs, ze;
     query_bounds(px, r, g.inv, g.dx, xs, xe);
@@ -122,7 +122,7 @@ __device__ __forceinline__ void for_each_candidate(const GridDev& g, float px, f
             if (se.x == hi && hi > lo) {
                 hi = se.y;
             } else {
-                for (int k = lo; k < hi; ++k) f(k);
+                if (hi > lo) run(lo, hi);
                 lo = se.x;
                 hi = se.y;
             }
@@ -158,7 +158,16 @@ __device__ __forceinline__ void for_each_candidate(const GridDev& g, float px, f
             }
         }
     }
-    for (int k = lo; k < hi; ++k) f(k);
+    if (hi > lo) run(lo, hi);
+}
+
+// Per-candidate form of for_each_run: f(k) for every k of every run, in order.
+template <class F>
+__device__ __forceinline__ void for_each_candidate(const GridDev& g, float px, float py, float pz, float r, F&& f)
+{
+    for_each_run(g, px, py, pz, r, [&](int lo, int hi) {
+        for (int k = lo; k < hi; ++k) f(k);
+    });
 }
 
 // ---------------------------------------------------------------------------

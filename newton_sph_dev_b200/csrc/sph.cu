@@ -26,7 +26,7 @@
 namespace nsph {
 namespace {
 
-constexpr int kSphThreads = 256;
+constexpr int kSphThreads = 128;
 
 // the neighbour test shared with the oracle (no contraction beyond the two
 // explicit FMAs): r2 = fma(dz, dz, fma(dy, dy, dx*dx))
@@ -71,12 +71,71 @@ __device__ __forceinline__ float eos(float rho, const nsph_sph_params& p)
     return pr;
 }
 
+// ---- hit compaction -------------------------------------------------------------
+// Only ~15% of the 27-cell candidates are neighbours, and in a warp some lane
+// hits on almost every candidate, so evaluating the SPH terms inside the
+// candidate loop would cost every lane the full term for every candidate.
+// Instead the cheap distance test runs first and each thread appends its hits,
+// in query order, to a private list in shared memory (column `tid` of a
+// [kHitCap][kSphThreads] array: conflict-free); the list is drained (terms
+// evaluated and accumulated in the same order) when full and at the end. The
+// per-particle summation order, and so every rounding, is unchanged.
+constexpr int kHitCap = 48;
+
+// density terms of the buffered hits, in order
+__device__ __forceinline__ float drain_density(const float4* __restrict__ xs, const int* buf, int nh, float4 xi,
+                                               const nsph_sph_params& p, float rho)
+{
+    for (int t = 0; t < nh; ++t) {
+        const float4 xj = __ldg(xs + buf[t * kSphThreads]);
+        float dx, dy, dz;
+        const float r2 = dist2(xi, xj, dx, dy, dz);
+        rho = __fmaf_rn(xj.w, kernel_w(__fmul_rn(__fsqrt_rn(r2), p.inv_h), p), rho);
+    }
+    return rho;
+}
+
+struct ForceAcc {
+    float ax, ay, az, dvx, dvy, dvz;
+};
+
+// pressure and XSPH terms of the buffered hits, in order
+__device__ __forceinline__ void drain_force(const float4* __restrict__ xs, const float4* __restrict__ vs,
+                                            const float2* __restrict__ aux, const int* buf, int nh, float4 xi,
+                                            float4 vi, float pr2_i, const nsph_sph_params& p, ForceAcc& acc)
+{
+    for (int t = 0; t < nh; ++t) {
+        const int j = buf[t * kSphThreads];
+        const float4 vj = __ldg(vs + j);
+        if (!(__float_as_int(vj.w) & kAttrActive)) continue;
+        const float4 xj = __ldg(xs + j);
+        const float2 aj = __ldg(aux + j);
+        float dx, dy, dz;
+        const float r2 = dist2(xi, xj, dx, dy, dz);
+        const float r = __fsqrt_rn(r2);
+        const float q = __fmul_rn(r, p.inv_h);
+        const float w = kernel_w(q, p);
+        if (r2 > 0.f) {
+            const float f = kernel_f(q, __frcp_rn(r), p);
+            const float s = __fmul_rn(__fmul_rn(xj.w, __fadd_rn(pr2_i, aj.y)), f);
+            acc.ax = __fmaf_rn(-s, dx, acc.ax);
+            acc.ay = __fmaf_rn(-s, dy, acc.ay);
+            acc.az = __fmaf_rn(-s, dz, acc.az);
+        }
+        const float c = __fmul_rn(aj.x, w);
+        acc.dvx = __fmaf_rn(c, __fsub_rn(vj.x, vi.x), acc.dvx);
+        acc.dvy = __fmaf_rn(c, __fsub_rn(vj.y, vi.y), acc.dvy);
+        acc.dvz = __fmaf_rn(c, __fsub_rn(vj.z, vi.z), acc.dvz);
+    }
+}
+
 // ---- pass 1: density + EOS --------------------------------------------------
-__global__ void __launch_bounds__(kSphThreads) k_density(GridDev g, const float4* __restrict__ xs,
+__global__ void __launch_bounds__(kSphThreads, 4) k_density(GridDev g, const float4* __restrict__ xs,
                                                          const float4* __restrict__ vs, int n,
-                                                         nsph_sph_params p, float2* __restrict__ aux,
+                                                         const __grid_constant__ nsph_sph_params p, float2* __restrict__ aux,
                                                          float2* __restrict__ rp, unsigned* __restrict__ status)
 {
+    __shared__ int hits[kHitCap * kSphThreads];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const float4 xi = xs[k];
@@ -86,13 +145,23 @@ __global__ void __launch_bounds__(kSphThreads) k_density(GridDev g, const float4
         rp[k] = make_float2(0.f, 0.f);
         return;
     }
+    int* buf = hits + threadIdx.x;
+    int nh = 0;
     float rho = 0.f;
-    for_each_candidate(g, xi.x, xi.y, xi.z, p.h, [&](int j) {
-        const float4 xj = __ldg(xs + j);
-        float dx, dy, dz;
-        const float r2 = dist2(xi, xj, dx, dy, dz);
-        if (r2 < p.h2) rho = __fmaf_rn(xj.w, kernel_w(__fmul_rn(__fsqrt_rn(r2), p.inv_h), p), rho);
+    for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
+        for (int j = lo; j < hi; ++j) {
+            const float4 xj = __ldg(xs + j);
+            float dx, dy, dz;
+            if (dist2(xi, xj, dx, dy, dz) < p.h2) {
+                buf[nh * kSphThreads] = j;
+                if (++nh == kHitCap) {
+                    rho = drain_density(xs, buf, nh, xi, p, rho);
+                    nh = 0;
+                }
+            }
+        }
     });
+    rho = drain_density(xs, buf, nh, xi, p, rho);
     float pr = 0.f, mor = 0.f, pr2 = 0.f;
     if (rho > 0.f) {
         pr = eos(rho, p);
@@ -106,10 +175,10 @@ __global__ void __launch_bounds__(kSphThreads) k_density(GridDev g, const float4
 }
 
 // ---- pass 2: pressure force + XSPH + integrate --------------------------------
-__global__ void __launch_bounds__(kSphThreads) k_force(GridDev g, const float4* __restrict__ xs,
+__global__ void __launch_bounds__(kSphThreads, 4) k_force(GridDev g, const float4* __restrict__ xs,
                                                        const float4* __restrict__ vs,
                                                        const float2* __restrict__ aux,
-                                                       const float2* __restrict__ rp, int n, nsph_sph_params p,
+                                                       const float2* __restrict__ rp, int n, const __grid_constant__ nsph_sph_params p,
                                                        const float* __restrict__ f_ext,
                                                        const float* __restrict__ inv_mass,
                                                        const float* __restrict__ gravity, float* __restrict__ x_out,
@@ -117,6 +186,7 @@ __global__ void __launch_bounds__(kSphThreads) k_force(GridDev g, const float4* 
                                                        float* __restrict__ p_out, float* __restrict__ a_out,
                                                        unsigned* __restrict__ status)
 {
+    __shared__ int hits[kHitCap * kSphThreads];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const float4 xi = xs[k];
@@ -136,33 +206,24 @@ __global__ void __launch_bounds__(kSphThreads) k_force(GridDev g, const float4* 
         return;
     }
     const float pr2_i = aux[k].y;
-    float ax = 0.f, ay = 0.f, az = 0.f;
-    float dvx = 0.f, dvy = 0.f, dvz = 0.f;
-    for_each_candidate(g, xi.x, xi.y, xi.z, p.h, [&](int j) {
-        const float4 xj = __ldg(xs + j);
-        float dx, dy, dz;
-        const float r2 = dist2(xi, xj, dx, dy, dz);
-        if (r2 < p.h2 && j != k) {
-            const float4 vj = __ldg(vs + j);
-            if (__float_as_int(vj.w) & kAttrActive) {
-                const float2 aj = __ldg(aux + j);
-                const float r = __fsqrt_rn(r2);
-                const float q = __fmul_rn(r, p.inv_h);
-                const float w = kernel_w(q, p);
-                if (r2 > 0.f) {
-                    const float f = kernel_f(q, __frcp_rn(r), p);
-                    const float s = __fmul_rn(__fmul_rn(xj.w, __fadd_rn(pr2_i, aj.y)), f);
-                    ax = __fmaf_rn(-s, dx, ax);
-                    ay = __fmaf_rn(-s, dy, ay);
-                    az = __fmaf_rn(-s, dz, az);
+    ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    int* buf = hits + threadIdx.x;
+    int nh = 0;
+    for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
+        for (int j = lo; j < hi; ++j) {
+            const float4 xj = __ldg(xs + j);
+            float dx, dy, dz;
+            if (dist2(xi, xj, dx, dy, dz) < p.h2 && j != k) {
+                buf[nh * kSphThreads] = j;
+                if (++nh == kHitCap) {
+                    drain_force(xs, vs, aux, buf, nh, xi, vi, pr2_i, p, acc);
+                    nh = 0;
                 }
-                const float c = __fmul_rn(aj.x, w);
-                dvx = __fmaf_rn(c, __fsub_rn(vj.x, vi.x), dvx);
-                dvy = __fmaf_rn(c, __fsub_rn(vj.y, vi.y), dvy);
-                dvz = __fmaf_rn(c, __fsub_rn(vj.z, vi.z), dvz);
             }
         }
     });
+    drain_force(xs, vs, aux, buf, nh, xi, vi, pr2_i, p, acc);
+    const float ax = acc.ax, ay = acc.ay, az = acc.az, dvx = acc.dvx, dvy = acc.dvy, dvz = acc.dvz;
     if (a_out) {
         a_out[3 * i + 0] = ax;
         a_out[3 * i + 1] = ay;
