@@ -26,7 +26,7 @@
 namespace nsph {
 namespace {
 
-constexpr int kSphThreads = 128;
+constexpr int kSphThreads = 256;
 
 // the neighbour test shared with the oracle (no contraction beyond the two
 // explicit FMAs): r2 = fma(dz, dz, fma(dy, dy, dx*dx))
@@ -71,71 +71,28 @@ __device__ __forceinline__ float eos(float rho, const nsph_sph_params& p)
     return pr;
 }
 
-// ---- hit compaction -------------------------------------------------------------
-// Only ~15% of the 27-cell candidates are neighbours, and in a warp some lane
-// hits on almost every candidate, so evaluating the SPH terms inside the
-// candidate loop would cost every lane the full term for every candidate.
-// Instead the cheap distance test runs first and each thread appends its hits,
-// in query order, to a private list in shared memory (column `tid` of a
-// [kHitCap][kSphThreads] array: conflict-free); the list is drained (terms
-// evaluated and accumulated in the same order) when full and at the end. The
-// per-particle summation order, and so every rounding, is unchanged.
-constexpr int kHitCap = 48;
-
-// density terms of the buffered hits, in order
-__device__ __forceinline__ float drain_density(const float4* __restrict__ xs, const int* buf, int nh, float4 xi,
-                                               const nsph_sph_params& p, float rho)
-{
-    for (int t = 0; t < nh; ++t) {
-        const float4 xj = __ldg(xs + buf[t * kSphThreads]);
-        float dx, dy, dz;
-        const float r2 = dist2(xi, xj, dx, dy, dz);
-        rho = __fmaf_rn(xj.w, kernel_w(__fmul_rn(__fsqrt_rn(r2), p.inv_h), p), rho);
-    }
-    return rho;
-}
-
-struct ForceAcc {
-    float ax, ay, az, dvx, dvy, dvz;
-};
-
-// pressure and XSPH terms of the buffered hits, in order
-__device__ __forceinline__ void drain_force(const float4* __restrict__ xs, const float4* __restrict__ vs,
-                                            const float2* __restrict__ aux, const int* buf, int nh, float4 xi,
-                                            float4 vi, float pr2_i, const nsph_sph_params& p, ForceAcc& acc)
-{
-    for (int t = 0; t < nh; ++t) {
-        const int j = buf[t * kSphThreads];
-        const float4 vj = __ldg(vs + j);
-        if (!(__float_as_int(vj.w) & kAttrActive)) continue;
-        const float4 xj = __ldg(xs + j);
-        const float2 aj = __ldg(aux + j);
-        float dx, dy, dz;
-        const float r2 = dist2(xi, xj, dx, dy, dz);
-        const float r = __fsqrt_rn(r2);
-        const float q = __fmul_rn(r, p.inv_h);
-        const float w = kernel_w(q, p);
-        if (r2 > 0.f) {
-            const float f = kernel_f(q, __frcp_rn(r), p);
-            const float s = __fmul_rn(__fmul_rn(xj.w, __fadd_rn(pr2_i, aj.y)), f);
-            acc.ax = __fmaf_rn(-s, dx, acc.ax);
-            acc.ay = __fmaf_rn(-s, dy, acc.ay);
-            acc.az = __fmaf_rn(-s, dz, acc.az);
-        }
-        const float c = __fmul_rn(aj.x, w);
-        acc.dvx = __fmaf_rn(c, __fsub_rn(vj.x, vi.x), acc.dvx);
-        acc.dvy = __fmaf_rn(c, __fsub_rn(vj.y, vi.y), acc.dvy);
-        acc.dvz = __fmaf_rn(c, __fsub_rn(vj.z, vi.z), acc.dvz);
-    }
-}
+// ---- neighbour masks ---------------------------------------------------------
+// The density pass and the force pass see the same positions x_n, so they
+// have the same candidate sequence (Warp query order) and the same
+// neighbours. The density pass records, for candidate number c of particle
+// k, whether it passed the distance test: bit (c & 31) of word
+// mask[(c >> 5) * n + k] (word-major, so a warp's stores coalesce), for the
+// first kMaskWords*32 candidates, and the candidate count in ncand[k]. The
+// force pass walks the same runs and visits only the set bits, in the same
+// order, so it skips ~85% of the candidates without changing any rounding.
+// A particle with more candidates than the mask holds (dense clusters or an
+// aliased grid) is re-tested candidate by candidate.
+constexpr int kMaskWords = 8;
+constexpr int kMaskBits = kMaskWords * 32;
 
 // ---- pass 1: density + EOS --------------------------------------------------
-__global__ void __launch_bounds__(kSphThreads, 4) k_density(GridDev g, const float4* __restrict__ xs,
+__global__ void __launch_bounds__(kSphThreads, 3) k_density(GridDev g, const float4* __restrict__ xs,
                                                          const float4* __restrict__ vs, int n,
-                                                         const __grid_constant__ nsph_sph_params p, float2* __restrict__ aux,
-                                                         float2* __restrict__ rp, unsigned* __restrict__ status)
+                                                         const __grid_constant__ nsph_sph_params p,
+                                                         float2* __restrict__ aux, float2* __restrict__ rp,
+                                                         unsigned* __restrict__ mask, int* __restrict__ ncand,
+                                                         unsigned* __restrict__ status)
 {
-    __shared__ int hits[kHitCap * kSphThreads];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const float4 xi = xs[k];
@@ -143,25 +100,29 @@ __global__ void __launch_bounds__(kSphThreads, 4) k_density(GridDev g, const flo
     if (!(attr & kAttrActive)) {
         aux[k] = make_float2(0.f, 0.f);
         rp[k] = make_float2(0.f, 0.f);
+        ncand[k] = 0;
         return;
     }
-    int* buf = hits + threadIdx.x;
-    int nh = 0;
     float rho = 0.f;
+    int pos = 0;
+    unsigned word = 0u;
     for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
         for (int j = lo; j < hi; ++j) {
             const float4 xj = __ldg(xs + j);
             float dx, dy, dz;
-            if (dist2(xi, xj, dx, dy, dz) < p.h2) {
-                buf[nh * kSphThreads] = j;
-                if (++nh == kHitCap) {
-                    rho = drain_density(xs, buf, nh, xi, p, rho);
-                    nh = 0;
-                }
+            const float r2 = dist2(xi, xj, dx, dy, dz);
+            const bool hit = r2 < p.h2;
+            if (hit) rho = __fmaf_rn(xj.w, kernel_w(__fmul_rn(__fsqrt_rn(r2), p.inv_h), p), rho);
+            word |= (unsigned)hit << (pos & 31);
+            ++pos;
+            if ((pos & 31) == 0) {
+                if (pos <= kMaskBits) mask[(size_t)((pos >> 5) - 1) * n + k] = word;
+                word = 0u;
             }
         }
     });
-    rho = drain_density(xs, buf, nh, xi, p, rho);
+    if ((pos & 31) != 0 && pos < kMaskBits) mask[(size_t)(pos >> 5) * n + k] = word;
+    ncand[k] = pos;
     float pr = 0.f, mor = 0.f, pr2 = 0.f;
     if (rho > 0.f) {
         pr = eos(rho, p);
@@ -174,11 +135,45 @@ __global__ void __launch_bounds__(kSphThreads, 4) k_density(GridDev g, const flo
     rp[k] = make_float2(rho, pr);
 }
 
+struct ForceAcc {
+    float ax, ay, az, dvx, dvy, dvz;
+};
+
+// pressure and XSPH terms of neighbour j (j != self), accumulated in order
+__device__ __forceinline__ void force_term(const float4* __restrict__ xs, const float4* __restrict__ vs,
+                                           const float2* __restrict__ aux, int j, float4 xi, float4 vi,
+                                           float pr2_i, const nsph_sph_params& p, ForceAcc& acc)
+{
+    const float4 vj = __ldg(vs + j);
+    if (!(__float_as_int(vj.w) & kAttrActive)) return;
+    const float4 xj = __ldg(xs + j);
+    const float2 aj = __ldg(aux + j);
+    float dx, dy, dz;
+    const float r2 = dist2(xi, xj, dx, dy, dz);
+    const float r = __fsqrt_rn(r2);
+    const float q = __fmul_rn(r, p.inv_h);
+    const float w = kernel_w(q, p);
+    if (r2 > 0.f) {
+        const float f = kernel_f(q, __frcp_rn(r), p);
+        const float s = __fmul_rn(__fmul_rn(xj.w, __fadd_rn(pr2_i, aj.y)), f);
+        acc.ax = __fmaf_rn(-s, dx, acc.ax);
+        acc.ay = __fmaf_rn(-s, dy, acc.ay);
+        acc.az = __fmaf_rn(-s, dz, acc.az);
+    }
+    const float c = __fmul_rn(aj.x, w);
+    acc.dvx = __fmaf_rn(c, __fsub_rn(vj.x, vi.x), acc.dvx);
+    acc.dvy = __fmaf_rn(c, __fsub_rn(vj.y, vi.y), acc.dvy);
+    acc.dvz = __fmaf_rn(c, __fsub_rn(vj.z, vi.z), acc.dvz);
+}
+
 // ---- pass 2: pressure force + XSPH + integrate --------------------------------
-__global__ void __launch_bounds__(kSphThreads, 4) k_force(GridDev g, const float4* __restrict__ xs,
+__global__ void __launch_bounds__(kSphThreads, 3) k_force(GridDev g, const float4* __restrict__ xs,
                                                        const float4* __restrict__ vs,
                                                        const float2* __restrict__ aux,
-                                                       const float2* __restrict__ rp, int n, const __grid_constant__ nsph_sph_params p,
+                                                       const float2* __restrict__ rp, int n,
+                                                       const __grid_constant__ nsph_sph_params p,
+                                                       const unsigned* __restrict__ mask,
+                                                       const int* __restrict__ ncand,
                                                        const float* __restrict__ f_ext,
                                                        const float* __restrict__ inv_mass,
                                                        const float* __restrict__ gravity, float* __restrict__ x_out,
@@ -186,7 +181,6 @@ __global__ void __launch_bounds__(kSphThreads, 4) k_force(GridDev g, const float
                                                        float* __restrict__ p_out, float* __restrict__ a_out,
                                                        unsigned* __restrict__ status)
 {
-    __shared__ int hits[kHitCap * kSphThreads];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const float4 xi = xs[k];
@@ -207,22 +201,34 @@ __global__ void __launch_bounds__(kSphThreads, 4) k_force(GridDev g, const float
     }
     const float pr2_i = aux[k].y;
     ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    int* buf = hits + threadIdx.x;
-    int nh = 0;
-    for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
-        for (int j = lo; j < hi; ++j) {
-            const float4 xj = __ldg(xs + j);
-            float dx, dy, dz;
-            if (dist2(xi, xj, dx, dy, dz) < p.h2 && j != k) {
-                buf[nh * kSphThreads] = j;
-                if (++nh == kHitCap) {
-                    drain_force(xs, vs, aux, buf, nh, xi, vi, pr2_i, p, acc);
-                    nh = 0;
+    if (ncand[k] <= kMaskBits) {
+        int pos = 0;
+        for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
+            const int end = pos + (hi - lo);
+            int c = pos;
+            while (c < end) {
+                const int nb = min(32 - (c & 31), end - c);
+                unsigned bits = __ldg(mask + (size_t)(c >> 5) * n + k) >> (c & 31);
+                if (nb < 32) bits &= (1u << nb) - 1u;
+                const int base = lo + (c - pos);
+                while (bits) {
+                    const int j = base + __ffs(bits) - 1;
+                    bits &= bits - 1u;
+                    if (j != k) force_term(xs, vs, aux, j, xi, vi, pr2_i, p, acc);
                 }
+                c += nb;
             }
-        }
-    });
-    drain_force(xs, vs, aux, buf, nh, xi, vi, pr2_i, p, acc);
+            pos = end;
+        });
+    } else {
+        for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
+            for (int j = lo; j < hi; ++j) {
+                float dx, dy, dz;
+                if (dist2(xi, __ldg(xs + j), dx, dy, dz) < p.h2 && j != k)
+                    force_term(xs, vs, aux, j, xi, vi, pr2_i, p, acc);
+            }
+        });
+    }
     const float ax = acc.ax, ay = acc.ay, az = acc.az, dvx = acc.dvx, dvy = acc.dvy, dvz = acc.dvz;
     if (a_out) {
         a_out[3 * i + 0] = ax;
@@ -313,6 +319,8 @@ struct nsph_sph {
     float4* vs = nullptr;
     float2* aux = nullptr;
     float2* rp = nullptr;
+    unsigned* mask = nullptr;  // kMaskWords x capacity neighbour bits (word-major)
+    int* ncand = nullptr;      // candidates per particle
     unsigned* status = nullptr;
     int last_n = 0;
     int last_launches = 0;
@@ -342,6 +350,8 @@ static void sph_free(nsph_sph* s)
     cudaFree(s->vs);
     cudaFree(s->aux);
     cudaFree(s->rp);
+    cudaFree(s->mask);
+    cudaFree(s->ncand);
     cudaFree(s->status);
     grid_free(s->grid);
 }
@@ -363,6 +373,8 @@ extern "C" int nsph_sph_create(int device, int capacity, const int grid_dims[3],
         if (e == cudaSuccess) e = cudaMalloc(&s->vs, sizeof(float4) * c);
         if (e == cudaSuccess) e = cudaMalloc(&s->aux, sizeof(float2) * c);
         if (e == cudaSuccess) e = cudaMalloc(&s->rp, sizeof(float2) * c);
+        if (e == cudaSuccess) e = cudaMalloc(&s->mask, sizeof(unsigned) * kMaskWords * c);
+        if (e == cudaSuccess) e = cudaMalloc(&s->ncand, sizeof(int) * c);
         if (e == cudaSuccess) e = cudaMalloc(&s->status, sizeof(unsigned));
         if (e == cudaSuccess) e = cudaMemset(s->status, 0, sizeof(unsigned));
         cudaFuncAttributes fa;
@@ -433,12 +445,13 @@ extern "C" int nsph_sph_step(nsph_sph* s, const nsph_sph_params* p, int n, const
     if (n > 0) {
         const GridDev g = s->grid.view();
         const int blocks = (n + kSphThreads - 1) / kSphThreads;
-        k_density<<<blocks, kSphThreads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->status);
+        k_density<<<blocks, kSphThreads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->mask, s->ncand,
+                                                  s->status);
         NSPH_LAUNCH_CHECK("k_density");
         ++launches;
         if (s->ev[2]) NSPH_CUDA_TRY(record_mark(s->ev[2], cs));
-        k_force<<<blocks, kSphThreads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, f_ext, inv_mass, gravity,
-                                                x_out, v_out, rho_out, p_out, a_out, s->status);
+        k_force<<<blocks, kSphThreads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->mask, s->ncand, f_ext,
+                                                inv_mass, gravity, x_out, v_out, rho_out, p_out, a_out, s->status);
         NSPH_LAUNCH_CHECK("k_force");
         ++launches;
     } else if (s->ev[2]) {
