@@ -85,14 +85,43 @@ __device__ __forceinline__ float eos(float rho, const nsph_sph_params& p)
 constexpr int kMaskWords = 8;
 constexpr int kMaskBits = kMaskWords * 32;
 
-// ---- pass 1: density + EOS --------------------------------------------------
-__global__ void __launch_bounds__(kSphThreads, 3) k_density(GridDev g, const float4* __restrict__ xs,
-                                                         const float4* __restrict__ vs, int n,
-                                                         const __grid_constant__ nsph_sph_params p,
-                                                         float2* __restrict__ aux, float2* __restrict__ rp,
-                                                         unsigned* __restrict__ mask, int* __restrict__ ncand,
-                                                         unsigned* __restrict__ status)
+// Walk the set bits of a particle's neighbour mask over the same runs the
+// traversal produced: visit(j) for each neighbour, in query order. `word(w)`
+// returns mask word w of this particle.
+template <class W, class V>
+__device__ __forceinline__ void for_each_masked(const GridDev& g, float4 xi, float h, W&& word, V&& visit)
 {
+    int pos = 0;
+    for_each_run(g, xi.x, xi.y, xi.z, h, [&](int lo, int hi) {
+        const int end = pos + (hi - lo);
+        int c = pos;
+        while (c < end) {
+            const int nb = min(32 - (c & 31), end - c);
+            unsigned bits = word(c >> 5) >> (c & 31);
+            if (nb < 32) bits &= (1u << nb) - 1u;
+            const int base = lo + (c - pos);
+            while (bits) {
+                visit(base + __ffs(bits) - 1);
+                bits &= bits - 1u;
+            }
+            c += nb;
+        }
+        pos = end;
+    });
+}
+
+// ---- pass 1: density + EOS --------------------------------------------------
+// Phase A tests every candidate (a tight loop: load, 6 flops, compare) and
+// builds the neighbour mask in shared memory (8 KB per block, column `tid`);
+// phase B walks the set bits and accumulates the density terms in order.
+__global__ void __launch_bounds__(kSphThreads, 3) k_density(GridDev g, const float4* __restrict__ xs,
+                                                            const float4* __restrict__ vs, int n,
+                                                            const __grid_constant__ nsph_sph_params p,
+                                                            float2* __restrict__ aux, float2* __restrict__ rp,
+                                                            unsigned* __restrict__ mask, int* __restrict__ ncand,
+                                                            unsigned* __restrict__ status)
+{
+    __shared__ unsigned smask[kMaskWords * kSphThreads];
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const float4 xi = xs[k];
@@ -103,26 +132,53 @@ __global__ void __launch_bounds__(kSphThreads, 3) k_density(GridDev g, const flo
         ncand[k] = 0;
         return;
     }
+    unsigned* my = smask + threadIdx.x;
     float rho = 0.f;
+    // phase A: candidate tests -> mask
     int pos = 0;
     unsigned word = 0u;
+    bool overflow = false;
     for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
-        for (int j = lo; j < hi; ++j) {
-            const float4 xj = __ldg(xs + j);
-            float dx, dy, dz;
-            const float r2 = dist2(xi, xj, dx, dy, dz);
-            const bool hit = r2 < p.h2;
-            if (hit) rho = __fmaf_rn(xj.w, kernel_w(__fmul_rn(__fsqrt_rn(r2), p.inv_h), p), rho);
-            word |= (unsigned)hit << (pos & 31);
-            ++pos;
+        int j = lo;
+        while (j < hi) {
+            // a chunk that ends at the current mask word's boundary
+            const int len = min(32 - (pos & 31), hi - j);
+            unsigned m = 0u;
+#pragma unroll 4
+            for (int t = 0; t < len; ++t) {
+                const float4 xj = __ldg(xs + j + t);
+                float dx, dy, dz;
+                m |= (unsigned)(dist2(xi, xj, dx, dy, dz) < p.h2) << t;
+            }
+            word |= m << (pos & 31);
+            pos += len;
+            j += len;
             if ((pos & 31) == 0) {
-                if (pos <= kMaskBits) mask[(size_t)((pos >> 5) - 1) * n + k] = word;
+                if (pos <= kMaskBits) my[((pos >> 5) - 1) * kSphThreads] = word;
                 word = 0u;
             }
         }
     });
-    if ((pos & 31) != 0 && pos < kMaskBits) mask[(size_t)(pos >> 5) * n + k] = word;
+    if ((pos & 31) != 0 && pos < kMaskBits) my[(pos >> 5) * kSphThreads] = word;
+    overflow = pos > kMaskBits;
     ncand[k] = pos;
+    // phase B: density terms of the neighbours, in query order
+    auto term = [&](int j) {
+        const float4 xj = __ldg(xs + j);
+        float dx, dy, dz;
+        const float r2 = dist2(xi, xj, dx, dy, dz);
+        rho = __fmaf_rn(xj.w, kernel_w(__fmul_rn(__fsqrt_rn(r2), p.inv_h), p), rho);
+    };
+    if (!overflow) {
+        const int nw = (pos + 31) >> 5;
+        for (int w = 0; w < nw; ++w) mask[(size_t)w * n + k] = my[w * kSphThreads];
+        for_each_masked(g, xi, p.h, [&](int w) { return my[w * kSphThreads]; }, term);
+    } else {
+        for_each_candidate(g, xi.x, xi.y, xi.z, p.h, [&](int j) {
+            float dx, dy, dz;
+            if (dist2(xi, __ldg(xs + j), dx, dy, dz) < p.h2) term(j);
+        });
+    }
     float pr = 0.f, mor = 0.f, pr2 = 0.f;
     if (rho > 0.f) {
         pr = eos(rho, p);
@@ -139,15 +195,11 @@ struct ForceAcc {
     float ax, ay, az, dvx, dvy, dvz;
 };
 
-// pressure and XSPH terms of neighbour j (j != self), accumulated in order
-__device__ __forceinline__ void force_term(const float4* __restrict__ xs, const float4* __restrict__ vs,
-                                           const float2* __restrict__ aux, int j, float4 xi, float4 vi,
-                                           float pr2_i, const nsph_sph_params& p, ForceAcc& acc)
+// pressure and XSPH terms of one neighbour (not self), accumulated in order
+__device__ __forceinline__ void force_term_data(float4 xj, float4 vj, float2 aj, float4 xi, float4 vi, float pr2_i,
+                                                const nsph_sph_params& p, ForceAcc& acc)
 {
-    const float4 vj = __ldg(vs + j);
     if (!(__float_as_int(vj.w) & kAttrActive)) return;
-    const float4 xj = __ldg(xs + j);
-    const float2 aj = __ldg(aux + j);
     float dx, dy, dz;
     const float r2 = dist2(xi, xj, dx, dy, dz);
     const float r = __fsqrt_rn(r2);
@@ -202,30 +254,31 @@ __global__ void __launch_bounds__(kSphThreads, 3) k_force(GridDev g, const float
     const float pr2_i = aux[k].y;
     ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (ncand[k] <= kMaskBits) {
-        int pos = 0;
-        for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
-            const int end = pos + (hi - lo);
-            int c = pos;
-            while (c < end) {
-                const int nb = min(32 - (c & 31), end - c);
-                unsigned bits = __ldg(mask + (size_t)(c >> 5) * n + k) >> (c & 31);
-                if (nb < 32) bits &= (1u << nb) - 1u;
-                const int base = lo + (c - pos);
-                while (bits) {
-                    const int j = base + __ffs(bits) - 1;
-                    bits &= bits - 1u;
-                    if (j != k) force_term(xs, vs, aux, j, xi, vi, pr2_i, p, acc);
-                }
-                c += nb;
-            }
-            pos = end;
-        });
+        // one-deep software pipeline: the loads of neighbour t+1 are issued
+        // before the terms of neighbour t are evaluated (order unchanged)
+        bool have = false;
+        float4 pxj = make_float4(0.f, 0.f, 0.f, 0.f), pvj = pxj;
+        float2 paj = make_float2(0.f, 0.f);
+        for_each_masked(
+            g, xi, p.h, [&](int w) { return __ldg(mask + (size_t)w * n + k); },
+            [&](int j) {
+                if (j == k) return;
+                const float4 nxj = __ldg(xs + j);
+                const float4 nvj = __ldg(vs + j);
+                const float2 naj = __ldg(aux + j);
+                if (have) force_term_data(pxj, pvj, paj, xi, vi, pr2_i, p, acc);
+                pxj = nxj;
+                pvj = nvj;
+                paj = naj;
+                have = true;
+            });
+        if (have) force_term_data(pxj, pvj, paj, xi, vi, pr2_i, p, acc);
     } else {
         for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
             for (int j = lo; j < hi; ++j) {
                 float dx, dy, dz;
                 if (dist2(xi, __ldg(xs + j), dx, dy, dz) < p.h2 && j != k)
-                    force_term(xs, vs, aux, j, xi, vi, pr2_i, p, acc);
+                    force_term_data(__ldg(xs + j), __ldg(vs + j), __ldg(aux + j), xi, vi, pr2_i, p, acc);
             }
         });
     }
