@@ -114,6 +114,31 @@ NSPH_API int nsph_grid_get_view(const nsph_grid* grid, nsph_grid_view* view);
 NSPH_API int nsph_grid_query(const nsph_grid* grid, const float* queries, int num_queries, float radius,
                     int* counts, const long long* offsets, int* out_ids, void* stream);
 
+/* Allocation-free HashGrid build. No counterpart in the reference: it exists
+ * for callers that must not allocate device memory, such as code that
+ * rebuilds the grid while a CUDA stream is being captured (cudaMalloc is not
+ * allowed during a global-mode capture) or a host program whose device
+ * memory belongs to another allocator (a caching allocator or a fixed arena
+ * that a library-side cudaMalloc would compete with).
+ *
+ * Same semantics as nsph_grid_create + nsph_grid_build(points, radius), but
+ * no grid object: the caller passes every output (device memory):
+ *   point_cells, point_ids: num_points ints (sorted cell ids / original ids)
+ *   cell_starts, cell_ends: dim_x*dim_y*dim_z ints each (cleared by the call,
+ *                           then the [start,end) of every occupied cell)
+ * The sort scratch is a fixed device array of the library (about 4 MiB,
+ * held by every GPU that loads the library until the process exits), so
+ * num_points may not exceed NSPH_NOALLOC_MAX_POINTS (NSPH_ERR_CAPACITY).
+ * All calls share that scratch: calls that overlap on the GPU (concurrent
+ * streams, other host threads) race and must be serialised by the caller.
+ * The first call on a device looks up the scratch's device address (a
+ * runtime call, once per device); make that first call before any stream
+ * capture. The call calls neither cudaMalloc nor cudaFree. */
+#define NSPH_NOALLOC_MAX_POINTS (1 << 18)
+NSPH_API int nsph_grid_build_noalloc(const float* points, int num_points, float radius, int dim_x, int dim_y,
+                                     int dim_z, int* point_cells, int* point_ids, int* cell_starts, int* cell_ends,
+                                     void* stream);
+
 /* ======================================================================== *
  *  integrate_particles — replaces newton/_src/solvers/solver.py:10-47      *
  *  v1 = v0 + (f*w + g[max(world,0)]*(w>0))*dt; |v1| clamped to v_max;     *

@@ -83,6 +83,11 @@ SIGNATURES = [
     ("nsph_grid_get_view", ctypes.c_int, [c_void_p, ctypes.POINTER(NsphGridView)]),
     ("nsph_grid_query", ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_float, c_void_p, c_void_p, c_void_p, c_void_p]),
     (
+        "nsph_grid_build_noalloc",
+        ctypes.c_int,
+        [c_void_p, ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_int] + [c_void_p] * 5,
+    ),
+    (
         "nsph_integrate_particles",
         ctypes.c_int,
         [c_void_p] * 7 + [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float, c_void_p, c_void_p, c_void_p],

@@ -18,6 +18,8 @@
 //   k_ranges      cell_starts / cell_ends from the sorted cell ids.
 #include <algorithm>
 #include <cstdio>
+#include <mutex>
+#include <string>
 
 #include "nsph_internal.cuh"
 
@@ -530,5 +532,130 @@ extern "C" int nsph_grid_query(const nsph_grid* grid, const float* queries, int 
     k_query<<<(num_queries + 127) / 128, 128, 0, (cudaStream_t)stream>>>(grid->g.view(), queries, num_queries,
                                                                          radius, counts, offsets, out_ids);
     NSPH_LAUNCH_CHECK("k_query");
+    return NSPH_OK;
+}
+
+// ==========================================================================
+// C ABI: allocation-free HashGrid build
+//
+// For callers that must not allocate device memory: code that rebuilds the
+// grid while a CUDA stream is being captured (cudaMalloc is not allowed
+// during a global-mode capture), and host programs whose device memory is
+// owned by another allocator (a framework's caching allocator or a fixed
+// arena, where a library-side cudaMalloc would compete for memory and
+// synchronise the device). The caller passes the points and every output;
+// the sort scratch lives in the fixed device array below.
+// ==========================================================================
+namespace nsph {
+namespace {
+
+constexpr int kNoAllocTiles = (NSPH_NOALLOC_MAX_POINTS + kSortTile - 1) / kSortTile;
+// keys_a, vals_a, keys_b, vals_b (NSPH_NOALLOC_MAX_POINTS ints each), then
+// the per-tile digit histograms and the kRadix digit totals
+constexpr size_t kNoAllocSortInts = 4 * (size_t)NSPH_NOALLOC_MAX_POINTS;
+constexpr size_t kNoAllocHistUints = (size_t)kRadix * (kNoAllocTiles + 1);
+constexpr size_t kNoAllocBytes = sizeof(int) * kNoAllocSortInts + sizeof(unsigned) * kNoAllocHistUints;
+
+// Held by every GPU that loads the library until the process exits. Shared by
+// all calls: the last call's contents stay behind, and calls that overlap on
+// the GPU race on it.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};  // device address per device
+std::mutex g_noalloc_mutex;
+
+// Device address of g_noalloc_scratch on the current device (looked up once
+// per device with that device current; in host code the symbol itself is only
+// a host-side stand-in and must never be handed to a kernel).
+int noalloc_scratch(int device, unsigned char** out)
+{
+    if (device < 0 || device >= kNoAllocMaxDevices) return fail(NSPH_ERR_INVALID_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[device]) {
+        void* ptr = nullptr;
+        NSPH_CUDA_TRY(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+        g_noalloc_ptr[device] = static_cast<unsigned char*>(ptr);
+    }
+    *out = g_noalloc_ptr[device];
+    return NSPH_OK;
+}
+
+// start / end of each cell into two caller arrays (Warp's layout)
+__global__ void k_ranges_split(const int* __restrict__ cells, int n, int* __restrict__ starts, int* __restrict__ ends)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int c = cells[k];
+    if (k == 0 || cells[k - 1] != c) starts[c] = k;
+    if (k == n - 1 || cells[k + 1] != c) ends[c] = k + 1;
+}
+
+}  // namespace
+}  // namespace nsph
+
+extern "C" int nsph_grid_build_noalloc(const float* points, int num_points, float radius, int dim_x, int dim_y,
+                                       int dim_z, int* point_cells, int* point_ids, int* cell_starts, int* cell_ends,
+                                       void* stream)
+{
+    clear_error();
+    if (num_points < 0) return fail(NSPH_ERR_INVALID_ARG, "negative point count");
+    if (num_points > NSPH_NOALLOC_MAX_POINTS)
+        return fail(NSPH_ERR_CAPACITY, "nsph_grid_build_noalloc: more than NSPH_NOALLOC_MAX_POINTS (" +
+                                           std::to_string(NSPH_NOALLOC_MAX_POINTS) + ") points");
+    if (dim_x <= 0 || dim_y <= 0 || dim_z <= 0) return fail(NSPH_ERR_INVALID_ARG, "grid dims must be positive");
+    const long long ncells = (long long)dim_x * dim_y * dim_z;
+    if (ncells > (1LL << 28)) return fail(NSPH_ERR_INVALID_ARG, "grid has more than 2^28 cells");
+    if (!(radius > 0.f) || !isfinite(radius)) return fail(NSPH_ERR_INVALID_ARG, "radius must be positive and finite");
+    if (!cell_starts || !cell_ends || (num_points > 0 && (!points || !point_cells || !point_ids)))
+        return fail(NSPH_ERR_INVALID_ARG, "null pointer");
+    int device = 0;
+    NSPH_CUDA_TRY(cudaGetDevice(&device));
+    unsigned char* scratch = nullptr;
+    int st = noalloc_scratch(device, &scratch);
+    if (st != NSPH_OK) return st;
+    cudaStream_t cs = (cudaStream_t)stream;
+    int* keys_a = reinterpret_cast<int*>(scratch);
+    int* vals_a = keys_a + NSPH_NOALLOC_MAX_POINTS;
+    int* keys_b = vals_a + NSPH_NOALLOC_MAX_POINTS;
+    int* vals_b = keys_b + NSPH_NOALLOC_MAX_POINTS;
+    unsigned* hist = reinterpret_cast<unsigned*>(vals_b + NSPH_NOALLOC_MAX_POINTS);
+    unsigned* digit_tot = hist + (size_t)kRadix * kNoAllocTiles;
+    // empty cells read 0/0
+    NSPH_CUDA_TRY(cudaMemsetAsync(cell_starts, 0, sizeof(int) * ncells, cs));
+    NSPH_CUDA_TRY(cudaMemsetAsync(cell_ends, 0, sizeof(int) * ncells, cs));
+    const int n = num_points;
+    if (n == 0) return NSPH_OK;
+    int bits = 1;
+    while ((1LL << bits) < ncells) ++bits;
+    const int passes = (bits + kRadixBits - 1) / kRadixBits;
+    auto mask_of = [&](int p) { return (1 << std::min(kRadixBits, bits - p * kRadixBits)) - 1; };
+    const int ntiles = ntiles_of(n);
+    const float inv = 1.0f / radius;
+    k_hash_hist<<<ntiles, kSortThreads, 0, cs>>>(points, n, inv, dim_x, dim_y, dim_z, keys_a, vals_a, hist, ntiles,
+                                                 mask_of(0), nullptr, 0, nullptr, nullptr);
+    NSPH_LAUNCH_CHECK("k_hash_hist");
+    const int* kin = keys_a;
+    const int* vin = vals_a;
+    for (int p = 0; p < passes; ++p) {
+        const bool last = (p == passes - 1);
+        int* kout = last ? point_cells : ((p & 1) ? keys_a : keys_b);
+        int* vout = last ? point_ids : ((p & 1) ? vals_a : vals_b);
+        const int shift = p * kRadixBits;
+        if (p > 0) {
+            k_upsweep<<<ntiles, kSortThreads, 0, cs>>>(kin, n, shift, mask_of(p), hist, ntiles);
+            NSPH_LAUNCH_CHECK("k_upsweep");
+        }
+        k_scan_rows<<<kRadix, kScanThreads, 0, cs>>>(hist, ntiles, digit_tot);
+        NSPH_LAUNCH_CHECK("k_scan_rows");
+        k_downsweep<false><<<ntiles, kSortThreads, sizeof(DownsweepSmem), cs>>>(kin, vin, kout, vout, n, shift,
+                                                                                mask_of(p), hist, ntiles, digit_tot,
+                                                                                GatherArgs{});
+        NSPH_LAUNCH_CHECK("k_downsweep");
+        kin = kout;
+        vin = vout;
+    }
+    k_ranges_split<<<(n + 255) / 256, 256, 0, cs>>>(point_cells, n, cell_starts, cell_ends);
+    NSPH_LAUNCH_CHECK("k_ranges_split");
     return NSPH_OK;
 }
