@@ -110,85 +110,173 @@ __device__ __forceinline__ void for_each_masked(const GridDev& g, float4 xi, flo
     });
 }
 
-// ---- pass 1: density + EOS --------------------------------------------------
-// Phase A tests every candidate (a tight loop: load, 6 flops, compare) and
-// builds the neighbour mask in shared memory (8 KB per block, column `tid`);
-// phase B walks the set bits and accumulates the density terms in order.
-__global__ void __launch_bounds__(kSphThreads, 3) k_density(GridDev g, const float4* __restrict__ xs,
-                                                            const float4* __restrict__ vs, int n,
-                                                            const __grid_constant__ nsph_sph_params p,
-                                                            float2* __restrict__ aux, float2* __restrict__ rp,
-                                                            unsigned* __restrict__ mask, int* __restrict__ ncand,
-                                                            unsigned* __restrict__ status)
+// ---- particle pairs ------------------------------------------------------------
+// Each thread owns two consecutive sorted particles k0 = 2t, k1 = 2t+1 (almost
+// always in the same cell). When their query boxes coincide they see the same
+// candidate sequence, so every candidate is loaded and tested once for both,
+// with the two distance computations packed into fp32x2 operations (each
+// lane of a packed op rounds exactly like its scalar form). Sums stay per
+// particle and in query order. Pairs whose boxes differ, or with an inactive
+// particle, take the single-particle path.
+constexpr int kPairThreads = 128;
+
+__device__ __forceinline__ bool same_box(const GridDev& g, float4 a, float4 b, float h)
 {
-    __shared__ unsigned smask[kMaskWords * kSphThreads];
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const float4 xi = xs[k];
-    const int attr = __float_as_int(vs[k].w);
-    if (!(attr & kAttrActive)) {
-        aux[k] = make_float2(0.f, 0.f);
-        rp[k] = make_float2(0.f, 0.f);
-        ncand[k] = 0;
-        return;
-    }
-    unsigned* my = smask + threadIdx.x;
+    long long a0, a1, b0, b1;
+    query_bounds(a.x, h, g.inv, g.dx, a0, a1);
+    query_bounds(b.x, h, g.inv, g.dx, b0, b1);
+    if (a0 != b0 || a1 != b1) return false;
+    query_bounds(a.y, h, g.inv, g.dy, a0, a1);
+    query_bounds(b.y, h, g.inv, g.dy, b0, b1);
+    if (a0 != b0 || a1 != b1) return false;
+    query_bounds(a.z, h, g.inv, g.dz, a0, a1);
+    query_bounds(b.z, h, g.inv, g.dz, b0, b1);
+    return a0 == b0 && a1 == b1;
+}
+
+__device__ __forceinline__ float wterm(float r2, const nsph_sph_params& p)
+{
+    return kernel_w(__fmul_rn(__fsqrt_rn(r2), p.inv_h), p);
+}
+
+// ---- pass 1: density + EOS --------------------------------------------------
+// single particle: direct accumulation in query order, neighbour mask built
+// candidate by candidate
+__device__ __forceinline__ float density_single(const GridDev& g, const float4* __restrict__ xs,
+                                                const nsph_sph_params& p, float4 xi, unsigned* __restrict__ mask,
+                                                int n, int k, int& ncand)
+{
     float rho = 0.f;
-    // phase A: candidate tests -> mask
     int pos = 0;
     unsigned word = 0u;
-    bool overflow = false;
     for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
-        int j = lo;
-        while (j < hi) {
-            // a chunk that ends at the current mask word's boundary
-            const int len = min(32 - (pos & 31), hi - j);
-            unsigned m = 0u;
-#pragma unroll 4
-            for (int t = 0; t < len; ++t) {
-                const float4 xj = __ldg(xs + j + t);
-                float dx, dy, dz;
-                m |= (unsigned)(dist2(xi, xj, dx, dy, dz) < p.h2) << t;
-            }
-            word |= m << (pos & 31);
-            pos += len;
-            j += len;
+        for (int j = lo; j < hi; ++j) {
+            const float4 xj = __ldg(xs + j);
+            float dx, dy, dz;
+            const float r2 = dist2(xi, xj, dx, dy, dz);
+            const bool hit = r2 < p.h2;
+            if (hit) rho = __fmaf_rn(xj.w, wterm(r2, p), rho);
+            word |= (unsigned)hit << (pos & 31);
+            ++pos;
             if ((pos & 31) == 0) {
-                if (pos <= kMaskBits) my[((pos >> 5) - 1) * kSphThreads] = word;
+                if (pos <= kMaskBits) mask[(size_t)((pos >> 5) - 1) * n + k] = word;
                 word = 0u;
             }
         }
     });
-    if ((pos & 31) != 0 && pos < kMaskBits) my[(pos >> 5) * kSphThreads] = word;
-    overflow = pos > kMaskBits;
-    ncand[k] = pos;
-    // phase B: density terms of the neighbours, in query order
-    auto term = [&](int j) {
-        const float4 xj = __ldg(xs + j);
-        float dx, dy, dz;
-        const float r2 = dist2(xi, xj, dx, dy, dz);
-        rho = __fmaf_rn(xj.w, kernel_w(__fmul_rn(__fsqrt_rn(r2), p.inv_h), p), rho);
-    };
-    if (!overflow) {
-        const int nw = (pos + 31) >> 5;
-        for (int w = 0; w < nw; ++w) mask[(size_t)w * n + k] = my[w * kSphThreads];
-        for_each_masked(g, xi, p.h, [&](int w) { return my[w * kSphThreads]; }, term);
-    } else {
-        for_each_candidate(g, xi.x, xi.y, xi.z, p.h, [&](int j) {
-            float dx, dy, dz;
-            if (dist2(xi, __ldg(xs + j), dx, dy, dz) < p.h2) term(j);
-        });
-    }
+    if ((pos & 31) != 0 && pos < kMaskBits) mask[(size_t)(pos >> 5) * n + k] = word;
+    ncand = pos;
+    return rho;
+}
+
+__device__ __forceinline__ void density_finish(int k, float m, float rho, const nsph_sph_params& p,
+                                               float2* __restrict__ aux, float2* __restrict__ rp,
+                                               unsigned* __restrict__ status)
+{
     float pr = 0.f, mor = 0.f, pr2 = 0.f;
     if (rho > 0.f) {
         pr = eos(rho, p);
-        mor = __fdiv_rn(xi.w, rho);
+        mor = __fdiv_rn(m, rho);
         pr2 = __fdiv_rn(pr, __fmul_rn(rho, rho));
     } else if (status) {
         atomicOr(status, (unsigned)NSPH_STATUS_ZERO_DENSITY);
     }
     aux[k] = make_float2(mor, pr2);
     rp[k] = make_float2(rho, pr);
+}
+
+__global__ void __launch_bounds__(kPairThreads, 5) k_density(GridDev g, const float4* __restrict__ xs,
+                                                             const float4* __restrict__ vs, int n,
+                                                             const __grid_constant__ nsph_sph_params p,
+                                                             float2* __restrict__ aux, float2* __restrict__ rp,
+                                                             unsigned* __restrict__ mask, int* __restrict__ ncand,
+                                                             unsigned* __restrict__ status)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k0 = 2 * t, k1 = 2 * t + 1;
+    if (k0 >= n) return;
+    const bool has1 = k1 < n;
+    const float4 a = xs[k0];
+    const float4 b = has1 ? xs[k1] : a;
+    const bool act0 = (__float_as_int(vs[k0].w) & kAttrActive) != 0;
+    const bool act1 = has1 && (__float_as_int(vs[k1].w) & kAttrActive) != 0;
+    if (act0 && act1 && same_box(g, a, b, p.h)) {
+        const float2 X = make_float2(a.x, b.x), Y = make_float2(a.y, b.y), Z = make_float2(a.z, b.z);
+        const float2 M1 = make_float2(-1.f, -1.f);
+        float rho0 = 0.f, rho1 = 0.f;
+        int pos = 0;
+        unsigned w0 = 0u, w1 = 0u;
+        for_each_run(g, a.x, a.y, a.z, p.h, [&](int lo, int hi) {
+            int j0 = lo;
+            while (j0 < hi) {
+                // a chunk of <= 8 candidates that does not straddle a mask word
+                const int len = min(min(8, hi - j0), 32 - (pos & 31));
+                unsigned m0 = 0u, m1 = 0u;
+                float2 r2s[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    if (u < len) {
+                        const float4 xj = __ldg(xs + j0 + u);
+                        const float2 dx = __ffma2_rn(make_float2(xj.x, xj.x), M1, X);
+                        const float2 dy = __ffma2_rn(make_float2(xj.y, xj.y), M1, Y);
+                        const float2 dz = __ffma2_rn(make_float2(xj.z, xj.z), M1, Z);
+                        r2s[u] = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                        m0 |= (unsigned)(r2s[u].x < p.h2) << u;
+                        m1 |= (unsigned)(r2s[u].y < p.h2) << u;
+                    }
+                }
+                if (m0 | m1) {
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        const unsigned bit = 1u << u;
+                        if ((m0 | m1) & bit) {
+                            const float mj = __ldg(xs + j0 + u).w;
+                            if (m0 & bit) rho0 = __fmaf_rn(mj, wterm(r2s[u].x, p), rho0);
+                            if (m1 & bit) rho1 = __fmaf_rn(mj, wterm(r2s[u].y, p), rho1);
+                        }
+                    }
+                }
+                w0 |= m0 << (pos & 31);
+                w1 |= m1 << (pos & 31);
+                pos += len;
+                j0 += len;
+                if ((pos & 31) == 0) {
+                    if (pos <= kMaskBits) {
+                        const size_t wi = (size_t)((pos >> 5) - 1) * n;
+                        mask[wi + k0] = w0;
+                        mask[wi + k1] = w1;
+                    }
+                    w0 = w1 = 0u;
+                }
+            }
+        });
+        if ((pos & 31) != 0 && pos < kMaskBits) {
+            const size_t wi = (size_t)(pos >> 5) * n;
+            mask[wi + k0] = w0;
+            mask[wi + k1] = w1;
+        }
+        ncand[k0] = pos;
+        ncand[k1] = pos;
+        density_finish(k0, a.w, rho0, p, aux, rp, status);
+        density_finish(k1, b.w, rho1, p, aux, rp, status);
+        return;
+    }
+    // single-particle path
+    for (int e = 0; e < 2; ++e) {
+        const int k = e ? k1 : k0;
+        if (e && !has1) break;
+        if (!(e ? act1 : act0)) {
+            aux[k] = make_float2(0.f, 0.f);
+            rp[k] = make_float2(0.f, 0.f);
+            ncand[k] = 0;
+            continue;
+        }
+        const float4 xi = e ? b : a;
+        int nc = 0;
+        const float rho = density_single(g, xs, p, xi, mask, n, k, nc);
+        ncand[k] = nc;
+        density_finish(k, xi.w, rho, p, aux, rp, status);
+    }
 }
 
 struct ForceAcc {
@@ -218,61 +306,18 @@ __device__ __forceinline__ void force_term_data(float4 xj, float4 vj, float2 aj,
     acc.dvz = __fmaf_rn(c, __fsub_rn(vj.z, vi.z), acc.dvz);
 }
 
-// ---- pass 2: pressure force + XSPH + integrate --------------------------------
-__global__ void __launch_bounds__(kSphThreads, 3) k_force(GridDev g, const float4* __restrict__ xs,
-                                                       const float4* __restrict__ vs,
-                                                       const float2* __restrict__ aux,
-                                                       const float2* __restrict__ rp, int n,
-                                                       const __grid_constant__ nsph_sph_params p,
-                                                       const unsigned* __restrict__ mask,
-                                                       const int* __restrict__ ncand,
-                                                       const float* __restrict__ f_ext,
-                                                       const float* __restrict__ inv_mass,
-                                                       const float* __restrict__ gravity, float* __restrict__ x_out,
-                                                       float* __restrict__ v_out, float* __restrict__ rho_out,
-                                                       float* __restrict__ p_out, float* __restrict__ a_out,
-                                                       unsigned* __restrict__ status)
+// single particle: walk its neighbour mask (or re-test when the mask overflowed)
+__device__ __forceinline__ void force_single(const GridDev& g, const float4* __restrict__ xs,
+                                             const float4* __restrict__ vs, const float2* __restrict__ aux,
+                                             const unsigned* __restrict__ mask, int nc, int n, int k, float4 xi,
+                                             float4 vi, float pr2_i, const nsph_sph_params& p, ForceAcc& acc)
 {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const float4 xi = xs[k];
-    const float4 vi = vs[k];
-    const int attr = __float_as_int(vi.w);
-    const size_t i = (size_t)g.ids[k];
-    if (rho_out || p_out) {
-        const float2 r = rp[k];
-        if (rho_out) rho_out[i] = r.x;
-        if (p_out) p_out[i] = r.y;
-    }
-    if (!(attr & kAttrActive)) {
-        x_out[3 * i + 0] = xi.x;
-        x_out[3 * i + 1] = xi.y;
-        x_out[3 * i + 2] = xi.z;
-        if (a_out) a_out[3 * i + 0] = a_out[3 * i + 1] = a_out[3 * i + 2] = 0.f;
-        return;
-    }
-    const float pr2_i = aux[k].y;
-    ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    if (ncand[k] <= kMaskBits) {
-        // one-deep software pipeline: the loads of neighbour t+1 are issued
-        // before the terms of neighbour t are evaluated (order unchanged)
-        bool have = false;
-        float4 pxj = make_float4(0.f, 0.f, 0.f, 0.f), pvj = pxj;
-        float2 paj = make_float2(0.f, 0.f);
+    if (nc <= kMaskBits) {
         for_each_masked(
             g, xi, p.h, [&](int w) { return __ldg(mask + (size_t)w * n + k); },
             [&](int j) {
-                if (j == k) return;
-                const float4 nxj = __ldg(xs + j);
-                const float4 nvj = __ldg(vs + j);
-                const float2 naj = __ldg(aux + j);
-                if (have) force_term_data(pxj, pvj, paj, xi, vi, pr2_i, p, acc);
-                pxj = nxj;
-                pvj = nvj;
-                paj = naj;
-                have = true;
+                if (j != k) force_term_data(__ldg(xs + j), __ldg(vs + j), __ldg(aux + j), xi, vi, pr2_i, p, acc);
             });
-        if (have) force_term_data(pxj, pvj, paj, xi, vi, pr2_i, p, acc);
     } else {
         for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
             for (int j = lo; j < hi; ++j) {
@@ -282,28 +327,55 @@ __global__ void __launch_bounds__(kSphThreads, 3) k_force(GridDev g, const float
             }
         });
     }
-    const float ax = acc.ax, ay = acc.ay, az = acc.az, dvx = acc.dvx, dvy = acc.dvy, dvz = acc.dvz;
-    if (a_out) {
-        a_out[3 * i + 0] = ax;
-        a_out[3 * i + 1] = ay;
-        a_out[3 * i + 2] = az;
+}
+
+struct StepOut {
+    const float* f_ext;
+    const float* inv_mass;
+    const float* gravity;
+    float* x_out;
+    float* v_out;
+    float* rho_out;
+    float* p_out;
+    float* a_out;
+    unsigned* status;
+};
+
+// integrate particle k (original index i) and scatter its outputs
+__device__ __forceinline__ void integrate_out(size_t i, float4 xi, float4 vi, int attr, float2 rpk,
+                                              const ForceAcc& acc, const nsph_sph_params& p, const StepOut& o)
+{
+    if (o.rho_out) o.rho_out[i] = rpk.x;
+    if (o.p_out) o.p_out[i] = rpk.y;
+    if (!(attr & kAttrActive)) {
+        o.x_out[3 * i + 0] = xi.x;
+        o.x_out[3 * i + 1] = xi.y;
+        o.x_out[3 * i + 2] = xi.z;
+        if (o.a_out) o.a_out[3 * i + 0] = o.a_out[3 * i + 1] = o.a_out[3 * i + 2] = 0.f;
+        return;
+    }
+    const float ax = acc.ax, ay = acc.ay, az = acc.az;
+    if (o.a_out) {
+        o.a_out[3 * i + 0] = ax;
+        o.a_out[3 * i + 1] = ay;
+        o.a_out[3 * i + 2] = az;
     }
     float v1x = vi.x, v1y = vi.y, v1z = vi.z;
     const bool dynamic = (attr & kAttrDynamic) != 0;
     if (dynamic) {
         const int gw = attr >> kAttrGravShift;
         float fx = 0.f, fy = 0.f, fz = 0.f;
-        if (f_ext) {
-            const float w = inv_mass[i];
-            fx = __fmul_rn(f_ext[3 * i + 0], w);
-            fy = __fmul_rn(f_ext[3 * i + 1], w);
-            fz = __fmul_rn(f_ext[3 * i + 2], w);
+        if (o.f_ext) {
+            const float w = o.inv_mass[i];
+            fx = __fmul_rn(o.f_ext[3 * i + 0], w);
+            fy = __fmul_rn(o.f_ext[3 * i + 1], w);
+            fz = __fmul_rn(o.f_ext[3 * i + 2], w);
         }
-        const float gx = gravity[3 * gw + 0], gy = gravity[3 * gw + 1], gz = gravity[3 * gw + 2];
+        const float gx = o.gravity[3 * gw + 0], gy = o.gravity[3 * gw + 1], gz = o.gravity[3 * gw + 2];
         // v1 = fma(eps, dv, fma((a + f w) + g, dt, v0))
-        v1x = __fmaf_rn(p.xsph_eps, dvx, __fmaf_rn(__fadd_rn(__fadd_rn(ax, fx), gx), p.dt, vi.x));
-        v1y = __fmaf_rn(p.xsph_eps, dvy, __fmaf_rn(__fadd_rn(__fadd_rn(ay, fy), gy), p.dt, vi.y));
-        v1z = __fmaf_rn(p.xsph_eps, dvz, __fmaf_rn(__fadd_rn(__fadd_rn(az, fz), gz), p.dt, vi.z));
+        v1x = __fmaf_rn(p.xsph_eps, acc.dvx, __fmaf_rn(__fadd_rn(__fadd_rn(ax, fx), gx), p.dt, vi.x));
+        v1y = __fmaf_rn(p.xsph_eps, acc.dvy, __fmaf_rn(__fadd_rn(__fadd_rn(ay, fy), gy), p.dt, vi.y));
+        v1z = __fmaf_rn(p.xsph_eps, acc.dvz, __fmaf_rn(__fadd_rn(__fadd_rn(az, fz), gz), p.dt, vi.z));
     }
     const float vm = __fsqrt_rn(__fmaf_rn(v1z, v1z, __fmaf_rn(v1y, v1y, __fmul_rn(v1x, v1x))));
     if (vm > p.v_max) {
@@ -321,15 +393,76 @@ __global__ void __launch_bounds__(kSphThreads, 3) k_force(GridDev g, const float
         if (x1z < p.box_lo[2]) { x1z = p.box_lo[2]; v1z = fmaxf(v1z, 0.f); }
         if (x1z > p.box_hi[2]) { x1z = p.box_hi[2]; v1z = fminf(v1z, 0.f); }
     }
-    if (status && !(isfinite(x1x) && isfinite(x1y) && isfinite(x1z) && isfinite(v1x) && isfinite(v1y) &&
-                    isfinite(v1z)))
-        atomicOr(status, (unsigned)NSPH_STATUS_NONFINITE_OUTPUT);
-    x_out[3 * i + 0] = x1x;
-    x_out[3 * i + 1] = x1y;
-    x_out[3 * i + 2] = x1z;
-    v_out[3 * i + 0] = v1x;
-    v_out[3 * i + 1] = v1y;
-    v_out[3 * i + 2] = v1z;
+    if (o.status && !(isfinite(x1x) && isfinite(x1y) && isfinite(x1z) && isfinite(v1x) && isfinite(v1y) &&
+                      isfinite(v1z)))
+        atomicOr(o.status, (unsigned)NSPH_STATUS_NONFINITE_OUTPUT);
+    o.x_out[3 * i + 0] = x1x;
+    o.x_out[3 * i + 1] = x1y;
+    o.x_out[3 * i + 2] = x1z;
+    o.v_out[3 * i + 0] = v1x;
+    o.v_out[3 * i + 1] = v1y;
+    o.v_out[3 * i + 2] = v1z;
+}
+
+// ---- pass 2: pressure force + XSPH + integrate --------------------------------
+// Pairs with the same query box walk the union of their two neighbour masks
+// once: each neighbour's data is loaded once and its terms are added to
+// whichever of the two particles it belongs to, in query order.
+__global__ void __launch_bounds__(kPairThreads, 5) k_force(GridDev g, const float4* __restrict__ xs,
+                                                           const float4* __restrict__ vs,
+                                                           const float2* __restrict__ aux,
+                                                           const float2* __restrict__ rp, int n,
+                                                           const __grid_constant__ nsph_sph_params p,
+                                                           const unsigned* __restrict__ mask,
+                                                           const int* __restrict__ ncand, const StepOut o)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k0 = 2 * t, k1 = 2 * t + 1;
+    if (k0 >= n) return;
+    const bool has1 = k1 < n;
+    const float4 a = xs[k0], va = vs[k0];
+    const float4 b = has1 ? xs[k1] : a, vb = has1 ? vs[k1] : va;
+    const int attr0 = __float_as_int(va.w), attr1 = has1 ? __float_as_int(vb.w) : 0;
+    const bool act0 = (attr0 & kAttrActive) != 0, act1 = (attr1 & kAttrActive) != 0;
+    const int nc0 = ncand[k0], nc1 = has1 ? ncand[k1] : 0;
+    ForceAcc A{0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, B{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const float pa = aux[k0].y, pb = has1 ? aux[k1].y : 0.f;
+    if (act0 && act1 && nc0 <= kMaskBits && nc1 <= kMaskBits && same_box(g, a, b, p.h)) {
+        int pos = 0;
+        for_each_run(g, a.x, a.y, a.z, p.h, [&](int lo, int hi) {
+            const int end = pos + (hi - lo);
+            int c = pos;
+            while (c < end) {
+                const int nb = min(32 - (c & 31), end - c);
+                const size_t wi = (size_t)(c >> 5) * n;
+                unsigned m0 = __ldg(mask + wi + k0) >> (c & 31);
+                unsigned m1 = __ldg(mask + wi + k1) >> (c & 31);
+                if (nb < 32) {
+                    m0 &= (1u << nb) - 1u;
+                    m1 &= (1u << nb) - 1u;
+                }
+                unsigned mu = m0 | m1;
+                const int base = lo + (c - pos);
+                while (mu) {
+                    const int bit = __ffs(mu) - 1;
+                    mu &= mu - 1u;
+                    const int j = base + bit;
+                    const float4 xj = __ldg(xs + j);
+                    const float4 vj = __ldg(vs + j);
+                    const float2 aj = __ldg(aux + j);
+                    if (((m0 >> bit) & 1u) && j != k0) force_term_data(xj, vj, aj, a, va, pa, p, A);
+                    if (((m1 >> bit) & 1u) && j != k1) force_term_data(xj, vj, aj, b, vb, pb, p, B);
+                }
+                c += nb;
+            }
+            pos = end;
+        });
+    } else {
+        if (act0) force_single(g, xs, vs, aux, mask, nc0, n, k0, a, va, pa, p, A);
+        if (has1 && act1) force_single(g, xs, vs, aux, mask, nc1, n, k1, b, vb, pb, p, B);
+    }
+    integrate_out((size_t)g.ids[k0], a, va, attr0, rp[k0], A, p, o);
+    if (has1) integrate_out((size_t)g.ids[k1], b, vb, attr1, rp[k1], B, p, o);
 }
 
 // ---- neighbour lists of the last build (parity export) ----------------------
@@ -497,14 +630,14 @@ extern "C" int nsph_sph_step(nsph_sph* s, const nsph_sph_params* p, int n, const
     if (s->ev[1]) NSPH_CUDA_TRY(record_mark(s->ev[1], cs));
     if (n > 0) {
         const GridDev g = s->grid.view();
-        const int blocks = (n + kSphThreads - 1) / kSphThreads;
-        k_density<<<blocks, kSphThreads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->mask, s->ncand,
-                                                  s->status);
+        const int blocks = ((n + 1) / 2 + kPairThreads - 1) / kPairThreads;
+        k_density<<<blocks, kPairThreads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->mask, s->ncand,
+                                                   s->status);
         NSPH_LAUNCH_CHECK("k_density");
         ++launches;
         if (s->ev[2]) NSPH_CUDA_TRY(record_mark(s->ev[2], cs));
-        k_force<<<blocks, kSphThreads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->mask, s->ncand, f_ext,
-                                                inv_mass, gravity, x_out, v_out, rho_out, p_out, a_out, s->status);
+        const StepOut o{f_ext, inv_mass, gravity, x_out, v_out, rho_out, p_out, a_out, s->status};
+        k_force<<<blocks, kPairThreads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->mask, s->ncand, o);
         NSPH_LAUNCH_CHECK("k_force");
         ++launches;
     } else if (s->ev[2]) {
