@@ -110,30 +110,6 @@ __device__ __forceinline__ void for_each_masked(const GridDev& g, float4 xi, flo
     });
 }
 
-// ---- particle pairs ------------------------------------------------------------
-// Each thread owns two consecutive sorted particles k0 = 2t, k1 = 2t+1 (almost
-// always in the same cell). When their query boxes coincide they see the same
-// candidate sequence, so every candidate is loaded and tested once for both,
-// with the two distance computations packed into fp32x2 operations (each
-// lane of a packed op rounds exactly like its scalar form). Sums stay per
-// particle and in query order. Pairs whose boxes differ, or with an inactive
-// particle, take the single-particle path.
-constexpr int kPairThreads = 128;
-
-__device__ __forceinline__ bool same_box(const GridDev& g, float4 a, float4 b, float h)
-{
-    long long a0, a1, b0, b1;
-    query_bounds(a.x, h, g.inv, g.dx, a0, a1);
-    query_bounds(b.x, h, g.inv, g.dx, b0, b1);
-    if (a0 != b0 || a1 != b1) return false;
-    query_bounds(a.y, h, g.inv, g.dy, a0, a1);
-    query_bounds(b.y, h, g.inv, g.dy, b0, b1);
-    if (a0 != b0 || a1 != b1) return false;
-    query_bounds(a.z, h, g.inv, g.dz, a0, a1);
-    query_bounds(b.z, h, g.inv, g.dz, b0, b1);
-    return a0 == b0 && a1 == b1;
-}
-
 __device__ __forceinline__ float wterm(float r2, const nsph_sph_params& p)
 {
     return kernel_w(__fmul_rn(__fsqrt_rn(r2), p.inv_h), p);
@@ -185,98 +161,26 @@ __device__ __forceinline__ void density_finish(int k, float m, float rho, const 
     rp[k] = make_float2(rho, pr);
 }
 
-__global__ void __launch_bounds__(kPairThreads, 5) k_density(GridDev g, const float4* __restrict__ xs,
-                                                             const float4* __restrict__ vs, int n,
-                                                             const __grid_constant__ nsph_sph_params p,
-                                                             float2* __restrict__ aux, float2* __restrict__ rp,
-                                                             unsigned* __restrict__ mask, int* __restrict__ ncand,
-                                                             unsigned* __restrict__ status)
+__global__ void __launch_bounds__(kSphThreads, 3) k_density(GridDev g, const float4* __restrict__ xs,
+                                                            const float4* __restrict__ vs, int n,
+                                                            const __grid_constant__ nsph_sph_params p,
+                                                            float2* __restrict__ aux, float2* __restrict__ rp,
+                                                            unsigned* __restrict__ mask, int* __restrict__ ncand,
+                                                            unsigned* __restrict__ status)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int k0 = 2 * t, k1 = 2 * t + 1;
-    if (k0 >= n) return;
-    const bool has1 = k1 < n;
-    const float4 a = xs[k0];
-    const float4 b = has1 ? xs[k1] : a;
-    const bool act0 = (__float_as_int(vs[k0].w) & kAttrActive) != 0;
-    const bool act1 = has1 && (__float_as_int(vs[k1].w) & kAttrActive) != 0;
-    if (act0 && act1 && same_box(g, a, b, p.h)) {
-        const float2 X = make_float2(a.x, b.x), Y = make_float2(a.y, b.y), Z = make_float2(a.z, b.z);
-        const float2 M1 = make_float2(-1.f, -1.f);
-        float rho0 = 0.f, rho1 = 0.f;
-        int pos = 0;
-        unsigned w0 = 0u, w1 = 0u;
-        for_each_run(g, a.x, a.y, a.z, p.h, [&](int lo, int hi) {
-            int j0 = lo;
-            while (j0 < hi) {
-                // a chunk of <= 8 candidates that does not straddle a mask word
-                const int len = min(min(8, hi - j0), 32 - (pos & 31));
-                unsigned m0 = 0u, m1 = 0u;
-                float2 r2s[8];
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    if (u < len) {
-                        const float4 xj = __ldg(xs + j0 + u);
-                        const float2 dx = __ffma2_rn(make_float2(xj.x, xj.x), M1, X);
-                        const float2 dy = __ffma2_rn(make_float2(xj.y, xj.y), M1, Y);
-                        const float2 dz = __ffma2_rn(make_float2(xj.z, xj.z), M1, Z);
-                        r2s[u] = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-                        m0 |= (unsigned)(r2s[u].x < p.h2) << u;
-                        m1 |= (unsigned)(r2s[u].y < p.h2) << u;
-                    }
-                }
-                if (m0 | m1) {
-#pragma unroll
-                    for (int u = 0; u < 8; ++u) {
-                        const unsigned bit = 1u << u;
-                        if ((m0 | m1) & bit) {
-                            const float mj = __ldg(xs + j0 + u).w;
-                            if (m0 & bit) rho0 = __fmaf_rn(mj, wterm(r2s[u].x, p), rho0);
-                            if (m1 & bit) rho1 = __fmaf_rn(mj, wterm(r2s[u].y, p), rho1);
-                        }
-                    }
-                }
-                w0 |= m0 << (pos & 31);
-                w1 |= m1 << (pos & 31);
-                pos += len;
-                j0 += len;
-                if ((pos & 31) == 0) {
-                    if (pos <= kMaskBits) {
-                        const size_t wi = (size_t)((pos >> 5) - 1) * n;
-                        mask[wi + k0] = w0;
-                        mask[wi + k1] = w1;
-                    }
-                    w0 = w1 = 0u;
-                }
-            }
-        });
-        if ((pos & 31) != 0 && pos < kMaskBits) {
-            const size_t wi = (size_t)(pos >> 5) * n;
-            mask[wi + k0] = w0;
-            mask[wi + k1] = w1;
-        }
-        ncand[k0] = pos;
-        ncand[k1] = pos;
-        density_finish(k0, a.w, rho0, p, aux, rp, status);
-        density_finish(k1, b.w, rho1, p, aux, rp, status);
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float4 xi = xs[k];
+    if (!(__float_as_int(vs[k].w) & kAttrActive)) {
+        aux[k] = make_float2(0.f, 0.f);
+        rp[k] = make_float2(0.f, 0.f);
+        ncand[k] = 0;
         return;
     }
-    // single-particle path
-    for (int e = 0; e < 2; ++e) {
-        const int k = e ? k1 : k0;
-        if (e && !has1) break;
-        if (!(e ? act1 : act0)) {
-            aux[k] = make_float2(0.f, 0.f);
-            rp[k] = make_float2(0.f, 0.f);
-            ncand[k] = 0;
-            continue;
-        }
-        const float4 xi = e ? b : a;
-        int nc = 0;
-        const float rho = density_single(g, xs, p, xi, mask, n, k, nc);
-        ncand[k] = nc;
-        density_finish(k, xi.w, rho, p, aux, rp, status);
-    }
+    int nc = 0;
+    const float rho = density_single(g, xs, p, xi, mask, n, k, nc);
+    ncand[k] = nc;
+    density_finish(k, xi.w, rho, p, aux, rp, status);
 }
 
 struct ForceAcc {
@@ -306,18 +210,32 @@ __device__ __forceinline__ void force_term_data(float4 xj, float4 vj, float2 aj,
     acc.dvz = __fmaf_rn(c, __fsub_rn(vj.z, vi.z), acc.dvz);
 }
 
-// single particle: walk its neighbour mask (or re-test when the mask overflowed)
+// single particle: walk its neighbour mask (or re-test when the mask overflowed).
+// One-deep software pipeline: the loads of neighbour t+1 are issued before the
+// terms of neighbour t are evaluated (order unchanged).
 __device__ __forceinline__ void force_single(const GridDev& g, const float4* __restrict__ xs,
                                              const float4* __restrict__ vs, const float2* __restrict__ aux,
                                              const unsigned* __restrict__ mask, int nc, int n, int k, float4 xi,
                                              float4 vi, float pr2_i, const nsph_sph_params& p, ForceAcc& acc)
 {
     if (nc <= kMaskBits) {
+        bool have = false;
+        float4 pxj = make_float4(0.f, 0.f, 0.f, 0.f), pvj = pxj;
+        float2 paj = make_float2(0.f, 0.f);
         for_each_masked(
             g, xi, p.h, [&](int w) { return __ldg(mask + (size_t)w * n + k); },
             [&](int j) {
-                if (j != k) force_term_data(__ldg(xs + j), __ldg(vs + j), __ldg(aux + j), xi, vi, pr2_i, p, acc);
+                if (j == k) return;
+                const float4 nxj = __ldg(xs + j);
+                const float4 nvj = __ldg(vs + j);
+                const float2 naj = __ldg(aux + j);
+                if (have) force_term_data(pxj, pvj, paj, xi, vi, pr2_i, p, acc);
+                pxj = nxj;
+                pvj = nvj;
+                paj = naj;
+                have = true;
             });
+        if (have) force_term_data(pxj, pvj, paj, xi, vi, pr2_i, p, acc);
     } else {
         for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
             for (int j = lo; j < hi; ++j) {
@@ -405,64 +323,21 @@ __device__ __forceinline__ void integrate_out(size_t i, float4 xi, float4 vi, in
 }
 
 // ---- pass 2: pressure force + XSPH + integrate --------------------------------
-// Pairs with the same query box walk the union of their two neighbour masks
-// once: each neighbour's data is loaded once and its terms are added to
-// whichever of the two particles it belongs to, in query order.
-__global__ void __launch_bounds__(kPairThreads, 5) k_force(GridDev g, const float4* __restrict__ xs,
-                                                           const float4* __restrict__ vs,
-                                                           const float2* __restrict__ aux,
-                                                           const float2* __restrict__ rp, int n,
-                                                           const __grid_constant__ nsph_sph_params p,
-                                                           const unsigned* __restrict__ mask,
-                                                           const int* __restrict__ ncand, const StepOut o)
+__global__ void __launch_bounds__(kSphThreads, 3) k_force(GridDev g, const float4* __restrict__ xs,
+                                                          const float4* __restrict__ vs,
+                                                          const float2* __restrict__ aux,
+                                                          const float2* __restrict__ rp, int n,
+                                                          const __grid_constant__ nsph_sph_params p,
+                                                          const unsigned* __restrict__ mask,
+                                                          const int* __restrict__ ncand, const StepOut o)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int k0 = 2 * t, k1 = 2 * t + 1;
-    if (k0 >= n) return;
-    const bool has1 = k1 < n;
-    const float4 a = xs[k0], va = vs[k0];
-    const float4 b = has1 ? xs[k1] : a, vb = has1 ? vs[k1] : va;
-    const int attr0 = __float_as_int(va.w), attr1 = has1 ? __float_as_int(vb.w) : 0;
-    const bool act0 = (attr0 & kAttrActive) != 0, act1 = (attr1 & kAttrActive) != 0;
-    const int nc0 = ncand[k0], nc1 = has1 ? ncand[k1] : 0;
-    ForceAcc A{0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, B{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    const float pa = aux[k0].y, pb = has1 ? aux[k1].y : 0.f;
-    if (act0 && act1 && nc0 <= kMaskBits && nc1 <= kMaskBits && same_box(g, a, b, p.h)) {
-        int pos = 0;
-        for_each_run(g, a.x, a.y, a.z, p.h, [&](int lo, int hi) {
-            const int end = pos + (hi - lo);
-            int c = pos;
-            while (c < end) {
-                const int nb = min(32 - (c & 31), end - c);
-                const size_t wi = (size_t)(c >> 5) * n;
-                unsigned m0 = __ldg(mask + wi + k0) >> (c & 31);
-                unsigned m1 = __ldg(mask + wi + k1) >> (c & 31);
-                if (nb < 32) {
-                    m0 &= (1u << nb) - 1u;
-                    m1 &= (1u << nb) - 1u;
-                }
-                unsigned mu = m0 | m1;
-                const int base = lo + (c - pos);
-                while (mu) {
-                    const int bit = __ffs(mu) - 1;
-                    mu &= mu - 1u;
-                    const int j = base + bit;
-                    const float4 xj = __ldg(xs + j);
-                    const float4 vj = __ldg(vs + j);
-                    const float2 aj = __ldg(aux + j);
-                    if (((m0 >> bit) & 1u) && j != k0) force_term_data(xj, vj, aj, a, va, pa, p, A);
-                    if (((m1 >> bit) & 1u) && j != k1) force_term_data(xj, vj, aj, b, vb, pb, p, B);
-                }
-                c += nb;
-            }
-            pos = end;
-        });
-    } else {
-        if (act0) force_single(g, xs, vs, aux, mask, nc0, n, k0, a, va, pa, p, A);
-        if (has1 && act1) force_single(g, xs, vs, aux, mask, nc1, n, k1, b, vb, pb, p, B);
-    }
-    integrate_out((size_t)g.ids[k0], a, va, attr0, rp[k0], A, p, o);
-    if (has1) integrate_out((size_t)g.ids[k1], b, vb, attr1, rp[k1], B, p, o);
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float4 xi = xs[k], vi = vs[k];
+    const int attr = __float_as_int(vi.w);
+    ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (attr & kAttrActive) force_single(g, xs, vs, aux, mask, ncand[k], n, k, xi, vi, aux[k].y, p, acc);
+    integrate_out((size_t)g.ids[k], xi, vi, attr, rp[k], acc, p, o);
 }
 
 // ---- neighbour lists of the last build (parity export) ----------------------
@@ -630,14 +505,14 @@ extern "C" int nsph_sph_step(nsph_sph* s, const nsph_sph_params* p, int n, const
     if (s->ev[1]) NSPH_CUDA_TRY(record_mark(s->ev[1], cs));
     if (n > 0) {
         const GridDev g = s->grid.view();
-        const int blocks = ((n + 1) / 2 + kPairThreads - 1) / kPairThreads;
-        k_density<<<blocks, kPairThreads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->mask, s->ncand,
+        const int blocks = (n + kSphThreads - 1) / kSphThreads;
+        k_density<<<blocks, kSphThreads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->mask, s->ncand,
                                                    s->status);
         NSPH_LAUNCH_CHECK("k_density");
         ++launches;
         if (s->ev[2]) NSPH_CUDA_TRY(record_mark(s->ev[2], cs));
         const StepOut o{f_ext, inv_mass, gravity, x_out, v_out, rho_out, p_out, a_out, s->status};
-        k_force<<<blocks, kPairThreads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->mask, s->ncand, o);
+        k_force<<<blocks, kSphThreads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->mask, s->ncand, o);
         NSPH_LAUNCH_CHECK("k_force");
         ++launches;
     } else if (s->ev[2]) {
