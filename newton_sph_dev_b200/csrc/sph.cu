@@ -116,8 +116,23 @@ __device__ __forceinline__ float wterm(float r2, const nsph_sph_params& p)
 }
 
 // ---- pass 1: density + EOS --------------------------------------------------
-// single particle: direct accumulation in query order, neighbour mask built
-// candidate by candidate
+// Append `cnt` (<= 4) mask bits for the candidates at positions pos.. to the
+// particle's mask (word-major in global memory, the first kMaskWords words).
+__device__ __forceinline__ void mask_append(unsigned bits, int cnt, int& pos, unsigned& word,
+                                            unsigned* __restrict__ mask, int n, int k)
+{
+    const int sh = pos & 31;
+    word |= bits << sh;
+    if (sh + cnt >= 32) {
+        const int w = pos >> 5;
+        if (w < kMaskWords) mask[(size_t)w * n + k] = word;
+        word = sh ? bits >> (32 - sh) : 0u;
+    }
+    pos += cnt;
+}
+
+// single particle: direct accumulation in query order (candidates tested four
+// at a time, terms added in order), neighbour mask built alongside
 __device__ __forceinline__ float density_single(const GridDev& g, const float4* __restrict__ xs,
                                                 const nsph_sph_params& p, float4 xi, unsigned* __restrict__ mask,
                                                 int n, int k, int& ncand)
@@ -126,21 +141,36 @@ __device__ __forceinline__ float density_single(const GridDev& g, const float4* 
     int pos = 0;
     unsigned word = 0u;
     for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
-        for (int j = lo; j < hi; ++j) {
+        int j = lo;
+        for (; j + 4 <= hi; j += 4) {
+            float4 xj[4];
+            float r2[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) xj[u] = __ldg(xs + j + u);
+            unsigned nib = 0u;
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                float dx, dy, dz;
+                r2[u] = dist2(xi, xj[u], dx, dy, dz);
+                nib |= (unsigned)(r2[u] < p.h2) << u;
+            }
+            if (nib) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (nib & (1u << u)) rho = __fmaf_rn(xj[u].w, wterm(r2[u], p), rho);
+            }
+            mask_append(nib, 4, pos, word, mask, n, k);
+        }
+        for (; j < hi; ++j) {
             const float4 xj = __ldg(xs + j);
             float dx, dy, dz;
             const float r2 = dist2(xi, xj, dx, dy, dz);
             const bool hit = r2 < p.h2;
             if (hit) rho = __fmaf_rn(xj.w, wterm(r2, p), rho);
-            word |= (unsigned)hit << (pos & 31);
-            ++pos;
-            if ((pos & 31) == 0) {
-                if (pos <= kMaskBits) mask[(size_t)((pos >> 5) - 1) * n + k] = word;
-                word = 0u;
-            }
+            mask_append((unsigned)hit, 1, pos, word, mask, n, k);
         }
     });
-    if ((pos & 31) != 0 && pos < kMaskBits) mask[(size_t)(pos >> 5) * n + k] = word;
+    if ((pos & 31) != 0 && (pos >> 5) < kMaskWords) mask[(size_t)(pos >> 5) * n + k] = word;
     ncand = pos;
     return rho;
 }
