@@ -11,7 +11,7 @@
 //   k_hash_hist   original order: cell id per point + digit-0 tile histograms;
 //                 also clears the cell ranges the previous build wrote.
 //   per 8-bit digit pass: [k_upsweep] -> k_scan_rows -> k_downsweep
-//                 stable multi-split per 4096-key tile (warp match_any ranks,
+//                 stable multi-split per 2048-key tile (warp match_any ranks,
 //                 shared-memory staging for coalesced scatter). The last pass
 //                 writes point_cells / point_ids and, in SPH mode, gathers the
 //                 sorted float4 mirrors of position and velocity.
@@ -151,14 +151,14 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_rows(unsigned* __restrict
 
 // --------------------------------------------------------------------------
 // k_downsweep: stable scatter of one digit pass.
-// Warp w owns tile elements [w*512, w*512+512) in 16 rounds of 32; within a
+// Warp w owns tile elements [w*256, w*256+256) in 8 rounds of 32; within a
 // round lanes with equal digits are ranked by __match_any_sync, and a
 // per-warp counter carries ranks across rounds, so the order inside a tile
 // is exactly the input order per digit. Keys are staged in shared memory in
 // tile-sorted order and written out in runs (coalesced).
 // --------------------------------------------------------------------------
 constexpr int kWarps = kSortThreads / 32;
-constexpr int kPerWarp = kSortTile / kWarps;  // 512
+constexpr int kPerWarp = kSortTile / kWarps;  // 256
 
 struct DownsweepSmem {
     unsigned warp_cnt[kWarps][kRadix];

@@ -174,8 +174,8 @@ __device__ __forceinline__ void for_each_candidate(const GridDev& g, float px, f
 // grid object (shared by the HashGrid API and the SPH solver)
 // ---------------------------------------------------------------------------
 constexpr int kSortThreads = 256;
-constexpr int kSortItems = 16;
-constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per CTA
+constexpr int kSortItems = 8;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per CTA
 constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
 
