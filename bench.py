@@ -52,12 +52,54 @@ WORKLOADS = {
                     desc="2,097,152 particles, 128^3 block at 0.005 m in a 2x1x1 m tank"),
     "dam_break_32k": dict(shape=(32, 32, 32), spacing=0.01, box=(1.0, 1.0, 1.0), dt=1e-4, vel_std=0.0,
                           desc="32,768 particles, 32^3 block at 0.01 m in a 1 m box"),
+    "worlds_4096": dict(worlds=4096, n_range=(256, 16384), s_range=(0.004, 0.01), box=(0.5, 0.5, 0.5), dt=1e-4,
+                        vel_std=0.0, seed=3,
+                        desc="4,096 independent scenes: particles log-uniform in [256, 16384], spacing uniform in "
+                             "[0.004, 0.01] m, h = 2 spacing, one jittered lattice block each in a 0.5 m cube"),
 }
+
+
+def worlds_layout(w):
+    """Per-world (lattice dims, spacing) of the batched-worlds workload (seeded)."""
+    rng = np.random.default_rng(w["seed"])
+    lo, hi = w["n_range"]
+    counts = np.rint(np.exp(rng.uniform(np.log(lo), np.log(hi), w["worlds"]))).astype(int)
+    spacing = rng.uniform(w["s_range"][0], w["s_range"][1], w["worlds"])
+    out = []
+    for nk, s in zip(counts, spacing):
+        a = max(2, int(np.floor(nk ** (1.0 / 3.0))))
+        c = max(1, int(round(nk / (a * a))))
+        out.append(((a, a, c), float(s)))
+    return out
+
+
+def make_worlds_scene(name: str, device: str, max_worlds: int | None = None):
+    import newton_sph_dev_b200 as nsph
+    from newton_sph_dev_b200.solvers import SolverSPH
+
+    w = WORKLOADS[name]
+    layout = worlds_layout(w)
+    if max_worlds is not None:
+        layout = layout[:max_worlds]
+    b = nsph.ModelBuilder()
+    cfgs = []
+    for shape, s in layout:
+        b.begin_world()
+        b.add_particle_grid(pos=(s / 2, s / 2, s / 2), rot=(0, 0, 0, 1), vel=(0, 0, 0), dim_x=shape[0],
+                            dim_y=shape[1], dim_z=shape[2], cell_x=s, cell_y=s, cell_z=s, mass=1000.0 * s**3,
+                            jitter=0.2 * s)
+        b.end_world()
+        cfgs.append(SolverSPH.Config(smoothing_length=2 * s, rest_density=1000.0, sound_speed=20.0, eos_gamma=7,
+                                     xsph=0.01, box_lo=(0.0, 0.0, 0.0), box_hi=w["box"]))
+    model = b.finalize(device)
+    return model, cfgs, w
 
 
 def make_scene(name: str, device: str):
     import torch
 
+    if "worlds" in WORKLOADS[name]:
+        return make_worlds_scene(name, device)
     import newton_sph_dev_b200 as nsph
     from newton_sph_dev_b200.solvers import SolverSPH
 
@@ -169,6 +211,26 @@ def cpu_oracle_rate(model_cpu, cfg, w, budget_s: float, max_steps: int, sample_s
     from oracle import oracle as O
 
     O.build()
+    if isinstance(cfg, list):  # batched worlds: one oracle step per world, on the first worlds
+        x = model_cpu.particle_q.numpy()
+        v = model_cpu.particle_qd.numpy()
+        world = model_cpu.particle_world.numpy()
+        m, inv = model_cpu.particle_mass.numpy(), model_cpu.particle_inv_mass.numpy()
+        fl, g = model_cpu.particle_flags.numpy(), model_cpu.gravity.numpy()
+        done = 0
+        t0 = time.perf_counter()
+        nw = 0
+        for k, c in enumerate(cfg):
+            sel = np.nonzero(world == k)[0]
+            O.sph_step(c.constants(w["dt"], model_cpu.particle_max_velocity), c.resolved_grid_dims(tight=True),
+                       x[sel], v[sel], m[sel], inv[sel], fl[sel], np.zeros(len(sel), np.int32), g[k:k + 1],
+                       f_ext=np.zeros((len(sel), 3), np.float32), v_out_init=v[sel], precision="f32")
+            done += len(sel)
+            nw += 1
+            if time.perf_counter() - t0 >= budget_s or nw >= max_steps:
+                break
+        el = time.perf_counter() - t0
+        return done / el, nw, el, O.get_threads()
     x = model_cpu.particle_q.numpy()
     v = model_cpu.particle_qd.numpy()
     args = dict(mass=model_cpu.particle_mass.numpy(), inv_mass=model_cpu.particle_inv_mass.numpy(),
@@ -408,9 +470,13 @@ def run_gpu(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         model_cpu, cfg_cpu, w_cpu = make_scene(args.workload, "cpu")
-        rate, steps_done, el, threads = cpu_oracle_rate(model_cpu, cfg_cpu, w_cpu, budget_s=15.0, max_steps=40)
-        cpu = {"value": rate, "unit": METRIC, "cores": threads, "kind": "port",
-               "sample": f"{steps_done} full steps of the {n}-particle workload in {el:.1f} s (fp32 oracle, OpenMP)"}
+        if isinstance(cfg_cpu, list):
+            rate, nw, el, threads = cpu_oracle_rate(model_cpu, cfg_cpu, w_cpu, budget_s=15.0, max_steps=len(cfg_cpu))
+            sample = f"one step of each of the first {nw} worlds in {el:.1f} s (fp32 oracle, OpenMP)"
+        else:
+            rate, steps_done, el, threads = cpu_oracle_rate(model_cpu, cfg_cpu, w_cpu, budget_s=15.0, max_steps=40)
+            sample = f"{steps_done} full steps of the {n}-particle workload in {el:.1f} s (fp32 oracle, OpenMP)"
+        cpu = {"value": rate, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample}
 
     if rank == 0:
         clocks = clk.summary()
@@ -431,7 +497,8 @@ def run_gpu(args):
                 "workload": args.workload,
                 "particles": n,
                 "desc": w["desc"],
-                "grid_dims": list(solver.grid_dims),
+                "grid_dims": list(solver.grid_dims) if solver.grid_dims is not None else "per world (tight)",
+                "worlds": model.world_count,
                 "graph": use_graph,
                 "l2": "flushed (256 MiB write) before every timed step, outside the timed interval",
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",

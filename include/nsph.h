@@ -205,6 +205,32 @@ NSPH_API int nsph_sph_step(nsph_sph* solver, const nsph_sph_params* params, int 
                   float* x_out, float* v_out, float* rho_out, float* p_out, float* a_out,
                   void* stream);
 
+/* ---- batched worlds ------------------------------------------------------
+ * Many independent scenes (Newton worlds: ModelBuilder.begin_world /
+ * add_world, builder.py:2815-2909, with Model.particle_world) in one solver.
+ * Each world has its own grid (dims world_dims[3w..3w+2], HashGrid semantics,
+ * cell width from its parameters) and its own parameters; a particle's
+ * neighbours are the particles of its own world only (world -1 counts as
+ * world 0). Sort keys are (world cell offset + cell), so one build, one
+ * density launch and one force launch cover every world.
+ *
+ * nsph_sph_create_worlds: allocates for `capacity` particles and the sum of
+ *   the worlds' cells.
+ * nsph_sph_set_world_params: copies world_count parameter blocks to the
+ *   device (synchronous; call before the first step and after changes; their
+ *   dt fields are ignored).
+ * nsph_sph_step_worlds: nsph_sph_step for all worlds with time step dt;
+ *   gravity has one row per world. */
+NSPH_API int nsph_sph_create_worlds(int device, int capacity, int world_count, const int* world_dims,
+                                    nsph_sph** out);
+NSPH_API int nsph_sph_set_world_params(nsph_sph* solver, const nsph_sph_params* params, int world_count);
+NSPH_API int nsph_sph_step_worlds(nsph_sph* solver, float dt, int n,
+                                  const float* x_in, const float* v_in, const float* f_ext,
+                                  const float* mass, const float* inv_mass, const int* flags, const int* world,
+                                  const float* gravity, int world_count,
+                                  float* x_out, float* v_out, float* rho_out, float* p_out, float* a_out,
+                                  void* stream);
+
 /* Neighbour lists of the last step's build, in original particle order: for
  * each particle i the ids j (self included) of active particles visited by
  * hash_grid_query(x_i, h) with fp32 r2 = fma(dz,dz,fma(dy,dy,dx*dx)) < h2,

@@ -103,6 +103,17 @@ SIGNATURES = [
         + [c_void_p] * 5
         + [c_void_p],
     ),
+    (
+        "nsph_sph_create_worlds",
+        ctypes.c_int,
+        [ctypes.c_int, ctypes.c_int, ctypes.c_int, c_void_p, ctypes.POINTER(c_void_p)],
+    ),
+    ("nsph_sph_set_world_params", ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int]),
+    (
+        "nsph_sph_step_worlds",
+        ctypes.c_int,
+        [c_void_p, ctypes.c_float, ctypes.c_int] + [c_void_p] * 8 + [ctypes.c_int] + [c_void_p] * 5 + [c_void_p],
+    ),
     ("nsph_sph_neighbors", ctypes.c_int, [c_void_p, ctypes.POINTER(NsphSphParams), c_void_p, c_void_p, c_void_p, c_void_p]),
     ("nsph_sph_get_grid_view", ctypes.c_int, [c_void_p, ctypes.POINTER(NsphGridView)]),
     ("nsph_sph_enable_phase_timing", ctypes.c_int, [c_void_p, ctypes.c_int]),

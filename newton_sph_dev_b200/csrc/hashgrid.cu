@@ -20,6 +20,7 @@
 #include <cstdio>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "nsph_internal.cuh"
 
@@ -42,7 +43,8 @@ __device__ __forceinline__ unsigned lanemask_lt()
 __global__ void __launch_bounds__(kSortThreads) k_hash_hist(
     const float* __restrict__ points, int n, float inv, int dx, int dy, int dz, int* __restrict__ keys,
     int* __restrict__ vals, unsigned* __restrict__ hist, int ntiles, int digit_mask,
-    const int* __restrict__ prev_cells, int prev_n, int2* __restrict__ ranges, unsigned* __restrict__ status)
+    const int* __restrict__ prev_cells, int prev_n, int2* __restrict__ ranges, unsigned* __restrict__ status,
+    const int* __restrict__ world, const WorldCells* __restrict__ wcells, int world_count)
 {
     __shared__ unsigned wh[kSortThreads / 32][kRadix];
     const int warp = threadIdx.x >> 5;
@@ -63,7 +65,15 @@ __global__ void __launch_bounds__(kSortThreads) k_hash_hist(
             const float y = points[3 * (size_t)idx + 1];
             const float z = points[3 * (size_t)idx + 2];
             bad |= !(isfinite(x) && isfinite(y) && isfinite(z));
-            const int key = point_cell(x, y, z, inv, dx, dy, dz);
+            int key;
+            if (wcells) {
+                int w = world ? world[idx] : 0;
+                w = w < 0 ? 0 : (w >= world_count ? world_count - 1 : w);
+                const WorldCells c = wcells[w];
+                key = (int)(c.off + point_cell(x, y, z, c.inv, c.dx, c.dy, c.dz));
+            } else {
+                key = point_cell(x, y, z, inv, dx, dy, dz);
+            }
             keys[idx] = key;
             vals[idx] = idx;
             atomicAdd(&wh[warp][key & digit_mask], 1u);
@@ -329,6 +339,42 @@ int grid_init(Grid& g, int dx, int dy, int dz, int device)
     return NSPH_OK;
 }
 
+int grid_init_worlds(Grid& g, const int* world_dims, int world_count, int device)
+{
+    if (world_count <= 0 || !world_dims) return fail(NSPH_ERR_INVALID_ARG, "world_count must be positive");
+    std::vector<WorldCells> wc((size_t)world_count);
+    long long off = 0;
+    for (int w = 0; w < world_count; ++w) {
+        const int dx = world_dims[3 * w], dy = world_dims[3 * w + 1], dz = world_dims[3 * w + 2];
+        if (dx <= 0 || dy <= 0 || dz <= 0) return fail(NSPH_ERR_INVALID_ARG, "world grid dims must be positive");
+        wc[w] = WorldCells{dx, dy, dz, 0.f, off};
+        off += (long long)dx * dy * dz;
+        if (off > (1LL << 30)) return fail(NSPH_ERR_INVALID_ARG, "the worlds' grids hold more than 2^30 cells");
+    }
+    g.device = device;
+    g.dx = g.dy = g.dz = 0;
+    g.ncells = off;
+    int bits = 1;
+    while ((1LL << bits) < off) ++bits;
+    g.key_bits = bits;
+    g.world_count = world_count;
+    DeviceGuard guard(device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    NSPH_CUDA_TRY(cudaMalloc(&g.cell_ranges, sizeof(int2) * off));
+    NSPH_CUDA_TRY(cudaMemset(g.cell_ranges, 0, sizeof(int2) * off));
+    NSPH_CUDA_TRY(cudaMalloc(&g.worlds, sizeof(WorldCells) * world_count));
+    NSPH_CUDA_TRY(cudaMemcpy(g.worlds, wc.data(), sizeof(WorldCells) * world_count, cudaMemcpyHostToDevice));
+    cudaFuncAttributes fa;
+    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_hash_hist));
+    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_upsweep));
+    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_scan_rows));
+    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_downsweep<false>));
+    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_downsweep<true>));
+    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_ranges));
+    NSPH_CUDA_TRY(cudaDeviceSynchronize());
+    return NSPH_OK;
+}
+
 int grid_reserve(Grid& g, int capacity)
 {
     if (capacity < 0) return fail(NSPH_ERR_INVALID_ARG, "negative capacity");
@@ -374,11 +420,12 @@ void grid_free(Grid& g)
     for (int* b : bufs) cudaFree(b);
     cudaFree(g.hist);
     cudaFree(g.cell_ranges);
+    cudaFree(g.worlds);
     g = Grid();
 }
 
 int grid_build(Grid& g, const float* points, int n, float cell_width, float cell_inv, const GatherArgs* gather,
-               unsigned int* status, cudaStream_t stream, int* launches)
+               unsigned int* status, cudaStream_t stream, int* launches, const int* world)
 {
     int local_launches = 0;
     int& nl = launches ? *launches : local_launches;
@@ -396,7 +443,8 @@ int grid_build(Grid& g, const float* points, int n, float cell_width, float cell
     if (launch_tiles > 0) {
         k_hash_hist<<<launch_tiles, kSortThreads, 0, stream>>>(points, n, cell_inv, g.dx, g.dy, g.dz, g.keys_a,
                                                                g.vals_a, g.hist, ntiles, mask_of(0),
-                                                               g.point_cells, prev_n, g.cell_ranges, status);
+                                                               g.point_cells, prev_n, g.cell_ranges, status, world,
+                                                               g.worlds, g.world_count);
         NSPH_LAUNCH_CHECK("k_hash_hist");
         ++nl;
     }
@@ -633,7 +681,7 @@ extern "C" int nsph_grid_build_noalloc(const float* points, int num_points, floa
     const int ntiles = ntiles_of(n);
     const float inv = 1.0f / radius;
     k_hash_hist<<<ntiles, kSortThreads, 0, cs>>>(points, n, inv, dim_x, dim_y, dim_z, keys_a, vals_a, hist, ntiles,
-                                                 mask_of(0), nullptr, 0, nullptr, nullptr);
+                                                 mask_of(0), nullptr, 0, nullptr, nullptr, nullptr, nullptr, 0);
     NSPH_LAUNCH_CHECK("k_hash_hist");
     const int* kin = keys_a;
     const int* vin = vals_a;

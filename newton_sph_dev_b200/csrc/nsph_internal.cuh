@@ -179,8 +179,20 @@ constexpr int kSortTile = kSortThreads * kSortItems;  // 2048 keys per CTA
 constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
 
+// One world of the batched-worlds mode: the world's own HashGrid dims, its
+// 1/cell_width, and where its cells start in the shared cell table. A
+// particle's sort key is off + (its cell in the world's grid), so worlds
+// occupy disjoint key ranges and never see each other's particles.
+struct WorldCells {
+    int dx, dy, dz;
+    float inv;
+    long long off;
+};
+
 struct Grid {
     int device = 0;
+    int world_count = 0;             // > 0: batched-worlds mode
+    WorldCells* worlds = nullptr;    // device table (world_count entries)
     int dx = 0, dy = 0, dz = 0;
     long long ncells = 0;
     int key_bits = 0;
@@ -223,11 +235,16 @@ constexpr int kAttrDynamic = 2;
 constexpr int kAttrGravShift = 2;
 
 int grid_init(Grid& g, int dx, int dy, int dz, int device);
+// Batched-worlds grid: world w has dims world_dims[3w..3w+2]; its cells start
+// at the sum of the previous worlds' cell counts.
+int grid_init_worlds(Grid& g, const int* world_dims, int world_count, int device);
 int grid_reserve(Grid& g, int capacity);
 void grid_free(Grid& g);
 // Build over `points` (n x 3 AoS float). gather may be null. status may be
 // null. launches (may be null) is incremented per kernel launched.
+// In batched-worlds mode `world` (original order, may be null = world 0) selects
+// each point's world; cell_width/cell_inv are ignored (per world).
 int grid_build(Grid& g, const float* points, int n, float cell_width, float cell_inv, const GatherArgs* gather,
-               unsigned int* status, cudaStream_t stream, int* launches = nullptr);
+               unsigned int* status, cudaStream_t stream, int* launches = nullptr, const int* world = nullptr);
 
 }  // namespace nsph

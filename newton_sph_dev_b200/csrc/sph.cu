@@ -19,7 +19,10 @@
 //   aux[k] float2 (m/rho, p/rho^2)   written by the density pass
 //   rp[k]  float2 (rho, p)           written by the density pass
 // Outputs are scattered back to original particle order through point_ids.
+#include <algorithm>
 #include <cmath>
+#include <string>
+#include <vector>
 
 #include "nsph_internal.cuh"
 
@@ -291,7 +294,8 @@ struct StepOut {
 
 // integrate particle k (original index i) and scatter its outputs
 __device__ __forceinline__ void integrate_out(size_t i, float4 xi, float4 vi, int attr, float2 rpk,
-                                              const ForceAcc& acc, const nsph_sph_params& p, const StepOut& o)
+                                              const ForceAcc& acc, const nsph_sph_params& p, float dt,
+                                              const StepOut& o)
 {
     if (o.rho_out) o.rho_out[i] = rpk.x;
     if (o.p_out) o.p_out[i] = rpk.y;
@@ -321,9 +325,9 @@ __device__ __forceinline__ void integrate_out(size_t i, float4 xi, float4 vi, in
         }
         const float gx = o.gravity[3 * gw + 0], gy = o.gravity[3 * gw + 1], gz = o.gravity[3 * gw + 2];
         // v1 = fma(eps, dv, fma((a + f w) + g, dt, v0))
-        v1x = __fmaf_rn(p.xsph_eps, acc.dvx, __fmaf_rn(__fadd_rn(__fadd_rn(ax, fx), gx), p.dt, vi.x));
-        v1y = __fmaf_rn(p.xsph_eps, acc.dvy, __fmaf_rn(__fadd_rn(__fadd_rn(ay, fy), gy), p.dt, vi.y));
-        v1z = __fmaf_rn(p.xsph_eps, acc.dvz, __fmaf_rn(__fadd_rn(__fadd_rn(az, fz), gz), p.dt, vi.z));
+        v1x = __fmaf_rn(p.xsph_eps, acc.dvx, __fmaf_rn(__fadd_rn(__fadd_rn(ax, fx), gx), dt, vi.x));
+        v1y = __fmaf_rn(p.xsph_eps, acc.dvy, __fmaf_rn(__fadd_rn(__fadd_rn(ay, fy), gy), dt, vi.y));
+        v1z = __fmaf_rn(p.xsph_eps, acc.dvz, __fmaf_rn(__fadd_rn(__fadd_rn(az, fz), gz), dt, vi.z));
     }
     const float vm = __fsqrt_rn(__fmaf_rn(v1z, v1z, __fmaf_rn(v1y, v1y, __fmul_rn(v1x, v1x))));
     if (vm > p.v_max) {
@@ -332,7 +336,7 @@ __device__ __forceinline__ void integrate_out(size_t i, float4 xi, float4 vi, in
         v1y = __fmul_rn(v1y, s);
         v1z = __fmul_rn(v1z, s);
     }
-    float x1x = __fmaf_rn(v1x, p.dt, xi.x), x1y = __fmaf_rn(v1y, p.dt, xi.y), x1z = __fmaf_rn(v1z, p.dt, xi.z);
+    float x1x = __fmaf_rn(v1x, dt, xi.x), x1y = __fmaf_rn(v1y, dt, xi.y), x1z = __fmaf_rn(v1z, dt, xi.z);
     if (dynamic && p.use_box) {
         if (x1x < p.box_lo[0]) { x1x = p.box_lo[0]; v1x = fmaxf(v1x, 0.f); }
         if (x1x > p.box_hi[0]) { x1x = p.box_hi[0]; v1x = fminf(v1x, 0.f); }
@@ -367,7 +371,101 @@ __global__ void __launch_bounds__(kSphThreads, 3) k_force(GridDev g, const float
     const int attr = __float_as_int(vi.w);
     ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (attr & kAttrActive) force_single(g, xs, vs, aux, mask, ncand[k], n, k, xi, vi, aux[k].y, p, acc);
-    integrate_out((size_t)g.ids[k], xi, vi, attr, rp[k], acc, p, o);
+    integrate_out((size_t)g.ids[k], xi, vi, attr, rp[k], acc, p, p.dt, o);
+}
+
+// ---- batched worlds ------------------------------------------------------------
+// One launch per pass covers every world. The kernels are persistent: a grid
+// of (SMs x resident blocks) threads strides over all particles, whose work
+// is similar whatever their world, so no work queue is needed. A particle's
+// world (attr >> kAttrGravShift, clamped at the gather) selects its grid
+// (dims, 1/cell width, cell-table offset) and its parameter block; its
+// neighbours are found and summed exactly as in the single-world kernels, in
+// its own world's query order.
+__device__ __forceinline__ GridDev world_grid(const WorldCells& c, const int2* __restrict__ ranges,
+                                              const int* __restrict__ ids)
+{
+    return GridDev{c.dx, c.dy, c.dz, c.inv, ranges + c.off, ids};
+}
+
+__global__ void __launch_bounds__(kSphThreads, 3) k_density_worlds(const WorldCells* __restrict__ wc,
+                                                                   const nsph_sph_params* __restrict__ wp,
+                                                                   const int2* __restrict__ ranges,
+                                                                   const int* __restrict__ ids,
+                                                                   const float4* __restrict__ xs,
+                                                                   const float4* __restrict__ vs, int n,
+                                                                   float2* __restrict__ aux, float2* __restrict__ rp,
+                                                                   unsigned* __restrict__ mask, int* __restrict__ ncand,
+                                                                   unsigned* __restrict__ status)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float4 xi = xs[k];
+        const int attr = __float_as_int(vs[k].w);
+        if (!(attr & kAttrActive)) {
+            aux[k] = make_float2(0.f, 0.f);
+            rp[k] = make_float2(0.f, 0.f);
+            ncand[k] = 0;
+            continue;
+        }
+        const int w = attr >> kAttrGravShift;
+        const nsph_sph_params& p = wp[w];
+        const GridDev g = world_grid(wc[w], ranges, ids);
+        int nc = 0;
+        const float rho = density_single(g, xs, p, xi, mask, n, k, nc);
+        ncand[k] = nc;
+        density_finish(k, xi.w, rho, p, aux, rp, status);
+    }
+}
+
+__global__ void __launch_bounds__(kSphThreads, 2) k_force_worlds(const WorldCells* __restrict__ wc,
+                                                                 const nsph_sph_params* __restrict__ wp,
+                                                                 const int2* __restrict__ ranges,
+                                                                 const int* __restrict__ ids,
+                                                                 const float4* __restrict__ xs,
+                                                                 const float4* __restrict__ vs,
+                                                                 const float2* __restrict__ aux,
+                                                                 const float2* __restrict__ rp, int n, float dt,
+                                                                 const unsigned* __restrict__ mask,
+                                                                 const int* __restrict__ ncand, const StepOut o)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float4 xi = xs[k], vi = vs[k];
+        const int attr = __float_as_int(vi.w);
+        const int w = attr >> kAttrGravShift;
+        const nsph_sph_params& p = wp[w];
+        const GridDev g = world_grid(wc[w], ranges, ids);
+        ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (attr & kAttrActive) force_single(g, xs, vs, aux, mask, ncand[k], n, k, xi, vi, aux[k].y, p, acc);
+        integrate_out((size_t)ids[k], xi, vi, attr, rp[k], acc, p, dt, o);
+    }
+}
+
+__global__ void k_neighbors_worlds(const WorldCells* __restrict__ wc, const nsph_sph_params* __restrict__ wp,
+                                   const int2* __restrict__ ranges, const int* __restrict__ ids,
+                                   const float4* __restrict__ xs, const float4* __restrict__ vs, int n,
+                                   int* __restrict__ counts, const long long* __restrict__ offsets,
+                                   int* __restrict__ out)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = ids[k];
+    const float4 xi = xs[k];
+    const int attr = __float_as_int(vs[k].w);
+    long long o = out ? offsets[i] : 0;
+    int c = 0;
+    if (attr & kAttrActive) {
+        const int w = attr >> kAttrGravShift;
+        const float h = wp[w].h, h2 = wp[w].h2;
+        const GridDev g = world_grid(wc[w], ranges, ids);
+        for_each_candidate(g, xi.x, xi.y, xi.z, h, [&](int j) {
+            float dx, dy, dz;
+            if (dist2(xi, xs[j], dx, dy, dz) < h2 && (__float_as_int(vs[j].w) & kAttrActive)) {
+                if (out) out[o++] = ids[j];
+                ++c;
+            }
+        });
+    }
+    if (!out) counts[i] = c;
 }
 
 // ---- neighbour lists of the last build (parity export) ----------------------
@@ -416,6 +514,9 @@ struct nsph_sph {
     int last_n = 0;
     int last_launches = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // start, built, density, end
+    nsph_sph_params* wparams = nullptr;  // batched worlds: per-world parameters (device)
+    int wparams_set = 0;
+    int persistent_blocks = 0;           // batched worlds: blocks of the persistent passes
 };
 
 // Record a timing event: as an external event node while the stream is being
@@ -443,9 +544,12 @@ static void sph_free(nsph_sph* s)
     cudaFree(s->rp);
     cudaFree(s->mask);
     cudaFree(s->ncand);
+    cudaFree(s->wparams);
     cudaFree(s->status);
     grid_free(s->grid);
 }
+
+static int sph_create_common(nsph_sph* s, int device, int capacity);
 
 extern "C" int nsph_sph_create(int device, int capacity, const int grid_dims[3], nsph_sph** out)
 {
@@ -456,7 +560,55 @@ extern "C" int nsph_sph_create(int device, int capacity, const int grid_dims[3],
     nsph_sph* s = new (std::nothrow) nsph_sph();
     if (!s) return fail(NSPH_ERR_OUT_OF_MEMORY, "host allocation failed");
     int st = grid_init(s->grid, grid_dims[0], grid_dims[1], grid_dims[2], device);
-    if (st == NSPH_OK) st = grid_reserve(s->grid, capacity);
+    if (st == NSPH_OK) st = sph_create_common(s, device, capacity);
+    if (st != NSPH_OK) {
+        sph_free(s);
+        delete s;
+        return st;
+    }
+    *out = s;
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_create_worlds(int device, int capacity, int world_count, const int* world_dims,
+                                      nsph_sph** out)
+{
+    clear_error();
+    if (!out || !world_dims) return fail(NSPH_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    if (capacity < 0) return fail(NSPH_ERR_INVALID_ARG, "negative capacity");
+    nsph_sph* s = new (std::nothrow) nsph_sph();
+    if (!s) return fail(NSPH_ERR_OUT_OF_MEMORY, "host allocation failed");
+    int st = grid_init_worlds(s->grid, world_dims, world_count, device);
+    if (st == NSPH_OK) st = sph_create_common(s, device, capacity);
+    if (st == NSPH_OK) {
+        DeviceGuard guard(device);
+        cudaError_t e = cudaMalloc(&s->wparams, sizeof(nsph_sph_params) * (size_t)world_count);
+        int sms = 0, per_sm = 0;
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_force_worlds, kSphThreads, 0);
+        cudaFuncAttributes fa;
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_density_worlds);
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_neighbors_worlds);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            st = fail(NSPH_ERR_CUDA, std::string("worlds setup: ") + cudaGetErrorString(e));
+        }
+        s->persistent_blocks = std::max(1, sms * std::max(1, per_sm));
+    }
+    if (st != NSPH_OK) {
+        sph_free(s);
+        delete s;
+        return st;
+    }
+    *out = s;
+    return NSPH_OK;
+}
+
+static int sph_create_common(nsph_sph* s, int device, int capacity)
+{
+    int st = grid_reserve(s->grid, capacity);
     if (st == NSPH_OK) {
         DeviceGuard guard(device);
         const size_t c = (size_t)(capacity > 0 ? capacity : 1);
@@ -478,14 +630,8 @@ extern "C" int nsph_sph_create(int device, int capacity, const int grid_dims[3],
             st = fail(NSPH_ERR_OUT_OF_MEMORY, std::string("solver allocation: ") + cudaGetErrorString(e));
         }
     }
-    if (st != NSPH_OK) {
-        sph_free(s);
-        delete s;
-        return st;
-    }
-    s->capacity = capacity;
-    *out = s;
-    return NSPH_OK;
+    if (st == NSPH_OK) s->capacity = capacity;
+    return st;
 }
 
 extern "C" int nsph_sph_destroy(nsph_sph* solver)
@@ -523,6 +669,8 @@ extern "C" int nsph_sph_step(nsph_sph* s, const nsph_sph_params* p, int n, const
         return fail(NSPH_ERR_INVALID_ARG, "null state or model array");
     if (n > 0 && (x_out == x_in || v_out == v_in))
         return fail(NSPH_ERR_INVALID_ARG, "state_out must not alias state_in");
+    if (s->grid.world_count > 0)
+        return fail(NSPH_ERR_INVALID_ARG, "solver was created for batched worlds: use nsph_sph_step_worlds");
     DeviceGuard guard(s->grid.device);
     if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
     cudaStream_t cs = (cudaStream_t)stream;
@@ -553,11 +701,96 @@ extern "C" int nsph_sph_step(nsph_sph* s, const nsph_sph_params* p, int n, const
     return NSPH_OK;
 }
 
+extern "C" int nsph_sph_set_world_params(nsph_sph* s, const nsph_sph_params* params, int world_count)
+{
+    clear_error();
+    if (!s || !params) return fail(NSPH_ERR_INVALID_ARG, "null argument");
+    if (s->grid.world_count <= 0) return fail(NSPH_ERR_INVALID_ARG, "solver was not created for batched worlds");
+    if (world_count != s->grid.world_count) return fail(NSPH_ERR_INVALID_ARG, "world_count differs from the solver's");
+    for (int w = 0; w < world_count; ++w) {
+        const int st = check_params(params + w);
+        if (st != NSPH_OK) return fail(st, "world " + std::to_string(w) + ": " + nsph_last_error());
+    }
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    std::vector<WorldCells> wc((size_t)world_count);
+    NSPH_CUDA_TRY(cudaMemcpy(wc.data(), s->grid.worlds, sizeof(WorldCells) * world_count, cudaMemcpyDeviceToHost));
+    for (int w = 0; w < world_count; ++w) wc[w].inv = params[w].cell_inv;
+    NSPH_CUDA_TRY(cudaMemcpy(s->grid.worlds, wc.data(), sizeof(WorldCells) * world_count, cudaMemcpyHostToDevice));
+    NSPH_CUDA_TRY(cudaMemcpy(s->wparams, params, sizeof(nsph_sph_params) * world_count, cudaMemcpyHostToDevice));
+    s->wparams_set = 1;
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_step_worlds(nsph_sph* s, float dt, int n, const float* x_in, const float* v_in,
+                                    const float* f_ext, const float* mass, const float* inv_mass, const int* flags,
+                                    const int* world, const float* gravity, int world_count, float* x_out,
+                                    float* v_out, float* rho_out, float* p_out, float* a_out, void* stream)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    if (s->grid.world_count <= 0) return fail(NSPH_ERR_INVALID_ARG, "solver was not created for batched worlds");
+    if (!s->wparams_set) return fail(NSPH_ERR_INVALID_ARG, "world parameters not set (nsph_sph_set_world_params)");
+    if (!isfinite(dt)) return fail(NSPH_ERR_INVALID_ARG, "dt must be finite");
+    if (n < 0) return fail(NSPH_ERR_INVALID_ARG, "negative particle count");
+    if (n > s->capacity) return fail(NSPH_ERR_CAPACITY, "more particles than the solver was created for");
+    if (world_count != s->grid.world_count || !gravity)
+        return fail(NSPH_ERR_INVALID_ARG, "gravity must have one row per world of the solver");
+    if (n > 0 && (!x_in || !v_in || !mass || !inv_mass || !flags || !x_out || !v_out))
+        return fail(NSPH_ERR_INVALID_ARG, "null state or model array");
+    if (n > 0 && (x_out == x_in || v_out == v_in))
+        return fail(NSPH_ERR_INVALID_ARG, "state_out must not alias state_in");
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    cudaStream_t cs = (cudaStream_t)stream;
+    GatherArgs ga{x_in, v_in, mass, inv_mass, flags, world, world_count, s->xs, s->vs};
+    int launches = 0;
+    if (s->ev[0]) NSPH_CUDA_TRY(record_mark(s->ev[0], cs));
+    int st = grid_build(s->grid, x_in, n, 0.f, 0.f, &ga, s->status, cs, &launches, world);
+    if (st != NSPH_OK) return st;
+    s->last_n = n;
+    if (s->ev[1]) NSPH_CUDA_TRY(record_mark(s->ev[1], cs));
+    if (n > 0) {
+        const int blocks = std::min(s->persistent_blocks, (n + kSphThreads - 1) / kSphThreads);
+        k_density_worlds<<<blocks, kSphThreads, 0, cs>>>(s->grid.worlds, s->wparams, s->grid.cell_ranges,
+                                                         s->grid.point_ids, s->xs, s->vs, n, s->aux, s->rp, s->mask,
+                                                         s->ncand, s->status);
+        NSPH_LAUNCH_CHECK("k_density_worlds");
+        ++launches;
+        if (s->ev[2]) NSPH_CUDA_TRY(record_mark(s->ev[2], cs));
+        const StepOut o{f_ext, inv_mass, gravity, x_out, v_out, rho_out, p_out, a_out, s->status};
+        k_force_worlds<<<blocks, kSphThreads, 0, cs>>>(s->grid.worlds, s->wparams, s->grid.cell_ranges,
+                                                       s->grid.point_ids, s->xs, s->vs, s->aux, s->rp, n, dt, s->mask,
+                                                       s->ncand, o);
+        NSPH_LAUNCH_CHECK("k_force_worlds");
+        ++launches;
+    } else if (s->ev[2]) {
+        NSPH_CUDA_TRY(record_mark(s->ev[2], cs));
+    }
+    if (s->ev[3]) NSPH_CUDA_TRY(record_mark(s->ev[3], cs));
+    s->last_launches = launches;
+    return NSPH_OK;
+}
+
 extern "C" int nsph_sph_neighbors(const nsph_sph* s, const nsph_sph_params* p, int* counts,
                                   const long long* offsets, int* out_ids, void* stream)
 {
     clear_error();
     if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    if (s->grid.world_count > 0) {
+        if (!s->grid.built) return fail(NSPH_ERR_NOT_BUILT, "no step has run yet");
+        if (out_ids ? !offsets : !counts)
+            return fail(NSPH_ERR_INVALID_ARG, "counts (count call) or offsets (fill call) required");
+        const int n = s->last_n;
+        if (n == 0) return NSPH_OK;
+        DeviceGuard guard(s->grid.device);
+        if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+        k_neighbors_worlds<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(
+            s->grid.worlds, s->wparams, s->grid.cell_ranges, s->grid.point_ids, s->xs, s->vs, n, counts, offsets,
+            out_ids);
+        NSPH_LAUNCH_CHECK("k_neighbors_worlds");
+        return NSPH_OK;
+    }
     int st = check_params(p);
     if (st != NSPH_OK) return st;
     if (!s->grid.built) return fail(NSPH_ERR_NOT_BUILT, "no step has run yet");

@@ -142,17 +142,22 @@ class SPHConfig:
         }
         return {"f32": f32, "f64": f64}
 
-    def resolved_grid_dims(self) -> tuple[int, int, int]:
+    def resolved_grid_dims(self, tight: bool = False) -> tuple[int, int, int]:
+        """Grid dims: `grid_dims` if given; else, with a box, the cells that
+        cover it plus one guard cell per side, rounded up to powers of two
+        (or exact when `tight`, as the batched-worlds grids use); else 128^3
+        (64^3 when tight)."""
         if self.grid_dims is not None:
             return tuple(int(d) for d in self.grid_dims)
         if self.box_lo is None or self.box_hi is None:
-            return (128, 128, 128)
+            return (64, 64, 64) if tight else (128, 128, 128)
         inv = float(F32(1.0) / F32(self.cell_width if self.cell_width is not None else self.smoothing_length))
         dims = []
         for a in range(3):
             lo = _trunc(float(F32(F32(self.box_lo[a]) * F32(inv))))
             hi = _trunc(float(F32(F32(self.box_hi[a]) * F32(inv))))
-            dims.append(min(2048, _next_pow2(max(4, hi - lo + 3))))
+            span = max(4, hi - lo + 3)
+            dims.append(min(2048, span if tight else _next_pow2(span)))
         while dims[0] * dims[1] * dims[2] > (1 << 26):
             k = int(np.argmax(dims))
             dims[k] //= 2
@@ -175,6 +180,14 @@ class SPHConfig:
 class SolverSPH(SolverBase):
     """WCSPH particle-fluid solver on one CUDA device.
 
+    With one ``Config`` every particle shares one grid and one parameter set
+    (particles of different worlds interact, as in the reference's particle
+    kernels, which ignore ``particle_world``). With a list of configs, one
+    per world (``model.world_count`` entries), the solver runs in
+    batched-worlds mode: each world has its own grid and parameters, a
+    particle only sees particles of its own world, and one launch per pass
+    covers all worlds.
+
     Example::
 
         builder = ModelBuilder()
@@ -188,16 +201,21 @@ class SolverSPH(SolverBase):
 
     Config = SPHConfig
 
-    def __init__(self, model: Model, config: SPHConfig | None = None):
+    def __init__(self, model: Model, config: SPHConfig | list[SPHConfig] | None = None):
         super().__init__(model)
-        self.config = config if config is not None else SPHConfig()
-        if self.config.smoothing_length <= 0.0:
-            raise ValueError("smoothing_length must be positive")
         if model.device.type != "cuda":
             raise RuntimeError("SolverSPH runs on CUDA only (there is no CPU fallback)")
         self._lib = _lib.load()
-        self.grid_dims = self.config.resolved_grid_dims()
         self._handle = ctypes.c_void_p()
+        self._dt = None
+        if isinstance(config, (list, tuple)):
+            self._init_worlds(model, list(config))
+            return
+        self.world_configs = None
+        self.config = config if config is not None else SPHConfig()
+        if self.config.smoothing_length <= 0.0:
+            raise ValueError("smoothing_length must be positive")
+        self.grid_dims = self.config.resolved_grid_dims()
         dims = (ctypes.c_int * 3)(*self.grid_dims)
         _lib.check(
             self._lib.nsph_sph_create(model.device.index or 0, int(model.particle_count), ctypes.byref(dims),
@@ -205,7 +223,37 @@ class SolverSPH(SolverBase):
             "SolverSPH()",
         )
         self._params = self.config.params(0.0, model.particle_max_velocity)
-        self._dt = None
+
+    def _init_worlds(self, model: Model, configs: list[SPHConfig]) -> None:
+        if len(configs) != model.world_count:
+            raise ValueError(f"{len(configs)} configs for {model.world_count} worlds")
+        for c in configs:
+            if c.smoothing_length <= 0.0:
+                raise ValueError("smoothing_length must be positive")
+        self.world_configs = configs
+        self.config = configs[0]
+        self.world_grid_dims = [c.resolved_grid_dims(tight=True) for c in configs]
+        self.grid_dims = None
+        dims = (ctypes.c_int * (3 * len(configs)))(*[d for wd in self.world_grid_dims for d in wd])
+        _lib.check(
+            self._lib.nsph_sph_create_worlds(model.device.index or 0, int(model.particle_count), len(configs), dims,
+                                             ctypes.byref(self._handle)),
+            "SolverSPH()",
+        )
+        self._upload_world_params()
+
+    def _upload_world_params(self) -> None:
+        arr = (_lib.NsphSphParams * len(self.world_configs))()
+        for w, c in enumerate(self.world_configs):
+            arr[w] = c.params(0.0, self.model.particle_max_velocity)
+        _lib.check(self._lib.nsph_sph_set_world_params(self._handle, arr, len(self.world_configs)),
+                   "SolverSPH.set_world_params")
+        self._params = arr[0]
+
+    @property
+    def batched(self) -> bool:
+        """True in batched-worlds mode (one config per world)."""
+        return self.world_configs is not None
 
     def __del__(self):
         h = getattr(self, "_handle", None)
@@ -254,6 +302,15 @@ class SolverSPH(SolverBase):
         rho = getattr(ns, "density", None) if ns is not None else None
         prs = getattr(ns, "pressure", None) if ns is not None else None
         acc = getattr(ns, "acceleration", None) if ns is not None else None
+        if self.batched:
+            st = self._lib.nsph_sph_step_worlds(
+                self._handle, float(F32(dt)), n, state_in.particle_q.data_ptr(), state_in.particle_qd.data_ptr(),
+                _lib.ptr(f_ext), model.particle_mass.data_ptr(), model.particle_inv_mass.data_ptr(),
+                model.particle_flags.data_ptr(), model.particle_world.data_ptr(), model.gravity.data_ptr(),
+                int(model.gravity.shape[0]), state_out.particle_q.data_ptr(), state_out.particle_qd.data_ptr(),
+                _lib.ptr(rho), _lib.ptr(prs), _lib.ptr(acc), _lib.stream_handle(model.device))
+            _lib.check(st, "SolverSPH.step")
+            return
         p = self.params_for(dt)
         st = self._lib.nsph_sph_step(
             self._handle,
@@ -281,8 +338,11 @@ class SolverSPH(SolverBase):
         """MODEL_PROPERTIES re-reads particle_max_velocity; gravity needs no
         action (read on the device every step)."""
         if flags & SolverNotifyFlags.MODEL_PROPERTIES:
-            self._params = self.config.params(0.0 if self._dt is None else self._dt,
-                                              self.model.particle_max_velocity)
+            if self.batched:
+                self._upload_world_params()
+            else:
+                self._params = self.config.params(0.0 if self._dt is None else self._dt,
+                                                  self.model.particle_max_velocity)
 
     @classmethod
     def register_custom_attributes(cls, builder: ModelBuilder) -> None:
@@ -328,6 +388,11 @@ class SolverSPH(SolverBase):
         v = _lib.NsphGridView()
         _lib.check(self._lib.nsph_sph_get_grid_view(self._handle, ctypes.byref(v)), "SolverSPH.grid_arrays")
         dev = self.model.device
+        if self.batched:  # cell tables of all worlds are one large table: return the sort only
+            return {
+                "point_cells": _view_int(v.point_cells, v.num_points, dev).clone(),
+                "point_ids": _view_int(v.point_ids, v.num_points, dev).clone(),
+            }
         nc = v.dim_x * v.dim_y * v.dim_z
         return {
             "point_cells": _view_int(v.point_cells, v.num_points, dev).clone(),
