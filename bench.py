@@ -375,6 +375,7 @@ def run_gpu(args):
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
     # the library records start / built / density / end events inside every
     # step (as external event nodes when captured), on the launching stream
+    tuned = solver.autotune(s0, s1, dt) if not args.no_autotune else None
     solver.enable_phase_timing(True)
 
     def step(a, b):
@@ -500,6 +501,8 @@ def run_gpu(args):
                 "grid_dims": list(solver.grid_dims) if solver.grid_dims is not None else "per world (tight)",
                 "worlds": model.world_count,
                 "graph": use_graph,
+                "launch": {"threads": solver.launch[0], "blocks_per_sm": solver.launch[1],
+                           "autotuned": tuned is not None} if hasattr(solver, "launch") else "default",
                 "l2": "flushed (256 MiB write) before every timed step, outside the timed interval",
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             },
@@ -530,6 +533,7 @@ def main(argv=None):
     ap.add_argument("--workload", choices=[k for k in WORKLOADS if not k.startswith("_")], default="tank_1m")
     ap.add_argument("--no-graph", action="store_true", help="time eager steps instead of graph replays")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

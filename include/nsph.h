@@ -251,6 +251,14 @@ NSPH_API int nsph_sph_get_grid_view(const nsph_sph* solver, nsph_grid_view* view
 NSPH_API int nsph_sph_enable_phase_timing(nsph_sph* solver, int enable);
 NSPH_API int nsph_sph_phase_times(nsph_sph* solver, float ms_out[3]);
 
+/* Launch shape of the two neighbour passes (density, force): `threads` per
+ * block (0 = default 256; else a multiple of 32 up to 256) and
+ * `blocks_per_sm` (-1 = default: one thread per particle for a single world,
+ * a persistent grid for batched worlds; 0 = one thread per particle; k > 0 =
+ * a persistent grid of k blocks per SM striding over the particles). Results
+ * do not depend on the shape; SolverSPH.autotune picks the fastest. */
+NSPH_API int nsph_sph_set_launch(nsph_sph* solver, int threads, int blocks_per_sm);
+
 /* Number of kernels the last nsph_sph_step launched. */
 NSPH_API int nsph_sph_last_launches(const nsph_sph* solver);
 

@@ -201,19 +201,19 @@ __global__ void __launch_bounds__(kSphThreads, 3) k_density(GridDev g, const flo
                                                             unsigned* __restrict__ mask, int* __restrict__ ncand,
                                                             unsigned* __restrict__ status)
 {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const float4 xi = xs[k];
-    if (!(__float_as_int(vs[k].w) & kAttrActive)) {
-        aux[k] = make_float2(0.f, 0.f);
-        rp[k] = make_float2(0.f, 0.f);
-        ncand[k] = 0;
-        return;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float4 xi = xs[k];
+        if (!(__float_as_int(vs[k].w) & kAttrActive)) {
+            aux[k] = make_float2(0.f, 0.f);
+            rp[k] = make_float2(0.f, 0.f);
+            ncand[k] = 0;
+            continue;
+        }
+        int nc = 0;
+        const float rho = density_single(g, xs, p, xi, mask, n, k, nc);
+        ncand[k] = nc;
+        density_finish(k, xi.w, rho, p, aux, rp, status);
     }
-    int nc = 0;
-    const float rho = density_single(g, xs, p, xi, mask, n, k, nc);
-    ncand[k] = nc;
-    density_finish(k, xi.w, rho, p, aux, rp, status);
 }
 
 struct ForceAcc {
@@ -365,13 +365,13 @@ __global__ void __launch_bounds__(kSphThreads, 3) k_force(GridDev g, const float
                                                           const unsigned* __restrict__ mask,
                                                           const int* __restrict__ ncand, const StepOut o)
 {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const float4 xi = xs[k], vi = vs[k];
-    const int attr = __float_as_int(vi.w);
-    ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    if (attr & kAttrActive) force_single(g, xs, vs, aux, mask, ncand[k], n, k, xi, vi, aux[k].y, p, acc);
-    integrate_out((size_t)g.ids[k], xi, vi, attr, rp[k], acc, p, p.dt, o);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float4 xi = xs[k], vi = vs[k];
+        const int attr = __float_as_int(vi.w);
+        ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (attr & kAttrActive) force_single(g, xs, vs, aux, mask, ncand[k], n, k, xi, vi, aux[k].y, p, acc);
+        integrate_out((size_t)g.ids[k], xi, vi, attr, rp[k], acc, p, p.dt, o);
+    }
 }
 
 // ---- batched worlds ------------------------------------------------------------
@@ -517,7 +517,27 @@ struct nsph_sph {
     nsph_sph_params* wparams = nullptr;  // batched worlds: per-world parameters (device)
     int wparams_set = 0;
     int persistent_blocks = 0;           // batched worlds: blocks of the persistent passes
+    int launch_threads = 0;              // neighbour passes: threads per block (0 = default)
+    int launch_blocks_per_sm = -1;       // neighbour passes: persistent blocks per SM (-1 = default, 0 = one thread per particle)
+    int sms = 0;
 };
+
+// grid of a neighbour pass: one thread per particle, or a persistent grid of
+// blocks_per_sm blocks per SM striding over the particles
+static void pass_launch(const nsph_sph* s, int n, bool persistent_default, int& blocks, int& threads)
+{
+    threads = s->launch_threads > 0 ? s->launch_threads : kSphThreads;
+    const int full = (n + threads - 1) / threads;
+    int bps = s->launch_blocks_per_sm;
+    if (bps < 0) bps = persistent_default ? -1 : 0;
+    if (bps < 0)
+        blocks = std::min(full, s->persistent_blocks > 0 ? s->persistent_blocks : full);
+    else if (bps == 0)
+        blocks = full;
+    else
+        blocks = std::min(full, std::max(1, s->sms * bps));
+    blocks = std::max(blocks, 1);
+}
 
 // Record a timing event: as an external event node while the stream is being
 // captured (so a replayed graph records it), as a plain record otherwise.
@@ -608,6 +628,10 @@ extern "C" int nsph_sph_create_worlds(int device, int capacity, int world_count,
 
 static int sph_create_common(nsph_sph* s, int device, int capacity)
 {
+    if (cudaDeviceGetAttribute(&s->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        cudaGetLastError();
+        s->sms = 1;
+    }
     int st = grid_reserve(s->grid, capacity);
     if (st == NSPH_OK) {
         DeviceGuard guard(device);
@@ -683,14 +707,15 @@ extern "C" int nsph_sph_step(nsph_sph* s, const nsph_sph_params* p, int n, const
     if (s->ev[1]) NSPH_CUDA_TRY(record_mark(s->ev[1], cs));
     if (n > 0) {
         const GridDev g = s->grid.view();
-        const int blocks = (n + kSphThreads - 1) / kSphThreads;
-        k_density<<<blocks, kSphThreads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->mask, s->ncand,
+        int blocks, threads;
+        pass_launch(s, n, false, blocks, threads);
+        k_density<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->mask, s->ncand,
                                                    s->status);
         NSPH_LAUNCH_CHECK("k_density");
         ++launches;
         if (s->ev[2]) NSPH_CUDA_TRY(record_mark(s->ev[2], cs));
         const StepOut o{f_ext, inv_mass, gravity, x_out, v_out, rho_out, p_out, a_out, s->status};
-        k_force<<<blocks, kSphThreads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->mask, s->ncand, o);
+        k_force<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->mask, s->ncand, o);
         NSPH_LAUNCH_CHECK("k_force");
         ++launches;
     } else if (s->ev[2]) {
@@ -751,15 +776,16 @@ extern "C" int nsph_sph_step_worlds(nsph_sph* s, float dt, int n, const float* x
     s->last_n = n;
     if (s->ev[1]) NSPH_CUDA_TRY(record_mark(s->ev[1], cs));
     if (n > 0) {
-        const int blocks = std::min(s->persistent_blocks, (n + kSphThreads - 1) / kSphThreads);
-        k_density_worlds<<<blocks, kSphThreads, 0, cs>>>(s->grid.worlds, s->wparams, s->grid.cell_ranges,
+        int blocks, threads;
+        pass_launch(s, n, true, blocks, threads);
+        k_density_worlds<<<blocks, threads, 0, cs>>>(s->grid.worlds, s->wparams, s->grid.cell_ranges,
                                                          s->grid.point_ids, s->xs, s->vs, n, s->aux, s->rp, s->mask,
                                                          s->ncand, s->status);
         NSPH_LAUNCH_CHECK("k_density_worlds");
         ++launches;
         if (s->ev[2]) NSPH_CUDA_TRY(record_mark(s->ev[2], cs));
         const StepOut o{f_ext, inv_mass, gravity, x_out, v_out, rho_out, p_out, a_out, s->status};
-        k_force_worlds<<<blocks, kSphThreads, 0, cs>>>(s->grid.worlds, s->wparams, s->grid.cell_ranges,
+        k_force_worlds<<<blocks, threads, 0, cs>>>(s->grid.worlds, s->wparams, s->grid.cell_ranges,
                                                        s->grid.point_ids, s->xs, s->vs, s->aux, s->rp, n, dt, s->mask,
                                                        s->ncand, o);
         NSPH_LAUNCH_CHECK("k_force_worlds");
@@ -850,6 +876,18 @@ extern "C" int nsph_sph_phase_times(nsph_sph* s, float ms_out[3])
     if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
     NSPH_CUDA_TRY(cudaEventSynchronize(s->ev[3]));
     for (int k = 0; k < 3; ++k) NSPH_CUDA_TRY(cudaEventElapsedTime(ms_out + k, s->ev[k], s->ev[k + 1]));
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_set_launch(nsph_sph* s, int threads, int blocks_per_sm)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    if (threads != 0 && (threads < 32 || threads > kSphThreads || (threads & 31)))
+        return fail(NSPH_ERR_INVALID_ARG, "threads must be 0 or a multiple of 32 in [32, 256]");
+    if (blocks_per_sm < -1 || blocks_per_sm > 64) return fail(NSPH_ERR_INVALID_ARG, "blocks_per_sm out of [-1, 64]");
+    s->launch_threads = threads;
+    s->launch_blocks_per_sm = blocks_per_sm;
     return NSPH_OK;
 }
 

@@ -415,6 +415,43 @@ class SolverSPH(SolverBase):
         _lib.check(self._lib.nsph_sph_phase_times(self._handle, ctypes.byref(ms)), "SolverSPH.phase_times")
         return float(ms[0]), float(ms[1]), float(ms[2])
 
+    def set_launch(self, threads: int = 0, blocks_per_sm: int = -1) -> None:
+        """Launch shape of the density and force passes (see nsph_sph_set_launch)."""
+        _lib.check(self._lib.nsph_sph_set_launch(self._handle, int(threads), int(blocks_per_sm)),
+                   "SolverSPH.set_launch")
+        self.launch = (int(threads), int(blocks_per_sm))
+
+    def autotune(self, state_in: State, state_out: State, dt: float, candidates=None, repeats: int = 3) -> dict:
+        """Pick the fastest launch shape of the neighbour passes.
+
+        Runs `repeats` steps state_in -> state_out per candidate (threads per
+        block, persistent blocks per SM; 0 = one thread per particle), timed
+        on the device with the library's phase events, and keeps the fastest
+        density + force time. Outside a CUDA graph capture only. Results do not
+        depend on the launch shape.
+
+        Returns:
+            {(threads, blocks_per_sm): ms of density + force per step, ...,
+             "best": (threads, blocks_per_sm)}
+        """
+        if candidates is None:
+            candidates = [(t, b) for t in (128, 256) for b in (0, 2, 3, 4, 8)]
+        self.enable_phase_timing(True)
+        results = {}
+        for t, b in candidates:
+            self.set_launch(t, b)
+            self.step(state_in, state_out, None, None, dt)  # warm-up of this shape
+            best = float("inf")
+            for _ in range(repeats):
+                self.step(state_in, state_out, None, None, dt)
+                _, d, f = self.phase_times()
+                best = min(best, d + f)
+            results[(t, b)] = best
+        choice = min(results, key=results.get)
+        self.set_launch(*choice)
+        results["best"] = choice
+        return results
+
     @property
     def last_launches(self) -> int:
         """Kernels launched by the last step."""

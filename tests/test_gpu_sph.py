@@ -302,3 +302,28 @@ def test_full_size_tank_properties(oracle_mod):
     interior = (np.linalg.norm(x - x.mean(0), axis=1) < 0.15)
     assert abs(float(np.median(rho[interior])) - 1000.0) < 20.0
     assert solver.status() == 0
+
+
+def test_launch_shape_does_not_change_results():
+    """The autotuner may pick any launch shape: every shape gives the same bits."""
+    from newton_sph_dev_b200.solvers import SolverSPH
+
+    model, cfg = lattice_scene((16, 12, 10), vel_std=0.1, device=DEV)
+    solver = SolverSPH(model, cfg)
+    s0, s1 = model.state(), model.state()
+    solver.step(s0, s1, None, None, 1e-4)
+    torch.cuda.synchronize()
+    ref = (s1.particle_q.clone(), s1.particle_qd.clone(), s1.sph.density.clone())
+    for shape in [(64, 0), (128, 1), (256, 4), (96, 2)]:
+        solver.set_launch(*shape)
+        solver.step(s0, s1, None, None, 1e-4)
+        torch.cuda.synchronize()
+        assert torch.equal(s1.particle_q, ref[0]) and torch.equal(s1.particle_qd, ref[1])
+        assert torch.equal(s1.sph.density, ref[2])
+    res = solver.autotune(s0, s1, 1e-4, candidates=[(128, 0), (256, 2)], repeats=1)
+    assert res["best"] in [(128, 0), (256, 2)]
+    solver.step(s0, s1, None, None, 1e-4)
+    torch.cuda.synchronize()
+    assert torch.equal(s1.particle_q, ref[0])
+    with pytest.raises(ValueError):
+        solver.set_launch(100, 0)
