@@ -231,6 +231,44 @@ NSPH_API int nsph_sph_step_worlds(nsph_sph* solver, float dt, int n,
                                   float* x_out, float* v_out, float* rho_out, float* p_out, float* a_out,
                                   void* stream);
 
+/* ---- adjoint (reverse mode) of nsph_sph_step ------------------------------
+ * Replaces the reference's wp.Tape gradient of a solver step
+ * (newton/solvers.py:359-395; examples/diffsim/example_diffsim_ball.py:
+ * 115-151): the vector-Jacobian product of one step, written by hand.
+ *
+ * nsph_sph_enable_adjoint: allocates the adjoint scratch (36 bytes per
+ *   particle of capacity); call once, outside graph capture. Single-world
+ *   solvers only.
+ * nsph_sph_step_adjoint: same model/state inputs as the nsph_sph_step it
+ *   reverses (x_in, v_in, f_ext, mass, ... of that step; it recomputes the
+ *   step's grid, density and forces from them, bit for bit). Given
+ *     x_out_adj, v_out_adj: adjoints of x_out, v_out (n x 3)
+ *     rho_out_adj:          adjoint of the step's density (float[n]) or NULL
+ *   it writes
+ *     x_in_adj, v_in_adj:   adjoints of x_in, v_in (n x 3, overwritten; may
+ *                           be the same memory as x_out_adj / v_out_adj
+ *                           respectively, which a reverse loop uses)
+ *   and accumulates (+=), so a reverse loop sums them over steps,
+ *     f_ext_adj:            adjoint of f_ext (n x 3) or NULL
+ *     eos_b_adj:            adjoint of params->eos_b (one float) or NULL.
+ * The neighbour set is held fixed (W and dW/dr vanish at r = h, so the step
+ * is C1 across its changes); the pressure clamp, |v| clamp and box are
+ * differentiated on the side the forward step took. Inactive particles
+ * pass their adjoints through (their velocity output is taken as a copy of
+ * the input). Deterministic: no atomics; adj(B) is reduced in a fixed order
+ * for a fixed launch shape. The call overwrites the solver's grid and
+ * neighbour scratch (as a step on x_in would). Kernels: grid build, density,
+ * force recompute + integrate reverse, pair gather, density gather, and the
+ * adj(B) reduction when eos_b_adj is given. */
+NSPH_API int nsph_sph_enable_adjoint(nsph_sph* solver);
+NSPH_API int nsph_sph_step_adjoint(nsph_sph* solver, const nsph_sph_params* params, int n,
+                                   const float* x_in, const float* v_in, const float* f_ext,
+                                   const float* mass, const float* inv_mass, const int* flags, const int* world,
+                                   const float* gravity, int world_count,
+                                   const float* x_out_adj, const float* v_out_adj, const float* rho_out_adj,
+                                   float* x_in_adj, float* v_in_adj, float* f_ext_adj, float* eos_b_adj,
+                                   void* stream);
+
 /* Neighbour lists of the last step's build, in original particle order: for
  * each particle i the ids j (self included) of active particles visited by
  * hash_grid_query(x_i, h) with fp32 r2 = fma(dz,dz,fma(dy,dy,dx*dx)) < h2,

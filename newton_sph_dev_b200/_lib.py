@@ -114,6 +114,16 @@ SIGNATURES = [
         ctypes.c_int,
         [c_void_p, ctypes.c_float, ctypes.c_int] + [c_void_p] * 8 + [ctypes.c_int] + [c_void_p] * 5 + [c_void_p],
     ),
+    ("nsph_sph_enable_adjoint", ctypes.c_int, [c_void_p]),
+    (
+        "nsph_sph_step_adjoint",
+        ctypes.c_int,
+        [c_void_p, ctypes.POINTER(NsphSphParams), ctypes.c_int]
+        + [c_void_p] * 8
+        + [ctypes.c_int]
+        + [c_void_p] * 7
+        + [c_void_p],
+    ),
     ("nsph_sph_neighbors", ctypes.c_int, [c_void_p, ctypes.POINTER(NsphSphParams), c_void_p, c_void_p, c_void_p, c_void_p]),
     ("nsph_sph_get_grid_view", ctypes.c_int, [c_void_p, ctypes.POINTER(NsphGridView)]),
     ("nsph_sph_enable_phase_timing", ctypes.c_int, [c_void_p, ctypes.c_int]),

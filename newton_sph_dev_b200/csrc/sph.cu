@@ -493,6 +493,299 @@ __global__ void k_neighbors(GridDev g, const float4* __restrict__ xs, const floa
     if (!out) counts[i] = c;
 }
 
+// ==========================================================================
+// Adjoint of the step (reverse mode): given the adjoints of x_{n+1}, v_{n+1}
+// (and optionally of rho), the adjoints of x_n, v_n, f_ext and of the EOS
+// stiffness B. The neighbour set is held fixed (it is piecewise constant in
+// x; W and dW/dr vanish at r = h, so the step is C1 across its changes); the
+// pressure clamp, |v| clamp and box are differentiated on the side the
+// forward step took, which the reverse pass recomputes bit for bit.
+//
+// The forward step sums pair terms into particle i only (a gather), so its
+// transpose scatters into both particles of a pair. Because the neighbour
+// relation is symmetric (the fp32 r2 of (i, j) and (j, i) are equal) every
+// scatter is rewritten as a gather over the same neighbour lists, with no
+// atomics, and each particle's adjoint is written by one thread:
+//   local   G_i = adj(a_i), D_i = adj(dv_i), and the integrate reverse
+//   pair    adj(p_i/rho_i^2) = sum_j F_ij (Z_ij . d_ij)
+//           adj(m_i/rho_i)   = sum_j W_ij D_j . (v_i - v_j)
+//           adj(x_i)        += sum_j S_ij [F Z + (F'/r)(d.Z) d]
+//                              + F ((v_j - v_i) . Y_ij) d
+//           adj(v_i)        -= sum_j W_ij Y_ij
+//           with Z = m_i G_j - m_j G_i, Y = mor_j D_i - mor_i D_j,
+//           S = p_i/rho_i^2 + p_j/rho_j^2, d = x_i - x_j, F = (dW/dr)/r
+//           then adj(rho_i) through the EOS and the m/rho, p/rho^2 factors
+//   density adj(x_i)        += sum_j F_ij (adj(rho_i) m_j + adj(rho_j) m_i) d_ij
+// ==========================================================================
+
+// (dF/dr)/r of F = (dW/dr)/r: near 3 c_near / (h r); far -c_far t (2/(h r^2) + t/r^3)
+__device__ __forceinline__ float kernel_df_over_r(float q, float inv_r, const nsph_sph_params& p)
+{
+    const float t = 1.f - q;
+    if (q <= 0.5f) return 3.f * p.c_near * p.inv_h * inv_r;
+    if (q < 1.f) return -p.c_far * t * (2.f * p.inv_h + t * inv_r) * inv_r * inv_r;
+    return 0.f;
+}
+
+// visit(j) for every neighbour j != k of sorted particle k, in query order,
+// from the density pass's masks (re-testing when they overflowed)
+template <class V>
+__device__ __forceinline__ void for_each_neighbor(const GridDev& g, const float4* __restrict__ xs,
+                                                  const unsigned* __restrict__ mask, int nc, int n, int k, float4 xi,
+                                                  const nsph_sph_params& p, V&& visit)
+{
+    if (nc <= kMaskBits) {
+        for_each_masked(
+            g, xi, p.h, [&](int w) { return __ldg(mask + (size_t)w * n + k); },
+            [&](int j) {
+                if (j != k) visit(j);
+            });
+    } else {
+        for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
+            for (int j = lo; j < hi; ++j) {
+                float dx, dy, dz;
+                if (j != k && dist2(xi, __ldg(xs + j), dx, dy, dz) < p.h2) visit(j);
+            }
+        });
+    }
+}
+
+struct AdjIO {
+    const float* x_out_adj;
+    const float* v_out_adj;
+    const float* rho_out_adj;
+    float* x_in_adj;
+    float* v_in_adj;
+    float* f_ext_adj;
+    const float* f_ext;
+    const float* inv_mass;
+    const float* gravity;
+    float4* g;     // sorted: adj(a)
+    float4* d;     // sorted: adj(dv)
+    float* rho;    // sorted: adj(rho)
+    float* bpart;  // per block: partial adj(B)
+};
+
+// reverse of integrate: recompute the forward particle update (bit for bit,
+// so the clamp decisions are the forward's), then transpose it
+__global__ void __launch_bounds__(kSphThreads, 2) k_adj_local(GridDev g, const float4* __restrict__ xs,
+                                                              const float4* __restrict__ vs,
+                                                              const float2* __restrict__ aux, int n,
+                                                              const __grid_constant__ nsph_sph_params p,
+                                                              const unsigned* __restrict__ mask,
+                                                              const int* __restrict__ ncand, const AdjIO io)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float4 xi = xs[k], vi = vs[k];
+        const int attr = __float_as_int(vi.w);
+        const size_t i = (size_t)g.ids[k];
+        const float xb1[3] = {io.x_out_adj[3 * i], io.x_out_adj[3 * i + 1], io.x_out_adj[3 * i + 2]};
+        const float vb1[3] = {io.v_out_adj[3 * i], io.v_out_adj[3 * i + 1], io.v_out_adj[3 * i + 2]};
+        float fb[3] = {0.f, 0.f, 0.f};
+        float4 gk = make_float4(0.f, 0.f, 0.f, 0.f), dk = gk;
+        if (!(attr & kAttrActive)) {
+            for (int c = 0; c < 3; ++c) {
+                io.x_in_adj[3 * i + c] = xb1[c];
+                io.v_in_adj[3 * i + c] = vb1[c];
+            }
+        } else {
+            ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            force_single(g, xs, vs, aux, mask, ncand[k], n, k, xi, vi, aux[k].y, p, acc);
+            const bool dynamic = (attr & kAttrDynamic) != 0;
+            float w = 0.f;
+            float u[3] = {vi.x, vi.y, vi.z};
+            if (dynamic) {  // the forward update of integrate_out, same rounding
+                const int gw = attr >> kAttrGravShift;
+                float fe[3] = {0.f, 0.f, 0.f};
+                if (io.f_ext) {
+                    w = io.inv_mass[i];
+                    for (int c = 0; c < 3; ++c) fe[c] = __fmul_rn(io.f_ext[3 * i + c], w);
+                }
+                const float a[3] = {acc.ax, acc.ay, acc.az}, dv[3] = {acc.dvx, acc.dvy, acc.dvz};
+                for (int c = 0; c < 3; ++c)
+                    u[c] = __fmaf_rn(p.xsph_eps, dv[c],
+                                     __fmaf_rn(__fadd_rn(__fadd_rn(a[c], fe[c]), io.gravity[3 * gw + c]), p.dt, u[c]));
+            }
+            const float vm = __fsqrt_rn(__fmaf_rn(u[2], u[2], __fmaf_rn(u[1], u[1], __fmul_rn(u[0], u[0]))));
+            const bool vclamp = vm > p.v_max;
+            const float s = vclamp ? __fdiv_rn(p.v_max, vm) : 1.f;
+            const float xin[3] = {xi.x, xi.y, xi.z};
+            float vcb[3], xpb[3];
+            for (int c = 0; c < 3; ++c) {
+                const float vc = vclamp ? __fmul_rn(u[c], s) : u[c];
+                const float xp = __fmaf_rn(vc, p.dt, xin[c]);
+                xpb[c] = xb1[c];
+                vcb[c] = vb1[c];
+                if (dynamic && p.use_box) {
+                    if (xp < p.box_lo[c]) {  // x = lo, v = max(v, 0)
+                        xpb[c] = 0.f;
+                        if (vc < 0.f) vcb[c] = 0.f;
+                    } else if (xp > p.box_hi[c]) {  // x = hi, v = min(v, 0)
+                        xpb[c] = 0.f;
+                        if (vc > 0.f) vcb[c] = 0.f;
+                    }
+                }
+                vcb[c] += xpb[c] * p.dt;
+            }
+            float ub[3] = {vcb[0], vcb[1], vcb[2]};
+            if (vclamp) {  // v = v_max u/|u|: adj(u) = (v_max/|u|)(adj(v) - u^ (u^ . adj(v)))
+                const float inv = 1.f / vm;
+                const float uh[3] = {u[0] * inv, u[1] * inv, u[2] * inv};
+                const float dot = uh[0] * vcb[0] + uh[1] * vcb[1] + uh[2] * vcb[2];
+                for (int c = 0; c < 3; ++c) ub[c] = s * (vcb[c] - uh[c] * dot);
+            }
+            for (int c = 0; c < 3; ++c) {
+                io.x_in_adj[3 * i + c] = xpb[c];
+                io.v_in_adj[3 * i + c] = ub[c];
+            }
+            if (dynamic) {
+                gk = make_float4(ub[0] * p.dt, ub[1] * p.dt, ub[2] * p.dt, 0.f);
+                dk = make_float4(ub[0] * p.xsph_eps, ub[1] * p.xsph_eps, ub[2] * p.xsph_eps, 0.f);
+                if (io.f_ext)
+                    for (int c = 0; c < 3; ++c) fb[c] = ub[c] * p.dt * w;
+            }
+        }
+        if (io.f_ext_adj)
+            for (int c = 0; c < 3; ++c) io.f_ext_adj[3 * i + c] += fb[c];
+        io.g[k] = gk;
+        io.d[k] = dk;
+    }
+}
+
+// sum of v over the block, valid in thread 0
+__device__ __forceinline__ float block_sum(float v)
+{
+    __shared__ float part[32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) part[warp] = v;
+    __syncthreads();
+    v = 0.f;
+    if (warp == 0) {
+        v = lane < (int)(blockDim.x >> 5) ? part[lane] : 0.f;
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    }
+    return v;
+}
+
+// gather of the transposed pressure and XSPH terms, then adj(rho) through
+// the EOS; per-block partial sums of adj(B)
+__global__ void __launch_bounds__(kSphThreads, 2) k_adj_pair(GridDev g, const float4* __restrict__ xs,
+                                                             const float4* __restrict__ vs,
+                                                             const float2* __restrict__ aux,
+                                                             const float2* __restrict__ rp, int n,
+                                                             const __grid_constant__ nsph_sph_params p,
+                                                             const unsigned* __restrict__ mask,
+                                                             const int* __restrict__ ncand, const AdjIO io)
+{
+    float bsum = 0.f;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float4 xi = xs[k], vi = vs[k];
+        const size_t i = (size_t)g.ids[k];
+        if (!(__float_as_int(vi.w) & kAttrActive)) {
+            io.rho[k] = 0.f;
+            continue;
+        }
+        const float2 ak = aux[k];
+        const float4 gk = io.g[k], dk = io.d[k];
+        const float mk = xi.w;
+        float pr2b = 0.f, morb = 0.f;
+        float xb[3] = {0.f, 0.f, 0.f}, vb[3] = {0.f, 0.f, 0.f};
+        for_each_neighbor(g, xs, mask, ncand[k], n, k, xi, p, [&](int j) {
+            const float4 vj = __ldg(vs + j);
+            if (!(__float_as_int(vj.w) & kAttrActive)) return;
+            const float4 xj = __ldg(xs + j);
+            const float2 aj = __ldg(aux + j);
+            const float4 gj = __ldg(io.g + j), dj = __ldg(io.d + j);
+            float dx, dy, dz;
+            const float r2 = dist2(xi, xj, dx, dy, dz);
+            const float r = __fsqrt_rn(r2);
+            const float q = r * p.inv_h;
+            const float w = kernel_w(q, p);
+            const float yx = aj.x * dk.x - ak.x * dj.x, yy = aj.x * dk.y - ak.x * dj.y, yz = aj.x * dk.z - ak.x * dj.z;
+            const float rvx = vj.x - vi.x, rvy = vj.y - vi.y, rvz = vj.z - vi.z;
+            if (r2 > 0.f) {
+                const float inv_r = 1.f / r;
+                const float f = kernel_f(q, inv_r, p);
+                const float dfr = kernel_df_over_r(q, inv_r, p);
+                const float zx = mk * gj.x - xj.w * gk.x, zy = mk * gj.y - xj.w * gk.y, zz = mk * gj.z - xj.w * gk.z;
+                const float zd = zx * dx + zy * dy + zz * dz;
+                pr2b += f * zd;
+                const float sp = ak.y + aj.y;
+                const float cx = sp * dfr * zd + f * (rvx * yx + rvy * yy + rvz * yz);
+                xb[0] += sp * f * zx + cx * dx;
+                xb[1] += sp * f * zy + cx * dy;
+                xb[2] += sp * f * zz + cx * dz;
+            }
+            vb[0] -= w * yx;
+            vb[1] -= w * yy;
+            vb[2] -= w * yz;
+            morb -= w * (dj.x * rvx + dj.y * rvy + dj.z * rvz);
+        });
+        // adj(rho) from p/rho^2 (through the EOS) and m/rho
+        const float2 rpk = rp[k];
+        float rb = io.rho_out_adj ? io.rho_out_adj[i] : 0.f;
+        if (rpk.x > 0.f) {
+            const float rho = rpk.x, ratio = __fmul_rn(rho, p.inv_rho0);
+            float pw1 = 1.f;  // ratio^(gamma-1)
+            for (int e = 1; e < p.eos_gamma; ++e) pw1 = __fmul_rn(pw1, ratio);
+            const float pw = p.eos_gamma > 0 ? __fmul_rn(pw1, ratio) : 1.f;
+            const float praw = __fmul_rn(p.eos_b, __fsub_rn(pw, 1.f));
+            const bool live = !(p.clamp_pressure && praw < 0.f);
+            const float inv_rho = 1.f / rho, inv_rho2 = inv_rho * inv_rho;
+            const float dp = (live && p.eos_gamma > 0) ? p.eos_b * (float)p.eos_gamma * pw1 * p.inv_rho0 : 0.f;
+            rb += pr2b * (dp - 2.f * rpk.y * inv_rho) * inv_rho2 - morb * mk * inv_rho2;
+            if (live) bsum += pr2b * (pw - 1.f) * inv_rho2;
+        }
+        io.rho[k] = rb;
+        for (int c = 0; c < 3; ++c) {
+            io.x_in_adj[3 * i + c] += xb[c];
+            io.v_in_adj[3 * i + c] += vb[c];
+        }
+    }
+    bsum = block_sum(bsum);
+    if (threadIdx.x == 0) io.bpart[blockIdx.x] = bsum;
+}
+
+// gather of the transposed density sum
+__global__ void __launch_bounds__(kSphThreads, 3) k_adj_density(GridDev g, const float4* __restrict__ xs,
+                                                                const float4* __restrict__ vs, int n,
+                                                                const __grid_constant__ nsph_sph_params p,
+                                                                const unsigned* __restrict__ mask,
+                                                                const int* __restrict__ ncand,
+                                                                const float* __restrict__ rho_adj,
+                                                                float* __restrict__ x_in_adj)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        if (!(__float_as_int(vs[k].w) & kAttrActive)) continue;
+        const float4 xi = xs[k];
+        const float rbk = rho_adj[k], mk = xi.w;
+        float xb[3] = {0.f, 0.f, 0.f};
+        for_each_neighbor(g, xs, mask, ncand[k], n, k, xi, p, [&](int j) {
+            const float4 xj = __ldg(xs + j);
+            float dx, dy, dz;
+            const float r2 = dist2(xi, xj, dx, dy, dz);
+            if (!(r2 > 0.f)) return;
+            const float r = __fsqrt_rn(r2);
+            const float c = kernel_f(r * p.inv_h, 1.f / r, p) * (rbk * xj.w + __ldg(rho_adj + j) * mk);
+            xb[0] += c * dx;
+            xb[1] += c * dy;
+            xb[2] += c * dz;
+        });
+        const size_t i = (size_t)g.ids[k];
+        for (int c = 0; c < 3; ++c) x_in_adj[3 * i + c] += xb[c];
+    }
+}
+
+// adj(B) += sum of the per-block partials, in a fixed order
+__global__ void k_adj_b_reduce(const float* __restrict__ bpart, int blocks, float* __restrict__ b_adj)
+{
+    float v = 0.f;
+    for (int b = threadIdx.x; b < blocks; b += blockDim.x) v += bpart[b];
+    v = block_sum(v);
+    if (threadIdx.x == 0) *b_adj += v;
+}
+
 }  // namespace
 }  // namespace nsph
 
@@ -520,6 +813,11 @@ struct nsph_sph {
     int launch_threads = 0;              // neighbour passes: threads per block (0 = default)
     int launch_blocks_per_sm = -1;       // neighbour passes: persistent blocks per SM (-1 = default, 0 = one thread per particle)
     int sms = 0;
+    float4* adj_g = nullptr;             // adjoint scratch (nsph_sph_enable_adjoint), sorted order: adj(a)
+    float4* adj_d = nullptr;             //   adj(dv)
+    float* adj_rho = nullptr;            //   adj(rho)
+    float* adj_bpart = nullptr;          //   per-block partial sums of adj(B)
+    int adj_bcap = 0;                    //   entries of adj_bpart
 };
 
 // grid of a neighbour pass: one thread per particle, or a persistent grid of
@@ -566,6 +864,10 @@ static void sph_free(nsph_sph* s)
     cudaFree(s->ncand);
     cudaFree(s->wparams);
     cudaFree(s->status);
+    cudaFree(s->adj_g);
+    cudaFree(s->adj_d);
+    cudaFree(s->adj_rho);
+    cudaFree(s->adj_bpart);
     grid_free(s->grid);
 }
 
@@ -911,5 +1213,95 @@ extern "C" int nsph_sph_reset_status(nsph_sph* s, void* stream)
     DeviceGuard guard(s->grid.device);
     if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
     NSPH_CUDA_TRY(cudaMemsetAsync(s->status, 0, sizeof(unsigned), (cudaStream_t)stream));
+    return NSPH_OK;
+}
+
+// ==========================================================================
+// C ABI: adjoint of the step
+// ==========================================================================
+extern "C" int nsph_sph_enable_adjoint(nsph_sph* s)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    if (s->grid.world_count > 0) return fail(NSPH_ERR_INVALID_ARG, "the adjoint supports single-world solvers only");
+    if (s->adj_g) return NSPH_OK;
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    const size_t c = (size_t)(s->capacity > 0 ? s->capacity : 1);
+    const int bcap = (int)((c + 31) / 32) + 1;  // blocks of a pass of >= 32 threads per block
+    cudaError_t e = cudaMalloc(&s->adj_g, sizeof(float4) * c);
+    if (e == cudaSuccess) e = cudaMalloc(&s->adj_d, sizeof(float4) * c);
+    if (e == cudaSuccess) e = cudaMalloc(&s->adj_rho, sizeof(float) * c);
+    if (e == cudaSuccess) e = cudaMalloc(&s->adj_bpart, sizeof(float) * (size_t)bcap);
+    cudaFuncAttributes fa;
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_adj_local);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_adj_pair);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_adj_density);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(s->adj_g);
+        cudaFree(s->adj_d);
+        cudaFree(s->adj_rho);
+        cudaFree(s->adj_bpart);
+        s->adj_g = s->adj_d = nullptr;
+        s->adj_rho = s->adj_bpart = nullptr;
+        return fail(NSPH_ERR_OUT_OF_MEMORY, std::string("adjoint allocation: ") + cudaGetErrorString(e));
+    }
+    s->adj_bcap = bcap;
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_step_adjoint(nsph_sph* s, const nsph_sph_params* p, int n, const float* x_in,
+                                     const float* v_in, const float* f_ext, const float* mass, const float* inv_mass,
+                                     const int* flags, const int* world, const float* gravity, int world_count,
+                                     const float* x_out_adj, const float* v_out_adj, const float* rho_out_adj,
+                                     float* x_in_adj, float* v_in_adj, float* f_ext_adj, float* eos_b_adj,
+                                     void* stream)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    int st = check_params(p);
+    if (st != NSPH_OK) return st;
+    if (s->grid.world_count > 0) return fail(NSPH_ERR_INVALID_ARG, "the adjoint supports single-world solvers only");
+    if (!s->adj_g) return fail(NSPH_ERR_INVALID_ARG, "adjoint scratch not allocated (nsph_sph_enable_adjoint)");
+    if (n < 0) return fail(NSPH_ERR_INVALID_ARG, "negative particle count");
+    if (n > s->capacity) return fail(NSPH_ERR_CAPACITY, "more particles than the solver was created for");
+    if (world_count < 1 || !gravity) return fail(NSPH_ERR_INVALID_ARG, "gravity needs world_count >= 1");
+    if (n > 0 && (!x_in || !v_in || !mass || !inv_mass || !flags))
+        return fail(NSPH_ERR_INVALID_ARG, "null state or model array");
+    if (n > 0 && (!x_out_adj || !v_out_adj || !x_in_adj || !v_in_adj))
+        return fail(NSPH_ERR_INVALID_ARG, "null adjoint array");
+    if (n > 0 && ((const float*)x_in_adj == v_out_adj || (const float*)v_in_adj == x_out_adj || x_in_adj == v_in_adj))
+        return fail(NSPH_ERR_INVALID_ARG, "position and velocity adjoints must not share memory");
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    cudaStream_t cs = (cudaStream_t)stream;
+    GatherArgs ga{x_in, v_in, mass, inv_mass, flags, world, world_count, s->xs, s->vs};
+    int launches = 0;
+    st = grid_build(s->grid, x_in, n, p->cell_width, p->cell_inv, &ga, s->status, cs, &launches);
+    if (st != NSPH_OK) return st;
+    s->last_n = n;
+    if (n > 0) {
+        const GridDev g = s->grid.view();
+        int blocks, threads;
+        pass_launch(s, n, false, blocks, threads);
+        k_density<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->mask, s->ncand, s->status);
+        NSPH_LAUNCH_CHECK("k_density");
+        const AdjIO io{x_out_adj, v_out_adj, rho_out_adj, x_in_adj, v_in_adj, f_ext_adj, f_ext, inv_mass, gravity,
+                       s->adj_g, s->adj_d, s->adj_rho, s->adj_bpart};
+        k_adj_local<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, n, *p, s->mask, s->ncand, io);
+        NSPH_LAUNCH_CHECK("k_adj_local");
+        k_adj_pair<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->mask, s->ncand, io);
+        NSPH_LAUNCH_CHECK("k_adj_pair");
+        k_adj_density<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->mask, s->ncand, s->adj_rho, x_in_adj);
+        NSPH_LAUNCH_CHECK("k_adj_density");
+        launches += 4;
+        if (eos_b_adj) {
+            k_adj_b_reduce<<<1, 256, 0, cs>>>(s->adj_bpart, blocks, eos_b_adj);
+            NSPH_LAUNCH_CHECK("k_adj_b_reduce");
+            ++launches;
+        }
+    }
+    s->last_launches = launches;
     return NSPH_OK;
 }

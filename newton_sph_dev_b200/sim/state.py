@@ -55,9 +55,11 @@ class State:
         forces accumulated before the step, cleared by clear_forces)."""
 
     def clear_forces(self) -> None:
-        """Zero ``particle_f`` (state.py:156-167)."""
+        """Zero ``particle_f`` (state.py:156-167). Not recorded by autograd
+        (the forces are inputs, as Warp's tape treats the cleared array)."""
         if self.particle_count:
-            self.particle_f.zero_()
+            with torch.no_grad():
+                self.particle_f.zero_()
 
     def assign(self, other: State) -> None:
         """Copy the arrays of another state into this one (state.py:169-229).

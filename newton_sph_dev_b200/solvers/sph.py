@@ -298,6 +298,20 @@ class SolverSPH(SolverBase):
             if t.dtype != torch.float32 or tuple(t.shape) != (n, 3) or not t.is_contiguous():
                 raise ValueError(f"{name} must be a contiguous ({n}, 3) float32 tensor")
         f_ext = state_in.particle_f if (self.config.apply_particle_f and state_in.particle_f is not None) else None
+        if torch.is_grad_enabled() and any(t is not None and t.requires_grad
+                                           for t in (state_in.particle_q, state_in.particle_qd, f_ext)):
+            # differentiable step (models finalized with requires_grad=True):
+            # state_out's arrays become the outputs of an autograd node whose
+            # backward is the hand-written adjoint, as wp.Tape records a step
+            # (newton/solvers.py:359-395). Inactive particles keep state_in's
+            # velocity; the sph namespace outputs are not written.
+            from .sph_diff import sph_step
+
+            if self.batched:
+                raise ValueError("differentiable steps need a single-world solver")
+            state_out.particle_q, state_out.particle_qd = sph_step(
+                self, state_in.particle_q, state_in.particle_qd, dt, None, f_ext)
+            return
         ns = getattr(state_out, "sph", None)
         rho = getattr(ns, "density", None) if ns is not None else None
         prs = getattr(ns, "pressure", None) if ns is not None else None
@@ -333,6 +347,110 @@ class SolverSPH(SolverBase):
             _lib.stream_handle(model.device),
         )
         _lib.check(st, "SolverSPH.step")
+
+    # ---- adjoint ---------------------------------------------------------
+    def enable_adjoint(self) -> None:
+        """Allocate the adjoint scratch (36 bytes per particle); called on
+        demand by :meth:`step_backward`, outside graph capture."""
+        if self.batched:
+            raise ValueError("the adjoint supports single-world solvers only")
+        if not getattr(self, "_adjoint_ready", False):
+            _lib.check(self._lib.nsph_sph_enable_adjoint(self._handle), "SolverSPH.enable_adjoint")
+            self._adjoint_ready = True
+
+    def step_params(self, dt: float, eos_b: float | None = None) -> _lib.NsphSphParams:
+        """A private copy of the fp32 parameter block for time step dt, with
+        the EOS stiffness B replaced by `eos_b` when given."""
+        p = _lib.NsphSphParams()
+        ctypes.memmove(ctypes.byref(p), ctypes.byref(self.params_for(dt)), ctypes.sizeof(p))
+        if eos_b is not None:
+            p.eos_b = float(F32(eos_b))
+        return p
+
+    def _check_vec(self, t: torch.Tensor, name: str) -> None:
+        n = self.model.particle_count
+        _require_cuda(t, name)
+        if t.dtype != torch.float32 or tuple(t.shape) != (n, 3) or not t.is_contiguous():
+            raise ValueError(f"{name} must be a contiguous ({n}, 3) float32 tensor")
+
+    def step_raw(self, x_in: torch.Tensor, v_in: torch.Tensor, x_out: torch.Tensor, v_out: torch.Tensor,
+                 params: _lib.NsphSphParams, f_ext: torch.Tensor | None = None) -> None:
+        """One step on plain (N, 3) tensors with an explicit parameter block
+        and external force (None = none). v_out keeps its contents for
+        inactive particles, as in :meth:`step`."""
+        model = self.model
+        n = model.particle_count
+        if self.batched:
+            raise ValueError("step_raw needs a single-world solver")
+        for t, name in ((x_in, "x_in"), (v_in, "v_in"), (x_out, "x_out"), (v_out, "v_out")):
+            self._check_vec(t, name)
+        if f_ext is not None:
+            self._check_vec(f_ext, "f_ext")
+        st = self._lib.nsph_sph_step(
+            self._handle, ctypes.byref(params), n, x_in.data_ptr(), v_in.data_ptr(), _lib.ptr(f_ext),
+            model.particle_mass.data_ptr(), model.particle_inv_mass.data_ptr(), model.particle_flags.data_ptr(),
+            model.particle_world.data_ptr(), model.gravity.data_ptr(), int(model.gravity.shape[0]),
+            x_out.data_ptr(), v_out.data_ptr(), None, None, None, _lib.stream_handle(model.device))
+        _lib.check(st, "SolverSPH.step_raw")
+
+    def step_backward_raw(self, x_in: torch.Tensor, v_in: torch.Tensor, params: _lib.NsphSphParams,
+                          x_out_grad: torch.Tensor, v_out_grad: torch.Tensor, x_in_grad: torch.Tensor,
+                          v_in_grad: torch.Tensor, f_ext: torch.Tensor | None = None,
+                          rho_out_grad: torch.Tensor | None = None, f_ext_grad: torch.Tensor | None = None,
+                          eos_b_grad: torch.Tensor | None = None) -> None:
+        """nsph_sph_step_adjoint on plain tensors: writes x_in_grad, v_in_grad
+        (which may be x_out_grad, v_out_grad themselves) and adds to
+        f_ext_grad (N, 3) and eos_b_grad (one float32) when given."""
+        model = self.model
+        n = model.particle_count
+        self.enable_adjoint()
+        for t, name in ((x_in, "x_in"), (v_in, "v_in"), (x_out_grad, "x_out_grad"), (v_out_grad, "v_out_grad"),
+                        (x_in_grad, "x_in_grad"), (v_in_grad, "v_in_grad")):
+            self._check_vec(t, name)
+        for t, name in ((f_ext, "f_ext"), (f_ext_grad, "f_ext_grad")):
+            if t is not None:
+                self._check_vec(t, name)
+        if rho_out_grad is not None and (rho_out_grad.dtype != torch.float32 or tuple(rho_out_grad.shape) != (n,)
+                                         or not rho_out_grad.is_cuda or not rho_out_grad.is_contiguous()):
+            raise ValueError(f"rho_out_grad must be a contiguous ({n},) float32 CUDA tensor")
+        if eos_b_grad is not None and (eos_b_grad.dtype != torch.float32 or eos_b_grad.numel() != 1
+                                       or not eos_b_grad.is_cuda):
+            raise ValueError("eos_b_grad must be a one-element float32 CUDA tensor")
+        st = self._lib.nsph_sph_step_adjoint(
+            self._handle, ctypes.byref(params), n, x_in.data_ptr(), v_in.data_ptr(), _lib.ptr(f_ext),
+            model.particle_mass.data_ptr(), model.particle_inv_mass.data_ptr(), model.particle_flags.data_ptr(),
+            model.particle_world.data_ptr(), model.gravity.data_ptr(), int(model.gravity.shape[0]),
+            x_out_grad.data_ptr(), v_out_grad.data_ptr(), _lib.ptr(rho_out_grad), x_in_grad.data_ptr(),
+            v_in_grad.data_ptr(), _lib.ptr(f_ext_grad), _lib.ptr(eos_b_grad), _lib.stream_handle(model.device))
+        _lib.check(st, "SolverSPH.step_backward")
+
+    def step_backward(self, state_in: State, dt: float, x_out_grad: torch.Tensor, v_out_grad: torch.Tensor,
+                      rho_out_grad: torch.Tensor | None = None) -> dict[str, torch.Tensor]:
+        """Reverse of ``step(state_in, state_out, None, None, dt)``: the
+        gradients of a scalar with respect to the step's inputs, given its
+        gradients with respect to state_out's positions, velocities (and
+        optionally densities). Replaces ``wp.Tape.backward`` over one step
+        (newton/solvers.py:359-395).
+
+        Returns:
+            {"particle_q": (N,3), "particle_qd": (N,3), "particle_f": (N,3)
+             (only with ``config.apply_particle_f`` and state_in.particle_f),
+             "eos_b": (1,)}
+        """
+        n = self.model.particle_count
+        dev = self.model.device
+        f_ext = state_in.particle_f if (self.config.apply_particle_f and state_in.particle_f is not None) else None
+        xg = torch.empty((n, 3), dtype=torch.float32, device=dev)
+        vg = torch.empty_like(xg)
+        fg = torch.zeros_like(xg) if f_ext is not None else None
+        bg = torch.zeros(1, dtype=torch.float32, device=dev)
+        self.step_backward_raw(state_in.particle_q, state_in.particle_qd, self.step_params(dt),
+                               x_out_grad.contiguous(), v_out_grad.contiguous(), xg, vg, f_ext=f_ext,
+                               rho_out_grad=rho_out_grad, f_ext_grad=fg, eos_b_grad=bg)
+        out = {"particle_q": xg, "particle_qd": vg, "eos_b": bg}
+        if fg is not None:
+            out["particle_f"] = fg
+        return out
 
     def notify_model_changed(self, flags: int) -> None:
         """MODEL_PROPERTIES re-reads particle_max_velocity; gravity needs no

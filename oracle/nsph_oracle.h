@@ -94,6 +94,19 @@ void oracle_integrate_particles_f64(const float* x, const float* v, const float*
                                     const int* flags, const int* world, const float* gravity, int world_count,
                                     int n, double dt, double v_max, double* x_new, double* v_new);
 
+/* ---- adjoint (sph_adjoint.c): fp64 state, fp64 neighbour sets ----------
+ * oracle_adj_step_f64: one step on a double state (inactive particles keep x
+ * and v). oracle_adj_vjp_f64: given the adjoints of x_out and v_out (and
+ * optionally of the step's density), the adjoints of x, v, f_ext (optional)
+ * and of the EOS stiffness B (optional, one double, overwritten). */
+int oracle_adj_step_f64(const oracle_phys_f64* ph, int n, const double* x, const double* v, const double* f_ext,
+                        const double* mass, const double* inv_mass, const int* flags, const int* world,
+                        const double* gravity, int world_count, double* x_out, double* v_out, double* rho_out);
+int oracle_adj_vjp_f64(const oracle_phys_f64* ph, int n, const double* x, const double* v, const double* f_ext,
+                       const double* mass, const double* inv_mass, const int* flags, const int* world,
+                       const double* gravity, int world_count, const double* x_out_adj, const double* v_out_adj,
+                       const double* rho_out_adj, double* x_adj, double* v_adj, double* f_adj, double* b_adj);
+
 /* Number of OpenMP threads the oracle uses (0 = OpenMP default). */
 void oracle_set_threads(int n);
 int  oracle_get_threads(void);

@@ -136,6 +136,12 @@ def lib() -> ctypes.CDLL:
     L.oracle_integrate_particles_f64.restype = None
     L.oracle_integrate_particles_f64.argtypes = [_f32p, _f32p, _f32p, _f32p, _i32p, _i32p, _f32p, ctypes.c_int,
                                                  ctypes.c_int, ctypes.c_double, ctypes.c_double, _f64p, _f64p]
+    L.oracle_adj_step_f64.restype = ctypes.c_int
+    L.oracle_adj_step_f64.argtypes = [ctypes.POINTER(Phys64), ctypes.c_int] + [ctypes.c_void_p] * 8 + \
+        [ctypes.c_int] + [ctypes.c_void_p] * 3
+    L.oracle_adj_vjp_f64.restype = ctypes.c_int
+    L.oracle_adj_vjp_f64.argtypes = [ctypes.POINTER(Phys64), ctypes.c_int] + [ctypes.c_void_p] * 8 + \
+        [ctypes.c_int] + [ctypes.c_void_p] * 7
     L.oracle_set_threads.restype = None
     L.oracle_set_threads.argtypes = [ctypes.c_int]
     L.oracle_get_threads.restype = ctypes.c_int
@@ -300,6 +306,101 @@ def integrate_particles(x, v, f, inv_mass, flags, world, gravity, dt, v_max, x_n
         lib().oracle_integrate_particles_f64(*args, x_new.reshape(-1), v_new.reshape(-1))
     else:
         lib().oracle_integrate_particles_f32(*args, x_new.reshape(-1), v_new.reshape(-1))
+
+
+# ---------------------------------------------------------------------------
+# adjoint (sph_adjoint.c): fp64 state, fp64 neighbour sets
+# ---------------------------------------------------------------------------
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class AdjScene:
+    """The fixed inputs of an fp64 rollout: constants and model arrays."""
+
+    def __init__(self, c64: dict, mass, inv_mass, flags, gravity, world=None, f_ext=None):
+        self.c64 = dict(c64)
+        self.mass = _f64(mass)
+        self.inv_mass = _f64(inv_mass)
+        self.flags = _i32(flags)
+        self.n = self.mass.shape[0]
+        self.world = _i32(world) if world is not None else np.zeros(self.n, np.int32)
+        self.gravity = _f64(gravity).reshape(-1, 3)
+        self.f_ext = _f64(f_ext) if f_ext is not None else None
+
+    def phys(self, eos_b: float | None = None) -> Phys64:
+        c = dict(self.c64)
+        if eos_b is not None:
+            c["eos_b"] = float(eos_b)
+        return phys64(c)
+
+    def _model_args(self):
+        return [_p(self.f_ext), _p(self.mass), _p(self.inv_mass), _p(self.flags), _p(self.world), _p(self.gravity),
+                self.gravity.shape[0]]
+
+
+def adj_step64(scene: AdjScene, x, v, eos_b: float | None = None):
+    """One fp64 step; returns (x1, v1, rho)."""
+    x, v = _f64(x), _f64(v)
+    n = scene.n
+    xo, vo, rho = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n)
+    ph = scene.phys(eos_b)
+    st = lib().oracle_adj_step_f64(ctypes.byref(ph), n, _p(x), _p(v), *scene._model_args(), _p(xo), _p(vo), _p(rho))
+    if st != 0:
+        raise RuntimeError(f"oracle_adj_step_f64 status {st}")
+    return xo, vo, rho
+
+
+def adj_vjp64(scene: AdjScene, x, v, x1_adj, v1_adj, rho_adj=None, eos_b: float | None = None):
+    """Reverse of one fp64 step: (x_adj, v_adj, f_adj, b_adj)."""
+    x, v = _f64(x), _f64(v)
+    x1_adj, v1_adj = _f64(x1_adj), _f64(v1_adj)
+    rho_adj = _f64(rho_adj) if rho_adj is not None else None
+    n = scene.n
+    xa, va, fa = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros((n, 3))
+    ba = ctypes.c_double(0.0)
+    ph = scene.phys(eos_b)
+    st = lib().oracle_adj_vjp_f64(ctypes.byref(ph), n, _p(x), _p(v), *scene._model_args(), _p(x1_adj), _p(v1_adj),
+                                  _p(rho_adj), _p(xa), _p(va), _p(fa), ctypes.byref(ba))
+    if st != 0:
+        raise RuntimeError(f"oracle_adj_vjp_f64 status {st}")
+    return xa, va, fa, float(ba.value)
+
+
+def rollout64(scene: AdjScene, x0, v0, steps: int, eos_b: float | None = None, keep: bool = False):
+    """`steps` fp64 steps from (x0, v0). Returns (x_T, v_T) or, with keep,
+    the lists of all states [x_0..x_T], [v_0..v_T]."""
+    xs, vs = [_f64(x0)], [_f64(v0)]
+    x, v = xs[0], vs[0]
+    for _ in range(steps):
+        x, v, _ = adj_step64(scene, x, v, eos_b)
+        if keep:
+            xs.append(x)
+            vs.append(v)
+    return (xs, vs) if keep else (x, v)
+
+
+def mse_loss(x, target) -> float:
+    """mean over particles of |x_i - y_i|^2"""
+    d = _f64(x) - _f64(target)
+    return float(np.sum(d * d) / d.shape[0])
+
+
+def rollout_grad64(scene: AdjScene, x0, v0, steps: int, target, eos_b: float | None = None):
+    """Loss mse_loss(x_T, target) and its gradient with respect to x0, v0
+    and the EOS stiffness B, by reverse steps over the stored trajectory.
+
+    Returns (loss, x0_adj, v0_adj, b_adj)."""
+    xs, vs = rollout64(scene, x0, v0, steps, eos_b, keep=True)
+    n = scene.n
+    loss = mse_loss(xs[-1], target)
+    xa = 2.0 * (xs[-1] - _f64(target)) / n
+    va = np.zeros((n, 3))
+    b_total = 0.0
+    for t in range(steps - 1, -1, -1):
+        xa, va, _, ba = adj_vjp64(scene, xs[t], vs[t], xa, va, None, eos_b)
+        b_total += ba
+    return loss, xa, va, b_total
 
 
 # ---------------------------------------------------------------------------
