@@ -52,6 +52,12 @@ WORKLOADS = {
                     desc="2,097,152 particles, 128^3 block at 0.005 m in a 2x1x1 m tank"),
     "dam_break_32k": dict(shape=(32, 32, 32), spacing=0.01, box=(1.0, 1.0, 1.0), dt=1e-4, vel_std=0.0,
                           desc="32,768 particles, 32^3 block at 0.01 m in a 1 m box"),
+    "rollout_grad_64k": dict(shape=(64, 64, 16), spacing=0.01, box=(1.0, 1.0, 1.0), dt=1e-4, vel_std=0.1, vel_seed=4,
+                             grad=dict(steps=50, checkpoint=10, target_seed=5),
+                             desc="differentiable rollout: 65,536 particles (64x64x16 block at 0.01 m in a 1 m box), "
+                                  "v0 ~ N(0, 0.1 m/s), 50 steps at dt = 1e-4 s, loss = mean |x_T - y|^2 against a "
+                                  "seeded target cloud, gradients w.r.t. x0, v0 and the EOS stiffness B, checkpoint "
+                                  "every 10 steps"),
     "worlds_4096": dict(worlds=4096, n_range=(256, 16384), s_range=(0.004, 0.01), box=(0.5, 0.5, 0.5), dt=1e-4,
                         vel_std=0.0, seed=3,
                         desc="4,096 independent scenes: particles log-uniform in [256, 16384], spacing uniform in "
@@ -111,7 +117,7 @@ def make_scene(name: str, device: str):
                         mass=1000.0 * s**3, jitter=0.2 * s)
     model = b.finalize(device)
     if w["vel_std"] > 0:
-        rng = np.random.default_rng(seed=2)
+        rng = np.random.default_rng(seed=w.get("vel_seed", 2))
         v = rng.normal(0.0, w["vel_std"], (model.particle_count, 3)).astype(np.float32)
         model.particle_qd.copy_(torch.from_numpy(v))
     cfg = SolverSPH.Config(smoothing_length=2 * s, rest_density=1000.0, sound_speed=20.0, eos_gamma=7, xsph=0.01,
@@ -524,6 +530,255 @@ def run_gpu(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# differentiable rollout (adjoint): forward + checkpointed backward
+# ---------------------------------------------------------------------------
+# algorithmic bytes per particle of the pair gather of the adjoint (read x, v,
+# the density-pass scratch, adj(a), adj(dv); read-modify-write adj(x), adj(v);
+# write adj(rho))
+B_ALG_ADJ_PAIR = 16 + 16 + 8 + 8 + 16 + 16 + 24 + 24 + 4
+
+
+def grad_target(x: np.ndarray, w: dict) -> np.ndarray:
+    """The seeded target cloud of the differentiable-rollout workload: the
+    initial block shifted by (s, 0, -s/2) plus N(0, (0.2 s)^2) noise."""
+    s = w["spacing"]
+    rng = np.random.default_rng(w["grad"]["target_seed"])
+    return (x + np.array([s, 0.0, -0.5 * s]) + rng.normal(0.0, 0.2 * s, x.shape)).astype(np.float32)
+
+
+def cpu_grad_rate(model_cpu, cfg, w, budget_s: float):
+    """Differentiable particle-steps/s of the fp64 adjoint oracle (forward
+    passes on all OpenMP threads, reverse pass on one thread) over a bounded
+    number of steps of the same scene."""
+    from oracle import oracle as O
+
+    O.build()
+    x = model_cpu.particle_q.numpy().astype(np.float64)
+    v = model_cpu.particle_qd.numpy().astype(np.float64)
+    y = grad_target(model_cpu.particle_q.numpy(), w)
+    sc = O.AdjScene(cfg.constants(w["dt"], model_cpu.particle_max_velocity)["f64"], model_cpu.particle_mass.numpy(),
+                    model_cpu.particle_inv_mass.numpy(), model_cpu.particle_flags.numpy(),
+                    model_cpu.gravity.numpy())
+    t0 = time.perf_counter()
+    O.rollout_grad64(sc, x, v, 1, y)
+    per_step = time.perf_counter() - t0
+    steps = int(max(1, min(w["grad"]["steps"], budget_s / max(per_step, 1e-6))))
+    t0 = time.perf_counter()
+    O.rollout_grad64(sc, x, v, steps, y)
+    el = time.perf_counter() - t0
+    n = x.shape[0]
+    return n * steps / el, steps, el, O.get_threads()
+
+
+def run_grad(args):
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = dist_env()
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", device_id=device, timeout=timedelta(seconds=120))
+    from newton_sph_dev_b200.solvers import SolverSPH, sph_rollout
+
+    model, cfg, w = make_scene(args.workload, str(device))
+    n = model.particle_count
+    g = w["grad"]
+    steps, every, dt = g["steps"], g["checkpoint"], w["dt"]
+    solver = SolverSPH(model, cfg)
+    s0, s1 = model.state(), model.state()
+    tuned = solver.autotune(s0, s1, dt) if not args.no_autotune else None
+    solver.enable_adjoint()
+    solver.enable_phase_timing(True)
+    x0d = model.particle_q.clone()
+    v0d = model.particle_qd.clone()
+    y = torch.from_numpy(grad_target(model.particle_q.cpu().numpy(), w)).to(device)
+    b0 = torch.tensor([float(solver.step_params(dt).eos_b)], dtype=torch.float32, device=device)
+    stream = torch.cuda.current_stream(device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+
+    def rollout(x0, v0, b, timed):
+        if timed:
+            ev[0].record(stream)
+        xT, _ = sph_rollout(solver, x0, v0, steps, dt, eos_b=b, checkpoint_every=every)
+        loss = ((xT - y) ** 2).sum(dim=1).mean()
+        if timed:
+            ev[1].record(stream)
+        loss.backward()
+        if timed:
+            ev[2].record(stream)
+        return loss
+
+    def leaves():
+        return (x0d.detach().clone().requires_grad_(True), v0d.detach().clone().requires_grad_(True),
+                b0.detach().clone().requires_grad_(True))
+
+    for _ in range(args.warmup):
+        rollout(*leaves(), timed=False)
+    torch.cuda.synchronize()
+    fwd_ms = bwd_ms = 0.0
+    dens_ms = pair_ms = 0.0
+    launches0 = solver.launches_total
+    barrier(device)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            x0, v0, b = leaves()
+            flush.zero_()
+            loss = rollout(x0, v0, b, timed=True)
+            ev[2].synchronize()
+            fwd_ms += ev[0].elapsed_time(ev[1])
+            bwd_ms += ev[1].elapsed_time(ev[2])
+            ph = solver.adjoint_phase_times()  # the last adjoint step of this rollout
+            dens_ms += ph[1]
+            pair_ms += ph[3]
+    torch.cuda.synchronize()
+    barrier(device)
+    launches = solver.launches_total - launches0
+    total_ms = max_over_ranks(fwd_ms + bwd_ms, device)
+    value = world * n * steps * args.steps / (total_ms * 1e-3)
+    grads_finite = bool(torch.isfinite(x0.grad).all() and torch.isfinite(v0.grad).all() and torch.isfinite(b.grad).all())
+
+    # ---- end to end through the public API, host buffers in and out ----
+    e2e_iters = min(args.steps, 20)
+    hx, hv = x0d.cpu().pin_memory(), v0d.cpu().pin_memory()
+    hgx, hgv = torch.empty_like(hx).pin_memory(), torch.empty_like(hv).pin_memory()
+    hb = torch.empty(2, dtype=torch.float32).pin_memory()
+    e2e_ms = 0.0
+    barrier(device)
+    torch.cuda.synchronize()
+    for _ in range(e2e_iters):
+        ev[0].record(stream)
+        x0 = hx.to(device, non_blocking=True).requires_grad_(True)
+        v0 = hv.to(device, non_blocking=True).requires_grad_(True)
+        b = b0.detach().clone().requires_grad_(True)
+        loss = rollout(x0, v0, b, timed=False)
+        hgx.copy_(x0.grad, non_blocking=True)
+        hgv.copy_(v0.grad, non_blocking=True)
+        hb[0:1].copy_(loss.detach().reshape(1), non_blocking=True)
+        hb[1:2].copy_(b.grad, non_blocking=True)
+        ev[2].record(stream)
+        ev[2].synchronize()
+        e2e_ms += ev[0].elapsed_time(ev[2])
+    barrier(device)
+    e2e_ms = max_over_ranks(e2e_ms, device)
+    e2e_value = world * n * steps * e2e_iters / (e2e_ms * 1e-3)
+
+    # ---- roofline: the density pass has the largest share of the rollout's
+    # kernel time (it runs in the forward, recompute and adjoint steps); the
+    # pair gather is the adjoint's largest single kernel ----
+    peak, peak_kind = load_peak()
+    t_dens = dens_ms / args.steps * 1e-3
+    t_pair = pair_ms / args.steps * 1e-3
+    achieved = B_ALG_DENSITY * n / t_dens / 1e9
+    roofline = {"bound": "hbm", "kernel": "k_density", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+                "alg_bytes_per_launch": B_ALG_DENSITY * n}
+    pair_ach = B_ALG_ADJ_PAIR * n / t_pair / 1e9
+    roofline_adj = {"bound": "hbm", "kernel": "k_adj_pair", "achieved": pair_ach, "peak": peak, "unit": "GB/s",
+                    "frac": pair_ach / peak, "alg_bytes_per_launch": B_ALG_ADJ_PAIR * n,
+                    "ms_per_launch": t_pair * 1e3}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        model_cpu, cfg_cpu, w_cpu = make_scene(args.workload, "cpu")
+        rate, csteps, el, threads = cpu_grad_rate(model_cpu, cfg_cpu, w_cpu, budget_s=15.0)
+        cpu = {"value": rate, "unit": "differentiable particle-steps/s", "cores": threads, "kind": "port",
+               "sample": f"forward + reverse of {csteps} steps of the full {n}-particle scene in {el:.1f} s "
+                         f"(fp64 adjoint oracle: forward passes on {threads} OpenMP threads, reverse pass on one)"}
+
+    if rank == 0:
+        clocks = clk.summary()
+        line = {
+            "metric": "differentiable particle-steps/s",
+            "value": value,
+            "unit": "differentiable particle-steps/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": {
+                "workload": args.workload,
+                "particles": n,
+                "desc": w["desc"],
+                "step": "one bench step = one forward rollout + loss + checkpointed backward "
+                        f"({steps} simulation steps); value counts particle x simulation steps",
+                "grid_dims": list(solver.grid_dims),
+                "launch": {"threads": solver.launch[0], "blocks_per_sm": solver.launch[1],
+                           "autotuned": tuned is not None} if hasattr(solver, "launch") else "default",
+                "l2": "flushed (256 MiB write) before every timed rollout, outside the timed interval",
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            },
+            "phase_ms_per_step": {"forward": fwd_ms / args.steps, "backward": bwd_ms / args.steps},
+            "roofline": roofline,
+            "roofline_adjoint_pair": roofline_adj,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "differentiable particle-steps/s",
+                    "h2d_bytes_per_step": 2 * n * 12, "d2h_bytes_per_step": 2 * n * 12 + 8, "steps": e2e_iters},
+            "gpu_launches": launches,
+            "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+            "grads_finite": grads_finite,
+            "loss": float(loss.item()),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def run_grad_reference(args):
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    model, cfg, w = make_scene(args.workload, "cpu")
+    n = model.particle_count
+    from oracle import oracle as O
+
+    O.build()
+    x = model.particle_q.numpy().astype(np.float64)
+    v = model.particle_qd.numpy().astype(np.float64)
+    y = grad_target(model.particle_q.numpy(), w)
+    sc = O.AdjScene(cfg.constants(w["dt"], model.particle_max_velocity)["f64"], model.particle_mass.numpy(),
+                    model.particle_inv_mass.numpy(), model.particle_flags.numpy(), model.gravity.numpy())
+    t0 = time.perf_counter()
+    O.rollout_grad64(sc, x, v, 1, y)
+    per_step = time.perf_counter() - t0
+    # each bench step: forward + reverse of a bounded number of simulation steps
+    budget = 150.0 / (args.steps + args.warmup)
+    sim_steps = int(max(1, min(w["grad"]["steps"], budget / max(per_step, 1e-6))))
+    for _ in range(args.warmup):
+        O.rollout_grad64(sc, x, v, sim_steps, y)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        O.rollout_grad64(sc, x, v, sim_steps, y)
+    el = time.perf_counter() - t0
+    value = n * sim_steps * args.steps / el
+    unit = "differentiable particle-steps/s"
+    threads = O.get_threads()
+    line = {
+        "impl": "reference", "metric": unit, "value": value, "unit": unit, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "particles": n, "desc": w["desc"]},
+        "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port",
+                         "sample": f"each step: forward + reverse of {sim_steps} simulation steps of the full scene "
+                                   f"(fp64 adjoint oracle; forward passes on {threads} OpenMP threads, reverse on "
+                                   f"one)"},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -537,9 +792,10 @@ def main(argv=None):
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    grad = "grad" in WORKLOADS[args.workload]
     if args.impl == "reference":
-        return run_reference(args)
-    return run_gpu(args)
+        return run_grad_reference(args) if grad else run_reference(args)
+    return run_grad(args) if grad else run_gpu(args)
 
 
 if __name__ == "__main__":

@@ -269,6 +269,29 @@ NSPH_API int nsph_sph_step_adjoint(nsph_sph* solver, const nsph_sph_params* para
                                    float* x_in_adj, float* v_in_adj, float* f_ext_adj, float* eos_b_adj,
                                    void* stream);
 
+/* Multi-step forms used by checkpointed rollouts (one call per segment, the
+ * step loop runs in the library).
+ * nsph_sph_rollout: `steps` steps from (x0, v0) with constant f_ext; the
+ *   state after step t goes to x_traj / v_traj + 3 n t (steps x n x 3 each;
+ *   must not overlap each other or x0 / v0, but x0 may directly precede
+ *   x_traj). Inactive particles keep their velocity.
+ * nsph_sph_rollout_adjoint: reverse of `steps` steps whose input states are
+ *   x_states / v_states + 3 n t, t = 0..steps-1 (the layout of x0 followed
+ *   by the first steps-1 states of nsph_sph_rollout). x_adj / v_adj hold the
+ *   adjoint of the last step's output on entry and of the first step's input
+ *   on return; f_ext_adj and eos_b_adj accumulate as in
+ *   nsph_sph_step_adjoint. */
+NSPH_API int nsph_sph_rollout(nsph_sph* solver, const nsph_sph_params* params, int n, int steps,
+                              const float* x0, const float* v0, const float* f_ext,
+                              const float* mass, const float* inv_mass, const int* flags, const int* world,
+                              const float* gravity, int world_count,
+                              float* x_traj, float* v_traj, void* stream);
+NSPH_API int nsph_sph_rollout_adjoint(nsph_sph* solver, const nsph_sph_params* params, int n, int steps,
+                                      const float* x_states, const float* v_states, const float* f_ext,
+                                      const float* mass, const float* inv_mass, const int* flags, const int* world,
+                                      const float* gravity, int world_count,
+                                      float* x_adj, float* v_adj, float* f_ext_adj, float* eos_b_adj, void* stream);
+
 /* Neighbour lists of the last step's build, in original particle order: for
  * each particle i the ids j (self included) of active particles visited by
  * hash_grid_query(x_i, h) with fp32 r2 = fma(dz,dz,fma(dy,dy,dx*dx)) < h2,
@@ -288,6 +311,12 @@ NSPH_API int nsph_sph_get_grid_view(const nsph_sph* solver, nsph_grid_view* view
  * build / density / force durations in ms. Enable/disable outside capture. */
 NSPH_API int nsph_sph_enable_phase_timing(nsph_sph* solver, int enable);
 NSPH_API int nsph_sph_phase_times(nsph_sph* solver, float ms_out[3]);
+/* With phase timing enabled, every adjoint step also records six events:
+ * start, after the grid build, after the density pass, after the force
+ * recompute + integrate reverse, after the pair gather, end (density gather
+ * and adj(B) reduction). Returns the five durations of the last executed
+ * adjoint step in ms. */
+NSPH_API int nsph_sph_adjoint_phase_times(nsph_sph* solver, float ms_out[5]);
 
 /* Launch shape of the two neighbour passes (density, force): `threads` per
  * block (0 = default 256; else a multiple of 32 up to 256) and

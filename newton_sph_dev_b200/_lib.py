@@ -124,10 +124,29 @@ SIGNATURES = [
         + [c_void_p] * 7
         + [c_void_p],
     ),
+    (
+        "nsph_sph_rollout",
+        ctypes.c_int,
+        [c_void_p, ctypes.POINTER(NsphSphParams), ctypes.c_int, ctypes.c_int]
+        + [c_void_p] * 8
+        + [ctypes.c_int]
+        + [c_void_p] * 2
+        + [c_void_p],
+    ),
+    (
+        "nsph_sph_rollout_adjoint",
+        ctypes.c_int,
+        [c_void_p, ctypes.POINTER(NsphSphParams), ctypes.c_int, ctypes.c_int]
+        + [c_void_p] * 8
+        + [ctypes.c_int]
+        + [c_void_p] * 4
+        + [c_void_p],
+    ),
     ("nsph_sph_neighbors", ctypes.c_int, [c_void_p, ctypes.POINTER(NsphSphParams), c_void_p, c_void_p, c_void_p, c_void_p]),
     ("nsph_sph_get_grid_view", ctypes.c_int, [c_void_p, ctypes.POINTER(NsphGridView)]),
     ("nsph_sph_enable_phase_timing", ctypes.c_int, [c_void_p, ctypes.c_int]),
     ("nsph_sph_phase_times", ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_float * 3)]),
+    ("nsph_sph_adjoint_phase_times", ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_float * 5)]),
     ("nsph_sph_set_launch", ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int]),
     ("nsph_sph_last_launches", ctypes.c_int, [c_void_p]),
     ("nsph_sph_status", ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_uint), c_void_p]),

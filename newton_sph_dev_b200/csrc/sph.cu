@@ -818,6 +818,7 @@ struct nsph_sph {
     float* adj_rho = nullptr;            //   adj(rho)
     float* adj_bpart = nullptr;          //   per-block partial sums of adj(B)
     int adj_bcap = 0;                    //   entries of adj_bpart
+    cudaEvent_t eva[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // adjoint phases (timing)
 };
 
 // grid of a neighbour pass: one thread per particle, or a persistent grid of
@@ -852,6 +853,11 @@ static void sph_free(nsph_sph* s)
 {
     DeviceGuard guard(s->grid.device);
     for (cudaEvent_t& e : s->ev)
+        if (e) {
+            cudaEventDestroy(e);
+            e = nullptr;
+        }
+    for (cudaEvent_t& e : s->eva)
         if (e) {
             cudaEventDestroy(e);
             e = nullptr;
@@ -979,31 +985,31 @@ static int check_params(const nsph_sph_params* p)
     return NSPH_OK;
 }
 
-extern "C" int nsph_sph_step(nsph_sph* s, const nsph_sph_params* p, int n, const float* x_in, const float* v_in,
-                             const float* f_ext, const float* mass, const float* inv_mass, const int* flags,
-                             const int* world, const float* gravity, int world_count, float* x_out,
-                             float* v_out, float* rho_out, float* p_out, float* a_out, void* stream)
+// Checks shared by the single-world step entry points (the caller has
+// checked the solver handle and the parameter block).
+static int check_step_inputs(const nsph_sph* s, int n, const float* x_in, const float* v_in, const float* mass,
+                             const float* inv_mass, const int* flags, const float* gravity, int world_count)
 {
-    clear_error();
-    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
-    int st = check_params(p);
-    if (st != NSPH_OK) return st;
     if (n < 0) return fail(NSPH_ERR_INVALID_ARG, "negative particle count");
     if (n > s->capacity) return fail(NSPH_ERR_CAPACITY, "more particles than the solver was created for");
     if (world_count < 1 || !gravity) return fail(NSPH_ERR_INVALID_ARG, "gravity needs world_count >= 1");
-    if (n > 0 && (!x_in || !v_in || !mass || !inv_mass || !flags || !x_out || !v_out))
+    if (n > 0 && (!x_in || !v_in || !mass || !inv_mass || !flags))
         return fail(NSPH_ERR_INVALID_ARG, "null state or model array");
-    if (n > 0 && (x_out == x_in || v_out == v_in))
-        return fail(NSPH_ERR_INVALID_ARG, "state_out must not alias state_in");
     if (s->grid.world_count > 0)
         return fail(NSPH_ERR_INVALID_ARG, "solver was created for batched worlds: use nsph_sph_step_worlds");
-    DeviceGuard guard(s->grid.device);
-    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
-    cudaStream_t cs = (cudaStream_t)stream;
+    return NSPH_OK;
+}
+
+// Enqueue one step on validated inputs: grid build + sorted gather, density,
+// force + integrate (with the phase events when enabled).
+static int step_enqueue(nsph_sph* s, const nsph_sph_params* p, int n, const float* x_in, const float* v_in,
+                        const float* f_ext, const float* mass, const float* inv_mass, const int* flags,
+                        const int* world, const float* gravity, int world_count, float* x_out, float* v_out,
+                        float* rho_out, float* p_out, float* a_out, cudaStream_t cs, int& launches)
+{
     GatherArgs ga{x_in, v_in, mass, inv_mass, flags, world, world_count, s->xs, s->vs};
-    int launches = 0;
     if (s->ev[0]) NSPH_CUDA_TRY(record_mark(s->ev[0], cs));
-    st = grid_build(s->grid, x_in, n, p->cell_width, p->cell_inv, &ga, s->status, cs, &launches);
+    int st = grid_build(s->grid, x_in, n, p->cell_width, p->cell_inv, &ga, s->status, cs, &launches);
     if (st != NSPH_OK) return st;
     s->last_n = n;
     if (s->ev[1]) NSPH_CUDA_TRY(record_mark(s->ev[1], cs));
@@ -1024,6 +1030,71 @@ extern "C" int nsph_sph_step(nsph_sph* s, const nsph_sph_params* p, int n, const
         NSPH_CUDA_TRY(record_mark(s->ev[2], cs));
     }
     if (s->ev[3]) NSPH_CUDA_TRY(record_mark(s->ev[3], cs));
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_step(nsph_sph* s, const nsph_sph_params* p, int n, const float* x_in, const float* v_in,
+                             const float* f_ext, const float* mass, const float* inv_mass, const int* flags,
+                             const int* world, const float* gravity, int world_count, float* x_out,
+                             float* v_out, float* rho_out, float* p_out, float* a_out, void* stream)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    int st = check_params(p);
+    if (st == NSPH_OK) st = check_step_inputs(s, n, x_in, v_in, mass, inv_mass, flags, gravity, world_count);
+    if (st != NSPH_OK) return st;
+    if (n > 0 && (!x_out || !v_out)) return fail(NSPH_ERR_INVALID_ARG, "null state or model array");
+    if (n > 0 && (x_out == x_in || v_out == v_in))
+        return fail(NSPH_ERR_INVALID_ARG, "state_out must not alias state_in");
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    int launches = 0;
+    st = step_enqueue(s, p, n, x_in, v_in, f_ext, mass, inv_mass, flags, world, gravity, world_count, x_out, v_out,
+                      rho_out, p_out, a_out, (cudaStream_t)stream, launches);
+    s->last_launches = launches;
+    return st;
+}
+
+// [a, a + na) and [b, b + nb) (in floats) share memory
+static bool overlaps(const float* a, size_t na, const float* b, size_t nb)
+{
+    return a < b + nb && b < a + na;
+}
+
+extern "C" int nsph_sph_rollout(nsph_sph* s, const nsph_sph_params* p, int n, int steps, const float* x0,
+                                const float* v0, const float* f_ext, const float* mass, const float* inv_mass,
+                                const int* flags, const int* world, const float* gravity, int world_count,
+                                float* x_traj, float* v_traj, void* stream)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    int st = check_params(p);
+    if (st == NSPH_OK) st = check_step_inputs(s, n, x0, v0, mass, inv_mass, flags, gravity, world_count);
+    if (st != NSPH_OK) return st;
+    if (steps < 0) return fail(NSPH_ERR_INVALID_ARG, "negative step count");
+    const size_t len = 3 * (size_t)n;
+    if (n > 0 && steps > 0) {
+        if (!x_traj || !v_traj) return fail(NSPH_ERR_INVALID_ARG, "null trajectory array");
+        const size_t tot = len * (size_t)steps;
+        if (overlaps(x_traj, tot, v_traj, tot) || overlaps(x0, len, x_traj, tot) || overlaps(v0, len, v_traj, tot) ||
+            overlaps(x0, len, v_traj, tot) || overlaps(v0, len, x_traj, tot))
+            return fail(NSPH_ERR_INVALID_ARG, "trajectory arrays overlap each other or the initial state");
+    }
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    cudaStream_t cs = (cudaStream_t)stream;
+    int launches = 0;
+    for (int t = 0; t < steps && n > 0; ++t) {
+        const float* xi = t == 0 ? x0 : x_traj + (size_t)(t - 1) * len;
+        const float* vi = t == 0 ? v0 : v_traj + (size_t)(t - 1) * len;
+        float* xo = x_traj + (size_t)t * len;
+        float* vo = v_traj + (size_t)t * len;
+        // inactive particles keep their velocity (the step leaves it untouched)
+        NSPH_CUDA_TRY(cudaMemcpyAsync(vo, vi, sizeof(float) * len, cudaMemcpyDeviceToDevice, cs));
+        st = step_enqueue(s, p, n, xi, vi, f_ext, mass, inv_mass, flags, world, gravity, world_count, xo, vo, nullptr,
+                          nullptr, nullptr, cs, launches);
+        if (st != NSPH_OK) return st;
+    }
     s->last_launches = launches;
     return NSPH_OK;
 }
@@ -1159,11 +1230,15 @@ extern "C" int nsph_sph_enable_phase_timing(nsph_sph* s, int enable)
     if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
     DeviceGuard guard(s->grid.device);
     if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
-    for (cudaEvent_t& e : s->ev) {
-        if (enable && !e) NSPH_CUDA_TRY(cudaEventCreate(&e));
-        if (!enable && e) {
-            NSPH_CUDA_TRY(cudaEventDestroy(e));
-            e = nullptr;
+    for (cudaEvent_t* set : {s->ev, s->eva}) {
+        const int count = set == s->ev ? 4 : 6;
+        for (int k = 0; k < count; ++k) {
+            cudaEvent_t& e = set[k];
+            if (enable && !e) NSPH_CUDA_TRY(cudaEventCreate(&e));
+            if (!enable && e) {
+                NSPH_CUDA_TRY(cudaEventDestroy(e));
+                e = nullptr;
+            }
         }
     }
     return NSPH_OK;
@@ -1251,6 +1326,59 @@ extern "C" int nsph_sph_enable_adjoint(nsph_sph* s)
     return NSPH_OK;
 }
 
+// Enqueue the reverse of one step on validated inputs.
+static int adjoint_enqueue(nsph_sph* s, const nsph_sph_params* p, int n, const float* x_in, const float* v_in,
+                           const float* f_ext, const float* mass, const float* inv_mass, const int* flags,
+                           const int* world, const float* gravity, int world_count, const float* x_out_adj,
+                           const float* v_out_adj, const float* rho_out_adj, float* x_in_adj, float* v_in_adj,
+                           float* f_ext_adj, float* eos_b_adj, cudaStream_t cs, int& launches)
+{
+    GatherArgs ga{x_in, v_in, mass, inv_mass, flags, world, world_count, s->xs, s->vs};
+    if (s->eva[0]) NSPH_CUDA_TRY(record_mark(s->eva[0], cs));
+    int st = grid_build(s->grid, x_in, n, p->cell_width, p->cell_inv, &ga, s->status, cs, &launches);
+    if (st != NSPH_OK) return st;
+    s->last_n = n;
+    if (s->eva[1]) NSPH_CUDA_TRY(record_mark(s->eva[1], cs));
+    if (n > 0) {
+        const GridDev g = s->grid.view();
+        int blocks, threads;
+        pass_launch(s, n, false, blocks, threads);
+        k_density<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->mask, s->ncand,
+                                                   s->status);
+        NSPH_LAUNCH_CHECK("k_density");
+        if (s->eva[2]) NSPH_CUDA_TRY(record_mark(s->eva[2], cs));
+        const AdjIO io{x_out_adj, v_out_adj, rho_out_adj, x_in_adj, v_in_adj, f_ext_adj, f_ext, inv_mass, gravity,
+                       s->adj_g, s->adj_d, s->adj_rho, s->adj_bpart};
+        k_adj_local<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, n, *p, s->mask, s->ncand, io);
+        NSPH_LAUNCH_CHECK("k_adj_local");
+        if (s->eva[3]) NSPH_CUDA_TRY(record_mark(s->eva[3], cs));
+        k_adj_pair<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->mask, s->ncand, io);
+        NSPH_LAUNCH_CHECK("k_adj_pair");
+        if (s->eva[4]) NSPH_CUDA_TRY(record_mark(s->eva[4], cs));
+        k_adj_density<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->mask, s->ncand, s->adj_rho,
+                                                       x_in_adj);
+        NSPH_LAUNCH_CHECK("k_adj_density");
+        launches += 4;
+        if (eos_b_adj) {
+            k_adj_b_reduce<<<1, 256, 0, cs>>>(s->adj_bpart, blocks, eos_b_adj);
+            NSPH_LAUNCH_CHECK("k_adj_b_reduce");
+            ++launches;
+        }
+    } else {
+        for (int k = 2; k < 5; ++k)
+            if (s->eva[k]) NSPH_CUDA_TRY(record_mark(s->eva[k], cs));
+    }
+    if (s->eva[5]) NSPH_CUDA_TRY(record_mark(s->eva[5], cs));
+    return NSPH_OK;
+}
+
+static int check_adjoint_ready(const nsph_sph* s)
+{
+    if (s->grid.world_count > 0) return fail(NSPH_ERR_INVALID_ARG, "the adjoint supports single-world solvers only");
+    if (!s->adj_g) return fail(NSPH_ERR_INVALID_ARG, "adjoint scratch not allocated (nsph_sph_enable_adjoint)");
+    return NSPH_OK;
+}
+
 extern "C" int nsph_sph_step_adjoint(nsph_sph* s, const nsph_sph_params* p, int n, const float* x_in,
                                      const float* v_in, const float* f_ext, const float* mass, const float* inv_mass,
                                      const int* flags, const int* world, const float* gravity, int world_count,
@@ -1261,47 +1389,67 @@ extern "C" int nsph_sph_step_adjoint(nsph_sph* s, const nsph_sph_params* p, int 
     clear_error();
     if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
     int st = check_params(p);
+    if (st == NSPH_OK) st = check_adjoint_ready(s);
+    if (st == NSPH_OK) st = check_step_inputs(s, n, x_in, v_in, mass, inv_mass, flags, gravity, world_count);
     if (st != NSPH_OK) return st;
-    if (s->grid.world_count > 0) return fail(NSPH_ERR_INVALID_ARG, "the adjoint supports single-world solvers only");
-    if (!s->adj_g) return fail(NSPH_ERR_INVALID_ARG, "adjoint scratch not allocated (nsph_sph_enable_adjoint)");
-    if (n < 0) return fail(NSPH_ERR_INVALID_ARG, "negative particle count");
-    if (n > s->capacity) return fail(NSPH_ERR_CAPACITY, "more particles than the solver was created for");
-    if (world_count < 1 || !gravity) return fail(NSPH_ERR_INVALID_ARG, "gravity needs world_count >= 1");
-    if (n > 0 && (!x_in || !v_in || !mass || !inv_mass || !flags))
-        return fail(NSPH_ERR_INVALID_ARG, "null state or model array");
     if (n > 0 && (!x_out_adj || !v_out_adj || !x_in_adj || !v_in_adj))
         return fail(NSPH_ERR_INVALID_ARG, "null adjoint array");
     if (n > 0 && ((const float*)x_in_adj == v_out_adj || (const float*)v_in_adj == x_out_adj || x_in_adj == v_in_adj))
         return fail(NSPH_ERR_INVALID_ARG, "position and velocity adjoints must not share memory");
     DeviceGuard guard(s->grid.device);
     if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
-    cudaStream_t cs = (cudaStream_t)stream;
-    GatherArgs ga{x_in, v_in, mass, inv_mass, flags, world, world_count, s->xs, s->vs};
     int launches = 0;
-    st = grid_build(s->grid, x_in, n, p->cell_width, p->cell_inv, &ga, s->status, cs, &launches);
+    st = adjoint_enqueue(s, p, n, x_in, v_in, f_ext, mass, inv_mass, flags, world, gravity, world_count, x_out_adj,
+                         v_out_adj, rho_out_adj, x_in_adj, v_in_adj, f_ext_adj, eos_b_adj, (cudaStream_t)stream,
+                         launches);
+    s->last_launches = launches;
+    return st;
+}
+
+extern "C" int nsph_sph_rollout_adjoint(nsph_sph* s, const nsph_sph_params* p, int n, int steps,
+                                        const float* x_states, const float* v_states, const float* f_ext,
+                                        const float* mass, const float* inv_mass, const int* flags, const int* world,
+                                        const float* gravity, int world_count, float* x_adj, float* v_adj,
+                                        float* f_ext_adj, float* eos_b_adj, void* stream)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    int st = check_params(p);
+    if (st == NSPH_OK) st = check_adjoint_ready(s);
+    if (st == NSPH_OK) st = check_step_inputs(s, n, x_states, v_states, mass, inv_mass, flags, gravity, world_count);
     if (st != NSPH_OK) return st;
-    s->last_n = n;
-    if (n > 0) {
-        const GridDev g = s->grid.view();
-        int blocks, threads;
-        pass_launch(s, n, false, blocks, threads);
-        k_density<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->mask, s->ncand, s->status);
-        NSPH_LAUNCH_CHECK("k_density");
-        const AdjIO io{x_out_adj, v_out_adj, rho_out_adj, x_in_adj, v_in_adj, f_ext_adj, f_ext, inv_mass, gravity,
-                       s->adj_g, s->adj_d, s->adj_rho, s->adj_bpart};
-        k_adj_local<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, n, *p, s->mask, s->ncand, io);
-        NSPH_LAUNCH_CHECK("k_adj_local");
-        k_adj_pair<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->mask, s->ncand, io);
-        NSPH_LAUNCH_CHECK("k_adj_pair");
-        k_adj_density<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->mask, s->ncand, s->adj_rho, x_in_adj);
-        NSPH_LAUNCH_CHECK("k_adj_density");
-        launches += 4;
-        if (eos_b_adj) {
-            k_adj_b_reduce<<<1, 256, 0, cs>>>(s->adj_bpart, blocks, eos_b_adj);
-            NSPH_LAUNCH_CHECK("k_adj_b_reduce");
-            ++launches;
-        }
+    if (steps < 0) return fail(NSPH_ERR_INVALID_ARG, "negative step count");
+    const size_t len = 3 * (size_t)n;
+    if (n > 0 && steps > 0) {
+        if (!x_adj || !v_adj) return fail(NSPH_ERR_INVALID_ARG, "null adjoint array");
+        const size_t tot = len * (size_t)steps;
+        if (overlaps(x_adj, len, v_adj, len) || overlaps(x_adj, len, x_states, tot) ||
+            overlaps(x_adj, len, v_states, tot) || overlaps(v_adj, len, x_states, tot) ||
+            overlaps(v_adj, len, v_states, tot))
+            return fail(NSPH_ERR_INVALID_ARG, "adjoint arrays overlap each other or the states");
+    }
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    cudaStream_t cs = (cudaStream_t)stream;
+    int launches = 0;
+    for (int t = steps - 1; t >= 0 && n > 0; --t) {
+        st = adjoint_enqueue(s, p, n, x_states + (size_t)t * len, v_states + (size_t)t * len, f_ext, mass, inv_mass,
+                             flags, world, gravity, world_count, x_adj, v_adj, nullptr, x_adj, v_adj, f_ext_adj,
+                             eos_b_adj, cs, launches);
+        if (st != NSPH_OK) return st;
     }
     s->last_launches = launches;
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_adjoint_phase_times(nsph_sph* s, float ms_out[5])
+{
+    clear_error();
+    if (!s || !ms_out) return fail(NSPH_ERR_INVALID_ARG, "null argument");
+    if (!s->eva[0]) return fail(NSPH_ERR_INVALID_ARG, "phase timing is not enabled");
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    NSPH_CUDA_TRY(cudaEventSynchronize(s->eva[5]));
+    for (int k = 0; k < 5; ++k) NSPH_CUDA_TRY(cudaEventElapsedTime(ms_out + k, s->eva[k], s->eva[k + 1]));
     return NSPH_OK;
 }

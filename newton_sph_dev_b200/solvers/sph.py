@@ -208,6 +208,7 @@ class SolverSPH(SolverBase):
         self._lib = _lib.load()
         self._handle = ctypes.c_void_p()
         self._dt = None
+        self.launches_total = 0  # kernels enqueued by this solver's library calls (step, rollout, adjoint)
         if isinstance(config, (list, tuple)):
             self._init_worlds(model, list(config))
             return
@@ -324,6 +325,7 @@ class SolverSPH(SolverBase):
                 int(model.gravity.shape[0]), state_out.particle_q.data_ptr(), state_out.particle_qd.data_ptr(),
                 _lib.ptr(rho), _lib.ptr(prs), _lib.ptr(acc), _lib.stream_handle(model.device))
             _lib.check(st, "SolverSPH.step")
+            self.launches_total += self.last_launches
             return
         p = self.params_for(dt)
         st = self._lib.nsph_sph_step(
@@ -347,6 +349,7 @@ class SolverSPH(SolverBase):
             _lib.stream_handle(model.device),
         )
         _lib.check(st, "SolverSPH.step")
+        self.launches_total += self.last_launches
 
     # ---- adjoint ---------------------------------------------------------
     def enable_adjoint(self) -> None:
@@ -392,6 +395,7 @@ class SolverSPH(SolverBase):
             model.particle_world.data_ptr(), model.gravity.data_ptr(), int(model.gravity.shape[0]),
             x_out.data_ptr(), v_out.data_ptr(), None, None, None, _lib.stream_handle(model.device))
         _lib.check(st, "SolverSPH.step_raw")
+        self.launches_total += self.last_launches
 
     def step_backward_raw(self, x_in: torch.Tensor, v_in: torch.Tensor, params: _lib.NsphSphParams,
                           x_out_grad: torch.Tensor, v_out_grad: torch.Tensor, x_in_grad: torch.Tensor,
@@ -423,6 +427,62 @@ class SolverSPH(SolverBase):
             x_out_grad.data_ptr(), v_out_grad.data_ptr(), _lib.ptr(rho_out_grad), x_in_grad.data_ptr(),
             v_in_grad.data_ptr(), _lib.ptr(f_ext_grad), _lib.ptr(eos_b_grad), _lib.stream_handle(model.device))
         _lib.check(st, "SolverSPH.step_backward")
+        self.launches_total += self.last_launches
+
+    def _model_ptrs(self):
+        m = self.model
+        return (m.particle_mass.data_ptr(), m.particle_inv_mass.data_ptr(), m.particle_flags.data_ptr(),
+                m.particle_world.data_ptr(), m.gravity.data_ptr(), int(m.gravity.shape[0]))
+
+    def rollout_raw(self, x0: torch.Tensor, v0: torch.Tensor, x_traj: torch.Tensor, v_traj: torch.Tensor,
+                    params: _lib.NsphSphParams, f_ext: torch.Tensor | None = None) -> None:
+        """nsph_sph_rollout: x_traj.shape[0] steps from (x0, v0); the state
+        after step t goes to x_traj[t], v_traj[t] ((steps, N, 3) float32)."""
+        n = self.model.particle_count
+        if self.batched:
+            raise ValueError("rollout_raw needs a single-world solver")
+        for t, name in ((x0, "x0"), (v0, "v0")):
+            self._check_vec(t, name)
+        steps = int(x_traj.shape[0])
+        for t, name in ((x_traj, "x_traj"), (v_traj, "v_traj")):
+            _require_cuda(t, name)
+            if t.dtype != torch.float32 or tuple(t.shape) != (steps, n, 3) or not t.is_contiguous():
+                raise ValueError(f"{name} must be a contiguous ({steps}, {n}, 3) float32 tensor")
+        if f_ext is not None:
+            self._check_vec(f_ext, "f_ext")
+        st = self._lib.nsph_sph_rollout(self._handle, ctypes.byref(params), n, steps, x0.data_ptr(), v0.data_ptr(),
+                                        _lib.ptr(f_ext), *self._model_ptrs(), x_traj.data_ptr(), v_traj.data_ptr(),
+                                        _lib.stream_handle(self.model.device))
+        _lib.check(st, "SolverSPH.rollout")
+        self.launches_total += self.last_launches
+
+    def rollout_backward_raw(self, x_states: torch.Tensor, v_states: torch.Tensor, params: _lib.NsphSphParams,
+                             x_grad: torch.Tensor, v_grad: torch.Tensor, f_ext: torch.Tensor | None = None,
+                             f_ext_grad: torch.Tensor | None = None, eos_b_grad: torch.Tensor | None = None) -> None:
+        """nsph_sph_rollout_adjoint: reverse of x_states.shape[0] steps whose
+        input states are x_states[t], v_states[t]; x_grad / v_grad (N, 3) go
+        from the last output's gradient to the first input's, in place."""
+        n = self.model.particle_count
+        self.enable_adjoint()
+        steps = int(x_states.shape[0])
+        for t, name in ((x_states, "x_states"), (v_states, "v_states")):
+            _require_cuda(t, name)
+            if t.dtype != torch.float32 or tuple(t.shape) != (steps, n, 3) or not t.is_contiguous():
+                raise ValueError(f"{name} must be a contiguous ({steps}, {n}, 3) float32 tensor")
+        for t, name in ((x_grad, "x_grad"), (v_grad, "v_grad")):
+            self._check_vec(t, name)
+        for t, name in ((f_ext, "f_ext"), (f_ext_grad, "f_ext_grad")):
+            if t is not None:
+                self._check_vec(t, name)
+        if eos_b_grad is not None and (eos_b_grad.dtype != torch.float32 or eos_b_grad.numel() != 1
+                                       or not eos_b_grad.is_cuda):
+            raise ValueError("eos_b_grad must be a one-element float32 CUDA tensor")
+        st = self._lib.nsph_sph_rollout_adjoint(
+            self._handle, ctypes.byref(params), n, steps, x_states.data_ptr(), v_states.data_ptr(), _lib.ptr(f_ext),
+            *self._model_ptrs(), x_grad.data_ptr(), v_grad.data_ptr(), _lib.ptr(f_ext_grad), _lib.ptr(eos_b_grad),
+            _lib.stream_handle(self.model.device))
+        _lib.check(st, "SolverSPH.rollout_backward")
+        self.launches_total += self.last_launches
 
     def step_backward(self, state_in: State, dt: float, x_out_grad: torch.Tensor, v_out_grad: torch.Tensor,
                       rho_out_grad: torch.Tensor | None = None) -> dict[str, torch.Tensor]:
@@ -532,6 +592,15 @@ class SolverSPH(SolverBase):
         ms = (ctypes.c_float * 3)()
         _lib.check(self._lib.nsph_sph_phase_times(self._handle, ctypes.byref(ms)), "SolverSPH.phase_times")
         return float(ms[0]), float(ms[1]), float(ms[2])
+
+    def adjoint_phase_times(self) -> tuple[float, float, float, float, float]:
+        """(build, density, force recompute + integrate reverse, pair gather,
+        density gather) milliseconds of the last executed adjoint step; waits
+        for it. Needs :meth:`enable_phase_timing`."""
+        ms = (ctypes.c_float * 5)()
+        _lib.check(self._lib.nsph_sph_adjoint_phase_times(self._handle, ctypes.byref(ms)),
+                   "SolverSPH.adjoint_phase_times")
+        return tuple(float(v) for v in ms)
 
     def set_launch(self, threads: int = 0, blocks_per_sm: int = -1) -> None:
         """Launch shape of the density and force passes (see nsph_sph_set_launch)."""

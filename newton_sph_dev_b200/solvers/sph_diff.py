@@ -45,14 +45,6 @@ def _forward_step(solver, x, v, params, f_ext):
     return x1, v1
 
 
-def _grads_out(eos_b, b_grad, f_ext, f_grad):
-    gb = None
-    if torch.is_tensor(eos_b):
-        gb = b_grad.to(eos_b.dtype).reshape(eos_b.shape)
-    gf = f_grad if f_ext is not None else None
-    return gb, gf
-
-
 class _SPHStep(torch.autograd.Function):
     @staticmethod
     def forward(ctx, x, v, eos_b, f_ext, solver, dt):
@@ -98,15 +90,18 @@ def sph_step(solver: SolverSPH, x: torch.Tensor, v: torch.Tensor, dt: float, eos
 class _SPHRollout(torch.autograd.Function):
     @staticmethod
     def forward(ctx, x0, v0, eos_b, f_ext, solver, steps, dt, every):
-        x = x0.detach().contiguous().clone()
+        x = x0.detach().contiguous().clone()  # the first checkpoint
         v = v0.detach().contiguous().clone()
+        n = x.shape[0]
         f = f_ext.detach().contiguous() if f_ext is not None else None
         params = solver.step_params(dt, _b_value(solver, eos_b))
+        tx = torch.empty((min(every, steps), n, 3), dtype=torch.float32, device=x.device)
+        tv = torch.empty_like(tx)
         checkpoints = []
-        for t in range(steps):
-            if t % every == 0:
-                checkpoints.append((x, v))
-            x, v = _forward_step(solver, x, v, params, f)
+        for start, length in reversed(checkpoint_schedule(steps, every)):
+            checkpoints.append((x, v))
+            solver.rollout_raw(x, v, tx[:length], tv[:length], params, f)
+            x, v = tx[length - 1].clone(), tv[length - 1].clone()
         ctx.solver, ctx.params, ctx.steps, ctx.every = solver, params, steps, every
         ctx.checkpoints = checkpoints
         ctx.f = f
@@ -117,24 +112,22 @@ class _SPHRollout(torch.autograd.Function):
     @staticmethod
     def backward(ctx, gx, gv):
         solver, params, steps, every, f = ctx.solver, ctx.params, ctx.steps, ctx.every, ctx.f
-        x0, v0 = ctx.checkpoints[0] if ctx.checkpoints else (None, None)
-        if x0 is None:
-            return gx, gv, None, None, None, None, None, None
+        x0 = ctx.checkpoints[0][0]
+        n = x0.shape[0]
         xa = torch.zeros_like(x0) if gx is None else gx.contiguous().float().clone()
-        va = torch.zeros_like(v0) if gv is None else gv.contiguous().float().clone()
+        va = torch.zeros_like(x0) if gv is None else gv.contiguous().float().clone()
         bg = torch.zeros(1, dtype=torch.float32, device=x0.device)
         fg = torch.zeros_like(x0) if f is not None else None
-        for c in range(len(ctx.checkpoints) - 1, -1, -1):
-            start = c * every
-            length = min(every, steps - start)
-            xs, vs = [ctx.checkpoints[c][0]], [ctx.checkpoints[c][1]]
-            for _ in range(length - 1):  # recompute the segment's states
-                x1, v1 = _forward_step(solver, xs[-1], vs[-1], params, f)
-                xs.append(x1)
-                vs.append(v1)
-            for t in range(length - 1, -1, -1):  # adjoints in place
-                solver.step_backward_raw(xs[t], vs[t], params, xa, va, xa, va, f_ext=f, f_ext_grad=fg,
-                                         eos_b_grad=bg)
+        sx = torch.empty((min(every, steps), n, 3), dtype=torch.float32, device=x0.device)
+        sv = torch.empty_like(sx)
+        for c, (start, length) in enumerate(checkpoint_schedule(steps, every)):
+            cx, cv = ctx.checkpoints[len(ctx.checkpoints) - 1 - c]
+            sx[0].copy_(cx)
+            sv[0].copy_(cv)
+            if length > 1:  # recompute the segment's input states from its checkpoint
+                solver.rollout_raw(sx[0], sv[0], sx[1:length], sv[1:length], params, f)
+            solver.rollout_backward_raw(sx[:length], sv[:length], params, xa, va, f_ext=f, f_ext_grad=fg,
+                                        eos_b_grad=bg)
         ctx.checkpoints = None
         gb = bg.to(ctx.b_meta[0]).reshape(ctx.b_meta[1]) if ctx.has_b else None
         return xa, va, gb, fg, None, None, None, None
