@@ -52,6 +52,7 @@ extern "C" {
 #define NSPH_STATUS_NONFINITE_INPUT   1u  /* a position was NaN/Inf at the build     */
 #define NSPH_STATUS_NONFINITE_OUTPUT  2u  /* a new position/velocity was NaN/Inf     */
 #define NSPH_STATUS_ZERO_DENSITY      4u  /* an active particle had density <= 0     */
+#define NSPH_STATUS_SURROGATE_TIMEOUT 8u  /* a tensor-core completion wait gave up   */
 
 /* Particle flag bit, newton/_src/geometry/flags.py:8-14 (ParticleFlags.ACTIVE). */
 #define NSPH_PARTICLE_ACTIVE 1
@@ -291,6 +292,67 @@ NSPH_API int nsph_sph_rollout_adjoint(nsph_sph* solver, const nsph_sph_params* p
                                       const float* mass, const float* inv_mass, const int* flags, const int* world,
                                       const float* gravity, int world_count,
                                       float* x_adj, float* v_adj, float* f_ext_adj, float* eos_b_adj, void* stream);
+
+/* ---- learned surrogate step (no counterpart in the reference) -------------
+ * A WCSPH step with a larger dt whose acceleration is corrected per particle
+ * by a small MLP (16 -> 64 -> 64 -> 3, SiLU; bf16 weights and activations,
+ * fp32 accumulation on the tcgen05 tensor cores) that reads 16
+ * dimensionless neighbour features (density, density error, kernel-weighted
+ * relative position and velocity moments, the SPH acceleration, ...; the
+ * list is in csrc/sph.cu). `model` is a device buffer of
+ * nsph_mlp_model_floats() floats: the fp32 weights W1[16][64], b1[64],
+ * W2[64][64], b2[64], W3[64][3], b3[3] at offsets 0, 1024, 1088, 5184, 5248,
+ * 5440, the feature means and inverse standard deviations at 5448 and 5464,
+ * and the output means and standard deviations at 5480 and 5484. The
+ * correction is acc_scale * (y * out_std + out_mean) with acc_scale = c0^2/h.
+ *
+ * nsph_sph_enable_surrogate: allocates the feature scratch (96 bytes per
+ *   particle of capacity); once, outside graph capture.
+ * nsph_sph_features: the step's grid build, density pass and feature pass
+ *   on (x_in, v_in): feat_out (n x 16) and acc_out (n x 6: SPH acceleration,
+ *   XSPH sum), original order, either may be NULL; rho_out optional.
+ * nsph_sph_step_surrogate: one surrogate step (time step params->dt).
+ *   stats: device float[4]; the step writes stats[0] = mean over active
+ *   particles of max(0, rho/rho0 - 1) at x_in (the compression error),
+ *   stats[1] = max(stats[1], stats[0]), stats[2] += 1 and
+ *   stats[3] += stats[0], so a host that zeroes stats[1..2] reads a
+ *   window's worst compression and step count with one copy. Kernels: grid
+ *   build, density, feature pass, compression reduction, MLP + integrate. */
+NSPH_API int nsph_sph_enable_surrogate(nsph_sph* solver);
+NSPH_API int nsph_sph_features(nsph_sph* solver, const nsph_sph_params* params, int n,
+                               const float* x_in, const float* v_in,
+                               const float* mass, const float* inv_mass, const int* flags, const int* world,
+                               const float* gravity, int world_count,
+                               float* feat_out, float* acc_out, float* rho_out, void* stream);
+NSPH_API int nsph_sph_step_surrogate(nsph_sph* solver, const nsph_sph_params* params, const float* model,
+                                     float acc_scale, int n,
+                                     const float* x_in, const float* v_in, const float* f_ext,
+                                     const float* mass, const float* inv_mass, const int* flags, const int* world,
+                                     const float* gravity, int world_count,
+                                     float* x_out, float* v_out, float* rho_out, float* p_out, float* stats,
+                                     void* stream);
+
+/* The MLP on its own (training and checks).
+ * nsph_mlp_model_floats: size of the model buffer in floats.
+ * nsph_mlp_forward: out (n x 3) = de-normalised MLP outputs of features
+ *   (n x 16, raw) on device `device`; err (device uint) gets bit 0 if a
+ *   tensor-core wait gave up.
+ * nsph_mlp_gradient: gradient of the mean squared error between the
+ *   normalised outputs and the normalised targets (n x 3, raw) over the
+ *   batch rows batch_idx[0..batch): grad (device, 5443 + 1 floats: the
+ *   gradient in model order, then the loss). partials: device scratch of
+ *   partial_rows x 5444 floats, partial_rows >= nsph_mlp_gradient_ctas().
+ * nsph_mlp_adam: one Adam step on the 5443 trainable floats of `model`
+ *   (m, v: device moment buffers of 5443 floats; step counts from 1). */
+NSPH_API int nsph_mlp_model_floats(void);
+NSPH_API int nsph_mlp_forward(int device, const float* model, const float* features, int n, float* out,
+                              unsigned int* err, void* stream);
+NSPH_API int nsph_mlp_gradient_ctas(int device, int batch);
+NSPH_API int nsph_mlp_gradient(int device, const float* model, const float* features, const float* targets,
+                               const int* batch_idx, int batch, float* partials, int partial_rows, float* grad,
+                               unsigned int* err, void* stream);
+NSPH_API int nsph_mlp_adam(int device, float* model, const float* grad, float* m, float* v, float lr, float beta1,
+                           float beta2, float eps, int step, void* stream);
 
 /* Neighbour lists of the last step's build, in original particle order: for
  * each particle i the ids j (self included) of active particles visited by

@@ -23,6 +23,7 @@ NSPH_ERR_OUT_OF_MEMORY = 5
 NSPH_STATUS_NONFINITE_INPUT = 1
 NSPH_STATUS_NONFINITE_OUTPUT = 2
 NSPH_STATUS_ZERO_DENSITY = 4
+NSPH_STATUS_SURROGATE_TIMEOUT = 8
 
 c_int_p = ctypes.POINTER(ctypes.c_int)
 c_float_p = ctypes.POINTER(ctypes.c_float)
@@ -141,6 +142,38 @@ SIGNATURES = [
         + [ctypes.c_int]
         + [c_void_p] * 4
         + [c_void_p],
+    ),
+    ("nsph_sph_enable_surrogate", ctypes.c_int, [c_void_p]),
+    (
+        "nsph_sph_features",
+        ctypes.c_int,
+        [c_void_p, ctypes.POINTER(NsphSphParams), ctypes.c_int]
+        + [c_void_p] * 7
+        + [ctypes.c_int]
+        + [c_void_p] * 3
+        + [c_void_p],
+    ),
+    (
+        "nsph_sph_step_surrogate",
+        ctypes.c_int,
+        [c_void_p, ctypes.POINTER(NsphSphParams), c_void_p, ctypes.c_float, ctypes.c_int]
+        + [c_void_p] * 8
+        + [ctypes.c_int]
+        + [c_void_p] * 5
+        + [c_void_p],
+    ),
+    ("nsph_mlp_model_floats", ctypes.c_int, []),
+    ("nsph_mlp_forward", ctypes.c_int, [ctypes.c_int, c_void_p, c_void_p, ctypes.c_int, c_void_p, c_void_p, c_void_p]),
+    ("nsph_mlp_gradient_ctas", ctypes.c_int, [ctypes.c_int, ctypes.c_int]),
+    (
+        "nsph_mlp_gradient",
+        ctypes.c_int,
+        [ctypes.c_int] + [c_void_p] * 4 + [ctypes.c_int, c_void_p, ctypes.c_int, c_void_p, c_void_p, c_void_p],
+    ),
+    (
+        "nsph_mlp_adam",
+        ctypes.c_int,
+        [ctypes.c_int, c_void_p, c_void_p, c_void_p, c_void_p] + [ctypes.c_float] * 4 + [ctypes.c_int, c_void_p],
     ),
     ("nsph_sph_neighbors", ctypes.c_int, [c_void_p, ctypes.POINTER(NsphSphParams), c_void_p, c_void_p, c_void_p, c_void_p]),
     ("nsph_sph_get_grid_view", ctypes.c_int, [c_void_p, ctypes.POINTER(NsphGridView)]),

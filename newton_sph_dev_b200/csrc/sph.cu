@@ -24,6 +24,7 @@
 #include <string>
 #include <vector>
 
+#include "mlp.cuh"
 #include "nsph_internal.cuh"
 
 namespace nsph {
@@ -652,7 +653,8 @@ __global__ void __launch_bounds__(kSphThreads, 2) k_adj_local(GridDev g, const f
     }
 }
 
-// sum of v over the block, valid in thread 0
+// sum of v over the block, valid in thread 0 (a second call needs a
+// __syncthreads() in between: the shared partials are reused)
 __device__ __forceinline__ float block_sum(float v)
 {
     __shared__ float part[32];
@@ -786,6 +788,247 @@ __global__ void k_adj_b_reduce(const float* __restrict__ bpart, int blocks, floa
     if (threadIdx.x == 0) *b_adj += v;
 }
 
+// ==========================================================================
+// Surrogate step: the plain step's build and density pass, a force pass that
+// also gathers 16 neighbour features per particle (k_force_features), and
+// one kernel that evaluates the MLP on the tensor cores (mlp.cuh) and
+// integrates with the corrected acceleration a + da (k_surrogate). The
+// features are dimensionless (lengths / h, velocities / c0, accelerations
+// h / c0^2, with c0^2 = B gamma / rho0):
+//   0 rho/rho0   1 rho/rho0 - 1   2-4 sum V_j W (x_j - x_i) / h
+//   5-7 sum V_j W (v_j - v_i) / c0 (the XSPH sum)   8-10 a h / c0^2
+//   11 sum V_j W r^2 / h^2   12 Shepard sum V_i W(0) + sum V_j W
+//   13 sum V_j F (v_j - v_i).(x_i - x_j) h / c0 (velocity divergence)
+//   14 p / (rho0 c0^2)   15 |a| h / c0^2
+// with V_j = m_j / rho_j and F = (dW/dr)/r.
+// ==========================================================================
+constexpr int kFeat = kMlpIn;
+
+struct FeatAcc {
+    float sw, mx, my, mz, m2, dvg;
+};
+
+// the pressure and XSPH terms of force_term_data (same statements, so the
+// same rounding) plus the feature sums
+__device__ __forceinline__ void force_feature_term(float4 xj, float4 vj, float2 aj, float4 xi, float4 vi, float pr2_i,
+                                                   const nsph_sph_params& p, ForceAcc& acc, FeatAcc& fa)
+{
+    if (!(__float_as_int(vj.w) & kAttrActive)) return;
+    float dx, dy, dz;
+    const float r2 = dist2(xi, xj, dx, dy, dz);
+    const float r = __fsqrt_rn(r2);
+    const float q = __fmul_rn(r, p.inv_h);
+    const float w = kernel_w(q, p);
+    float f = 0.f;
+    if (r2 > 0.f) {
+        f = kernel_f(q, __frcp_rn(r), p);
+        const float s = __fmul_rn(__fmul_rn(xj.w, __fadd_rn(pr2_i, aj.y)), f);
+        acc.ax = __fmaf_rn(-s, dx, acc.ax);
+        acc.ay = __fmaf_rn(-s, dy, acc.ay);
+        acc.az = __fmaf_rn(-s, dz, acc.az);
+    }
+    const float c = __fmul_rn(aj.x, w);
+    const float rvx = __fsub_rn(vj.x, vi.x), rvy = __fsub_rn(vj.y, vi.y), rvz = __fsub_rn(vj.z, vi.z);
+    acc.dvx = __fmaf_rn(c, rvx, acc.dvx);
+    acc.dvy = __fmaf_rn(c, rvy, acc.dvy);
+    acc.dvz = __fmaf_rn(c, rvz, acc.dvz);
+    fa.sw += c;
+    fa.mx -= c * dx;
+    fa.my -= c * dy;
+    fa.mz -= c * dz;
+    fa.m2 += c * r2;
+    fa.dvg += aj.x * f * (rvx * dx + rvy * dy + rvz * dz);
+}
+
+__device__ __forceinline__ void force_features_single(const GridDev& g, const float4* __restrict__ xs,
+                                                      const float4* __restrict__ vs, const float2* __restrict__ aux,
+                                                      const unsigned* __restrict__ mask, int nc, int n, int k,
+                                                      float4 xi, float4 vi, float pr2_i, const nsph_sph_params& p,
+                                                      ForceAcc& acc, FeatAcc& fa)
+{
+    if (nc <= kMaskBits) {
+        for_each_masked(
+            g, xi, p.h, [&](int w) { return __ldg(mask + (size_t)w * n + k); },
+            [&](int j) {
+                if (j != k) force_feature_term(__ldg(xs + j), __ldg(vs + j), __ldg(aux + j), xi, vi, pr2_i, p, acc, fa);
+            });
+    } else {
+        for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
+            for (int j = lo; j < hi; ++j) {
+                float dx, dy, dz;
+                if (dist2(xi, __ldg(xs + j), dx, dy, dz) < p.h2 && j != k)
+                    force_feature_term(__ldg(xs + j), __ldg(vs + j), __ldg(aux + j), xi, vi, pr2_i, p, acc, fa);
+            }
+        });
+    }
+}
+
+// per sorted particle k: feat[16 k ..] and sacc[2k] = (a, 0), sacc[2k+1] =
+// (dv, 0); per block: (sum of max(0, rho/rho0 - 1), active count)
+__global__ void __launch_bounds__(kSphThreads, 2) k_force_features(GridDev g, const float4* __restrict__ xs,
+                                                                   const float4* __restrict__ vs,
+                                                                   const float2* __restrict__ aux,
+                                                                   const float2* __restrict__ rp, int n,
+                                                                   const __grid_constant__ nsph_sph_params p,
+                                                                   const unsigned* __restrict__ mask,
+                                                                   const int* __restrict__ ncand,
+                                                                   float* __restrict__ feat, float4* __restrict__ sacc,
+                                                                   float* __restrict__ cpart)
+{
+    float csum = 0.f, ccount = 0.f;
+    const float c0sq = fmaxf(p.eos_b * (float)p.eos_gamma * p.inv_rho0, 1e-30f);
+    const float inv_c0 = rsqrtf(c0sq);
+    const float ascale = p.h / c0sq;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float4 xi = xs[k], vi = vs[k];
+        float f[kFeat];
+        ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (__float_as_int(vi.w) & kAttrActive) {
+            const float2 ak = aux[k];
+            FeatAcc fa{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            force_features_single(g, xs, vs, aux, mask, ncand[k], n, k, xi, vi, ak.y, p, acc, fa);
+            const float2 rpk = rp[k];
+            const float ratio = rpk.x * p.inv_rho0;
+            f[0] = ratio;
+            f[1] = ratio - 1.f;
+            f[2] = fa.mx * p.inv_h;
+            f[3] = fa.my * p.inv_h;
+            f[4] = fa.mz * p.inv_h;
+            f[5] = acc.dvx * inv_c0;
+            f[6] = acc.dvy * inv_c0;
+            f[7] = acc.dvz * inv_c0;
+            f[8] = acc.ax * ascale;
+            f[9] = acc.ay * ascale;
+            f[10] = acc.az * ascale;
+            f[11] = fa.m2 * p.inv_h * p.inv_h;
+            f[12] = fa.sw + ak.x * p.sigma;
+            f[13] = fa.dvg * p.h * inv_c0;
+            f[14] = rpk.y * p.inv_rho0 / c0sq;
+            f[15] = sqrtf(f[8] * f[8] + f[9] * f[9] + f[10] * f[10]);
+            csum += fmaxf(ratio - 1.f, 0.f);
+            ccount += 1.f;
+        } else {
+#pragma unroll
+            for (int j = 0; j < kFeat; ++j) f[j] = 0.f;
+        }
+        float4* fo = reinterpret_cast<float4*>(feat + (size_t)k * kFeat);
+#pragma unroll
+        for (int j = 0; j < kFeat; j += 4) fo[j / 4] = make_float4(f[j], f[j + 1], f[j + 2], f[j + 3]);
+        sacc[2 * (size_t)k] = make_float4(acc.ax, acc.ay, acc.az, 0.f);
+        sacc[2 * (size_t)k + 1] = make_float4(acc.dvx, acc.dvy, acc.dvz, 0.f);
+    }
+    csum = block_sum(csum);
+    __syncthreads();  // block_sum's shared partials are reused
+    ccount = block_sum(ccount);
+    if (threadIdx.x == 0) {
+        cpart[2 * blockIdx.x] = csum;
+        cpart[2 * blockIdx.x + 1] = ccount;
+    }
+}
+
+// stats[0] = mean compression of this step; stats[1] = max since reset;
+// stats[2] += 1; stats[3] += stats[0]
+__global__ void k_compression_reduce(const float* __restrict__ cpart, int blocks, float* __restrict__ stats)
+{
+    float s = 0.f, c = 0.f;
+    for (int b = threadIdx.x; b < blocks; b += blockDim.x) {
+        s += cpart[2 * b];
+        c += cpart[2 * b + 1];
+    }
+    s = block_sum(s);
+    __syncthreads();
+    c = block_sum(c);
+    if (threadIdx.x == 0) {
+        const float e = c > 0.f ? s / c : 0.f;
+        stats[0] = e;
+        stats[1] = fmaxf(stats[1], e);
+        stats[2] += 1.f;
+        stats[3] += e;
+    }
+}
+
+// the MLP on the tensor cores, then integrate with a + da (dynamic particles)
+__global__ void __launch_bounds__(kMlpTile, 1) k_surrogate(const float* __restrict__ model, float acc_scale,
+                                                           GridDev g, const float4* __restrict__ xs,
+                                                           const float4* __restrict__ vs,
+                                                           const float2* __restrict__ rp, int n,
+                                                           const __grid_constant__ nsph_sph_params p,
+                                                           const float* __restrict__ feat,
+                                                           const float4* __restrict__ sacc, const StepOut o)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    MlpFwdSmem& s = *reinterpret_cast<MlpFwdSmem*>(smem_raw);
+    const uint32_t tmem = mlp_cta_begin(model, s, 128);
+    uint32_t phase = 0;
+    bool ok = true;
+    const int tiles = (n + kMlpTile - 1) / kMlpTile;
+    for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+        const int k = t * kMlpTile + threadIdx.x;
+        float f[kFeat];
+        if (k < n) {
+            const float4* fi = reinterpret_cast<const float4*>(feat + (size_t)k * kFeat);
+#pragma unroll
+            for (int j = 0; j < kFeat; j += 4) {
+                const float4 q4 = fi[j / 4];
+                f[j] = q4.x;
+                f[j + 1] = q4.y;
+                f[j + 2] = q4.z;
+                f[j + 3] = q4.w;
+            }
+        } else {
+#pragma unroll
+            for (int j = 0; j < kFeat; ++j) f[j] = 0.f;
+        }
+        mlp_stage_input(s, f);
+        mlp_sync();
+        float y[kMlpOut];
+        ok = mlp_forward_tile(s, tmem, 0, 64, 0, phase, y);
+        if (ok && k < n) {
+            const float4 xi = xs[k], vi = vs[k];
+            const int attr = __float_as_int(vi.w);
+            const float4 a = sacc[2 * (size_t)k], dv = sacc[2 * (size_t)k + 1];
+            ForceAcc acc{a.x, a.y, a.z, dv.x, dv.y, dv.z};
+            if (attr & kAttrDynamic) {
+                acc.ax = __fadd_rn(acc.ax, acc_scale * mlp_denorm(s, y, 0));
+                acc.ay = __fadd_rn(acc.ay, acc_scale * mlp_denorm(s, y, 1));
+                acc.az = __fadd_rn(acc.az, acc_scale * mlp_denorm(s, y, 2));
+            }
+            integrate_out((size_t)g.ids[k], xi, vi, attr, rp[k], acc, p, p.dt, o);
+        }
+        __syncthreads();
+    }
+    if (!ok && o.status && threadIdx.x == 0) atomicOr(o.status, (unsigned)NSPH_STATUS_SURROGATE_TIMEOUT);
+    mlp_cta_end(s, tmem, 128, !ok, phase);
+}
+
+// sorted scratch -> original order: feat (n x 16), acc (n x 6: a, dv)
+__global__ void k_scatter_features(const int* __restrict__ ids, int n, const float* __restrict__ sfeat,
+                                   const float4* __restrict__ sacc, float* __restrict__ feat_out,
+                                   float* __restrict__ acc_out)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const size_t i = (size_t)ids[k];
+    if (feat_out)
+        for (int j = 0; j < kFeat; ++j) feat_out[i * kFeat + j] = sfeat[(size_t)k * kFeat + j];
+    if (acc_out) {
+        const float4 a = sacc[2 * (size_t)k], dv = sacc[2 * (size_t)k + 1];
+        acc_out[6 * i + 0] = a.x;
+        acc_out[6 * i + 1] = a.y;
+        acc_out[6 * i + 2] = a.z;
+        acc_out[6 * i + 3] = dv.x;
+        acc_out[6 * i + 4] = dv.y;
+        acc_out[6 * i + 5] = dv.z;
+    }
+}
+
+__global__ void k_scatter_rho(const int* __restrict__ ids, int n, const float2* __restrict__ rp,
+                              float* __restrict__ rho_out)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) rho_out[ids[k]] = rp[k].x;
+}
+
 }  // namespace
 }  // namespace nsph
 
@@ -819,6 +1062,10 @@ struct nsph_sph {
     float* adj_bpart = nullptr;          //   per-block partial sums of adj(B)
     int adj_bcap = 0;                    //   entries of adj_bpart
     cudaEvent_t eva[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // adjoint phases (timing)
+    float* sfeat = nullptr;              // surrogate scratch (nsph_sph_enable_surrogate), sorted: 16 features
+    float4* sacc = nullptr;              //   (a, 0), (dv, 0)
+    float* cpart = nullptr;              //   per-block (compression sum, active count)
+    int surr_sms = 0;                    //   SMs (grid of the MLP kernel)
 };
 
 // grid of a neighbour pass: one thread per particle, or a persistent grid of
@@ -874,6 +1121,9 @@ static void sph_free(nsph_sph* s)
     cudaFree(s->adj_d);
     cudaFree(s->adj_rho);
     cudaFree(s->adj_bpart);
+    cudaFree(s->sfeat);
+    cudaFree(s->sacc);
+    cudaFree(s->cpart);
     grid_free(s->grid);
 }
 
@@ -1451,5 +1701,137 @@ extern "C" int nsph_sph_adjoint_phase_times(nsph_sph* s, float ms_out[5])
     if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
     NSPH_CUDA_TRY(cudaEventSynchronize(s->eva[5]));
     for (int k = 0; k < 5; ++k) NSPH_CUDA_TRY(cudaEventElapsedTime(ms_out + k, s->eva[k], s->eva[k + 1]));
+    return NSPH_OK;
+}
+
+// ==========================================================================
+// C ABI: surrogate step
+// ==========================================================================
+extern "C" int nsph_sph_enable_surrogate(nsph_sph* s)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    if (s->grid.world_count > 0) return fail(NSPH_ERR_INVALID_ARG, "the surrogate supports single-world solvers only");
+    if (s->sfeat) return NSPH_OK;
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    const size_t c = (size_t)(s->capacity > 0 ? s->capacity : 1);
+    const size_t blocks = (c + 31) / 32 + 1;
+    cudaError_t e = cudaMalloc(&s->sfeat, sizeof(float) * kFeat * c);
+    if (e == cudaSuccess) e = cudaMalloc(&s->sacc, sizeof(float4) * 2 * c);
+    if (e == cudaSuccess) e = cudaMalloc(&s->cpart, sizeof(float) * 2 * blocks);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_surrogate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpFwdSmem));
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->surr_sms, cudaDevAttrMultiProcessorCount, s->grid.device);
+    cudaFuncAttributes fa;
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_force_features);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(s->sfeat);
+        cudaFree(s->sacc);
+        cudaFree(s->cpart);
+        s->sfeat = s->cpart = nullptr;
+        s->sacc = nullptr;
+        return fail(NSPH_ERR_OUT_OF_MEMORY, std::string("surrogate allocation: ") + cudaGetErrorString(e));
+    }
+    return NSPH_OK;
+}
+
+// grid build, density pass and feature pass into the sorted scratch
+static int features_enqueue(nsph_sph* s, const nsph_sph_params* p, int n, const float* x_in, const float* v_in,
+                            const float* mass, const float* inv_mass, const int* flags, const int* world,
+                            int world_count, cudaStream_t cs, int& launches, int& blocks)
+{
+    GatherArgs ga{x_in, v_in, mass, inv_mass, flags, world, world_count, s->xs, s->vs};
+    int st = grid_build(s->grid, x_in, n, p->cell_width, p->cell_inv, &ga, s->status, cs, &launches);
+    if (st != NSPH_OK) return st;
+    s->last_n = n;
+    blocks = 0;
+    if (n == 0) return NSPH_OK;
+    const GridDev g = s->grid.view();
+    int threads;
+    pass_launch(s, n, false, blocks, threads);
+    k_density<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->mask, s->ncand, s->status);
+    NSPH_LAUNCH_CHECK("k_density");
+    k_force_features<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->mask, s->ncand, s->sfeat,
+                                                  s->sacc, s->cpart);
+    NSPH_LAUNCH_CHECK("k_force_features");
+    launches += 2;
+    return NSPH_OK;
+}
+
+static int check_surrogate_ready(const nsph_sph* s)
+{
+    if (s->grid.world_count > 0) return fail(NSPH_ERR_INVALID_ARG, "the surrogate supports single-world solvers only");
+    if (!s->sfeat) return fail(NSPH_ERR_INVALID_ARG, "surrogate scratch not allocated (nsph_sph_enable_surrogate)");
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_features(nsph_sph* s, const nsph_sph_params* p, int n, const float* x_in, const float* v_in,
+                                 const float* mass, const float* inv_mass, const int* flags, const int* world,
+                                 const float* gravity, int world_count, float* feat_out, float* acc_out,
+                                 float* rho_out, void* stream)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    int st = check_params(p);
+    if (st == NSPH_OK) st = check_surrogate_ready(s);
+    if (st == NSPH_OK) st = check_step_inputs(s, n, x_in, v_in, mass, inv_mass, flags, gravity, world_count);
+    if (st != NSPH_OK) return st;
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    cudaStream_t cs = (cudaStream_t)stream;
+    int launches = 0, blocks = 0;
+    st = features_enqueue(s, p, n, x_in, v_in, mass, inv_mass, flags, world, world_count, cs, launches, blocks);
+    if (st != NSPH_OK) return st;
+    if (n > 0 && (feat_out || acc_out)) {
+        k_scatter_features<<<(n + 255) / 256, 256, 0, cs>>>(s->grid.point_ids, n, s->sfeat, s->sacc, feat_out,
+                                                              acc_out);
+        NSPH_LAUNCH_CHECK("k_scatter_features");
+        ++launches;
+    }
+    if (n > 0 && rho_out) {
+        k_scatter_rho<<<(n + 255) / 256, 256, 0, cs>>>(s->grid.point_ids, n, s->rp, rho_out);
+        NSPH_LAUNCH_CHECK("k_scatter_rho");
+        ++launches;
+    }
+    s->last_launches = launches;
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_step_surrogate(nsph_sph* s, const nsph_sph_params* p, const float* model, float acc_scale,
+                                       int n, const float* x_in, const float* v_in, const float* f_ext,
+                                       const float* mass, const float* inv_mass, const int* flags, const int* world,
+                                       const float* gravity, int world_count, float* x_out, float* v_out,
+                                       float* rho_out, float* p_out, float* stats, void* stream)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    int st = check_params(p);
+    if (st == NSPH_OK) st = check_surrogate_ready(s);
+    if (st == NSPH_OK) st = check_step_inputs(s, n, x_in, v_in, mass, inv_mass, flags, gravity, world_count);
+    if (st != NSPH_OK) return st;
+    if (n > 0 && (!x_out || !v_out || !model || !stats)) return fail(NSPH_ERR_INVALID_ARG, "null argument");
+    if (n > 0 && (x_out == x_in || v_out == v_in))
+        return fail(NSPH_ERR_INVALID_ARG, "state_out must not alias state_in");
+    if (!isfinite(acc_scale)) return fail(NSPH_ERR_INVALID_ARG, "acc_scale must be finite");
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    cudaStream_t cs = (cudaStream_t)stream;
+    int launches = 0, blocks = 0;
+    st = features_enqueue(s, p, n, x_in, v_in, mass, inv_mass, flags, world, world_count, cs, launches, blocks);
+    if (st != NSPH_OK) return st;
+    if (n > 0) {
+        k_compression_reduce<<<1, 256, 0, cs>>>(s->cpart, blocks, stats);
+        NSPH_LAUNCH_CHECK("k_compression_reduce");
+        const int tiles = (n + kMlpTile - 1) / kMlpTile;
+        const int grid = std::min(tiles, 4 * std::max(1, s->surr_sms));
+        const StepOut o{f_ext, inv_mass, gravity, x_out, v_out, rho_out, p_out, nullptr, s->status};
+        k_surrogate<<<grid, kMlpTile, sizeof(MlpFwdSmem), cs>>>(model, acc_scale, s->grid.view(), s->xs, s->vs,
+                                                                    s->rp, n, *p, s->sfeat, s->sacc, o);
+        NSPH_LAUNCH_CHECK("k_surrogate");
+        launches += 2;
+    }
+    s->last_launches = launches;
     return NSPH_OK;
 }

@@ -484,6 +484,55 @@ class SolverSPH(SolverBase):
         _lib.check(st, "SolverSPH.rollout_backward")
         self.launches_total += self.last_launches
 
+    # ---- surrogate ---------------------------------------------------------
+    def enable_surrogate(self) -> None:
+        """Allocate the surrogate's feature scratch (96 bytes per particle);
+        outside graph capture."""
+        if self.batched:
+            raise ValueError("the surrogate supports single-world solvers only")
+        if not getattr(self, "_surrogate_ready", False):
+            _lib.check(self._lib.nsph_sph_enable_surrogate(self._handle), "SolverSPH.enable_surrogate")
+            self._surrogate_ready = True
+
+    def features_raw(self, x: torch.Tensor, v: torch.Tensor, feat_out: torch.Tensor | None = None,
+                     acc_out: torch.Tensor | None = None, rho_out: torch.Tensor | None = None,
+                     params: _lib.NsphSphParams | None = None) -> None:
+        """nsph_sph_features on (x, v): the 16 surrogate features (N, 16) and
+        the SPH acceleration + XSPH sum (N, 6) of each particle."""
+        n = self.model.particle_count
+        self.enable_surrogate()
+        self._check_vec(x, "x")
+        self._check_vec(v, "v")
+        for t, name, w in ((feat_out, "feat_out", 16), (acc_out, "acc_out", 6)):
+            if t is not None and (t.dtype != torch.float32 or tuple(t.shape) != (n, w) or not t.is_contiguous()
+                                  or not t.is_cuda):
+                raise ValueError(f"{name} must be a contiguous ({n}, {w}) float32 CUDA tensor")
+        p = params if params is not None else self.step_params(self._dt or 0.0)
+        st = self._lib.nsph_sph_features(self._handle, ctypes.byref(p), n, x.data_ptr(), v.data_ptr(),
+                                         *self._model_ptrs(), _lib.ptr(feat_out), _lib.ptr(acc_out), _lib.ptr(rho_out),
+                                         _lib.stream_handle(self.model.device))
+        _lib.check(st, "SolverSPH.features")
+        self.launches_total += self.last_launches
+
+    def step_surrogate_raw(self, x_in: torch.Tensor, v_in: torch.Tensor, x_out: torch.Tensor, v_out: torch.Tensor,
+                           params: _lib.NsphSphParams, model, acc_scale: float, stats: torch.Tensor,
+                           f_ext: torch.Tensor | None = None, rho_out: torch.Tensor | None = None,
+                           p_out: torch.Tensor | None = None) -> None:
+        """nsph_sph_step_surrogate: one corrected step of params.dt with the
+        MLP `model` (a SurrogateModel); stats: device float[4] monitor."""
+        n = self.model.particle_count
+        self.enable_surrogate()
+        for t, name in ((x_in, "x_in"), (v_in, "v_in"), (x_out, "x_out"), (v_out, "v_out")):
+            self._check_vec(t, name)
+        if stats.dtype != torch.float32 or stats.numel() < 4 or not stats.is_cuda:
+            raise ValueError("stats must be a float32 CUDA tensor of 4 entries")
+        st = self._lib.nsph_sph_step_surrogate(
+            self._handle, ctypes.byref(params), model.buf.data_ptr(), float(acc_scale), n, x_in.data_ptr(),
+            v_in.data_ptr(), _lib.ptr(f_ext), *self._model_ptrs(), x_out.data_ptr(), v_out.data_ptr(),
+            _lib.ptr(rho_out), _lib.ptr(p_out), stats.data_ptr(), _lib.stream_handle(self.model.device))
+        _lib.check(st, "SolverSPH.step_surrogate")
+        self.launches_total += self.last_launches
+
     def step_backward(self, state_in: State, dt: float, x_out_grad: torch.Tensor, v_out_grad: torch.Tensor,
                       rho_out_grad: torch.Tensor | None = None) -> dict[str, torch.Tensor]:
         """Reverse of ``step(state_in, state_out, None, None, dt)``: the
