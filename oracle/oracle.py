@@ -404,6 +404,85 @@ def rollout_grad64(scene: AdjScene, x0, v0, steps: int, target, eos_b: float | N
 
 
 # ---------------------------------------------------------------------------
+# surrogate features (fp64 restatement on the fp32 neighbour lists)
+# ---------------------------------------------------------------------------
+def surrogate_features_py(consts: dict, dims, x, v, mass, flags):
+    """The 16 dimensionless neighbour features of the surrogate step,
+    restated in fp64 numpy from fp32 inputs, on the oracle's fp32 neighbour
+    lists (the device's). Feature k of particle i:
+      0 rho/rho0, 1 rho/rho0 - 1, 2-4 sum_j V_j W (x_j - x_i)/h,
+      5-7 sum_j V_j W (v_j - v_i)/c0, 8-10 a h/c0^2, 11 sum_j V_j W r^2/h^2,
+      12 V_i W(0) + sum_j V_j W, 13 sum_j V_j F (v_j - v_i).(x_i - x_j) h/c0,
+      14 p/(rho0 c0^2), 15 |a| h/c0^2
+    with V_j = m_j/rho_j, F = (dW/dr)/r, c0^2 = B gamma / rho0, sums over
+    active neighbours j != i. Returns (features (n, 16), rho, a, dv)."""
+    c32, c64 = consts["f32"], consts["f64"]
+    x = _f32(x).astype(np.float64)
+    v = _f32(v).astype(np.float64)
+    m = _f32(mass).astype(np.float64)
+    fl = _i32(flags)
+    n = x.shape[0]
+    off, ids = sph_neighbors(c32, dims, _f32(x), fl)
+    h, sigma = c64["h"], c64["sigma"]
+    counts = np.diff(off)
+    ii = np.repeat(np.arange(n), counts)
+    jj = ids.astype(np.int64)
+    act = (fl & 1) != 0
+    d = x[ii] - x[jj]
+    r = np.sqrt(np.sum(d * d, axis=1))
+    q = r / h
+    t = 1.0 - q
+    W = sigma * np.where(q <= 0.5, 6.0 * q * q * (q - 1.0) + 1.0, np.where(q < 1.0, 2.0 * t ** 3, 0.0))
+    safe_r = np.where(r > 0, r, 1.0)
+    F = np.where(r > 0, np.where(q <= 0.5, c64["c_near"] * (3.0 * q - 2.0), c64["c_far"] * t * t / safe_r), 0.0)
+    mj = np.where(act[jj], m[jj], 0.0)
+    rho = np.zeros(n)
+    np.add.at(rho, ii, mj * W)
+    ratio = rho / c64["rho0"]
+    B, gam = c64["eos_b"], c64["eos_gamma"]
+    p = np.where(rho > 0, B * (ratio ** gam - 1.0), 0.0)
+    if c64["clamp_pressure"]:
+        p = np.maximum(p, 0.0)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        V = np.where(rho > 0, np.where(act, m, 0.0) / rho, 0.0)
+        pr2 = np.where(rho > 0, p / (rho * rho), 0.0)
+    nself = jj != ii
+    pair = nself & act[jj] & act[ii]
+    Vj, Wp, Fp = V[jj], W, F
+    a = np.zeros((n, 3))
+    dv = np.zeros((n, 3))
+    mx = np.zeros((n, 3))
+    sw = np.zeros(n)
+    m2 = np.zeros(n)
+    dvg = np.zeros(n)
+    s = np.where(pair, mj * (pr2[ii] + pr2[jj]) * Fp, 0.0)
+    rv = v[jj] - v[ii]
+    c = np.where(pair, Vj * Wp, 0.0)
+    for k in range(3):
+        np.add.at(a[:, k], ii, -s * d[:, k])
+        np.add.at(dv[:, k], ii, c * rv[:, k])
+        np.add.at(mx[:, k], ii, -c * d[:, k])
+    np.add.at(sw, ii, c)
+    np.add.at(m2, ii, c * r * r)
+    np.add.at(dvg, ii, np.where(pair, Vj * Fp * np.sum(rv * d, axis=1), 0.0))
+    c0sq = float(np.float32(c32["eos_b"]) * np.float32(c32["eos_gamma"]) * np.float32(c32["inv_rho0"]))
+    c0 = np.sqrt(c0sq)
+    f = np.zeros((n, 16))
+    f[:, 0] = ratio
+    f[:, 1] = ratio - 1.0
+    f[:, 2:5] = mx / h
+    f[:, 5:8] = dv / c0
+    f[:, 8:11] = a * h / c0sq
+    f[:, 11] = m2 / (h * h)
+    f[:, 12] = sw + V * sigma
+    f[:, 13] = dvg * h / c0
+    f[:, 14] = p / c64["rho0"] / c0sq
+    f[:, 15] = np.linalg.norm(f[:, 8:11], axis=1)
+    f[~act] = 0.0
+    return f, rho, a, dv
+
+
+# ---------------------------------------------------------------------------
 # pure-Python restatements (small cases; checks of the C oracle)
 # ---------------------------------------------------------------------------
 def trunc_sat_py(v: np.float32) -> int:
