@@ -58,6 +58,12 @@ WORKLOADS = {
                                   "v0 ~ N(0, 0.1 m/s), 50 steps at dt = 1e-4 s, loss = mean |x_T - y|^2 against a "
                                   "seeded target cloud, gradients w.r.t. x0, v0 and the EOS stiffness B, checkpoint "
                                   "every 10 steps"),
+    "tank_1m_surrogate": dict(shape=(128, 128, 64), spacing=0.005, box=(2.0, 1.0, 1.0), dt=5e-5, vel_std=0.01,
+                              surrogate=dict(substeps=4, threshold=0.01, window=10),
+                              metric="effective particle-steps/s",
+                              desc="learned surrogate on the 1,048,576-particle tank: one step of 4 x 5e-5 s with "
+                                   "the MLP acceleration correction (tcgen05) per call, plain steps as fallback when "
+                                   "the window's mean compression error exceeds 1%"),
     "worlds_4096": dict(worlds=4096, n_range=(256, 16384), s_range=(0.004, 0.01), box=(0.5, 0.5, 0.5), dt=1e-4,
                         vel_std=0.0, seed=3,
                         desc="4,096 independent scenes: particles log-uniform in [256, 16384], spacing uniform in "
@@ -311,11 +317,12 @@ def run_reference(args):
     sample = (f"{args.steps} steps of the {sample_n}-particle "
               + (f"{sub[0]}x{sub[1]}x{sub[2]} sub-block of the workload (same spacing and physics)" if sub
                  else "full workload"))
+    metric = WORKLOADS[name].get("metric", METRIC)
     line = {
         "impl": "reference",
-        "metric": METRIC,
+        "metric": metric,
         "value": value,
-        "unit": METRIC,
+        "unit": metric,
         "n_gpus": args.gpus,
         "steps": args.steps,
         "warmup": args.warmup,
@@ -326,8 +333,8 @@ def run_reference(args):
         "dtype": "f32",
         "data": "synthetic",
         "config": {"workload": name, "particles": n, "desc": WORKLOADS[name]["desc"]},
-        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port", "sample": sample},
-        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": value, "unit": metric, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": metric, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -779,6 +786,200 @@ def run_grad_reference(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# learned surrogate step (4 x dt per step, plain step as fallback and judge)
+# ---------------------------------------------------------------------------
+# algorithmic bytes per particle: feature pass (read x, v, m/rho p/rho^2, rho p;
+# write 16 features, a, dv) and MLP + integrate (read them back with x, v,
+# rho p and the sort permutation; write x, v)
+B_ALG_FEATURES = 16 + 16 + 8 + 8 + 64 + 32
+B_ALG_MLP = 64 + 32 + 16 + 16 + 8 + 4 + 24
+MLP_FLOPS = 2 * (16 * 64 + 64 * 64 + 64 * 16)  # per particle, as issued (layer 3 padded to N = 16)
+
+
+def load_tensor_peak():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["bf16_tflops"]), "measured"
+        except (ValueError, KeyError, OSError):
+            pass
+    return 1590.0, "fallback"
+
+
+def run_surrogate(args):
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = dist_env()
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", device_id=device, timeout=timedelta(seconds=120))
+    from newton_sph_dev_b200.solvers import SolverSPH
+    from newton_sph_dev_b200.solvers.sph_surrogate import SurrogateModel, SurrogateSPH
+
+    model, cfg, w = make_scene(args.workload, str(device))
+    n = model.particle_count
+    sw = w["surrogate"]
+    sub, dt = sw["substeps"], w["dt"]
+    solver = SolverSPH(model, cfg)
+    s0, s1 = model.state(), model.state()
+    tuned = solver.autotune(s0, s1, dt) if not args.no_autotune else None
+    solver.enable_phase_timing(True)
+    net = SurrogateModel.pretrained(device)
+    stepper = SurrogateSPH(solver, net, substeps=sub, threshold=sw["threshold"], window=sw["window"], graphs=True)
+    stream = torch.cuda.current_stream(device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    # the plain step on the same scene and device, graph-replayed, for the ratio
+    p0, p1 = model.state(), model.state()
+    for _ in range(3):
+        solver.step(p0, p1, None, None, dt)
+    gp = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(gp):
+        solver.step(p0, p1, None, None, dt)
+    plain_steps = min(4 * args.steps, 400)
+    plain_ms = 0.0
+    for _ in range(plain_steps):
+        flush.zero_()
+        e0.record(stream)
+        gp.replay()
+        e1.record(stream)
+        e1.synchronize()
+        plain_ms += e0.elapsed_time(e1)
+    del gp
+    plain_value = n * plain_steps / (plain_ms * 1e-3)
+
+    # surrogate run: warm-up macro steps (graph capture of both directions), then timed steps
+    for i in range(max(args.warmup, 3)):
+        stepper.step(s0, s1, dt) if i % 2 == 0 else stepper.step(s1, s0, dt)
+    cur, nxt = (s1, s0) if max(args.warmup, 3) % 2 == 1 else (s0, s1)
+    stepper.stats.zero_()
+    sur0, fb0 = stepper.surrogate_steps, stepper.fallback_calls
+    total_ms = 0.0
+    feat_ms = mlp_ms = 0.0
+    timed_sur = 0
+    barrier(device)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            before = stepper.surrogate_steps
+            e0.record(stream)
+            stepper.step(cur, nxt, dt)
+            e1.record(stream)
+            e1.synchronize()
+            total_ms += e0.elapsed_time(e1)
+            if stepper.surrogate_steps > before:
+                ph = solver.surrogate_phase_times()
+                feat_ms += ph[2]
+                mlp_ms += ph[3]
+                timed_sur += 1
+            cur, nxt = nxt, cur
+    torch.cuda.synchronize()
+    barrier(device)
+    total_ms = max_over_ranks(total_ms, device)
+    value = world * n * sub * args.steps / (total_ms * 1e-3)
+    st = stepper.stats.cpu()
+    n_sur = stepper.surrogate_steps - sur0
+    mean_comp = float(st[3]) / max(1, n_sur)
+    fallbacks = stepper.fallback_calls - fb0
+    status = solver.status()
+    finite = bool(torch.isfinite(cur.particle_q).all() and torch.isfinite(cur.particle_qd).all())
+
+    # end to end through the public API: host state in, one call, host state out
+    e2e_steps = min(args.steps, 50)
+    hx, hv = cur.particle_q.cpu().pin_memory(), cur.particle_qd.cpu().pin_memory()
+    e2e_ms = 0.0
+    for _ in range(e2e_steps):
+        e0.record(stream)
+        cur.particle_q.copy_(hx, non_blocking=True)
+        cur.particle_qd.copy_(hv, non_blocking=True)
+        stepper.step(cur, nxt, dt)
+        hx.copy_(nxt.particle_q, non_blocking=True)
+        hv.copy_(nxt.particle_qd, non_blocking=True)
+        e1.record(stream)
+        e1.synchronize()
+        e2e_ms += e0.elapsed_time(e1)
+    e2e_ms = max_over_ranks(e2e_ms, device)
+    e2e_value = world * n * sub * e2e_steps / (e2e_ms * 1e-3)
+
+    peak, peak_kind = load_peak()
+    tpeak, tpeak_kind = load_tensor_peak()
+    t_feat = feat_ms / max(1, timed_sur) * 1e-3
+    t_mlp = mlp_ms / max(1, timed_sur) * 1e-3
+    ach = B_ALG_FEATURES * n / t_feat / 1e9 if t_feat > 0 else None
+    roofline = {"bound": "hbm", "kernel": "k_force_features", "achieved": ach, "peak": peak, "peak_kind": peak_kind,
+                "unit": "GB/s", "frac": ach / peak if ach else None, "traffic": None,
+                "alg_bytes_per_launch": B_ALG_FEATURES * n, "ms_per_launch": t_feat * 1e3}
+    tflops = MLP_FLOPS * n / t_mlp / 1e12 if t_mlp > 0 else None
+    roofline_mlp = {"bound": "tensor", "kernel": "k_surrogate (MLP + integrate)", "achieved": tflops, "peak": tpeak,
+                    "peak_kind": tpeak_kind, "unit": "TFLOP/s", "frac": tflops / tpeak if tflops else None,
+                    "flops_per_particle": MLP_FLOPS, "ms_per_launch": t_mlp * 1e3,
+                    "hbm_achieved_gbs": B_ALG_MLP * n / t_mlp / 1e9 if t_mlp > 0 else None}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        model_cpu, cfg_cpu, w_cpu = make_scene(args.workload, "cpu")
+        rate, steps_done, el, threads = cpu_oracle_rate(model_cpu, cfg_cpu, w_cpu, budget_s=15.0, max_steps=40)
+        cpu = {"value": rate, "unit": w["metric"], "cores": threads, "kind": "port",
+               "sample": f"{steps_done} plain fp32 oracle steps (dt = {dt} s) of the full {n}-particle scene in "
+                         f"{el:.1f} s (OpenMP); the CPU has no surrogate, one plain step is one dt of simulated time"}
+    if rank == 0:
+        clocks = clk.summary()
+        line = {
+            "metric": w["metric"],
+            "value": value,
+            "unit": w["metric"],
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32 (MLP bf16, fp32 accumulate)",
+            "data": "synthetic",
+            "config": {
+                "workload": args.workload, "particles": n, "desc": w["desc"],
+                "step": f"one bench step = one call advancing {sub} x {dt} s of simulated time; value counts "
+                        f"particles x plain-dt steps of simulated time",
+                "substeps": sub, "dt_plain": dt, "dt_surrogate": sub * dt, "fallback_threshold": sw["threshold"],
+                "window": sw["window"], "graph": True,
+                "launch": {"threads": solver.launch[0], "blocks_per_sm": solver.launch[1],
+                           "autotuned": tuned is not None} if hasattr(solver, "launch") else "default",
+                "l2": "flushed (256 MiB write) before every timed step, outside the timed interval",
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            },
+            "plain": {"value": plain_value, "unit": "particle-steps/s", "steps": plain_steps,
+                      "ms_per_step": plain_ms / plain_steps},
+            "speedup_vs_plain": value / plain_value,
+            "compression_error": {"mean": mean_comp, "max_window": float(max(stepper.window_worst or [0.0])),
+                                  "definition": "mean over active particles of max(0, rho/rho0 - 1), per surrogate "
+                                                "step, averaged over the timed surrogate steps"},
+            "surrogate_steps": n_sur, "fallback_calls": fallbacks,
+            "phase_ms_per_surrogate_step": {"feature_pass": t_feat * 1e3, "mlp_integrate": t_mlp * 1e3},
+            "roofline": roofline,
+            "roofline_mlp": roofline_mlp,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": w["metric"], "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n,
+                    "steps": e2e_steps},
+            "gpu_launches": stepper.launches_per_step * n_sur + fallbacks * sub * solver.last_launches,
+            "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+            "status": status,
+            "finite": finite,
+        }
+        print(json.dumps(line), flush=True)
+    stepper._graphs.clear()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -795,6 +996,8 @@ def main(argv=None):
     grad = "grad" in WORKLOADS[args.workload]
     if args.impl == "reference":
         return run_grad_reference(args) if grad else run_reference(args)
+    if "surrogate" in WORKLOADS[args.workload]:
+        return run_surrogate(args)
     return run_grad(args) if grad else run_gpu(args)
 
 

@@ -379,6 +379,11 @@ NSPH_API int nsph_sph_phase_times(nsph_sph* solver, float ms_out[3]);
  * and adj(B) reduction). Returns the five durations of the last executed
  * adjoint step in ms. */
 NSPH_API int nsph_sph_adjoint_phase_times(nsph_sph* solver, float ms_out[5]);
+/* With phase timing enabled, every surrogate step records five events:
+ * start, after the grid build, after the density pass, after the feature
+ * pass, end (compression reduction and MLP + integrate). Returns the four
+ * durations of the last executed surrogate step in ms. */
+NSPH_API int nsph_sph_surrogate_phase_times(nsph_sph* solver, float ms_out[4]);
 
 /* Launch shape of the two neighbour passes (density, force): `threads` per
  * block (0 = default 256; else a multiple of 32 up to 256) and

@@ -847,11 +847,25 @@ __device__ __forceinline__ void force_features_single(const GridDev& g, const fl
                                                       ForceAcc& acc, FeatAcc& fa)
 {
     if (nc <= kMaskBits) {
+        // one-deep software pipeline, as in force_single: the loads of
+        // neighbour t+1 are issued before the terms of neighbour t
+        bool have = false;
+        float4 pxj = make_float4(0.f, 0.f, 0.f, 0.f), pvj = pxj;
+        float2 paj = make_float2(0.f, 0.f);
         for_each_masked(
             g, xi, p.h, [&](int w) { return __ldg(mask + (size_t)w * n + k); },
             [&](int j) {
-                if (j != k) force_feature_term(__ldg(xs + j), __ldg(vs + j), __ldg(aux + j), xi, vi, pr2_i, p, acc, fa);
+                if (j == k) return;
+                const float4 nxj = __ldg(xs + j);
+                const float4 nvj = __ldg(vs + j);
+                const float2 naj = __ldg(aux + j);
+                if (have) force_feature_term(pxj, pvj, paj, xi, vi, pr2_i, p, acc, fa);
+                pxj = nxj;
+                pvj = nvj;
+                paj = naj;
+                have = true;
             });
+        if (have) force_feature_term(pxj, pvj, paj, xi, vi, pr2_i, p, acc, fa);
     } else {
         for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
             for (int j = lo; j < hi; ++j) {
@@ -865,7 +879,7 @@ __device__ __forceinline__ void force_features_single(const GridDev& g, const fl
 
 // per sorted particle k: feat[16 k ..] and sacc[2k] = (a, 0), sacc[2k+1] =
 // (dv, 0); per block: (sum of max(0, rho/rho0 - 1), active count)
-__global__ void __launch_bounds__(kSphThreads, 2) k_force_features(GridDev g, const float4* __restrict__ xs,
+__global__ void __launch_bounds__(kSphThreads, 3) k_force_features(GridDev g, const float4* __restrict__ xs,
                                                                    const float4* __restrict__ vs,
                                                                    const float2* __restrict__ aux,
                                                                    const float2* __restrict__ rp, int n,
@@ -1061,7 +1075,7 @@ struct nsph_sph {
     float* adj_rho = nullptr;            //   adj(rho)
     float* adj_bpart = nullptr;          //   per-block partial sums of adj(B)
     int adj_bcap = 0;                    //   entries of adj_bpart
-    cudaEvent_t eva[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // adjoint phases (timing)
+    cudaEvent_t eva[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // adjoint / surrogate phases
     float* sfeat = nullptr;              // surrogate scratch (nsph_sph_enable_surrogate), sorted: 16 features
     float4* sacc = nullptr;              //   (a, 0), (dv, 0)
     float* cpart = nullptr;              //   per-block (compression sum, active count)
@@ -1738,25 +1752,35 @@ extern "C" int nsph_sph_enable_surrogate(nsph_sph* s)
 }
 
 // grid build, density pass and feature pass into the sorted scratch
+// (with `mark`, records phase events 0-3 when phase timing is enabled:
+// start, built, after the density pass, after the feature pass)
 static int features_enqueue(nsph_sph* s, const nsph_sph_params* p, int n, const float* x_in, const float* v_in,
                             const float* mass, const float* inv_mass, const int* flags, const int* world,
-                            int world_count, cudaStream_t cs, int& launches, int& blocks)
+                            int world_count, cudaStream_t cs, int& launches, int& blocks, bool mark = false)
 {
     GatherArgs ga{x_in, v_in, mass, inv_mass, flags, world, world_count, s->xs, s->vs};
+    if (mark && s->eva[0]) NSPH_CUDA_TRY(record_mark(s->eva[0], cs));
     int st = grid_build(s->grid, x_in, n, p->cell_width, p->cell_inv, &ga, s->status, cs, &launches);
     if (st != NSPH_OK) return st;
     s->last_n = n;
     blocks = 0;
-    if (n == 0) return NSPH_OK;
-    const GridDev g = s->grid.view();
-    int threads;
-    pass_launch(s, n, false, blocks, threads);
-    k_density<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->mask, s->ncand, s->status);
-    NSPH_LAUNCH_CHECK("k_density");
-    k_force_features<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->mask, s->ncand, s->sfeat,
-                                                  s->sacc, s->cpart);
-    NSPH_LAUNCH_CHECK("k_force_features");
-    launches += 2;
+    if (mark && s->eva[1]) NSPH_CUDA_TRY(record_mark(s->eva[1], cs));
+    if (n > 0) {
+        const GridDev g = s->grid.view();
+        int threads;
+        pass_launch(s, n, false, blocks, threads);
+        k_density<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->mask, s->ncand,
+                                                   s->status);
+        NSPH_LAUNCH_CHECK("k_density");
+        if (mark && s->eva[2]) NSPH_CUDA_TRY(record_mark(s->eva[2], cs));
+        k_force_features<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->mask, s->ncand,
+                                                          s->sfeat, s->sacc, s->cpart);
+        NSPH_LAUNCH_CHECK("k_force_features");
+        launches += 2;
+    } else if (mark && s->eva[2]) {
+        NSPH_CUDA_TRY(record_mark(s->eva[2], cs));
+    }
+    if (mark && s->eva[3]) NSPH_CUDA_TRY(record_mark(s->eva[3], cs));
     return NSPH_OK;
 }
 
@@ -1819,7 +1843,8 @@ extern "C" int nsph_sph_step_surrogate(nsph_sph* s, const nsph_sph_params* p, co
     if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
     cudaStream_t cs = (cudaStream_t)stream;
     int launches = 0, blocks = 0;
-    st = features_enqueue(s, p, n, x_in, v_in, mass, inv_mass, flags, world, world_count, cs, launches, blocks);
+    st = features_enqueue(s, p, n, x_in, v_in, mass, inv_mass, flags, world, world_count, cs, launches, blocks,
+                          true);
     if (st != NSPH_OK) return st;
     if (n > 0) {
         k_compression_reduce<<<1, 256, 0, cs>>>(s->cpart, blocks, stats);
@@ -1832,6 +1857,19 @@ extern "C" int nsph_sph_step_surrogate(nsph_sph* s, const nsph_sph_params* p, co
         NSPH_LAUNCH_CHECK("k_surrogate");
         launches += 2;
     }
+    if (s->eva[4]) NSPH_CUDA_TRY(record_mark(s->eva[4], cs));
     s->last_launches = launches;
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_surrogate_phase_times(nsph_sph* s, float ms_out[4])
+{
+    clear_error();
+    if (!s || !ms_out) return fail(NSPH_ERR_INVALID_ARG, "null argument");
+    if (!s->eva[0]) return fail(NSPH_ERR_INVALID_ARG, "phase timing is not enabled");
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    NSPH_CUDA_TRY(cudaEventSynchronize(s->eva[4]));
+    for (int k = 0; k < 4; ++k) NSPH_CUDA_TRY(cudaEventElapsedTime(ms_out + k, s->eva[k], s->eva[k + 1]));
     return NSPH_OK;
 }

@@ -651,6 +651,15 @@ class SolverSPH(SolverBase):
                    "SolverSPH.adjoint_phase_times")
         return tuple(float(v) for v in ms)
 
+    def surrogate_phase_times(self) -> tuple[float, float, float, float]:
+        """(build, density, feature pass, MLP + integrate) milliseconds of the
+        last executed surrogate step; waits for it. Needs
+        :meth:`enable_phase_timing`."""
+        ms = (ctypes.c_float * 4)()
+        _lib.check(self._lib.nsph_sph_surrogate_phase_times(self._handle, ctypes.byref(ms)),
+                   "SolverSPH.surrogate_phase_times")
+        return tuple(float(v) for v in ms)
+
     def set_launch(self, threads: int = 0, blocks_per_sm: int = -1) -> None:
         """Launch shape of the density and force passes (see nsph_sph_set_launch)."""
         _lib.check(self._lib.nsph_sph_set_launch(self._handle, int(threads), int(blocks_per_sm)),

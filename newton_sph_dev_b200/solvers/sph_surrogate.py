@@ -31,6 +31,7 @@ dimensionless step dt c0 / h.
 from __future__ import annotations
 
 import math
+from pathlib import Path
 
 import numpy as np
 import torch
@@ -47,6 +48,9 @@ W1, B1, W2, B2, W3, B3 = 0, 1024, 1088, 5184, 5248, 5440
 N_PARAMS = 5443
 IN_MEAN, IN_INV_STD, OUT_MEAN, OUT_STD = 5448, 5464, 5480, 5484
 MODEL_FLOATS = 5488
+# weights trained by newton_sph_dev_b200.train_surrogate (defaults: 200
+# trajectories of 32,768 particles at spacing 0.01 m, dt 1e-4 s, 4 substeps)
+PRETRAINED = Path(__file__).resolve().parents[1] / "surrogate_weights.npz"
 
 
 def c0_squared(config: SPHConfig) -> float:
@@ -143,6 +147,11 @@ class SurrogateModel:
     def save(self, path) -> None:
         meta = {k: (v if isinstance(v, (int, float, str)) else str(v)) for k, v in self.meta.items()}
         np.savez(path, buf=self.buf.detach().cpu().numpy(), meta=np.array([repr(meta)]))
+
+    @classmethod
+    def pretrained(cls, device: str | torch.device = "cuda:0") -> "SurrogateModel":
+        """The weights shipped with the package (PRETRAINED)."""
+        return cls.load(PRETRAINED, device)
 
     @classmethod
     def load(cls, path, device: str | torch.device = "cuda:0") -> "SurrogateModel":
@@ -355,7 +364,7 @@ class SurrogateSPH:
     suspended by the fallback rule (see the module docstring)."""
 
     def __init__(self, solver: SolverSPH, model: SurrogateModel, substeps: int = 4, threshold: float = 0.01,
-                 window: int = 10, cooldown: int = 1):
+                 window: int = 10, cooldown: int = 1, graphs: bool = False):
         if solver.batched:
             raise ValueError("the surrogate needs a single-world solver")
         self.solver = solver
@@ -372,15 +381,16 @@ class SurrogateSPH:
         self.window_worst: list[float] = []
         self._window_mode = True
         self.acc_scale = accel_scale(solver.config)
+        self.graphs = bool(graphs)  # replay each (state_in, state_out, dt) surrogate step from a CUDA graph
+        self._graphs: dict = {}
+        self.launches_per_step = 0
 
     def step(self, state_in, state_out, dt: float) -> None:
         """Advance state_in by substeps x dt into state_out."""
         if self.calls % self.window == 0:
             self._window_mode = self.monitor.use_surrogate()
         if self._window_mode:
-            self.solver.step_surrogate_raw(state_in.particle_q, state_in.particle_qd, state_out.particle_q,
-                                           state_out.particle_qd, self.solver.step_params(self.substeps * dt),
-                                           self.model, self.acc_scale, self.stats)
+            self._surrogate_step(state_in, state_out, dt)
             self.surrogate_steps += 1
         else:
             n = self.solver.model.particle_count
@@ -396,6 +406,29 @@ class SurrogateSPH:
         self.calls += 1
         if self.calls % self.window == 0:
             self._end_window()
+
+    def _surrogate_call(self, state_in, state_out, dt):
+        self.solver.step_surrogate_raw(state_in.particle_q, state_in.particle_qd, state_out.particle_q,
+                                       state_out.particle_qd, self.solver.step_params(self.substeps * dt),
+                                       self.model, self.acc_scale, self.stats)
+
+    def _surrogate_step(self, state_in, state_out, dt):
+        if not self.graphs:
+            self._surrogate_call(state_in, state_out, dt)
+            self.launches_per_step = self.solver.last_launches
+            return
+        key = (state_in.particle_q.data_ptr(), state_in.particle_qd.data_ptr(), state_out.particle_q.data_ptr(),
+               state_out.particle_qd.data_ptr(), float(dt))
+        g = self._graphs.get(key)
+        if g is None:  # run eagerly this time, then capture for the next calls
+            self._surrogate_call(state_in, state_out, dt)
+            self.launches_per_step = self.solver.last_launches
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._surrogate_call(state_in, state_out, dt)
+            self._graphs[key] = g
+            return
+        g.replay()
 
     def _end_window(self) -> None:
         if self._window_mode:
