@@ -961,7 +961,27 @@ __global__ void k_compression_reduce(const float* __restrict__ cpart, int blocks
     }
 }
 
-// the MLP on the tensor cores, then integrate with a + da (dynamic particles)
+__device__ __forceinline__ void load_features(const float* __restrict__ feat, int k, int n, float (&f)[kFeat])
+{
+    if (k < n) {
+        const float4* fi = reinterpret_cast<const float4*>(feat + (size_t)k * kFeat);
+#pragma unroll
+        for (int j = 0; j < kFeat; j += 4) {
+            const float4 q4 = __ldg(fi + j / 4);
+            f[j] = q4.x;
+            f[j + 1] = q4.y;
+            f[j + 2] = q4.z;
+            f[j + 3] = q4.w;
+        }
+    } else {
+#pragma unroll
+        for (int j = 0; j < kFeat; ++j) f[j] = 0.f;
+    }
+}
+
+// the MLP on the tensor cores, then integrate with a + da (dynamic
+// particles). Loads are issued ahead of the MMA chain that hides them: the
+// current tile's integrate inputs and the next tile's features.
 __global__ void __launch_bounds__(kMlpTile, 1) k_surrogate(const float* __restrict__ model, float acc_scale,
                                                            GridDev g, const float4* __restrict__ xs,
                                                            const float4* __restrict__ vs,
@@ -976,38 +996,30 @@ __global__ void __launch_bounds__(kMlpTile, 1) k_surrogate(const float* __restri
     uint32_t phase = 0;
     bool ok = true;
     const int tiles = (n + kMlpTile - 1) / kMlpTile;
+    float f[kFeat];
+    load_features(feat, (int)blockIdx.x * kMlpTile + (int)threadIdx.x, n, f);
     for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
         const int k = t * kMlpTile + threadIdx.x;
-        float f[kFeat];
-        if (k < n) {
-            const float4* fi = reinterpret_cast<const float4*>(feat + (size_t)k * kFeat);
-#pragma unroll
-            for (int j = 0; j < kFeat; j += 4) {
-                const float4 q4 = fi[j / 4];
-                f[j] = q4.x;
-                f[j + 1] = q4.y;
-                f[j + 2] = q4.z;
-                f[j + 3] = q4.w;
-            }
-        } else {
-#pragma unroll
-            for (int j = 0; j < kFeat; ++j) f[j] = 0.f;
-        }
         mlp_stage_input(s, f);
         mlp_sync();
+        // in flight during the MMA chain
+        const int kk = k < n ? k : 0;
+        const float4 xi = __ldg(xs + kk), vi = __ldg(vs + kk);
+        const float4 a = __ldg(sacc + 2 * (size_t)kk), dv = __ldg(sacc + 2 * (size_t)kk + 1);
+        const float2 rpk = __ldg(rp + kk);
+        const int ik = __ldg(g.ids + kk);
+        load_features(feat, k + (int)gridDim.x * kMlpTile, n, f);
         float y[kMlpOut];
         ok = mlp_forward_tile(s, tmem, 0, 64, 0, phase, y);
         if (ok && k < n) {
-            const float4 xi = xs[k], vi = vs[k];
             const int attr = __float_as_int(vi.w);
-            const float4 a = sacc[2 * (size_t)k], dv = sacc[2 * (size_t)k + 1];
             ForceAcc acc{a.x, a.y, a.z, dv.x, dv.y, dv.z};
             if (attr & kAttrDynamic) {
                 acc.ax = __fadd_rn(acc.ax, acc_scale * mlp_denorm(s, y, 0));
                 acc.ay = __fadd_rn(acc.ay, acc_scale * mlp_denorm(s, y, 1));
                 acc.az = __fadd_rn(acc.az, acc_scale * mlp_denorm(s, y, 2));
             }
-            integrate_out((size_t)g.ids[k], xi, vi, attr, rp[k], acc, p, p.dt, o);
+            integrate_out((size_t)ik, xi, vi, attr, rpk, acc, p, p.dt, o);
         }
         __syncthreads();
     }
