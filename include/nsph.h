@@ -293,6 +293,43 @@ NSPH_API int nsph_sph_rollout_adjoint(nsph_sph* solver, const nsph_sph_params* p
                                       const float* gravity, int world_count,
                                       float* x_adj, float* v_adj, float* f_ext_adj, float* eos_b_adj, void* stream);
 
+/* ---- particle-particle contact on the HashGrid ------------------------------
+ * The reference's other consumers of the grid, rebuilt on nsph_grid (same
+ * query: the candidates of hash_grid_query(grid, x_i, r_i + max_radius +
+ * cohesion) in Warp's order; one thread per grid point in sorted order).
+ * `grid` must have been built on x (n == its point count), with a cell
+ * width covering the query radius (the reference builds it with
+ * 2 max_radius + cohesion, solver_xpbd.py:315-319).
+ *
+ * nsph_particle_contact_forces replaces eval_particle_contact
+ *   (newton/_src/solvers/semi_implicit/kernels_contact.py:35-84 with
+ *   particle_force :11-32, launched by eval_particle_contact_forces
+ *   :559-579): for every active particle i, f_out[i] = the sum over active
+ *   j != i with err = |x_i - x_j| - r_i - r_j <= cohesion of the normal
+ *   force err k_contact + min(v_rel.n, 0) k_damp along -n and the Coulomb
+ *   friction min(|v_t| k_friction, mu |f_n|) along -v_t/|v_t|. Inactive
+ *   particles' f_out rows are not written.
+ * nsph_particle_contact_deltas replaces solve_particle_particle_contacts
+ *   (newton/_src/solvers/xpbd/kernels.py:225-289, launched at
+ *   solver_xpbd.py:420-440): adds the XPBD position correction of every
+ *   active particle to deltas[i] (one writer per particle, no atomics).
+ * Every fp32 operation is rounded as written (no contraction). */
+typedef struct nsph_contact_params {
+    float k_contact;   /* Model.particle_ke */
+    float k_damp;      /* Model.particle_kd */
+    float k_friction;  /* Model.particle_kf */
+    float k_mu;        /* Model.particle_mu */
+    float k_cohesion;  /* Model.particle_cohesion */
+    float max_radius;  /* Model.particle_max_radius */
+} nsph_contact_params;
+NSPH_API int nsph_particle_contact_forces(const nsph_grid* grid, const nsph_contact_params* params, int n,
+                                          const float* x, const float* v, const float* radius, const int* flags,
+                                          float* f_out, void* stream);
+NSPH_API int nsph_particle_contact_deltas(const nsph_grid* grid, int n, const float* x, const float* v,
+                                          const float* inv_mass, const float* radius, const int* flags, float k_mu,
+                                          float k_cohesion, float max_radius, float dt, float relaxation,
+                                          float* deltas, void* stream);
+
 /* ---- learned surrogate step (no counterpart in the reference) -------------
  * A WCSPH step with a larger dt whose acceleration is corrected per particle
  * by a small MLP (16 -> 64 -> 64 -> 3, SiLU; bf16 weights and activations,

@@ -72,6 +72,19 @@ class NsphSphParams(ctypes.Structure):
     ]
 
 
+class NsphContactParams(ctypes.Structure):
+    """Layout of nsph_contact_params (include/nsph.h)."""
+
+    _fields_ = [
+        ("k_contact", ctypes.c_float),
+        ("k_damp", ctypes.c_float),
+        ("k_friction", ctypes.c_float),
+        ("k_mu", ctypes.c_float),
+        ("k_cohesion", ctypes.c_float),
+        ("max_radius", ctypes.c_float),
+    ]
+
+
 # (name, restype, argtypes) of every exported entry point, in header order.
 SIGNATURES = [
     ("nsph_version", ctypes.c_int, []),
@@ -142,6 +155,16 @@ SIGNATURES = [
         + [ctypes.c_int]
         + [c_void_p] * 4
         + [c_void_p],
+    ),
+    (
+        "nsph_particle_contact_forces",
+        ctypes.c_int,
+        [c_void_p, ctypes.POINTER(NsphContactParams), ctypes.c_int] + [c_void_p] * 5 + [c_void_p],
+    ),
+    (
+        "nsph_particle_contact_deltas",
+        ctypes.c_int,
+        [c_void_p, ctypes.c_int] + [c_void_p] * 5 + [ctypes.c_float] * 5 + [c_void_p, c_void_p],
     ),
     ("nsph_sph_enable_surrogate", ctypes.c_int, [c_void_p]),
     (

@@ -495,9 +495,6 @@ int grid_build(Grid& g, const float* points, int n, float cell_width, float cell
 // ==========================================================================
 // C ABI: HashGrid
 // ==========================================================================
-struct nsph_grid {
-    nsph::Grid g;
-};
 
 using namespace nsph;
 

@@ -248,3 +248,8 @@ int grid_build(Grid& g, const float* points, int n, float cell_width, float cell
                unsigned int* status, cudaStream_t stream, int* launches = nullptr, const int* world = nullptr);
 
 }  // namespace nsph
+
+// the opaque handle of the nsph_grid_* C ABI (a HashGrid object)
+struct nsph_grid {
+    nsph::Grid g;
+};

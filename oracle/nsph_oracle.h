@@ -107,6 +107,17 @@ int oracle_adj_vjp_f64(const oracle_phys_f64* ph, int n, const double* x, const 
                        const double* gravity, int world_count, const double* x_out_adj, const double* v_out_adj,
                        const double* rho_out_adj, double* x_adj, double* v_adj, double* f_adj, double* b_adj);
 
+/* ---- particle-particle contact (contact.c), fp32 ------------------------
+ * The grid is built on x with cell width grid_radius (HashGrid.build(x,
+ * grid_radius)) and dims; f_out rows of inactive particles are not written;
+ * deltas are accumulated (+=). */
+int oracle_particle_contact_forces(const nsph_contact_params* p, float grid_radius, const int* dims, int n,
+                                   const float* x, const float* v, const float* radius, const int* flags,
+                                   float* f_out);
+int oracle_particle_contact_deltas(float grid_radius, const int* dims, int n, const float* x, const float* v,
+                                   const float* inv_mass, const float* radius, const int* flags, float k_mu,
+                                   float k_cohesion, float max_radius, float dt, float relaxation, float* deltas);
+
 /* Number of OpenMP threads the oracle uses (0 = OpenMP default). */
 void oracle_set_threads(int n);
 int  oracle_get_threads(void);

@@ -142,6 +142,12 @@ def lib() -> ctypes.CDLL:
     L.oracle_adj_vjp_f64.restype = ctypes.c_int
     L.oracle_adj_vjp_f64.argtypes = [ctypes.POINTER(Phys64), ctypes.c_int] + [ctypes.c_void_p] * 8 + \
         [ctypes.c_int] + [ctypes.c_void_p] * 7
+    L.oracle_particle_contact_forces.restype = ctypes.c_int
+    L.oracle_particle_contact_forces.argtypes = [ctypes.c_void_p, ctypes.c_float, _i32p, ctypes.c_int] + \
+        [ctypes.c_void_p] * 5
+    L.oracle_particle_contact_deltas.restype = ctypes.c_int
+    L.oracle_particle_contact_deltas.argtypes = [ctypes.c_float, _i32p, ctypes.c_int] + [ctypes.c_void_p] * 5 + \
+        [ctypes.c_float] * 5 + [ctypes.c_void_p]
     L.oracle_set_threads.restype = None
     L.oracle_set_threads.argtypes = [ctypes.c_int]
     L.oracle_get_threads.restype = ctypes.c_int
@@ -480,6 +486,46 @@ def surrogate_features_py(consts: dict, dims, x, v, mass, flags):
     f[:, 15] = np.linalg.norm(f[:, 8:11], axis=1)
     f[~act] = 0.0
     return f, rho, a, dv
+
+
+# ---------------------------------------------------------------------------
+# particle-particle contact (contact.c)
+# ---------------------------------------------------------------------------
+class ContactParams(ctypes.Structure):
+    """Layout of nsph_contact_params (include/nsph.h)."""
+
+    _fields_ = [(k, ctypes.c_float) for k in ("k_contact", "k_damp", "k_friction", "k_mu", "k_cohesion",
+                                              "max_radius")]
+
+
+def particle_contact_forces(x, v, radius, flags, grid_radius: float, dims, k_contact, k_damp, k_friction, k_mu,
+                            k_cohesion, max_radius, f_init=None):
+    """eval_particle_contact restated (fp32): forces (n, 3); rows of inactive
+    particles keep f_init (zeros by default)."""
+    x, v, r, fl = _f32(x), _f32(v), _f32(radius), _i32(flags)
+    n = x.shape[0]
+    f = np.array(f_init if f_init is not None else np.zeros((n, 3)), dtype=np.float32)
+    p = ContactParams(*[float(np.float32(t)) for t in (k_contact, k_damp, k_friction, k_mu, k_cohesion, max_radius)])
+    st = lib().oracle_particle_contact_forces(ctypes.byref(p), float(np.float32(grid_radius)), _i32(dims), n, _p(x),
+                                              _p(v), _p(r), _p(fl), _p(f))
+    if st != 0:
+        raise RuntimeError(f"oracle_particle_contact_forces status {st}")
+    return f
+
+
+def particle_contact_deltas(x, v, inv_mass, radius, flags, grid_radius: float, dims, k_mu, k_cohesion, max_radius,
+                            dt, relaxation, deltas_init=None):
+    """solve_particle_particle_contacts restated (fp32): deltas_init + corrections."""
+    x, v, w, r, fl = _f32(x), _f32(v), _f32(inv_mass), _f32(radius), _i32(flags)
+    n = x.shape[0]
+    d = np.array(deltas_init if deltas_init is not None else np.zeros((n, 3)), dtype=np.float32)
+    st = lib().oracle_particle_contact_deltas(float(np.float32(grid_radius)), _i32(dims), n, _p(x), _p(v), _p(w),
+                                              _p(r), _p(fl), *[float(np.float32(t)) for t in
+                                                               (k_mu, k_cohesion, max_radius, dt, relaxation)],
+                                              _p(d))
+    if st != 0:
+        raise RuntimeError(f"oracle_particle_contact_deltas status {st}")
+    return d
 
 
 # ---------------------------------------------------------------------------

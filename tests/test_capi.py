@@ -67,7 +67,8 @@ def _c_layout(struct: str, fields: list[str]) -> list[int]:
     return [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
 
 
-@pytest.mark.parametrize("pyname,cname", [("NsphSphParams", "nsph_sph_params"), ("NsphGridView", "nsph_grid_view")])
+@pytest.mark.parametrize("pyname,cname", [("NsphSphParams", "nsph_sph_params"), ("NsphGridView", "nsph_grid_view"),
+                                          ("NsphContactParams", "nsph_contact_params")])
 def test_struct_layouts_match_header(pyname, cname):
     from newton_sph_dev_b200 import _lib
 
