@@ -75,8 +75,9 @@ def test_contact_deltas_bit_exact(oracle_mod):
     T = lambda a: torch.from_numpy(a).to(DEV)
     d = T(init.copy())
     L = _lib.load()
-    st = L.nsph_particle_contact_deltas(g.id, n, T(x).data_ptr(), T(v).data_ptr(), T(w).data_ptr(), T(r).data_ptr(),
-                                        T(flags).data_ptr(), 0.5, cohesion, rmax, dt, relax, d.data_ptr(),
+    xt, vt, wt, rt, ft = T(x), T(v), T(w), T(r), T(flags)  # kept alive across the launch
+    st = L.nsph_particle_contact_deltas(g.id, n, xt.data_ptr(), vt.data_ptr(), wt.data_ptr(), rt.data_ptr(),
+                                        ft.data_ptr(), 0.5, cohesion, rmax, dt, relax, d.data_ptr(),
                                         _lib.stream_handle(torch.device(DEV)))
     assert st == 0
     torch.cuda.synchronize()
