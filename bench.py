@@ -64,6 +64,11 @@ WORKLOADS = {
                               desc="learned surrogate on the 1,048,576-particle tank: one step of 4 x 5e-5 s with "
                                    "the MLP acceleration correction (tcgen05) per call, plain steps as fallback when "
                                    "the window's mean compression error exceeds 1%"),
+    "contact_1m": dict(shape=(128, 128, 64), spacing=0.0095, radius=0.005, vel_std=0.1, contact=True,
+                       metric="particle-steps/s",
+                       desc="particle-particle contact (eval_particle_contact): 1,048,576 spheres of radius 0.005 m "
+                            "on a jittered 0.0095 m lattice (touching neighbours), v ~ N(0, 0.1 m/s); one step = "
+                            "HashGrid build at 2 r_max + cohesion + contact forces"),
     "worlds_4096": dict(worlds=4096, n_range=(256, 16384), s_range=(0.004, 0.01), box=(0.5, 0.5, 0.5), dt=1e-4,
                         vel_std=0.0, seed=3,
                         desc="4,096 independent scenes: particles log-uniform in [256, 16384], spacing uniform in "
@@ -988,6 +993,186 @@ def run_surrogate(args):
     return 0
 
 
+# ---------------------------------------------------------------------------
+# particle-particle contact (the reference's semi-implicit contact forces)
+# ---------------------------------------------------------------------------
+B_ALG_CONTACT = 12 + 12 + 4 + 4 + 12  # read x, v, radius, flags; write f
+
+
+def make_contact_scene(w, device):
+    import newton_sph_dev_b200 as nsph
+    import torch
+
+    s = w["spacing"]
+    b = nsph.ModelBuilder()
+    b.add_particle_grid(pos=(s / 2, s / 2, s / 2), rot=(0, 0, 0, 1), vel=(0, 0, 0), dim_x=w["shape"][0],
+                        dim_y=w["shape"][1], dim_z=w["shape"][2], cell_x=s, cell_y=s, cell_z=s, mass=1.0,
+                        jitter=0.2 * s, radius_mean=w["radius"])
+    model = b.finalize(device)
+    rng = np.random.default_rng(seed=2)
+    model.particle_qd.copy_(torch.from_numpy(rng.normal(0.0, w["vel_std"], (model.particle_count, 3))
+                                             .astype(np.float32)))
+    model.particle_cohesion = 0.0
+    return model
+
+
+def run_contact(args):
+    import torch
+
+    from newton_sph_dev_b200.contacts import eval_particle_contact_forces
+
+    world, rank, local = dist_env()
+    if world > 1:
+        raise SystemExit("contact_1m runs on one GPU (replicas are not wired for it)")
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    w = WORKLOADS[args.workload]
+    model = make_contact_scene(w, str(device))
+    n = model.particle_count
+    state = model.state()
+    f = torch.zeros_like(state.particle_q)
+    gr = 2.0 * model.particle_max_radius + model.particle_cohesion
+    grid = model.particle_grid
+    stream = torch.cuda.current_stream(device)
+
+    def step():
+        grid.build(state.particle_q, gr)
+        eval_particle_contact_forces(model, state, f)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        step()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    total = build_ms = 0.0
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            ev[0].record(stream)
+            grid.build(state.particle_q, gr)
+            ev[1].record(stream)
+            eval_particle_contact_forces(model, state, f)
+            ev[2].record(stream)
+            ev[2].synchronize()
+            build_ms += ev[0].elapsed_time(ev[1])
+            total += ev[0].elapsed_time(ev[2])
+    # graph-replayed steps (the same work, one launch sequence)
+    gtotal = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        ev[0].record(stream)
+        g.replay()
+        ev[2].record(stream)
+        ev[2].synchronize()
+        gtotal += ev[0].elapsed_time(ev[2])
+    del g
+    best = min(total, gtotal)
+    value = n * args.steps / (best * 1e-3)
+    t_contact = (total - build_ms) / args.steps * 1e-3
+    peak, peak_kind = load_peak()
+    ach = B_ALG_CONTACT * n / t_contact / 1e9
+    roofline = {"bound": "hbm", "kernel": "k_contact_forces", "achieved": ach, "peak": peak, "peak_kind": peak_kind,
+                "unit": "GB/s", "frac": ach / peak, "traffic": None, "alg_bytes_per_launch": B_ALG_CONTACT * n,
+                "ms_per_launch": t_contact * 1e3}
+    # end to end: host positions and velocities in, forces out
+    hx, hv = state.particle_q.cpu().pin_memory(), state.particle_qd.cpu().pin_memory()
+    hf = torch.empty_like(hx).pin_memory()
+    e2e_steps = min(args.steps, 50)
+    e2e = 0.0
+    for _ in range(e2e_steps):
+        ev[0].record(stream)
+        state.particle_q.copy_(hx, non_blocking=True)
+        state.particle_qd.copy_(hv, non_blocking=True)
+        step()
+        hf.copy_(f, non_blocking=True)
+        ev[2].record(stream)
+        ev[2].synchronize()
+        e2e += ev[0].elapsed_time(ev[2])
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+
+        O.build()
+        m = model
+        xs, vs = state.particle_q.cpu().numpy(), state.particle_qd.cpu().numpy()
+        rr, fl = m.particle_radius.cpu().numpy(), m.particle_flags.cpu().numpy()
+        t0 = time.perf_counter()
+        reps = 0
+        while True:
+            O.particle_contact_forces(xs, vs, rr, fl, float(np.float32(gr)), (128, 128, 128), m.particle_ke,
+                                      m.particle_kd, m.particle_kf, m.particle_mu, m.particle_cohesion,
+                                      m.particle_max_radius)
+            reps += 1
+            el = time.perf_counter() - t0
+            if el > 10.0 or reps >= 20:
+                break
+        cpu = {"value": n * reps / el, "unit": METRIC, "cores": O.get_threads(), "kind": "port",
+               "sample": f"{reps} steps (grid build + contact forces) of the full scene in {el:.1f} s "
+                         "(fp32 restatement of eval_particle_contact, OpenMP)"}
+    clocks = clk.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": best / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "particles": n, "desc": w["desc"], "grid_dims": [128, 128, 128],
+                   "graph": gtotal <= total,
+                   "l2": "flushed (256 MiB write) before every timed step, outside the timed interval"},
+        "phase_ms_per_step": {"build": build_ms / args.steps, "contact": t_contact * 1e3},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": {"value": n * e2e_steps / (e2e * 1e-3), "unit": METRIC, "h2d_bytes_per_step": 24 * n,
+                "d2h_bytes_per_step": 12 * n, "steps": e2e_steps},
+        "gpu_launches": (grid.last_launches + 1) * args.steps,
+        "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_contact_reference(args):
+    """The fp32 CPU restatement of eval_particle_contact (with its grid
+    build) on the same scene, all host threads."""
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import oracle as O
+
+    w = WORKLOADS[args.workload]
+    model = make_contact_scene(w, "cpu")
+    n = model.particle_count
+    O.build()
+    xs, vs = model.particle_q.numpy(), model.particle_qd.numpy()
+    rr, fl = model.particle_radius.numpy(), model.particle_flags.numpy()
+    gr = float(np.float32(2.0 * model.particle_max_radius + model.particle_cohesion))
+
+    def step():
+        O.particle_contact_forces(xs, vs, rr, fl, gr, (128, 128, 128), model.particle_ke, model.particle_kd,
+                                  model.particle_kf, model.particle_mu, model.particle_cohesion,
+                                  model.particle_max_radius)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    el = time.perf_counter() - t0
+    value = n * args.steps / el
+    threads = O.get_threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "particles": n, "desc": w["desc"]},
+        "cpu_baseline": {"value": value, "unit": METRIC, "cores": threads, "kind": "port",
+                         "sample": f"{args.steps} full steps (grid build + contact forces, fp32 restatement, OpenMP)"},
+        "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -1003,9 +1188,13 @@ def main(argv=None):
         ap.error("--warmup must be >= 3")
     grad = "grad" in WORKLOADS[args.workload]
     if args.impl == "reference":
+        if "contact" in WORKLOADS[args.workload]:
+            return run_contact_reference(args)
         return run_grad_reference(args) if grad else run_reference(args)
     if "surrogate" in WORKLOADS[args.workload]:
         return run_surrogate(args)
+    if "contact" in WORKLOADS[args.workload]:
+        return run_contact(args)
     return run_grad(args) if grad else run_gpu(args)
 
 

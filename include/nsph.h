@@ -105,6 +105,8 @@ typedef struct nsph_grid_view {
     int   built;
 } nsph_grid_view;
 NSPH_API int nsph_grid_get_view(const nsph_grid* grid, nsph_grid_view* view);
+/* Number of kernels the last nsph_grid_build launched. */
+NSPH_API int nsph_grid_last_launches(const nsph_grid* grid);
 
 /* Batched hash_grid_query(grid, pos, radius) + hash_grid_query_next:
  * enumerate, for each of num_queries positions (device, num_queries x 3

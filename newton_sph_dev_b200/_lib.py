@@ -95,6 +95,7 @@ SIGNATURES = [
     ("nsph_grid_reserve", ctypes.c_int, [c_void_p, ctypes.c_int]),
     ("nsph_grid_build", ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_float, c_void_p]),
     ("nsph_grid_get_view", ctypes.c_int, [c_void_p, ctypes.POINTER(NsphGridView)]),
+    ("nsph_grid_last_launches", ctypes.c_int, [c_void_p]),
     ("nsph_grid_query", ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_float, c_void_p, c_void_p, c_void_p, c_void_p]),
     (
         "nsph_grid_build_noalloc",

@@ -539,8 +539,14 @@ extern "C" int nsph_grid_build(nsph_grid* grid, const float* points, int num_poi
     DeviceGuard guard(grid->g.device);
     if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
     const float inv = 1.0f / radius;
-    return grid_build(grid->g, points, num_points, radius, inv, nullptr, nullptr, (cudaStream_t)stream);
+    int launches = 0;
+    const int st = grid_build(grid->g, points, num_points, radius, inv, nullptr, nullptr, (cudaStream_t)stream,
+                              &launches);
+    grid->g.last_launches = launches;
+    return st;
 }
+
+extern "C" int nsph_grid_last_launches(const nsph_grid* grid) { return grid ? grid->g.last_launches : 0; }
 
 extern "C" int nsph_grid_get_view(const nsph_grid* grid, nsph_grid_view* view)
 {

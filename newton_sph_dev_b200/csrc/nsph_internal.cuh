@@ -198,6 +198,7 @@ struct Grid {
     int key_bits = 0;
     int capacity = 0;
     int num_points = 0;   // points of the last build
+    int last_launches = 0;  // kernels launched by the last nsph_grid_build
     int built = 0;
     float cell_width = 0.f;
     float cell_inv = 0.f;

@@ -93,6 +93,11 @@ class HashGrid:
                                        _lib.stream_handle(self.device))
         _lib.check(st, "HashGrid.build")
 
+    @property
+    def last_launches(self) -> int:
+        """Kernels launched by the last build."""
+        return int(self._lib.nsph_grid_last_launches(self._handle))
+
     # ---- host-visible views for tests and consumers --------------------
     def _view(self) -> _lib.NsphGridView:
         v = _lib.NsphGridView()
