@@ -996,7 +996,7 @@ def run_surrogate(args):
 # ---------------------------------------------------------------------------
 # particle-particle contact (the reference's semi-implicit contact forces)
 # ---------------------------------------------------------------------------
-B_ALG_CONTACT = 12 + 12 + 4 + 4 + 12  # read x, v, radius, flags; write f
+B_ALG_CONTACT = 12 + 12 + 4 + 4 + 12  # read x, v, radius, flags; write f (the sorted mirrors are scratch)
 
 
 def make_contact_scene(w, device):
@@ -1124,7 +1124,7 @@ def run_contact(args):
         "cpu_baseline": cpu,
         "e2e": {"value": n * e2e_steps / (e2e * 1e-3), "unit": METRIC, "h2d_bytes_per_step": 24 * n,
                 "d2h_bytes_per_step": 12 * n, "steps": e2e_steps},
-        "gpu_launches": (grid.last_launches + 1) * args.steps,
+        "gpu_launches": (grid.last_launches + 2) * args.steps,  # grid build + mirror gather + contact
         "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
     }
     print(json.dumps(line), flush=True)

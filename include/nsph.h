@@ -315,7 +315,10 @@ NSPH_API int nsph_sph_rollout_adjoint(nsph_sph* solver, const nsph_sph_params* p
  *   (newton/_src/solvers/xpbd/kernels.py:225-289, launched at
  *   solver_xpbd.py:420-440): adds the XPBD position correction of every
  *   active particle to deltas[i] (one writer per particle, no atomics).
- * Every fp32 operation is rounded as written (no contraction). */
+ * Every fp32 operation is rounded as written (no contraction). Both calls
+ * first copy the particles into sorted mirrors owned by the grid (32 bytes
+ * per point, allocated by nsph_grid_reserve), then run the contact kernel:
+ * two launches, no allocation. */
 typedef struct nsph_contact_params {
     float k_contact;   /* Model.particle_ke */
     float k_damp;      /* Model.particle_kd */

@@ -13,7 +13,11 @@
 // One thread per grid point, taken in sorted order (the reference's
 // hash_grid_point_id(grid, tid)); each particle gathers over the candidates
 // of hash_grid_query(grid, x_i, r_i + max_radius + cohesion) in Warp's
-// iteration order. Every fp32 operation is an explicit round-to-nearest
+// iteration order. A first kernel copies the particles into sorted float4
+// mirrors held by the grid object, m0 = (x, r) and m1 = (v, inverse mass),
+// so that the candidates of a cell run are read contiguously; an inactive
+// particle's radius slot holds -inf (radii of active particles are
+// finite). Every fp32 operation is an explicit round-to-nearest
 // intrinsic in the order the reference's expressions are written (dot
 // products ((x + y) + z), no contraction), so the CPU restatement reproduces
 // the results bit for bit.
@@ -51,76 +55,91 @@ __device__ __forceinline__ void particle_force(float nx, float ny, float nz, flo
     fz = __fsub_rn(__fmul_rn(-nz, fn), __fmul_rn(tz, ft));
 }
 
-__global__ void k_contact_forces(GridDev g, int n, const float* __restrict__ x, const float* __restrict__ v,
-                                 const float* __restrict__ radius, const int* __restrict__ flags,
+__device__ __forceinline__ bool mirror_active(float4 m0) { return m0.w != -INFINITY; }
+
+// sorted mirrors: m0[k] = (x, r or -inf if inactive), m1[k] = (v, inverse mass or 0)
+__global__ void k_contact_gather(const int* __restrict__ ids, int n, const float* __restrict__ x,
+                                 const float* __restrict__ v, const float* __restrict__ radius,
+                                 const int* __restrict__ flags, const float* __restrict__ inv_mass,
+                                 float4* __restrict__ m0, float4* __restrict__ m1)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const size_t i = (size_t)ids[k];
+    const bool active = (flags[i] & NSPH_PARTICLE_ACTIVE) != 0;
+    m0[k] = make_float4(x[3 * i], x[3 * i + 1], x[3 * i + 2], active ? radius[i] : -INFINITY);
+    m1[k] = make_float4(v[3 * i], v[3 * i + 1], v[3 * i + 2], inv_mass ? inv_mass[i] : 0.f);
+}
+
+__global__ void k_contact_forces(GridDev g, int n, const float4* __restrict__ m0, const float4* __restrict__ m1,
                                  const nsph_contact_params p, float* __restrict__ f_out)
 {
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= n) return;
-    const int i = g.ids[tid];
-    if (!(flags[i] & NSPH_PARTICLE_ACTIVE)) return;
-    const float xi = x[3 * (size_t)i], yi = x[3 * (size_t)i + 1], zi = x[3 * (size_t)i + 2];
-    const float vxi = v[3 * (size_t)i], vyi = v[3 * (size_t)i + 1], vzi = v[3 * (size_t)i + 2];
-    const float ri = radius[i];
+    const int kk = blockIdx.x * blockDim.x + threadIdx.x;
+    if (kk >= n) return;
+    const float4 a = m0[kk];
+    if (!mirror_active(a)) return;
+    const float4 va = m1[kk];
+    const float ri = a.w;
     const float qr = __fadd_rn(__fadd_rn(ri, p.max_radius), p.k_cohesion);
     float fx = 0.f, fy = 0.f, fz = 0.f;
-    for_each_candidate(g, xi, yi, zi, qr, [&](int k) {
-        const int j = g.ids[k];
-        if (!(flags[j] & NSPH_PARTICLE_ACTIVE) || j == i) return;
-        float nx = __fsub_rn(xi, x[3 * (size_t)j]);
-        float ny = __fsub_rn(yi, x[3 * (size_t)j + 1]);
-        float nz = __fsub_rn(zi, x[3 * (size_t)j + 2]);
+    for_each_candidate(g, a.x, a.y, a.z, qr, [&](int k) {
+        const float4 b = __ldg(m0 + k);
+        if (!mirror_active(b) || k == kk) return;
+        float nx = __fsub_rn(a.x, b.x);
+        float ny = __fsub_rn(a.y, b.y);
+        float nz = __fsub_rn(a.z, b.z);
         const float d = __fsqrt_rn(dot3(nx, ny, nz, nx, ny, nz));
-        const float err = __fsub_rn(__fsub_rn(d, ri), radius[j]);
+        const float err = __fsub_rn(__fsub_rn(d, ri), b.w);
         if (err <= p.k_cohesion) {
+            const float4 vb = __ldg(m1 + k);
             nx = __fdiv_rn(nx, d);
             ny = __fdiv_rn(ny, d);
             nz = __fdiv_rn(nz, d);
             float cx, cy, cz;
-            particle_force(nx, ny, nz, __fsub_rn(vxi, v[3 * (size_t)j]), __fsub_rn(vyi, v[3 * (size_t)j + 1]),
-                           __fsub_rn(vzi, v[3 * (size_t)j + 2]), err, p, cx, cy, cz);
+            particle_force(nx, ny, nz, __fsub_rn(va.x, vb.x), __fsub_rn(va.y, vb.y), __fsub_rn(va.z, vb.z), err, p,
+                           cx, cy, cz);
             fx = __fadd_rn(fx, cx);
             fy = __fadd_rn(fy, cy);
             fz = __fadd_rn(fz, cz);
         }
     });
-    f_out[3 * (size_t)i] = fx;
-    f_out[3 * (size_t)i + 1] = fy;
-    f_out[3 * (size_t)i + 2] = fz;
+    const size_t i = (size_t)g.ids[kk];
+    f_out[3 * i] = fx;
+    f_out[3 * i + 1] = fy;
+    f_out[3 * i + 2] = fz;
 }
 
 // solve_particle_particle_contacts (xpbd/kernels.py:225-289)
-__global__ void k_contact_deltas(GridDev g, int n, const float* __restrict__ x, const float* __restrict__ v,
-                                 const float* __restrict__ inv_mass, const float* __restrict__ radius,
-                                 const int* __restrict__ flags, float k_mu, float k_cohesion, float max_radius,
-                                 float dt, float relaxation, float* __restrict__ deltas)
+__global__ void k_contact_deltas(GridDev g, int n, const float4* __restrict__ m0, const float4* __restrict__ m1,
+                                 float k_mu, float k_cohesion, float max_radius, float dt, float relaxation,
+                                 float* __restrict__ deltas)
 {
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= n) return;
-    const int i = g.ids[tid];
-    if (!(flags[i] & NSPH_PARTICLE_ACTIVE)) return;
-    const float xi = x[3 * (size_t)i], yi = x[3 * (size_t)i + 1], zi = x[3 * (size_t)i + 2];
-    const float vxi = v[3 * (size_t)i], vyi = v[3 * (size_t)i + 1], vzi = v[3 * (size_t)i + 2];
-    const float ri = radius[i];
-    const float w1 = inv_mass[i];
+    const int kk = blockIdx.x * blockDim.x + threadIdx.x;
+    if (kk >= n) return;
+    const float4 a = m0[kk];
+    if (!mirror_active(a)) return;
+    const float4 va = m1[kk];
+    const float ri = a.w;
+    const float w1 = va.w;
     const float qr = __fadd_rn(__fadd_rn(ri, max_radius), k_cohesion);
     float dx = 0.f, dy = 0.f, dz = 0.f;
-    for_each_candidate(g, xi, yi, zi, qr, [&](int k) {
-        const int j = g.ids[k];
-        if (!(flags[j] & NSPH_PARTICLE_ACTIVE) || j == i) return;
-        float nx = __fsub_rn(xi, x[3 * (size_t)j]);
-        float ny = __fsub_rn(yi, x[3 * (size_t)j + 1]);
-        float nz = __fsub_rn(zi, x[3 * (size_t)j + 2]);
+    for_each_candidate(g, a.x, a.y, a.z, qr, [&](int k) {
+        const float4 b = __ldg(m0 + k);
+        if (!mirror_active(b) || k == kk) return;
+        float nx = __fsub_rn(a.x, b.x);
+        float ny = __fsub_rn(a.y, b.y);
+        float nz = __fsub_rn(a.z, b.z);
         const float d = __fsqrt_rn(dot3(nx, ny, nz, nx, ny, nz));
-        const float err = __fsub_rn(__fsub_rn(d, ri), radius[j]);
-        const float denom = __fadd_rn(w1, inv_mass[j]);
+        const float err = __fsub_rn(__fsub_rn(d, ri), b.w);
+        const float4 vb = __ldg(m1 + k);
+        const float denom = __fadd_rn(w1, vb.w);
         if (err <= k_cohesion && denom > 0.f) {
             nx = __fdiv_rn(nx, d);
             ny = __fdiv_rn(ny, d);
             nz = __fdiv_rn(nz, d);
-            const float rx = __fsub_rn(vxi, v[3 * (size_t)j]);
-            const float ry = __fsub_rn(vyi, v[3 * (size_t)j + 1]);
-            const float rz = __fsub_rn(vzi, v[3 * (size_t)j + 2]);
+            const float rx = __fsub_rn(va.x, vb.x);
+            const float ry = __fsub_rn(va.y, vb.y);
+            const float rz = __fsub_rn(va.z, vb.z);
             // normal
             const float lambda_n = err;
             const float dnx = __fmul_rn(nx, lambda_n), dny = __fmul_rn(ny, lambda_n), dnz = __fmul_rn(nz, lambda_n);
@@ -144,9 +163,10 @@ __global__ void k_contact_deltas(GridDev g, int n, const float* __restrict__ x, 
         }
     });
     // deltas[i] += delta * w1 * relaxation (one writer per particle: no atomics)
-    deltas[3 * (size_t)i] = __fadd_rn(deltas[3 * (size_t)i], __fmul_rn(__fmul_rn(dx, w1), relaxation));
-    deltas[3 * (size_t)i + 1] = __fadd_rn(deltas[3 * (size_t)i + 1], __fmul_rn(__fmul_rn(dy, w1), relaxation));
-    deltas[3 * (size_t)i + 2] = __fadd_rn(deltas[3 * (size_t)i + 2], __fmul_rn(__fmul_rn(dz, w1), relaxation));
+    const size_t i = (size_t)g.ids[kk];
+    deltas[3 * i] = __fadd_rn(deltas[3 * i], __fmul_rn(__fmul_rn(dx, w1), relaxation));
+    deltas[3 * i + 1] = __fadd_rn(deltas[3 * i + 1], __fmul_rn(__fmul_rn(dy, w1), relaxation));
+    deltas[3 * i + 2] = __fadd_rn(deltas[3 * i + 2], __fmul_rn(__fmul_rn(dz, w1), relaxation));
 }
 
 int check_grid(const nsph_grid* grid, int n)
@@ -157,6 +177,7 @@ int check_grid(const nsph_grid* grid, int n)
     if (n < 0) return fail(NSPH_ERR_INVALID_ARG, "negative particle count");
     if (n != grid->g.num_points)
         return fail(NSPH_ERR_INVALID_ARG, "particle count differs from the points of the grid's last build");
+    if (n > grid->mirror_cap) return fail(NSPH_ERR_CAPACITY, "grid not reserved through nsph_grid_reserve");
     return NSPH_OK;
 }
 
@@ -177,8 +198,12 @@ extern "C" int nsph_particle_contact_forces(const nsph_grid* grid, const nsph_co
     if (!x || !v || !radius || !flags || !f_out) return fail(NSPH_ERR_INVALID_ARG, "null array");
     DeviceGuard guard(grid->g.device);
     if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
-    k_contact_forces<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(grid->g.view(), n, x, v, radius, flags,
-                                                                         *params, f_out);
+    cudaStream_t cs = (cudaStream_t)stream;
+    float4* m0 = grid->mirror;
+    float4* m1 = grid->mirror + grid->mirror_cap;
+    k_contact_gather<<<(n + 255) / 256, 256, 0, cs>>>(grid->g.point_ids, n, x, v, radius, flags, nullptr, m0, m1);
+    NSPH_LAUNCH_CHECK("k_contact_gather");
+    k_contact_forces<<<(n + 127) / 128, 128, 0, cs>>>(grid->g.view(), n, m0, m1, *params, f_out);
     NSPH_LAUNCH_CHECK("k_contact_forces");
     return NSPH_OK;
 }
@@ -195,9 +220,13 @@ extern "C" int nsph_particle_contact_deltas(const nsph_grid* grid, int n, const 
     if (!x || !v || !inv_mass || !radius || !flags || !deltas) return fail(NSPH_ERR_INVALID_ARG, "null array");
     DeviceGuard guard(grid->g.device);
     if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
-    k_contact_deltas<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(grid->g.view(), n, x, v, inv_mass, radius,
-                                                                         flags, k_mu, k_cohesion, max_radius, dt,
-                                                                         relaxation, deltas);
+    cudaStream_t cs = (cudaStream_t)stream;
+    float4* m0 = grid->mirror;
+    float4* m1 = grid->mirror + grid->mirror_cap;
+    k_contact_gather<<<(n + 255) / 256, 256, 0, cs>>>(grid->g.point_ids, n, x, v, radius, flags, inv_mass, m0, m1);
+    NSPH_LAUNCH_CHECK("k_contact_gather");
+    k_contact_deltas<<<(n + 127) / 128, 128, 0, cs>>>(grid->g.view(), n, m0, m1, k_mu, k_cohesion, max_radius, dt,
+                                                       relaxation, deltas);
     NSPH_LAUNCH_CHECK("k_contact_deltas");
     return NSPH_OK;
 }

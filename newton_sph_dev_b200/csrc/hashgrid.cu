@@ -519,6 +519,10 @@ extern "C" int nsph_grid_destroy(nsph_grid* grid)
 {
     clear_error();
     if (!grid) return NSPH_OK;
+    {
+        DeviceGuard guard(grid->g.device);
+        cudaFree(grid->mirror);
+    }
     grid_free(grid->g);
     delete grid;
     return NSPH_OK;
@@ -528,7 +532,22 @@ extern "C" int nsph_grid_reserve(nsph_grid* grid, int num_points)
 {
     clear_error();
     if (!grid) return fail(NSPH_ERR_INVALID_ARG, "null grid");
-    return grid_reserve(grid->g, num_points);
+    const int st = grid_reserve(grid->g, num_points);
+    if (st != NSPH_OK || grid->mirror_cap >= grid->g.capacity) return st;
+    // sorted mirrors for the contact kernels (32 bytes per point)
+    DeviceGuard guard(grid->g.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    cudaFree(grid->mirror);
+    grid->mirror = nullptr;
+    grid->mirror_cap = 0;
+    const size_t c = (size_t)std::max(1, grid->g.capacity);
+    if (cudaMalloc(&grid->mirror, sizeof(float4) * 2 * c) != cudaSuccess) {
+        cudaGetLastError();
+        grid->mirror = nullptr;
+        return fail(NSPH_ERR_OUT_OF_MEMORY, "grid reserve: contact mirror allocation failed");
+    }
+    grid->mirror_cap = grid->g.capacity;
+    return NSPH_OK;
 }
 
 extern "C" int nsph_grid_build(nsph_grid* grid, const float* points, int num_points, float radius, void* stream)

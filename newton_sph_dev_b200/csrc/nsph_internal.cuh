@@ -253,4 +253,6 @@ int grid_build(Grid& g, const float* points, int n, float cell_width, float cell
 // the opaque handle of the nsph_grid_* C ABI (a HashGrid object)
 struct nsph_grid {
     nsph::Grid g;
+    float4* mirror = nullptr;  // contact scratch: 2 x mirror_cap sorted float4 ((x, r), (v, inv_mass))
+    int mirror_cap = 0;
 };
