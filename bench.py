@@ -348,6 +348,57 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+def pipelined_e2e(model, step, hx, hv, steps: int, device, outputs=None) -> float:
+    """Milliseconds for `steps` end-to-end steps through the public API:
+    upload (x, v) from the pinned host tensors hx, hv, step(state_in,
+    state_out), download outputs(state_out) (default: x, v) into pinned host
+    tensors. Three streams
+    (upload, compute, download) and two device state pairs let the upload of
+    step k+1 and the download of step k-1 run while step k computes; events
+    order every reuse of a buffer. Timed with CUDA events from a common start
+    to the last download."""
+    import torch
+
+    if outputs is None:
+        outputs = lambda st: (st.particle_q, st.particle_qd)  # noqa: E731
+    s_in, s_c, s_out = (torch.cuda.Stream(device) for _ in range(3))
+    ins = [model.state(), model.state()]
+    outs = [model.state(), model.state()]
+    host_out = [[torch.empty(t.shape, dtype=t.dtype).pin_memory() for t in outputs(outs[b])] for b in range(2)]
+    up = [torch.cuda.Event() for _ in range(2)]
+    done = [torch.cuda.Event() for _ in range(2)]
+    down = [torch.cuda.Event() for _ in range(2)]
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    cur = torch.cuda.current_stream(device)
+    # one untimed round to warm the streams' first launches
+    for k in range(steps + 2):
+        b = k % 2
+        if k == 2:
+            torch.cuda.synchronize()
+            start.record(cur)
+            for st in (s_in, s_c, s_out):
+                st.wait_event(start)
+        with torch.cuda.stream(s_in):
+            if k >= 2:
+                s_in.wait_event(done[b])  # step k-2 no longer reads ins[b]
+            ins[b].particle_q.copy_(hx, non_blocking=True)
+            ins[b].particle_qd.copy_(hv, non_blocking=True)
+            up[b].record(s_in)
+        with torch.cuda.stream(s_c):
+            s_c.wait_event(up[b])
+            if k >= 2:
+                s_c.wait_event(down[b])  # the download of step k-2 has read outs[b]
+            step(ins[b], outs[b])
+            done[b].record(s_c)
+        with torch.cuda.stream(s_out):
+            s_out.wait_event(done[b])
+            for h, t in zip(host_out[b], outputs(outs[b])):
+                h.copy_(t, non_blocking=True)
+            down[b].record(s_out)
+    end.record(s_out)
+    end.synchronize()
+    return start.elapsed_time(end)
+
 def load_traffic(kernel: str):
     p = REPO / "profiles" / "ncu_traffic.json"
     if not p.exists():
@@ -453,8 +504,18 @@ def run_gpu(args):
     hv = model.particle_qd.cpu().pin_memory()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e2e_ms = 0.0
+    # (a) pipelined: every step uploads its inputs from pinned host memory,
+    # runs SolverSPH.step and downloads its result; the upload of step k+1
+    # and the download of step k-1 overlap the step k on their own streams
     barrier(device)
+    torch.cuda.synchronize()
+    e2e_ms = pipelined_e2e(model, lambda a, b: solver.step(a, b, None, None, dt), hx, hv, e2e_steps, device)
+    barrier(device)
+    e2e_ms_max = max_over_ranks(e2e_ms, device)
+    e2e_value = world * n * e2e_steps / (e2e_ms_max * 1e-3)
+    # (b) serial host round trip: upload, step, download, and the next step
+    # starts from the downloaded state
+    serial_ms = 0.0
     torch.cuda.synchronize()
     for _ in range(e2e_steps):
         e0.record(stream)
@@ -465,10 +526,10 @@ def run_gpu(args):
         hv.copy_(s1.particle_qd, non_blocking=True)
         e1.record(stream)
         e1.synchronize()
-        e2e_ms += e0.elapsed_time(e1)
+        serial_ms += e0.elapsed_time(e1)
     barrier(device)
-    e2e_ms_max = max_over_ranks(e2e_ms, device)
-    e2e_value = world * n * e2e_steps / (e2e_ms_max * 1e-3)
+    serial_ms = max_over_ranks(serial_ms, device)
+    e2e_serial = world * n * e2e_steps / (serial_ms * 1e-3)
     state_bytes = n * 3 * 4 * 2
 
     # ---- roofline of the dominant single-kernel pass ----
@@ -529,7 +590,12 @@ def run_gpu(args):
             "roofline_step": roofline_step,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": state_bytes,
-                    "d2h_bytes_per_step": state_bytes, "steps": e2e_steps},
+                    "d2h_bytes_per_step": state_bytes, "steps": e2e_steps,
+                    "how": "each step uploads x, v from pinned host memory, runs SolverSPH.step and downloads x, v; "
+                           "independent steps from the same host state, uploads and downloads overlapping other "
+                           "steps' compute on separate streams (double-buffered device states)",
+                    "serial_round_trip": {"value": e2e_serial, "how": "upload, step, download, next step from the "
+                                                                      "downloaded state, no overlap"}},
             "gpu_launches": launches_per_step * args.steps,
             "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
             "status": status,
@@ -903,20 +969,11 @@ def run_surrogate(args):
     status = solver.status()
     finite = bool(torch.isfinite(cur.particle_q).all() and torch.isfinite(cur.particle_qd).all())
 
-    # end to end through the public API: host state in, one call, host state out
+    # end to end through the public API: host state in, one call, host state
+    # out, every call (pipelined over independent calls, as for tank_1m)
     e2e_steps = min(args.steps, 50)
     hx, hv = cur.particle_q.cpu().pin_memory(), cur.particle_qd.cpu().pin_memory()
-    e2e_ms = 0.0
-    for _ in range(e2e_steps):
-        e0.record(stream)
-        cur.particle_q.copy_(hx, non_blocking=True)
-        cur.particle_qd.copy_(hv, non_blocking=True)
-        stepper.step(cur, nxt, dt)
-        hx.copy_(nxt.particle_q, non_blocking=True)
-        hv.copy_(nxt.particle_qd, non_blocking=True)
-        e1.record(stream)
-        e1.synchronize()
-        e2e_ms += e0.elapsed_time(e1)
+    e2e_ms = pipelined_e2e(model, lambda a, b: stepper.step(a, b, dt), hx, hv, e2e_steps, device)
     e2e_ms = max_over_ranks(e2e_ms, device)
     e2e_value = world * n * sub * e2e_steps / (e2e_ms * 1e-3)
 
@@ -980,7 +1037,8 @@ def run_surrogate(args):
             "roofline_mlp": roofline_mlp,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": w["metric"], "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n,
-                    "steps": e2e_steps},
+                    "steps": e2e_steps, "how": "pinned upload, one SurrogateSPH.step call, download, every call; "
+                                              "independent calls pipelined on upload / compute / download streams"},
             "gpu_launches": stepper.launches_per_step * n_sur + fallbacks * sub * solver.last_launches,
             "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
             "status": status,
@@ -1076,20 +1134,16 @@ def run_contact(args):
     roofline = {"bound": "hbm", "kernel": "k_contact_forces", "achieved": ach, "peak": peak, "peak_kind": peak_kind,
                 "unit": "GB/s", "frac": ach / peak, "traffic": None, "alg_bytes_per_launch": B_ALG_CONTACT * n,
                 "ms_per_launch": t_contact * 1e3}
-    # end to end: host positions and velocities in, forces out
+    # end to end: host positions and velocities in, forces out, every step
+    # (pipelined over independent steps, as for tank_1m)
     hx, hv = state.particle_q.cpu().pin_memory(), state.particle_qd.cpu().pin_memory()
-    hf = torch.empty_like(hx).pin_memory()
     e2e_steps = min(args.steps, 50)
-    e2e = 0.0
-    for _ in range(e2e_steps):
-        ev[0].record(stream)
-        state.particle_q.copy_(hx, non_blocking=True)
-        state.particle_qd.copy_(hv, non_blocking=True)
-        step()
-        hf.copy_(f, non_blocking=True)
-        ev[2].record(stream)
-        ev[2].synchronize()
-        e2e += ev[0].elapsed_time(ev[2])
+
+    def e2e_step(a, b):
+        grid.build(a.particle_q, gr)
+        eval_particle_contact_forces(model, a, b.particle_f)
+
+    e2e = pipelined_e2e(model, e2e_step, hx, hv, e2e_steps, device, outputs=lambda st: (st.particle_f,))
     cpu = None
     if not args.no_cpu_baseline:
         from oracle import oracle as O
@@ -1123,7 +1177,9 @@ def run_contact(args):
         "roofline": roofline,
         "cpu_baseline": cpu,
         "e2e": {"value": n * e2e_steps / (e2e * 1e-3), "unit": METRIC, "h2d_bytes_per_step": 24 * n,
-                "d2h_bytes_per_step": 12 * n, "steps": e2e_steps},
+                "d2h_bytes_per_step": 12 * n, "steps": e2e_steps,
+                "how": "pinned upload of x, v, grid build + contact forces, download of f, every step; independent "
+                       "steps pipelined on upload / compute / download streams"},
         "gpu_launches": (grid.last_launches + 2) * args.steps,  # grid build + mirror gather + contact
         "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
     }
