@@ -23,7 +23,7 @@
 namespace nsph {
 namespace {
 
-constexpr uint32_t kFwdCols = 128;    // inference TMEM: z1 @0, z2 @64, y @0
+constexpr uint32_t kFwdCols = 64;     // inference TMEM: z1, z2 and y in turn at column 0
 constexpr uint32_t kTrainCols = 256;  // training TMEM: z1 @0, z2 @64, y @128, dA1 @192
 constexpr int kPartialStride = kMlpParams + 1;  // gradient + loss per CTA
 
@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(kMlpTile, 1) k_mlp_forward(const float* __rest
         mlp_stage_input(s, f);
         mlp_sync();
         float y[kMlpOut];
-        ok = mlp_forward_tile(s, tmem, 0, 64, 0, phase, y);
+        ok = mlp_forward_tile(s, tmem, 0, 0, 0, phase, y);
         if (ok && r < n)
             for (int o = 0; o < kMlpOut; ++o) out[(size_t)r * kMlpOut + o] = mlp_denorm(s, y, o);
         __syncthreads();
@@ -313,7 +313,8 @@ extern "C" int nsph_mlp_forward(int device, const float* model, const float* fea
     if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
     NSPH_CUDA_TRY(mlp_kernel_attrs(device));
     const int tiles = (n + kMlpTile - 1) / kMlpTile;
-    const int grid = std::min(tiles, 4 * sm_count(device));
+    // 8 CTAs x 64 TMEM columns fill an SM's 512 columns; shared memory lets 6 run at once
+    const int grid = std::min(tiles, 8 * sm_count(device));
     k_mlp_forward<<<grid, kMlpTile, sizeof(MlpFwdSmem), (cudaStream_t)stream>>>(model, features, n, out, err);
     NSPH_LAUNCH_CHECK("k_mlp_forward");
     return NSPH_OK;

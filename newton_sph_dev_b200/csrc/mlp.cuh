@@ -39,19 +39,29 @@ constexpr int kOutStd = kOutMean + 4;
 constexpr int kMlpModelFloats = kOutStd + 4;  // 5488
 constexpr int kMlpWaitLimit = 1 << 22;        // polls of an MMA-completion wait before giving up
 
-// shared memory of the forward pass (the training kernel extends it)
+// shared memory of inference: one hidden tile serves both layers (layer 2's
+// MMA has completed, so h1 is no longer read, before its epilogue writes
+// silu(z2) over it), which keeps a CTA at about 34 KB
 struct MlpFwdSmem {
     __nv_bfloat16 w1t[kMlpHid * kMlpIn];      // B of layer 1: [out][in], K = 16
     __nv_bfloat16 w2t[kMlpHid * kMlpHid];     // B of layer 2: [out][in], K = 64
     __nv_bfloat16 w3t[kMlpOutPad * kMlpHid];  // B of layer 3: [out (padded)][in], K = 64
     __nv_bfloat16 x[kMlpTile * kMlpIn];       // A of layer 1
-    __nv_bfloat16 h1[kMlpTile * kMlpHid];     // A of layer 2: silu(z1)
-    __nv_bfloat16 h2[kMlpTile * kMlpHid];     // A of layer 3: silu(z2)
+    __nv_bfloat16 h1[kMlpTile * kMlpHid];     // A of layer 2 (silu(z1)), then of layer 3 (silu(z2))
     float b1[kMlpHid], b2[kMlpHid], b3[kMlpOutPad];
     float norm[kMlpModelFloats - kInMean];    // feature / output normalisation
     uint64_t bar;
     uint32_t tmem;
 };
+
+// the A tile of layer 3: its own buffer where the smem layout has one (the
+// training kernel keeps silu(z2) for the weight gradients), else h1
+template <class S>
+__device__ __forceinline__ __nv_bfloat16* hidden2(S& s)
+{
+    return s.h2;
+}
+__device__ __forceinline__ __nv_bfloat16* hidden2(MlpFwdSmem& s) { return s.h1; }
 
 __device__ __forceinline__ float tanh_approx(float x)
 {
@@ -155,7 +165,8 @@ __device__ __forceinline__ bool mlp_wait(S& s, uint32_t& phase)
 
 // Forward of one tile whose normalised bf16 inputs are already in s.x (and
 // made visible with mlp_sync). Accumulators: z1 at TMEM column c1, z2 at c2,
-// the output at c3 (each without bias). Returns false if an MMA wait gave up
+// the output at c3 (each without bias); c2 may equal c1 and c3 may equal
+// either, since each accumulator is read out before the next MMA is issued. Returns false if an MMA wait gave up
 // (then no further MMA is issued). `phase` is the parity of the next
 // completion of s.bar.
 template <class S>
@@ -165,7 +176,7 @@ __device__ bool mlp_forward_tile(S& s, uint32_t tmem, uint32_t c1, uint32_t c2, 
     using namespace umma;
     const int row = threadIdx.x;
     const uint32_t tmem_row = tmem + ((uint32_t)((threadIdx.x >> 5) * 32) << 16);
-    const uint32_t xa = smem_addr(s.x), h1a = smem_addr(s.h1), h2a = smem_addr(s.h2);
+    const uint32_t xa = smem_addr(s.x), h1a = smem_addr(s.h1), h2a = smem_addr(hidden2(s));
     const uint32_t w1a = smem_addr(s.w1t), w2a = smem_addr(s.w2t), w3a = smem_addr(s.w3t);
     // layer 1: z1 = x W1 (K = 16, one MMA)
     if (threadIdx.x == 0) {
@@ -184,7 +195,7 @@ __device__ bool mlp_forward_tile(S& s, uint32_t tmem, uint32_t c1, uint32_t c2, 
         mma_commit(&s.bar);
     }
     if (!mlp_wait(s, phase)) return false;
-    mlp_hidden_epilogue(tmem_row, c2, s.b2, s.h2, row);
+    mlp_hidden_epilogue(tmem_row, c2, s.b2, hidden2(s), row);
     mlp_sync();
     // layer 3: out = h2 W3 (K = 64, N = 16 of which 3 are used)
     if (threadIdx.x == 0) {

@@ -992,7 +992,7 @@ __global__ void __launch_bounds__(kMlpTile, 1) k_surrogate(const float* __restri
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     MlpFwdSmem& s = *reinterpret_cast<MlpFwdSmem*>(smem_raw);
-    const uint32_t tmem = mlp_cta_begin(model, s, 128);
+    const uint32_t tmem = mlp_cta_begin(model, s, 64);
     uint32_t phase = 0;
     bool ok = true;
     const int tiles = (n + kMlpTile - 1) / kMlpTile;
@@ -1010,7 +1010,7 @@ __global__ void __launch_bounds__(kMlpTile, 1) k_surrogate(const float* __restri
         const int ik = __ldg(g.ids + kk);
         load_features(feat, k + (int)gridDim.x * kMlpTile, n, f);
         float y[kMlpOut];
-        ok = mlp_forward_tile(s, tmem, 0, 64, 0, phase, y);
+        ok = mlp_forward_tile(s, tmem, 0, 0, 0, phase, y);
         if (ok && k < n) {
             const int attr = __float_as_int(vi.w);
             ForceAcc acc{a.x, a.y, a.z, dv.x, dv.y, dv.z};
@@ -1024,7 +1024,7 @@ __global__ void __launch_bounds__(kMlpTile, 1) k_surrogate(const float* __restri
         __syncthreads();
     }
     if (!ok && o.status && threadIdx.x == 0) atomicOr(o.status, (unsigned)NSPH_STATUS_SURROGATE_TIMEOUT);
-    mlp_cta_end(s, tmem, 128, !ok, phase);
+    mlp_cta_end(s, tmem, 64, !ok, phase);
 }
 
 // sorted scratch -> original order: feat (n x 16), acc (n x 6: a, dv)
@@ -1862,7 +1862,8 @@ extern "C" int nsph_sph_step_surrogate(nsph_sph* s, const nsph_sph_params* p, co
         k_compression_reduce<<<1, 256, 0, cs>>>(s->cpart, blocks, stats);
         NSPH_LAUNCH_CHECK("k_compression_reduce");
         const int tiles = (n + kMlpTile - 1) / kMlpTile;
-        const int grid = std::min(tiles, 4 * std::max(1, s->surr_sms));
+        // 8 CTAs x 64 TMEM columns fill an SM's 512 columns; shared memory lets 6 run at once
+        const int grid = std::min(tiles, 8 * std::max(1, s->surr_sms));
         const StepOut o{f_ext, inv_mass, gravity, x_out, v_out, rho_out, p_out, nullptr, s->status};
         k_surrogate<<<grid, kMlpTile, sizeof(MlpFwdSmem), cs>>>(model, acc_scale, s->grid.view(), s->xs, s->vs,
                                                                     s->rp, n, *p, s->sfeat, s->sacc, o);
