@@ -23,7 +23,6 @@
 namespace nsph {
 namespace {
 
-constexpr uint32_t kFwdCols = 64;     // inference TMEM: z1, z2 and y in turn at column 0
 constexpr uint32_t kTrainCols = 256;  // training TMEM: z1 @0, z2 @64, y @128, dA1 @192
 constexpr int kPartialStride = kMlpParams + 1;  // gradient + loss per CTA
 
@@ -70,7 +69,7 @@ __global__ void __launch_bounds__(kMlpTile, 1) k_mlp_forward(const float* __rest
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     MlpFwdSmem& s = *reinterpret_cast<MlpFwdSmem*>(smem_raw);
-    const uint32_t tmem = mlp_cta_begin(model, s, kFwdCols);
+    const uint32_t tmem = mlp_cta_begin(model, s, kMlpFwdCols);
     uint32_t phase = 0;
     bool ok = true;
     const int tiles = (n + kMlpTile - 1) / kMlpTile;
@@ -88,7 +87,7 @@ __global__ void __launch_bounds__(kMlpTile, 1) k_mlp_forward(const float* __rest
         __syncthreads();
     }
     if (!ok && threadIdx.x == 0) atomicOr(err, 1u);
-    mlp_cta_end(s, tmem, kFwdCols, !ok, phase);
+    mlp_cta_end(s, tmem, kMlpFwdCols, !ok, phase);
 }
 
 __global__ void __launch_bounds__(kMlpTile, 1) k_mlp_grad(const float* __restrict__ model,
@@ -313,8 +312,9 @@ extern "C" int nsph_mlp_forward(int device, const float* model, const float* fea
     if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
     NSPH_CUDA_TRY(mlp_kernel_attrs(device));
     const int tiles = (n + kMlpTile - 1) / kMlpTile;
-    // 8 CTAs x 64 TMEM columns fill an SM's 512 columns; shared memory lets 6 run at once
-    const int grid = std::min(tiles, 8 * sm_count(device));
+    const int resident = mlp_resident_grid(k_mlp_forward, sizeof(MlpFwdSmem), device);
+    if (resident <= 0) return fail(NSPH_ERR_CUDA, "cannot size the k_mlp_forward grid");
+    const int grid = std::min(tiles, resident);
     k_mlp_forward<<<grid, kMlpTile, sizeof(MlpFwdSmem), (cudaStream_t)stream>>>(model, features, n, out, err);
     NSPH_LAUNCH_CHECK("k_mlp_forward");
     return NSPH_OK;

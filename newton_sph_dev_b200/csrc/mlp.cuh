@@ -38,6 +38,8 @@ constexpr int kOutMean = kInInvStd + kMlpIn;
 constexpr int kOutStd = kOutMean + 4;
 constexpr int kMlpModelFloats = kOutStd + 4;  // 5488
 constexpr int kMlpWaitLimit = 1 << 22;        // polls of an MMA-completion wait before giving up
+constexpr uint32_t kMlpFwdCols = 64;          // inference TMEM: z1, z2 and the output in turn at column 0
+constexpr int kTmemCols = 512;                // TMEM columns per SM
 
 // shared memory of inference: one hidden tile serves both layers (layer 2's
 // MMA has completed, so h1 is no longer read, before its epilogue writes
@@ -211,6 +213,32 @@ __device__ bool mlp_forward_tile(S& s, uint32_t tmem, uint32_t c1, uint32_t c2, 
 #pragma unroll
     for (int o = 0; o < kMlpOut; ++o) y[o] = v[o] + s.b3[o];
     return true;
+}
+
+// Grid of an inference kernel: as many CTAs as can be resident at once, so
+// every CTA runs in the first wave and strides over the tiles. Residency is
+// computed from the kernel's registers (allocated per warp in units of 256),
+// its shared memory (plus the per-CTA reservation) and the SM's TMEM columns;
+// 0 on a CUDA error.
+template <class K>
+inline int mlp_resident_grid(K kernel, size_t smem, int device)
+{
+    cudaFuncAttributes fa;
+    int sms = 0, smem_sm = 0, reserved = 0, regs_sm = 0;
+    if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, device) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    const int warp_regs = ((fa.numRegs * 32 + 255) / 256) * 256;
+    const int by_regs = regs_sm / (warp_regs * (kMlpTile / 32));
+    const int by_smem = smem_sm / (int)(smem + fa.sharedSizeBytes + reserved);
+    int per_sm = by_regs < by_smem ? by_regs : by_smem;
+    per_sm = per_sm > kTmemCols / (int)kMlpFwdCols ? kTmemCols / (int)kMlpFwdCols : per_sm;
+    return (sms > 0 ? sms : 1) * (per_sm > 0 ? per_sm : 1);
 }
 
 // CTA start: stage the weights, initialise the barrier, allocate `ncols`

@@ -992,7 +992,7 @@ __global__ void __launch_bounds__(kMlpTile, 1) k_surrogate(const float* __restri
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     MlpFwdSmem& s = *reinterpret_cast<MlpFwdSmem*>(smem_raw);
-    const uint32_t tmem = mlp_cta_begin(model, s, 64);
+    const uint32_t tmem = mlp_cta_begin(model, s, kMlpFwdCols);
     uint32_t phase = 0;
     bool ok = true;
     const int tiles = (n + kMlpTile - 1) / kMlpTile;
@@ -1024,7 +1024,7 @@ __global__ void __launch_bounds__(kMlpTile, 1) k_surrogate(const float* __restri
         __syncthreads();
     }
     if (!ok && o.status && threadIdx.x == 0) atomicOr(o.status, (unsigned)NSPH_STATUS_SURROGATE_TIMEOUT);
-    mlp_cta_end(s, tmem, 64, !ok, phase);
+    mlp_cta_end(s, tmem, kMlpFwdCols, !ok, phase);
 }
 
 // sorted scratch -> original order: feat (n x 16), acc (n x 6: a, dv)
@@ -1091,7 +1091,7 @@ struct nsph_sph {
     float* sfeat = nullptr;              // surrogate scratch (nsph_sph_enable_surrogate), sorted: 16 features
     float4* sacc = nullptr;              //   (a, 0), (dv, 0)
     float* cpart = nullptr;              //   per-block (compression sum, active count)
-    int surr_sms = 0;                    //   SMs (grid of the MLP kernel)
+    int surr_ctas = 0;                   //   resident CTAs of k_surrogate (its grid)
 };
 
 // grid of a neighbour pass: one thread per particle, or a persistent grid of
@@ -1748,7 +1748,10 @@ extern "C" int nsph_sph_enable_surrogate(nsph_sph* s)
     if (e == cudaSuccess) e = cudaMalloc(&s->cpart, sizeof(float) * 2 * blocks);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_surrogate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpFwdSmem));
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->surr_sms, cudaDevAttrMultiProcessorCount, s->grid.device);
+    if (e == cudaSuccess) {
+        s->surr_ctas = mlp_resident_grid(k_surrogate, sizeof(MlpFwdSmem), s->grid.device);
+        if (s->surr_ctas <= 0) e = cudaErrorUnknown;
+    }
     cudaFuncAttributes fa;
     if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_force_features);
     if (e != cudaSuccess) {
@@ -1862,8 +1865,7 @@ extern "C" int nsph_sph_step_surrogate(nsph_sph* s, const nsph_sph_params* p, co
         k_compression_reduce<<<1, 256, 0, cs>>>(s->cpart, blocks, stats);
         NSPH_LAUNCH_CHECK("k_compression_reduce");
         const int tiles = (n + kMlpTile - 1) / kMlpTile;
-        // 8 CTAs x 64 TMEM columns fill an SM's 512 columns; shared memory lets 6 run at once
-        const int grid = std::min(tiles, 8 * std::max(1, s->surr_sms));
+        const int grid = std::min(tiles, std::max(1, s->surr_ctas));
         const StepOut o{f_ext, inv_mass, gravity, x_out, v_out, rho_out, p_out, nullptr, s->status};
         k_surrogate<<<grid, kMlpTile, sizeof(MlpFwdSmem), cs>>>(model, acc_scale, s->grid.view(), s->xs, s->vs,
                                                                     s->rp, n, *p, s->sfeat, s->sacc, o);
