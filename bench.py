@@ -712,7 +712,7 @@ def run_grad(args):
             fwd_ms += ev[0].elapsed_time(ev[1])
             bwd_ms += ev[1].elapsed_time(ev[2])
             ph = solver.adjoint_phase_times()  # the last adjoint step of this rollout
-            dens_ms += ph[1]
+            dens_ms += solver.phase_times()[1]  # the last forward step's density pass
             pair_ms += ph[3]
     torch.cuda.synchronize()
     barrier(device)
@@ -747,7 +747,7 @@ def run_grad(args):
     e2e_value = world * n * steps * e2e_iters / (e2e_ms * 1e-3)
 
     # ---- roofline: the density pass has the largest share of the rollout's
-    # kernel time (it runs in the forward, recompute and adjoint steps); the
+    # kernel time (it runs in the forward and the segment recompute steps); the
     # pair gather is the adjoint's largest single kernel ----
     peak, peak_kind = load_peak()
     t_dens = dens_ms / args.steps * 1e-3

@@ -295,6 +295,29 @@ NSPH_API int nsph_sph_rollout_adjoint(nsph_sph* solver, const nsph_sph_params* p
                                       const float* gravity, int world_count,
                                       float* x_adj, float* v_adj, float* f_ext_adj, float* eos_b_adj, void* stream);
 
+/* Segment form with a tape: one call recomputes a checkpointed segment and
+ * reverses it, replacing nsph_sph_rollout (of steps - 1 steps) followed by
+ * nsph_sph_rollout_adjoint, with bit-identical results.
+ * nsph_sph_segment_adjoint: `steps` steps from (x0, v0). The forward keeps,
+ *   per step, the grid build and density pass that the step's reverse reads
+ *   (sorted mirrors, cell table, sorted ids, m/rho, p/rho^2, rho, p,
+ *   neighbour masks), so the reverse skips the rebuild and the density pass;
+ *   the last step's force pass is not run. x_adj / v_adj hold the adjoint of
+ *   the state after `steps` steps on entry and of (x0, v0) on return (they
+ *   must not overlap each other or x0 / v0); f_ext_adj and eos_b_adj
+ *   accumulate as in nsph_sph_step_adjoint. Afterwards the solver's grid
+ *   describes the last step's input.
+ * nsph_sph_reserve_segment: allocates the tape for segments of up to
+ *   `steps` steps (88 bytes per particle of capacity plus 8 bytes per grid
+ *   cell, per step, and two states); nsph_sph_segment_adjoint reserves on
+ *   demand, so call this first where the call is captured in a graph. */
+NSPH_API int nsph_sph_reserve_segment(nsph_sph* solver, int steps);
+NSPH_API int nsph_sph_segment_adjoint(nsph_sph* solver, const nsph_sph_params* params, int n, int steps,
+                                      const float* x0, const float* v0, const float* f_ext,
+                                      const float* mass, const float* inv_mass, const int* flags, const int* world,
+                                      const float* gravity, int world_count,
+                                      float* x_adj, float* v_adj, float* f_ext_adj, float* eos_b_adj, void* stream);
+
 /* ---- particle-particle contact on the HashGrid ------------------------------
  * The reference's other consumers of the grid, rebuilt on nsph_grid (same
  * query: the candidates of hash_grid_query(grid, x_i, r_i + max_radius +

@@ -157,6 +157,16 @@ SIGNATURES = [
         + [c_void_p] * 4
         + [c_void_p],
     ),
+    ("nsph_sph_reserve_segment", ctypes.c_int, [c_void_p, ctypes.c_int]),
+    (
+        "nsph_sph_segment_adjoint",
+        ctypes.c_int,
+        [c_void_p, ctypes.POINTER(NsphSphParams), ctypes.c_int, ctypes.c_int]
+        + [c_void_p] * 8
+        + [ctypes.c_int]
+        + [c_void_p] * 4
+        + [c_void_p],
+    ),
     (
         "nsph_particle_contact_forces",
         ctypes.c_int,

@@ -1092,7 +1092,62 @@ struct nsph_sph {
     float4* sacc = nullptr;              //   (a, 0), (dv, 0)
     float* cpart = nullptr;              //   per-block (compression sum, active count)
     int surr_ctas = 0;                   //   resident CTAs of k_surrogate (its grid)
+    char* tape = nullptr;                // segment tape (nsph_sph_segment_adjoint): per step of a segment,
+    int tape_steps = 0;                  //   the build and density outputs the step's reverse reads,
+    size_t tape_step_bytes = 0;          //   tape_steps slots of tape_step_bytes, then two states
 };
+
+// One step's slot of the segment tape: the sorted mirrors, the density
+// pass's outputs and neighbour masks, and the grid (sorted ids, cell table).
+struct TapeStep {
+    float4* xs;
+    float4* vs;
+    float2* aux;
+    float2* rp;
+    unsigned* mask;
+    int* ncand;
+    int* ids;
+    int2* ranges;
+};
+
+static size_t tape_align(size_t b) { return (b + 255) & ~(size_t)255; }
+
+static size_t tape_slot_bytes(size_t c, long long ncells)
+{
+    return 2 * tape_align(sizeof(float4) * c) + 2 * tape_align(sizeof(float2) * c) +
+           tape_align(sizeof(unsigned) * kMaskWords * c) + 2 * tape_align(sizeof(int) * c) +
+           tape_align(sizeof(int2) * (size_t)ncells);
+}
+
+static TapeStep tape_slot(const nsph_sph* s, int t)
+{
+    const size_t c = (size_t)s->capacity;
+    char* b = s->tape + (size_t)t * s->tape_step_bytes;
+    TapeStep ts;
+    ts.xs = reinterpret_cast<float4*>(b);
+    b += tape_align(sizeof(float4) * c);
+    ts.vs = reinterpret_cast<float4*>(b);
+    b += tape_align(sizeof(float4) * c);
+    ts.aux = reinterpret_cast<float2*>(b);
+    b += tape_align(sizeof(float2) * c);
+    ts.rp = reinterpret_cast<float2*>(b);
+    b += tape_align(sizeof(float2) * c);
+    ts.mask = reinterpret_cast<unsigned*>(b);
+    b += tape_align(sizeof(unsigned) * kMaskWords * c);
+    ts.ncand = reinterpret_cast<int*>(b);
+    b += tape_align(sizeof(int) * c);
+    ts.ids = reinterpret_cast<int*>(b);
+    b += tape_align(sizeof(int) * c);
+    ts.ranges = reinterpret_cast<int2*>(b);
+    return ts;
+}
+
+// the two recompute states (x then v, 3 x capacity floats each) after the slots
+static float* tape_state(const nsph_sph* s, int which)
+{
+    return reinterpret_cast<float*>(s->tape + (size_t)s->tape_steps * s->tape_step_bytes) +
+           (size_t)which * 6 * (size_t)s->capacity;
+}
 
 // grid of a neighbour pass: one thread per particle, or a persistent grid of
 // blocks_per_sm blocks per SM striding over the particles
@@ -1148,6 +1203,7 @@ static void sph_free(nsph_sph* s)
     cudaFree(s->adj_rho);
     cudaFree(s->adj_bpart);
     cudaFree(s->sfeat);
+    cudaFree(s->tape);
     cudaFree(s->sacc);
     cudaFree(s->cpart);
     grid_free(s->grid);
@@ -1602,6 +1658,30 @@ extern "C" int nsph_sph_enable_adjoint(nsph_sph* s)
     return NSPH_OK;
 }
 
+// The adjoint kernels of one step whose build and density outputs are `ts`
+// (its grid seen through g). mark: record the adjoint phase events.
+static int adjoint_kernels(nsph_sph* s, const nsph_sph_params* p, int n, const GridDev& g, const TapeStep& ts,
+                           const AdjIO& io, float* eos_b_adj, cudaStream_t cs, int& launches, bool mark)
+{
+    int blocks, threads;
+    pass_launch(s, n, false, blocks, threads);
+    k_adj_local<<<blocks, threads, 0, cs>>>(g, ts.xs, ts.vs, ts.aux, n, *p, ts.mask, ts.ncand, io);
+    NSPH_LAUNCH_CHECK("k_adj_local");
+    if (mark && s->eva[3]) NSPH_CUDA_TRY(record_mark(s->eva[3], cs));
+    k_adj_pair<<<blocks, threads, 0, cs>>>(g, ts.xs, ts.vs, ts.aux, ts.rp, n, *p, ts.mask, ts.ncand, io);
+    NSPH_LAUNCH_CHECK("k_adj_pair");
+    if (mark && s->eva[4]) NSPH_CUDA_TRY(record_mark(s->eva[4], cs));
+    k_adj_density<<<blocks, threads, 0, cs>>>(g, ts.xs, ts.vs, n, *p, ts.mask, ts.ncand, io.rho, io.x_in_adj);
+    NSPH_LAUNCH_CHECK("k_adj_density");
+    launches += 3;
+    if (eos_b_adj) {
+        k_adj_b_reduce<<<1, 256, 0, cs>>>(io.bpart, blocks, eos_b_adj);
+        NSPH_LAUNCH_CHECK("k_adj_b_reduce");
+        ++launches;
+    }
+    return NSPH_OK;
+}
+
 // Enqueue the reverse of one step on validated inputs.
 static int adjoint_enqueue(nsph_sph* s, const nsph_sph_params* p, int n, const float* x_in, const float* v_in,
                            const float* f_ext, const float* mass, const float* inv_mass, const int* flags,
@@ -1623,23 +1703,12 @@ static int adjoint_enqueue(nsph_sph* s, const nsph_sph_params* p, int n, const f
                                                    s->status);
         NSPH_LAUNCH_CHECK("k_density");
         if (s->eva[2]) NSPH_CUDA_TRY(record_mark(s->eva[2], cs));
+        ++launches;
         const AdjIO io{x_out_adj, v_out_adj, rho_out_adj, x_in_adj, v_in_adj, f_ext_adj, f_ext, inv_mass, gravity,
                        s->adj_g, s->adj_d, s->adj_rho, s->adj_bpart};
-        k_adj_local<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, n, *p, s->mask, s->ncand, io);
-        NSPH_LAUNCH_CHECK("k_adj_local");
-        if (s->eva[3]) NSPH_CUDA_TRY(record_mark(s->eva[3], cs));
-        k_adj_pair<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->mask, s->ncand, io);
-        NSPH_LAUNCH_CHECK("k_adj_pair");
-        if (s->eva[4]) NSPH_CUDA_TRY(record_mark(s->eva[4], cs));
-        k_adj_density<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->mask, s->ncand, s->adj_rho,
-                                                       x_in_adj);
-        NSPH_LAUNCH_CHECK("k_adj_density");
-        launches += 4;
-        if (eos_b_adj) {
-            k_adj_b_reduce<<<1, 256, 0, cs>>>(s->adj_bpart, blocks, eos_b_adj);
-            NSPH_LAUNCH_CHECK("k_adj_b_reduce");
-            ++launches;
-        }
+        const TapeStep ts{s->xs, s->vs, s->aux, s->rp, s->mask, s->ncand, nullptr, nullptr};
+        st = adjoint_kernels(s, p, n, g, ts, io, eos_b_adj, cs, launches, true);
+        if (st != NSPH_OK) return st;
     } else {
         for (int k = 2; k < 5; ++k)
             if (s->eva[k]) NSPH_CUDA_TRY(record_mark(s->eva[k], cs));
@@ -1713,6 +1782,119 @@ extern "C" int nsph_sph_rollout_adjoint(nsph_sph* s, const nsph_sph_params* p, i
                              flags, world, gravity, world_count, x_adj, v_adj, nullptr, x_adj, v_adj, f_ext_adj,
                              eos_b_adj, cs, launches);
         if (st != NSPH_OK) return st;
+    }
+    s->last_launches = launches;
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_reserve_segment(nsph_sph* s, int steps)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    if (s->grid.world_count > 0) return fail(NSPH_ERR_INVALID_ARG, "the adjoint supports single-world solvers only");
+    if (steps < 0) return fail(NSPH_ERR_INVALID_ARG, "negative step count");
+    if (steps <= s->tape_steps) return NSPH_OK;
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    const size_t c = (size_t)(s->capacity > 0 ? s->capacity : 1);
+    const size_t slot = tape_slot_bytes(c, s->grid.ncells);
+    const size_t bytes = slot * (size_t)steps + tape_align(sizeof(float) * 12 * c);
+    char* t = nullptr;
+    const cudaError_t e = cudaMalloc(&t, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(NSPH_ERR_OUT_OF_MEMORY, "segment tape of " + std::to_string(bytes) + " bytes: " +
+                                                cudaGetErrorString(e));
+    }
+    cudaFree(s->tape);
+    s->tape = t;
+    s->tape_steps = steps;
+    s->tape_step_bytes = slot;
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_segment_adjoint(nsph_sph* s, const nsph_sph_params* p, int n, int steps, const float* x0,
+                                        const float* v0, const float* f_ext, const float* mass,
+                                        const float* inv_mass, const int* flags, const int* world,
+                                        const float* gravity, int world_count, float* x_adj, float* v_adj,
+                                        float* f_ext_adj, float* eos_b_adj, void* stream)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    int st = check_params(p);
+    if (st == NSPH_OK) st = check_adjoint_ready(s);
+    if (st == NSPH_OK) st = check_step_inputs(s, n, x0, v0, mass, inv_mass, flags, gravity, world_count);
+    if (st != NSPH_OK) return st;
+    if (steps < 0) return fail(NSPH_ERR_INVALID_ARG, "negative step count");
+    const size_t len = 3 * (size_t)n;
+    if (n > 0 && steps > 0) {
+        if (!x_adj || !v_adj) return fail(NSPH_ERR_INVALID_ARG, "null adjoint array");
+        if (overlaps(x_adj, len, v_adj, len) || overlaps(x_adj, len, x0, len) || overlaps(x_adj, len, v0, len) ||
+            overlaps(v_adj, len, x0, len) || overlaps(v_adj, len, v0, len))
+            return fail(NSPH_ERR_INVALID_ARG, "adjoint arrays overlap each other or the initial state");
+    }
+    if (n == 0 || steps == 0) {
+        s->last_launches = 0;
+        return NSPH_OK;
+    }
+    st = nsph_sph_reserve_segment(s, steps);
+    if (st != NSPH_OK) return st;
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    cudaStream_t cs = (cudaStream_t)stream;
+    int launches = 0;
+    int blocks, threads;
+    pass_launch(s, n, false, blocks, threads);
+    // forward: the build and density pass of every step into its slot; the
+    // force pass of every step but the last (whose output is not needed)
+    for (int t = 0; t < steps; ++t) {
+        const float* xi = t == 0 ? x0 : tape_state(s, t & 1);
+        const float* vi = t == 0 ? v0 : tape_state(s, t & 1) + len;
+        const TapeStep ts = tape_slot(s, t);
+        GatherArgs ga{xi, vi, mass, inv_mass, flags, world, world_count, ts.xs, ts.vs};
+        st = grid_build(s->grid, xi, n, p->cell_width, p->cell_inv, &ga, s->status, cs, &launches);
+        if (st != NSPH_OK) return st;
+        NSPH_CUDA_TRY(cudaMemcpyAsync(ts.ranges, s->grid.cell_ranges, sizeof(int2) * (size_t)s->grid.ncells,
+                                      cudaMemcpyDeviceToDevice, cs));
+        NSPH_CUDA_TRY(cudaMemcpyAsync(ts.ids, s->grid.point_ids, sizeof(int) * (size_t)n, cudaMemcpyDeviceToDevice,
+                                      cs));
+        GridDev g = s->grid.view();
+        g.ranges = ts.ranges;
+        g.ids = ts.ids;
+        k_density<<<blocks, threads, 0, cs>>>(g, ts.xs, ts.vs, n, *p, ts.aux, ts.rp, ts.mask, ts.ncand, s->status);
+        NSPH_LAUNCH_CHECK("k_density");
+        ++launches;
+        if (t + 1 < steps) {
+            float* xo = tape_state(s, (t + 1) & 1);
+            float* vo = xo + len;
+            // inactive particles keep their velocity (the step leaves it untouched)
+            NSPH_CUDA_TRY(cudaMemcpyAsync(vo, vi, sizeof(float) * len, cudaMemcpyDeviceToDevice, cs));
+            const StepOut o{f_ext, inv_mass, gravity, xo, vo, nullptr, nullptr, nullptr, s->status};
+            k_force<<<blocks, threads, 0, cs>>>(g, ts.xs, ts.vs, ts.aux, ts.rp, n, *p, ts.mask, ts.ncand, o);
+            NSPH_LAUNCH_CHECK("k_force");
+            ++launches;
+        }
+    }
+    // the solver's mirrors describe its grid's last build (the last step's input)
+    const TapeStep last = tape_slot(s, steps - 1);
+    NSPH_CUDA_TRY(cudaMemcpyAsync(s->xs, last.xs, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToDevice, cs));
+    NSPH_CUDA_TRY(cudaMemcpyAsync(s->vs, last.vs, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToDevice, cs));
+    s->last_n = n;
+    // reverse, from the slots
+    const AdjIO io{x_adj, v_adj, nullptr, x_adj, v_adj, f_ext_adj, f_ext, inv_mass, gravity,
+                   s->adj_g, s->adj_d, s->adj_rho, s->adj_bpart};
+    for (int t = steps - 1; t >= 0; --t) {
+        const TapeStep ts = tape_slot(s, t);
+        GridDev g = s->grid.view();
+        g.ranges = ts.ranges;
+        g.ids = ts.ids;
+        // phase events: the build and density phases of a step reversed from
+        // the tape are empty (the recompute ran them)
+        for (int k = 0; k < 3; ++k)
+            if (s->eva[k]) NSPH_CUDA_TRY(record_mark(s->eva[k], cs));
+        st = adjoint_kernels(s, p, n, g, ts, io, eos_b_adj, cs, launches, true);
+        if (st != NSPH_OK) return st;
+        if (s->eva[5]) NSPH_CUDA_TRY(record_mark(s->eva[5], cs));
     }
     s->last_launches = launches;
     return NSPH_OK;

@@ -484,6 +484,36 @@ class SolverSPH(SolverBase):
         _lib.check(st, "SolverSPH.rollout_backward")
         self.launches_total += self.last_launches
 
+    def segment_backward_raw(self, x0: torch.Tensor, v0: torch.Tensor, steps: int, params: _lib.NsphSphParams,
+                             x_grad: torch.Tensor, v_grad: torch.Tensor, f_ext: torch.Tensor | None = None,
+                             f_ext_grad: torch.Tensor | None = None, eos_b_grad: torch.Tensor | None = None) -> None:
+        """nsph_sph_segment_adjoint: recompute `steps` steps from (x0, v0)
+        keeping each step's grid and density scratch, then reverse them;
+        x_grad / v_grad (N, 3) go from the gradient of the state after
+        `steps` steps to that of (x0, v0), in place. Equal, bit for bit, to
+        rollout_raw of the segment followed by rollout_backward_raw."""
+        n = self.model.particle_count
+        self.enable_adjoint()
+        for t, name in ((x0, "x0"), (v0, "v0"), (x_grad, "x_grad"), (v_grad, "v_grad")):
+            self._check_vec(t, name)
+        for t, name in ((f_ext, "f_ext"), (f_ext_grad, "f_ext_grad")):
+            if t is not None:
+                self._check_vec(t, name)
+        if eos_b_grad is not None and (eos_b_grad.dtype != torch.float32 or eos_b_grad.numel() != 1
+                                       or not eos_b_grad.is_cuda):
+            raise ValueError("eos_b_grad must be a one-element float32 CUDA tensor")
+        st = self._lib.nsph_sph_segment_adjoint(
+            self._handle, ctypes.byref(params), n, int(steps), x0.data_ptr(), v0.data_ptr(), _lib.ptr(f_ext),
+            *self._model_ptrs(), x_grad.data_ptr(), v_grad.data_ptr(), _lib.ptr(f_ext_grad), _lib.ptr(eos_b_grad),
+            _lib.stream_handle(self.model.device))
+        _lib.check(st, "SolverSPH.segment_backward")
+        self.launches_total += self.last_launches
+
+    def reserve_segment(self, steps: int) -> None:
+        """Allocate the segment tape of segment_backward_raw for up to
+        `steps` steps (outside graph capture)."""
+        _lib.check(self._lib.nsph_sph_reserve_segment(self._handle, int(steps)), "SolverSPH.reserve_segment")
+
     # ---- surrogate ---------------------------------------------------------
     def enable_surrogate(self) -> None:
         """Allocate the surrogate's feature scratch (96 bytes per particle);
@@ -645,7 +675,9 @@ class SolverSPH(SolverBase):
     def adjoint_phase_times(self) -> tuple[float, float, float, float, float]:
         """(build, density, force recompute + integrate reverse, pair gather,
         density gather) milliseconds of the last executed adjoint step; waits
-        for it. Needs :meth:`enable_phase_timing`."""
+        for it. Needs :meth:`enable_phase_timing`. A step reversed by
+        :meth:`segment_backward_raw` reads its build and density from the
+        segment tape, so those two phases are 0 there."""
         ms = (ctypes.c_float * 5)()
         _lib.check(self._lib.nsph_sph_adjoint_phase_times(self._handle, ctypes.byref(ms)),
                    "SolverSPH.adjoint_phase_times")

@@ -11,8 +11,10 @@ run under the tape, every intermediate array is kept, and
   them keeps every state; any torch code may sit between steps.
 - :func:`sph_rollout` — ``steps`` steps as one node with checkpointing: the
   forward keeps only every ``checkpoint_every``-th state, and the backward
-  recomputes each segment from its checkpoint before reversing it, so memory
-  is O(N (steps / K + K)) instead of O(N steps). The forward step is
+  recomputes each segment from its checkpoint before reversing it
+  (``nsph_sph_segment_adjoint``, which keeps each recomputed step's grid and
+  density scratch so that the reverse does not rebuild them), so memory is
+  O(N (steps / K + K)) instead of O(N steps). The forward step is
   deterministic, so the recomputed states are bit-identical to the first
   pass.
 
@@ -118,16 +120,11 @@ class _SPHRollout(torch.autograd.Function):
         va = torch.zeros_like(x0) if gv is None else gv.contiguous().float().clone()
         bg = torch.zeros(1, dtype=torch.float32, device=x0.device)
         fg = torch.zeros_like(x0) if f is not None else None
-        sx = torch.empty((min(every, steps), n, 3), dtype=torch.float32, device=x0.device)
-        sv = torch.empty_like(sx)
         for c, (start, length) in enumerate(checkpoint_schedule(steps, every)):
+            # recompute the segment from its checkpoint, keeping each step's
+            # grid and density scratch, and reverse it
             cx, cv = ctx.checkpoints[len(ctx.checkpoints) - 1 - c]
-            sx[0].copy_(cx)
-            sv[0].copy_(cv)
-            if length > 1:  # recompute the segment's input states from its checkpoint
-                solver.rollout_raw(sx[0], sv[0], sx[1:length], sv[1:length], params, f)
-            solver.rollout_backward_raw(sx[:length], sv[:length], params, xa, va, f_ext=f, f_ext_grad=fg,
-                                        eos_b_grad=bg)
+            solver.segment_backward_raw(cx, cv, length, params, xa, va, f_ext=f, f_ext_grad=fg, eos_b_grad=bg)
         ctx.checkpoints = None
         gb = bg.to(ctx.b_meta[0]).reshape(ctx.b_meta[1]) if ctx.has_b else None
         return xa, va, gb, fg, None, None, None, None
@@ -138,9 +135,11 @@ def sph_rollout(solver: SolverSPH, x0: torch.Tensor, v0: torch.Tensor, steps: in
                 checkpoint_every: int = 10) -> tuple[torch.Tensor, torch.Tensor]:
     """`steps` differentiable WCSPH steps from (x0, v0), checkpointed.
 
-    The backward pass costs one extra forward step per step (segment
-    recompute) plus the adjoint step, and holds steps / checkpoint_every
-    checkpoints plus one segment of states.
+    The backward pass costs one extra forward step per step (the segment
+    recompute, whose grid build and density pass the adjoint step then
+    reuses) plus the adjoint step, and holds steps / checkpoint_every
+    checkpoints plus one segment's tape (88 bytes per particle and 8 per
+    grid cell, per step).
 
     Returns:
         (x_T, v_T), each (N, 3) float32.

@@ -267,3 +267,95 @@ def test_adjoint_argument_checks():
     torch.cuda.synchronize()
     with pytest.raises(ValueError):
         solver.step_backward_raw(xt, vt, p, g1[:5], g2, g1, g2)
+
+
+def test_segment_tape_equals_recompute_then_reverse():
+    """nsph_sph_segment_adjoint (recompute keeping each step's grid and
+    density scratch, then reverse from it) is bit-identical to
+    nsph_sph_rollout of the segment followed by nsph_sph_rollout_adjoint,
+    with every branch live: walls, the |v| clamp, inactive and kinematic
+    particles, an external force and the B gradient; and it leaves the
+    solver's grid describing the segment's last input state."""
+    from newton_sph_dev_b200.solvers import SolverSPH
+
+    dt, steps = 1e-4, 7
+    model, cfg, x, v, rng = block_scene((12, 12, 8), 0.01, 5, 0.3, v_max=0.5, n_inactive=17, n_kinematic=13,
+                                        floor_shift=0.004, floor_speed=0.5)
+    solver = SolverSPH(model, cfg)
+    n = len(x)
+    p = solver.step_params(dt)
+    x0, v0 = torch.from_numpy(x).to(DEV), torch.from_numpy(v).to(DEV)
+    f = torch.from_numpy(rng.normal(0, 1e-3, x.shape).astype(np.float32)).to(DEV)
+    gx = torch.from_numpy(rng.normal(0, 1, x.shape).astype(np.float32)).to(DEV)
+    gv = torch.from_numpy(rng.normal(0, 1, x.shape).astype(np.float32)).to(DEV)
+
+    # recompute, then reverse
+    sx = torch.empty((steps, n, 3), dtype=torch.float32, device=DEV)
+    sv = torch.empty_like(sx)
+    sx[0].copy_(x0)
+    sv[0].copy_(v0)
+    solver.rollout_raw(sx[0], sv[0], sx[1:], sv[1:], p, f)
+    xa, va = gx.clone(), gv.clone()
+    fa, ba = torch.zeros_like(x0), torch.zeros(1, device=DEV)
+    solver.rollout_backward_raw(sx, sv, p, xa, va, f_ext=f, f_ext_grad=fa, eos_b_grad=ba)
+
+    # the tape
+    xb, vb = gx.clone(), gv.clone()
+    fb, bb = torch.zeros_like(x0), torch.zeros(1, device=DEV)
+    solver.segment_backward_raw(x0, v0, steps, p, xb, vb, f_ext=f, f_ext_grad=fb, eos_b_grad=bb)
+    torch.cuda.synchronize()
+    assert torch.isfinite(xa).all() and float(xa.abs().max()) > 0.0
+    for a, b in ((xa, xb), (va, vb), (fa, fb), (ba, bb)):
+        assert torch.equal(a, b)
+    assert solver.status() == 0
+
+    # the solver's grid and mirrors now describe the last input state: its
+    # neighbour lists equal those of a plain step on that state
+    after = solver.neighbors()
+    solver.step_raw(sx[steps - 1], sv[steps - 1], torch.empty_like(x0), sv[steps - 1].clone(), p, f)
+    ref = solver.neighbors()
+    assert all(torch.equal(a, b) for a, b in zip(after, ref))
+
+    # a longer segment than the tape holds grows it; a shorter one reuses it
+    xc, vc = gx.clone(), gv.clone()
+    solver.segment_backward_raw(x0, v0, 2, p, xc, vc, f_ext=f)
+    solver.segment_backward_raw(x0, v0, steps + 3, p, xc, vc, f_ext=f)
+    torch.cuda.synchronize()
+    assert torch.isfinite(xc).all()
+
+
+def test_segment_adjoint_argument_checks():
+    import ctypes
+
+    from newton_sph_dev_b200 import _lib
+    from newton_sph_dev_b200.solvers import SolverSPH
+
+    model, cfg, x, v, _ = block_scene((4, 4, 4), 0.01, 0, 0.0)
+    solver = SolverSPH(model, cfg)
+    xt, vt = torch.from_numpy(x).to(DEV), torch.from_numpy(v).to(DEV)
+    p = solver.step_params(1e-4)
+    L = _lib.load()
+    n = len(x)
+
+    def call(x0, v0, xa, va, steps=3):
+        return L.nsph_sph_segment_adjoint(solver._handle, ctypes.byref(p), n, steps, x0, v0, None,
+                                          model.particle_mass.data_ptr(), model.particle_inv_mass.data_ptr(),
+                                          model.particle_flags.data_ptr(), model.particle_world.data_ptr(),
+                                          model.gravity.data_ptr(), 1, xa, va, None, None,
+                                          _lib.stream_handle(model.device))
+
+    g1, g2 = torch.zeros_like(xt), torch.zeros_like(xt)
+    # adjoint scratch not enabled yet
+    assert call(xt.data_ptr(), vt.data_ptr(), g1.data_ptr(), g2.data_ptr()) == _lib.NSPH_ERR_INVALID_ARG
+    solver.enable_adjoint()
+    assert call(xt.data_ptr(), vt.data_ptr(), g1.data_ptr(), g2.data_ptr()) == _lib.NSPH_OK
+    assert call(xt.data_ptr(), vt.data_ptr(), None, g2.data_ptr()) == _lib.NSPH_ERR_INVALID_ARG
+    # adjoints overlapping each other or the initial state
+    assert call(xt.data_ptr(), vt.data_ptr(), g1.data_ptr(), g1.data_ptr()) == _lib.NSPH_ERR_INVALID_ARG
+    assert call(xt.data_ptr(), vt.data_ptr(), xt.data_ptr(), g2.data_ptr()) == _lib.NSPH_ERR_INVALID_ARG
+    assert call(xt.data_ptr(), vt.data_ptr(), g1.data_ptr(), g2.data_ptr(), steps=-1) == _lib.NSPH_ERR_INVALID_ARG
+    assert call(xt.data_ptr(), vt.data_ptr(), g1.data_ptr(), g2.data_ptr(), steps=0) == _lib.NSPH_OK
+    assert L.nsph_sph_reserve_segment(solver._handle, -1) == _lib.NSPH_ERR_INVALID_ARG
+    torch.cuda.synchronize()
+    with pytest.raises(ValueError):
+        solver.segment_backward_raw(xt, vt, 2, p, g1[:5], g2)
