@@ -299,16 +299,16 @@ NSPH_API int nsph_sph_rollout_adjoint(nsph_sph* solver, const nsph_sph_params* p
  * reverses it, replacing nsph_sph_rollout (of steps - 1 steps) followed by
  * nsph_sph_rollout_adjoint, with bit-identical results.
  * nsph_sph_segment_adjoint: `steps` steps from (x0, v0). The forward keeps,
- *   per step, the grid build and density pass that the step's reverse reads
- *   (sorted mirrors, cell table, sorted ids, m/rho, p/rho^2, rho, p,
- *   neighbour masks), so the reverse skips the rebuild and the density pass;
- *   the last step's force pass is not run. x_adj / v_adj hold the adjoint of
+ *   per step, the grid build, density pass and force sums that the step's
+ *   reverse reads (sorted mirrors, cell table, sorted ids, m/rho, p/rho^2,
+ *   rho, p, neighbour masks, a and the XSPH sum), so the reverse skips the
+ *   rebuild, the density pass and the force recompute. x_adj / v_adj hold the adjoint of
  *   the state after `steps` steps on entry and of (x0, v0) on return (they
  *   must not overlap each other or x0 / v0); f_ext_adj and eos_b_adj
  *   accumulate as in nsph_sph_step_adjoint. Afterwards the solver's grid
  *   describes the last step's input.
  * nsph_sph_reserve_segment: allocates the tape for segments of up to
- *   `steps` steps (88 bytes per particle of capacity plus 8 bytes per grid
+ *   `steps` steps (120 bytes per particle of capacity plus 8 bytes per grid
  *   cell, per step, and two states); nsph_sph_segment_adjoint reserves on
  *   demand, so call this first where the call is captured in a graph. */
 NSPH_API int nsph_sph_reserve_segment(nsph_sph* solver, int steps);

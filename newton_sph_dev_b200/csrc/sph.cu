@@ -291,6 +291,7 @@ struct StepOut {
     float* p_out;
     float* a_out;
     unsigned* status;
+    float4* acc_sorted;  // or null: (a, 0), (dv, 0) of sorted particle k at 2k, 2k + 1 (the segment tape)
 };
 
 // integrate particle k (original index i) and scatter its outputs
@@ -371,6 +372,10 @@ __global__ void __launch_bounds__(kSphThreads, 3) k_force(GridDev g, const float
         const int attr = __float_as_int(vi.w);
         ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (attr & kAttrActive) force_single(g, xs, vs, aux, mask, ncand[k], n, k, xi, vi, aux[k].y, p, acc);
+        if (o.acc_sorted) {
+            o.acc_sorted[2 * (size_t)k] = make_float4(acc.ax, acc.ay, acc.az, 0.f);
+            o.acc_sorted[2 * (size_t)k + 1] = make_float4(acc.dvx, acc.dvy, acc.dvz, 0.f);
+        }
         integrate_out((size_t)g.ids[k], xi, vi, attr, rp[k], acc, p, p.dt, o);
     }
 }
@@ -565,10 +570,12 @@ struct AdjIO {
     float4* d;     // sorted: adj(dv)
     float* rho;    // sorted: adj(rho)
     float* bpart;  // per block: partial adj(B)
+    const float4* acc;  // or null: the forward's sorted (a, 0), (dv, 0) (the segment tape), else recomputed
 };
 
 // reverse of integrate: recompute the forward particle update (bit for bit,
-// so the clamp decisions are the forward's), then transpose it
+// so the clamp decisions are the forward's), then transpose it. The force
+// sums a, dv are the forward's, stored (io.acc) or recomputed here.
 __global__ void __launch_bounds__(kSphThreads, 2) k_adj_local(GridDev g, const float4* __restrict__ xs,
                                                               const float4* __restrict__ vs,
                                                               const float2* __restrict__ aux, int n,
@@ -591,7 +598,12 @@ __global__ void __launch_bounds__(kSphThreads, 2) k_adj_local(GridDev g, const f
             }
         } else {
             ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            force_single(g, xs, vs, aux, mask, ncand[k], n, k, xi, vi, aux[k].y, p, acc);
+            if (io.acc) {
+                const float4 a = io.acc[2 * (size_t)k], d = io.acc[2 * (size_t)k + 1];
+                acc = ForceAcc{a.x, a.y, a.z, d.x, d.y, d.z};
+            } else {
+                force_single(g, xs, vs, aux, mask, ncand[k], n, k, xi, vi, aux[k].y, p, acc);
+            }
             const bool dynamic = (attr & kAttrDynamic) != 0;
             float w = 0.f;
             float u[3] = {vi.x, vi.y, vi.z};
@@ -1098,7 +1110,8 @@ struct nsph_sph {
 };
 
 // One step's slot of the segment tape: the sorted mirrors, the density
-// pass's outputs and neighbour masks, and the grid (sorted ids, cell table).
+// pass's outputs and neighbour masks, the grid (sorted ids, cell table) and
+// the force pass's sums.
 struct TapeStep {
     float4* xs;
     float4* vs;
@@ -1108,6 +1121,7 @@ struct TapeStep {
     int* ncand;
     int* ids;
     int2* ranges;
+    float4* acc;  // the force pass's (a, 0), (dv, 0) per sorted particle
 };
 
 static size_t tape_align(size_t b) { return (b + 255) & ~(size_t)255; }
@@ -1116,7 +1130,7 @@ static size_t tape_slot_bytes(size_t c, long long ncells)
 {
     return 2 * tape_align(sizeof(float4) * c) + 2 * tape_align(sizeof(float2) * c) +
            tape_align(sizeof(unsigned) * kMaskWords * c) + 2 * tape_align(sizeof(int) * c) +
-           tape_align(sizeof(int2) * (size_t)ncells);
+           tape_align(sizeof(int2) * (size_t)ncells) + tape_align(sizeof(float4) * 2 * c);
 }
 
 static TapeStep tape_slot(const nsph_sph* s, int t)
@@ -1139,6 +1153,8 @@ static TapeStep tape_slot(const nsph_sph* s, int t)
     ts.ids = reinterpret_cast<int*>(b);
     b += tape_align(sizeof(int) * c);
     ts.ranges = reinterpret_cast<int2*>(b);
+    b += tape_align(sizeof(int2) * (size_t)s->grid.ncells);
+    ts.acc = reinterpret_cast<float4*>(b);
     return ts;
 }
 
@@ -1706,7 +1722,7 @@ static int adjoint_enqueue(nsph_sph* s, const nsph_sph_params* p, int n, const f
         ++launches;
         const AdjIO io{x_out_adj, v_out_adj, rho_out_adj, x_in_adj, v_in_adj, f_ext_adj, f_ext, inv_mass, gravity,
                        s->adj_g, s->adj_d, s->adj_rho, s->adj_bpart};
-        const TapeStep ts{s->xs, s->vs, s->aux, s->rp, s->mask, s->ncand, nullptr, nullptr};
+        const TapeStep ts{s->xs, s->vs, s->aux, s->rp, s->mask, s->ncand, nullptr, nullptr, nullptr};
         st = adjoint_kernels(s, p, n, g, ts, io, eos_b_adj, cs, launches, true);
         if (st != NSPH_OK) return st;
     } else {
@@ -1845,8 +1861,8 @@ extern "C" int nsph_sph_segment_adjoint(nsph_sph* s, const nsph_sph_params* p, i
     int launches = 0;
     int blocks, threads;
     pass_launch(s, n, false, blocks, threads);
-    // forward: the build and density pass of every step into its slot; the
-    // force pass of every step but the last (whose output is not needed)
+    // forward: the build, density and force passes of every step, their
+    // outputs into the step's slot (the last step's new state is not used)
     for (int t = 0; t < steps; ++t) {
         const float* xi = t == 0 ? x0 : tape_state(s, t & 1);
         const float* vi = t == 0 ? v0 : tape_state(s, t & 1) + len;
@@ -1864,16 +1880,14 @@ extern "C" int nsph_sph_segment_adjoint(nsph_sph* s, const nsph_sph_params* p, i
         k_density<<<blocks, threads, 0, cs>>>(g, ts.xs, ts.vs, n, *p, ts.aux, ts.rp, ts.mask, ts.ncand, s->status);
         NSPH_LAUNCH_CHECK("k_density");
         ++launches;
-        if (t + 1 < steps) {
-            float* xo = tape_state(s, (t + 1) & 1);
-            float* vo = xo + len;
-            // inactive particles keep their velocity (the step leaves it untouched)
-            NSPH_CUDA_TRY(cudaMemcpyAsync(vo, vi, sizeof(float) * len, cudaMemcpyDeviceToDevice, cs));
-            const StepOut o{f_ext, inv_mass, gravity, xo, vo, nullptr, nullptr, nullptr, s->status};
-            k_force<<<blocks, threads, 0, cs>>>(g, ts.xs, ts.vs, ts.aux, ts.rp, n, *p, ts.mask, ts.ncand, o);
-            NSPH_LAUNCH_CHECK("k_force");
-            ++launches;
-        }
+        float* xo = tape_state(s, (t + 1) & 1);
+        float* vo = xo + len;
+        // inactive particles keep their velocity (the step leaves it untouched)
+        if (t + 1 < steps) NSPH_CUDA_TRY(cudaMemcpyAsync(vo, vi, sizeof(float) * len, cudaMemcpyDeviceToDevice, cs));
+        const StepOut o{f_ext, inv_mass, gravity, xo, vo, nullptr, nullptr, nullptr, s->status, ts.acc};
+        k_force<<<blocks, threads, 0, cs>>>(g, ts.xs, ts.vs, ts.aux, ts.rp, n, *p, ts.mask, ts.ncand, o);
+        NSPH_LAUNCH_CHECK("k_force");
+        ++launches;
     }
     // the solver's mirrors describe its grid's last build (the last step's input)
     const TapeStep last = tape_slot(s, steps - 1);
@@ -1881,10 +1895,11 @@ extern "C" int nsph_sph_segment_adjoint(nsph_sph* s, const nsph_sph_params* p, i
     NSPH_CUDA_TRY(cudaMemcpyAsync(s->vs, last.vs, sizeof(float4) * (size_t)n, cudaMemcpyDeviceToDevice, cs));
     s->last_n = n;
     // reverse, from the slots
-    const AdjIO io{x_adj, v_adj, nullptr, x_adj, v_adj, f_ext_adj, f_ext, inv_mass, gravity,
-                   s->adj_g, s->adj_d, s->adj_rho, s->adj_bpart};
+    AdjIO io{x_adj, v_adj, nullptr, x_adj, v_adj, f_ext_adj, f_ext, inv_mass, gravity,
+             s->adj_g, s->adj_d, s->adj_rho, s->adj_bpart, nullptr};
     for (int t = steps - 1; t >= 0; --t) {
         const TapeStep ts = tape_slot(s, t);
+        io.acc = ts.acc;
         GridDev g = s->grid.view();
         g.ranges = ts.ranges;
         g.ids = ts.ids;

@@ -12,8 +12,9 @@ run under the tape, every intermediate array is kept, and
 - :func:`sph_rollout` — ``steps`` steps as one node with checkpointing: the
   forward keeps only every ``checkpoint_every``-th state, and the backward
   recomputes each segment from its checkpoint before reversing it
-  (``nsph_sph_segment_adjoint``, which keeps each recomputed step's grid and
-  density scratch so that the reverse does not rebuild them), so memory is
+  (``nsph_sph_segment_adjoint``, which keeps each recomputed step's grid,
+  density scratch and force sums so that the reverse does not recompute
+  them), so memory is
   O(N (steps / K + K)) instead of O(N steps). The forward step is
   deterministic, so the recomputed states are bit-identical to the first
   pass.
@@ -136,10 +137,10 @@ def sph_rollout(solver: SolverSPH, x0: torch.Tensor, v0: torch.Tensor, steps: in
     """`steps` differentiable WCSPH steps from (x0, v0), checkpointed.
 
     The backward pass costs one extra forward step per step (the segment
-    recompute, whose grid build and density pass the adjoint step then
-    reuses) plus the adjoint step, and holds steps / checkpoint_every
-    checkpoints plus one segment's tape (88 bytes per particle and 8 per
-    grid cell, per step).
+    recompute, whose grid build, density pass and force sums the adjoint
+    step then reuses) plus the adjoint step, and holds steps /
+    checkpoint_every checkpoints plus one segment's tape (120 bytes per
+    particle and 8 per grid cell, per step).
 
     Returns:
         (x_T, v_T), each (N, 3) float32.
