@@ -11,7 +11,10 @@
 //   k_hash_hist   original order: cell id per point + digit-0 tile histograms;
 //                 also clears the cell ranges the previous build wrote.
 //   per 8-bit digit pass: [k_upsweep] -> k_scan_rows -> k_downsweep
-//                 stable multi-split per 2048-key tile (warp match_any ranks,
+//                 stable multi-split per tile of 256 x kItems keys (2048,
+//                 or 512 for builds of at most kSmallBuildPoints points, so
+//                 that small builds still spread over the SMs; the sorted
+//                 result does not depend on the tile) (warp match_any ranks,
 //                 shared-memory staging for coalesced scatter). The last pass
 //                 writes point_cells / point_ids and, in SPH mode, gathers the
 //                 sorted float4 mirrors of position and velocity.
@@ -40,6 +43,7 @@ __device__ __forceinline__ unsigned lanemask_lt()
 // Also clears the previous build's occupied cells (their first sorted entry
 // resets start/end to 0), so no full memset of the cell tables is needed.
 // --------------------------------------------------------------------------
+template <int kItems>
 __global__ void __launch_bounds__(kSortThreads) k_hash_hist(
     const float* __restrict__ points, int n, float inv, int dx, int dy, int dz, int* __restrict__ keys,
     int* __restrict__ vals, unsigned* __restrict__ hist, int ntiles, int digit_mask,
@@ -51,10 +55,10 @@ __global__ void __launch_bounds__(kSortThreads) k_hash_hist(
     for (int i = threadIdx.x; i < (kSortThreads / 32) * kRadix; i += kSortThreads) (&wh[0][0])[i] = 0u;
     __syncthreads();
 
-    const int base = blockIdx.x * kSortTile;
+    const int base = blockIdx.x * (kSortThreads * kItems);
     bool bad = false;
 #pragma unroll 4
-    for (int it = 0; it < kSortItems; ++it) {
+    for (int it = 0; it < kItems; ++it) {
         const int idx = base + it * kSortThreads + threadIdx.x;
         if (idx < prev_n) {
             const int c = prev_cells[idx];
@@ -92,6 +96,7 @@ __global__ void __launch_bounds__(kSortThreads) k_hash_hist(
 }
 
 // Histogram of one digit per tile (passes after the first).
+template <int kItems>
 __global__ void __launch_bounds__(kSortThreads) k_upsweep(const int* __restrict__ keys, int n, int shift,
                                                           int digit_mask, unsigned* __restrict__ hist,
                                                           int ntiles)
@@ -100,9 +105,9 @@ __global__ void __launch_bounds__(kSortThreads) k_upsweep(const int* __restrict_
     const int warp = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < (kSortThreads / 32) * kRadix; i += kSortThreads) (&wh[0][0])[i] = 0u;
     __syncthreads();
-    const int base = blockIdx.x * kSortTile;
+    const int base = blockIdx.x * (kSortThreads * kItems);
 #pragma unroll 4
-    for (int it = 0; it < kSortItems; ++it) {
+    for (int it = 0; it < kItems; ++it) {
         const int idx = base + it * kSortThreads + threadIdx.x;
         if (idx < n) atomicAdd(&wh[warp][(keys[idx] >> shift) & digit_mask], 1u);
     }
@@ -161,24 +166,24 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_rows(unsigned* __restrict
 
 // --------------------------------------------------------------------------
 // k_downsweep: stable scatter of one digit pass.
-// Warp w owns tile elements [w*256, w*256+256) in 8 rounds of 32; within a
-// round lanes with equal digits are ranked by __match_any_sync, and a
+// Warp w owns tile elements [w*32*kItems, (w+1)*32*kItems) in kItems rounds
+// of 32; within a round lanes with equal digits are ranked by __match_any_sync, and a
 // per-warp counter carries ranks across rounds, so the order inside a tile
 // is exactly the input order per digit. Keys are staged in shared memory in
 // tile-sorted order and written out in runs (coalesced).
 // --------------------------------------------------------------------------
 constexpr int kWarps = kSortThreads / 32;
-constexpr int kPerWarp = kSortTile / kWarps;  // 256
 
+template <int kItems>
 struct DownsweepSmem {
     unsigned warp_cnt[kWarps][kRadix];
     unsigned tile_off[kRadix];
     unsigned glob_off[kRadix];
-    int keys[kSortTile];
-    int vals[kSortTile];
+    int keys[kSortThreads * kItems];
+    int vals[kSortThreads * kItems];
 };
 
-template <bool kGather>
+template <bool kGather, int kItems>
 __global__ void __launch_bounds__(kSortThreads) k_downsweep(const int* __restrict__ keys_in,
                                                             const int* __restrict__ vals_in,
                                                             int* __restrict__ keys_out, int* __restrict__ vals_out,
@@ -187,19 +192,21 @@ __global__ void __launch_bounds__(kSortThreads) k_downsweep(const int* __restric
                                                             const unsigned* __restrict__ digit_tot,
                                                             GatherArgs gather)
 {
+    constexpr int kTile = kSortThreads * kItems;
+    constexpr int kPerWarp = kTile / kWarps;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    DownsweepSmem& sm = *reinterpret_cast<DownsweepSmem*>(smem_raw);
+    DownsweepSmem<kItems>& sm = *reinterpret_cast<DownsweepSmem<kItems>*>(smem_raw);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < kWarps * kRadix; i += kSortThreads) (&sm.warp_cnt[0][0])[i] = 0u;
     __syncthreads();
 
-    const int tile_base = blockIdx.x * kSortTile;
-    const int tile_n = min(kSortTile, n - tile_base);
-    int key[kSortItems], val[kSortItems];
-    unsigned rank[kSortItems];
+    const int tile_base = blockIdx.x * kTile;
+    const int tile_n = min(kTile, n - tile_base);
+    int key[kItems], val[kItems];
+    unsigned rank[kItems];
     const unsigned lt = lanemask_lt();
 #pragma unroll
-    for (int r = 0; r < kSortItems; ++r) {
+    for (int r = 0; r < kItems; ++r) {
         const int local = warp * kPerWarp + r * 32 + lane;
         const bool valid = local < tile_n;
         key[r] = valid ? keys_in[tile_base + local] : 0;
@@ -234,7 +241,7 @@ __global__ void __launch_bounds__(kSortThreads) k_downsweep(const int* __restric
     sm.tile_off[d] = block_exclusive_scan(total, dummy, ws);
     __syncthreads();
 #pragma unroll
-    for (int r = 0; r < kSortItems; ++r) {
+    for (int r = 0; r < kItems; ++r) {
         const int local = warp * kPerWarp + r * 32 + lane;
         if (local < tile_n) {
             const int d = (key[r] >> shift) & digit_mask;
@@ -297,7 +304,38 @@ __global__ void k_query(GridDev g, const float* __restrict__ q, int nq, float ra
     }
 }
 
-inline int ntiles_of(int n) { return (n + kSortTile - 1) / kSortTile; }
+inline int ntiles_of(int n, int items = kSortItems)
+{
+    const int tile = kSortThreads * items;
+    return (n + tile - 1) / tile;
+}
+
+// Small builds use tiles of 512 keys (2 per thread), so that a build of 65k
+// points runs 128 CTAs instead of 32.
+constexpr int kSmallItems = 2;
+constexpr int kSmallBuildPoints = 1 << 18;
+inline int items_for(int n) { return n <= kSmallBuildPoints ? kSmallItems : kSortItems; }
+
+// per-tile histogram rows the table needs for builds of up to `capacity` points
+inline int hist_tiles(int capacity)
+{
+    return std::max(ntiles_of(capacity, kSortItems), ntiles_of(std::min(capacity, kSmallBuildPoints), kSmallItems));
+}
+
+template <int kItems>
+cudaError_t load_sort_kernels()
+{
+    cudaFuncAttributes fa;
+    cudaError_t e = cudaFuncGetAttributes(&fa, k_hash_hist<kItems>);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_upsweep<kItems>);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_downsweep<false, kItems>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(DownsweepSmem<kItems>));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_downsweep<true, kItems>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(DownsweepSmem<kItems>));
+    return e;
+}
 
 }  // namespace
 
@@ -324,17 +362,11 @@ int grid_init(Grid& g, int dx, int dy, int dz, int device)
     // load every kernel now, so that a later stream capture never triggers
     // lazy module loading
     cudaFuncAttributes fa;
-    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_hash_hist));
-    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_upsweep));
+    NSPH_CUDA_TRY(load_sort_kernels<kSortItems>());
+    NSPH_CUDA_TRY(load_sort_kernels<kSmallItems>());
     NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_scan_rows));
-    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_downsweep<false>));
-    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_downsweep<true>));
     NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_ranges));
     NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_query));
-    NSPH_CUDA_TRY(cudaFuncSetAttribute(k_downsweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sizeof(DownsweepSmem)));
-    NSPH_CUDA_TRY(cudaFuncSetAttribute(k_downsweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)sizeof(DownsweepSmem)));
     NSPH_CUDA_TRY(cudaDeviceSynchronize());
     return NSPH_OK;
 }
@@ -365,11 +397,9 @@ int grid_init_worlds(Grid& g, const int* world_dims, int world_count, int device
     NSPH_CUDA_TRY(cudaMalloc(&g.worlds, sizeof(WorldCells) * world_count));
     NSPH_CUDA_TRY(cudaMemcpy(g.worlds, wc.data(), sizeof(WorldCells) * world_count, cudaMemcpyHostToDevice));
     cudaFuncAttributes fa;
-    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_hash_hist));
-    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_upsweep));
+    NSPH_CUDA_TRY(load_sort_kernels<kSortItems>());
+    NSPH_CUDA_TRY(load_sort_kernels<kSmallItems>());
     NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_scan_rows));
-    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_downsweep<false>));
-    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_downsweep<true>));
     NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_ranges));
     NSPH_CUDA_TRY(cudaDeviceSynchronize());
     return NSPH_OK;
@@ -404,7 +434,7 @@ int grid_reserve(Grid& g, int capacity)
     if (e == cudaSuccess) e = cudaMalloc(&g.point_ids, sz);
     // per-tile digit histograms plus kRadix digit totals
     if (e == cudaSuccess)
-        e = cudaMalloc(&g.hist, sizeof(unsigned) * kRadix * ((size_t)std::max(1, ntiles_of(capacity)) + 1));
+        e = cudaMalloc(&g.hist, sizeof(unsigned) * kRadix * ((size_t)std::max(1, hist_tiles(capacity)) + 1));
     if (e != cudaSuccess) {
         cudaGetLastError();
         return fail(NSPH_ERR_OUT_OF_MEMORY, std::string("reserve: ") + cudaGetErrorString(e));
@@ -424,54 +454,52 @@ void grid_free(Grid& g)
     g = Grid();
 }
 
-int grid_build(Grid& g, const float* points, int n, float cell_width, float cell_inv, const GatherArgs* gather,
-               unsigned int* status, cudaStream_t stream, int* launches, const int* world)
+namespace {
+
+// hash, digit passes and ranges of one build with tiles of 256 x kItems keys
+template <int kItems>
+int build_passes(Grid& g, const float* points, int n, float cell_inv, const GatherArgs* gather, unsigned int* status,
+                 cudaStream_t stream, int& nl, const int* world, int prev_n)
 {
-    int local_launches = 0;
-    int& nl = launches ? *launches : local_launches;
-    if (n < 0) return fail(NSPH_ERR_INVALID_ARG, "negative point count");
-    if (n > g.capacity) return fail(NSPH_ERR_CAPACITY, "build: more points than reserved");
-    if (n > 0 && !points) return fail(NSPH_ERR_INVALID_ARG, "build: null points");
-    const int prev_n = g.built ? g.num_points : 0;
-    const int ntiles = ntiles_of(n);
-    const int launch_tiles = std::max(ntiles, ntiles_of(prev_n));
+    constexpr size_t kSmem = sizeof(DownsweepSmem<kItems>);
+    const int ntiles = ntiles_of(n, kItems);
+    const int launch_tiles = std::max(ntiles, ntiles_of(prev_n, kItems));
     const int passes = (g.key_bits + kRadixBits - 1) / kRadixBits;
     auto mask_of = [&](int p) {
         const int bits = std::min(kRadixBits, g.key_bits - p * kRadixBits);
         return (1 << bits) - 1;
     };
     if (launch_tiles > 0) {
-        k_hash_hist<<<launch_tiles, kSortThreads, 0, stream>>>(points, n, cell_inv, g.dx, g.dy, g.dz, g.keys_a,
-                                                               g.vals_a, g.hist, ntiles, mask_of(0),
-                                                               g.point_cells, prev_n, g.cell_ranges, status, world,
-                                                               g.worlds, g.world_count);
+        k_hash_hist<kItems><<<launch_tiles, kSortThreads, 0, stream>>>(
+            points, n, cell_inv, g.dx, g.dy, g.dz, g.keys_a, g.vals_a, g.hist, ntiles, mask_of(0), g.point_cells,
+            prev_n, g.cell_ranges, status, world, g.worlds, g.world_count);
         NSPH_LAUNCH_CHECK("k_hash_hist");
         ++nl;
     }
     if (n > 0) {
         const int* kin = g.keys_a;
         const int* vin = g.vals_a;
+        unsigned* digit_tot = g.hist + (size_t)kRadix * hist_tiles(g.capacity);
         for (int p = 0; p < passes; ++p) {
             const bool last = (p == passes - 1);
             int* kout = last ? g.point_cells : ((p & 1) ? g.keys_a : g.keys_b);
             int* vout = last ? g.point_ids : ((p & 1) ? g.vals_a : g.vals_b);
             const int shift = p * kRadixBits;
             if (p > 0) {
-                k_upsweep<<<ntiles, kSortThreads, 0, stream>>>(kin, n, shift, mask_of(p), g.hist, ntiles);
+                k_upsweep<kItems><<<ntiles, kSortThreads, 0, stream>>>(kin, n, shift, mask_of(p), g.hist, ntiles);
                 NSPH_LAUNCH_CHECK("k_upsweep");
                 ++nl;
             }
-            unsigned* digit_tot = g.hist + (size_t)kRadix * ntiles_of(g.capacity);
             k_scan_rows<<<kRadix, kScanThreads, 0, stream>>>(g.hist, ntiles, digit_tot);
             NSPH_LAUNCH_CHECK("k_scan_rows");
             ++nl;
             GatherArgs ga{};
             if (last && gather) {
                 ga = *gather;
-                k_downsweep<true><<<ntiles, kSortThreads, sizeof(DownsweepSmem), stream>>>(
+                k_downsweep<true, kItems><<<ntiles, kSortThreads, kSmem, stream>>>(
                     kin, vin, kout, vout, n, shift, mask_of(p), g.hist, ntiles, digit_tot, ga);
             } else {
-                k_downsweep<false><<<ntiles, kSortThreads, sizeof(DownsweepSmem), stream>>>(
+                k_downsweep<false, kItems><<<ntiles, kSortThreads, kSmem, stream>>>(
                     kin, vin, kout, vout, n, shift, mask_of(p), g.hist, ntiles, digit_tot, ga);
             }
             NSPH_LAUNCH_CHECK("k_downsweep");
@@ -483,6 +511,24 @@ int grid_build(Grid& g, const float* points, int n, float cell_width, float cell
         NSPH_LAUNCH_CHECK("k_ranges");
         ++nl;
     }
+    return NSPH_OK;
+}
+
+}  // namespace
+
+int grid_build(Grid& g, const float* points, int n, float cell_width, float cell_inv, const GatherArgs* gather,
+               unsigned int* status, cudaStream_t stream, int* launches, const int* world)
+{
+    int local_launches = 0;
+    int& nl = launches ? *launches : local_launches;
+    if (n < 0) return fail(NSPH_ERR_INVALID_ARG, "negative point count");
+    if (n > g.capacity) return fail(NSPH_ERR_CAPACITY, "build: more points than reserved");
+    if (n > 0 && !points) return fail(NSPH_ERR_INVALID_ARG, "build: null points");
+    const int prev_n = g.built ? g.num_points : 0;
+    const int st = items_for(n) == kSmallItems
+                       ? build_passes<kSmallItems>(g, points, n, cell_inv, gather, status, stream, nl, world, prev_n)
+                       : build_passes<kSortItems>(g, points, n, cell_inv, gather, status, stream, nl, world, prev_n);
+    if (st != NSPH_OK) return st;
     g.num_points = n;
     g.cell_width = cell_width;
     g.cell_inv = cell_inv;
@@ -702,8 +748,9 @@ extern "C" int nsph_grid_build_noalloc(const float* points, int num_points, floa
     auto mask_of = [&](int p) { return (1 << std::min(kRadixBits, bits - p * kRadixBits)) - 1; };
     const int ntiles = ntiles_of(n);
     const float inv = 1.0f / radius;
-    k_hash_hist<<<ntiles, kSortThreads, 0, cs>>>(points, n, inv, dim_x, dim_y, dim_z, keys_a, vals_a, hist, ntiles,
-                                                 mask_of(0), nullptr, 0, nullptr, nullptr, nullptr, nullptr, 0);
+    k_hash_hist<kSortItems><<<ntiles, kSortThreads, 0, cs>>>(points, n, inv, dim_x, dim_y, dim_z, keys_a, vals_a,
+                                                             hist, ntiles, mask_of(0), nullptr, 0, nullptr, nullptr,
+                                                             nullptr, nullptr, 0);
     NSPH_LAUNCH_CHECK("k_hash_hist");
     const int* kin = keys_a;
     const int* vin = vals_a;
@@ -713,14 +760,13 @@ extern "C" int nsph_grid_build_noalloc(const float* points, int num_points, floa
         int* vout = last ? point_ids : ((p & 1) ? vals_a : vals_b);
         const int shift = p * kRadixBits;
         if (p > 0) {
-            k_upsweep<<<ntiles, kSortThreads, 0, cs>>>(kin, n, shift, mask_of(p), hist, ntiles);
+            k_upsweep<kSortItems><<<ntiles, kSortThreads, 0, cs>>>(kin, n, shift, mask_of(p), hist, ntiles);
             NSPH_LAUNCH_CHECK("k_upsweep");
         }
         k_scan_rows<<<kRadix, kScanThreads, 0, cs>>>(hist, ntiles, digit_tot);
         NSPH_LAUNCH_CHECK("k_scan_rows");
-        k_downsweep<false><<<ntiles, kSortThreads, sizeof(DownsweepSmem), cs>>>(kin, vin, kout, vout, n, shift,
-                                                                                mask_of(p), hist, ntiles, digit_tot,
-                                                                                GatherArgs{});
+        k_downsweep<false, kSortItems><<<ntiles, kSortThreads, sizeof(DownsweepSmem<kSortItems>), cs>>>(
+            kin, vin, kout, vout, n, shift, mask_of(p), hist, ntiles, digit_tot, GatherArgs{});
         NSPH_LAUNCH_CHECK("k_downsweep");
         kin = kout;
         vin = vout;
