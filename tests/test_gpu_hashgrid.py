@@ -70,6 +70,27 @@ def test_rebuild_clears_previous_ranges(oracle_mod):
     assert int(grid.cell_starts.abs().sum()) == 0 and int(grid.cell_ends.abs().sum()) == 0
 
 
+def test_rebuilds_across_the_sort_tile_sizes(oracle_mod):
+    """Builds of at most 262,144 points sort in 512-key tiles, larger ones in
+    2048-key tiles; each rebuild clears the previous build's cells in its own
+    tile size. Alternating sizes across that boundary (exactly at it, one
+    above, far above and far below) gives the oracle's grid every time."""
+    from newton_sph_dev_b200 import HashGrid
+
+    dims = (128, 128, 128)
+    radius = 0.02
+    grid = HashGrid(*dims, device=DEV)
+    grid.reserve(400000)
+    for i, n in enumerate([262144, 262145, 400000, 5000, 300001, 262144, 1]):
+        pts = _points(n, seed=100 + i, lo=-0.3 + 0.1 * i, hi=1.2 + 0.1 * i)
+        grid.build(torch.from_numpy(pts).to(DEV), radius)
+        torch.cuda.synchronize()
+        got = _grid_arrays(grid)
+        ref = oracle_mod.grid_build(pts, radius, dims)
+        for k in ref:
+            np.testing.assert_array_equal(got[k], ref[k], err_msg=f"build {i} (n={n}): {k}")
+
+
 @pytest.mark.parametrize("dims,radius,qradius", [((128, 128, 128), 0.05, 0.05), ((16, 8, 4), 0.05, 0.12),
                                                  ((64, 64, 64), 0.1, 0.03)])
 def test_query_matches_oracle(oracle_mod, dims, radius, qradius):
