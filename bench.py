@@ -69,6 +69,14 @@ WORKLOADS = {
                        desc="particle-particle contact (eval_particle_contact): 1,048,576 spheres of radius 0.005 m "
                             "on a jittered 0.0095 m lattice (touching neighbours), v ~ N(0, 0.1 m/s); one step = "
                             "HashGrid build at 2 r_max + cohesion + contact forces"),
+    "raycast_1m": dict(shape=(128, 128, 64), spacing=0.0095, radius=0.005, vel_std=0.0,
+                       raycast=dict(width=640, height=480, fov=1.0, position=(2.2, -1.0, 1.6), target=(0.6, 0.6, 0.3),
+                                    max_distance=4.0),
+                       metric="rays/s",
+                       desc="SensorRaycast particle depth image: 640x480 rays against 1,048,576 spheres of radius "
+                            "0.005 m on a jittered 0.0095 m lattice (a 1.22 x 1.22 x 0.61 m block) seen from 2.6 m; "
+                            "one step = HashGrid(128,128,128) build at r_max + 1e-6, the march (step half of that, "
+                            "max distance 4 m) and the no-hit clamp"),
     "worlds_4096": dict(worlds=4096, n_range=(256, 16384), s_range=(0.004, 0.01), box=(0.5, 0.5, 0.5), dt=1e-4,
                         vel_std=0.0, seed=3,
                         desc="4,096 independent scenes: particles log-uniform in [256, 16384], spacing uniform in "
@@ -890,7 +898,7 @@ def run_surrogate(args):
 
         dist.init_process_group("nccl", device_id=device, timeout=timedelta(seconds=120))
     from newton_sph_dev_b200.solvers import SolverSPH
-    from newton_sph_dev_b200.solvers.sph_surrogate import SurrogateModel, SurrogateSPH
+    from newton_sph_dev_b200.solvers.sph_surrogate import FallbackMonitor, SurrogateModel, SurrogateSPH
 
     model, cfg, w = make_scene(args.workload, str(device))
     n = model.particle_count
@@ -970,12 +978,19 @@ def run_surrogate(args):
     finite = bool(torch.isfinite(cur.particle_q).all() and torch.isfinite(cur.particle_qd).all())
 
     # end to end through the public API: host state in, one call, host state
-    # out, every call (pipelined over independent calls, as for tank_1m)
+    # out, every call (pipelined over independent calls, as for tank_1m). The
+    # calls all start from the timed run's first state, with the fallback
+    # rule reset: repeating one state repeats its compression, so a state
+    # whose surrogate step trips the rule would make every other window plain
     e2e_steps = min(args.steps, 50)
-    hx, hv = cur.particle_q.cpu().pin_memory(), cur.particle_qd.cpu().pin_memory()
+    hx, hv = start_q.cpu().pin_memory(), start_qd.cpu().pin_memory()
+    stepper.monitor = FallbackMonitor(sw["threshold"])
+    stepper.calls = 0
+    fb_e2e0 = stepper.fallback_calls
     e2e_ms = pipelined_e2e(model, lambda a, b: stepper.step(a, b, dt), hx, hv, e2e_steps, device)
     e2e_ms = max_over_ranks(e2e_ms, device)
     e2e_value = world * n * sub * e2e_steps / (e2e_ms * 1e-3)
+    e2e_fallbacks = stepper.fallback_calls - fb_e2e0
 
     peak, peak_kind = load_peak()
     tpeak, tpeak_kind = load_tensor_peak()
@@ -1038,7 +1053,8 @@ def run_surrogate(args):
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": w["metric"], "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n,
                     "steps": e2e_steps, "how": "pinned upload, one SurrogateSPH.step call, download, every call; "
-                                              "independent calls pipelined on upload / compute / download streams"},
+                                              "independent calls pipelined on upload / compute / download streams",
+                    "state": "the timed run's first state, fallback rule reset", "fallback_calls": e2e_fallbacks},
             "gpu_launches": stepper.launches_per_step * n_sur + fallbacks * sub * solver.last_launches,
             "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
             "status": status,
@@ -1229,6 +1245,181 @@ def run_contact_reference(args):
     return 0
 
 
+def make_raycast_sensor(model, w):
+    import warnings
+
+    from newton_sph_dev_b200.sensors import SensorRaycast
+
+    rc = w["raycast"]
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore", DeprecationWarning)
+        sensor = SensorRaycast(model, rc["position"], (1.0, 0.0, 0.0), (0.0, 0.0, 1.0), rc["fov"], rc["width"],
+                               rc["height"], max_distance=rc["max_distance"])
+    sensor.point_camera_at(target=rc["target"], position=rc["position"], up=(0.0, 0.0, 1.0))
+    return sensor
+
+
+def raycast_cpu(model, sensor, x, rows: int):
+    """The oracle's raycast (its own grid build included) of the sensor's
+    camera at `rows` rows instead of its height: the same frustum, fewer
+    rays. Returns (rays, seconds)."""
+    from oracle import oracle as O
+
+    from newton_sph_dev_b200.sensors import march_steps
+
+    O.build()
+    r = model.particle_radius.cpu().numpy()
+    sr = float(model.particle_max_radius) + 1e-6
+    step = 0.5 * sr
+    steps = march_steps(sensor.max_distance, step)[0]
+    cam = O.raycast_camera(sensor.camera_position, sensor.camera_direction, sensor.camera_up, sensor.camera_right,
+                           sensor.fov_scale, sensor.aspect_ratio, sensor.width, rows, sensor.max_distance)
+    t0 = time.perf_counter()
+    O.raycast_particles(x, r, (128, 128, 128), cam, sr, step, steps)
+    return sensor.width * rows, time.perf_counter() - t0
+
+
+def run_raycast(args):
+    import torch
+
+    world, rank, local = dist_env()
+    if world > 1:
+        raise SystemExit("raycast_1m runs on one GPU (replicas are not wired for it)")
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    w = WORKLOADS[args.workload]
+    model = make_contact_scene(w, str(device))
+    n = model.particle_count
+    state = model.state()
+    sensor = make_raycast_sensor(model, w)
+    rays = sensor.width * sensor.height
+    stream = torch.cuda.current_stream(device)
+
+    def step():
+        sensor.update(state, include_particles=True)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        step()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    total = build_ms = 0.0
+    grid = sensor._get_particle_grid()
+    sr = float(model.particle_max_radius) + 1e-6
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            ev[0].record(stream)
+            grid.build(state.particle_q, sr)
+            ev[1].record(stream)
+            step()
+            ev[2].record(stream)
+            ev[2].synchronize()
+            build_ms += ev[0].elapsed_time(ev[1])
+            total += ev[1].elapsed_time(ev[2])
+    gtotal = 0.0
+    for _ in range(args.steps):
+        flush.zero_()
+        ev[0].record(stream)
+        g.replay()
+        ev[2].record(stream)
+        ev[2].synchronize()
+        gtotal += ev[0].elapsed_time(ev[2])
+    del g
+    depth = sensor.get_depth_image_numpy()
+    best = min(total, gtotal)
+    value = rays * args.steps / (best * 1e-3)
+    # the march kernel alone: one update minus its grid build
+    t_march = max(total - build_ms, 1e-9) / args.steps * 1e-3
+    peak, peak_kind = load_peak()
+    alg = 32 * n + 4 * rays  # gather (read x, r; write the sorted mirror) once, depth once
+    roofline = {"bound": "hbm", "kernel": "k_raycast (+ gather, clamp)", "achieved": alg / t_march / 1e9,
+                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": alg / t_march / 1e9 / peak,
+                "traffic": None, "alg_bytes_per_launch": alg, "ms_per_launch": t_march * 1e3,
+                "note": "the march reads the 16.8 MB cell table and the sorted mirror from L2; it is latency-bound"}
+    # end to end: host positions in, depth image out, every frame; two sensors
+    # so that frames pipeline on upload / compute / download streams
+    sensors = {}
+
+    def e2e_step(a, b):
+        sn = sensors.setdefault(id(b), make_raycast_sensor(model, w))
+        sn.update(a, include_particles=True)
+
+    hx, hv = state.particle_q.cpu().pin_memory(), state.particle_qd.cpu().pin_memory()
+    e2e_steps = min(args.steps, 50)
+
+    def outputs(st):
+        sn = sensors.setdefault(id(st), make_raycast_sensor(model, w))
+        return (sn.get_depth_image(),)
+
+    e2e = pipelined_e2e(model, e2e_step, hx, hv, e2e_steps, device, outputs=outputs)
+    cpu = None
+    if not args.no_cpu_baseline:
+        nr, el = raycast_cpu(model, sensor, state.particle_q.cpu().numpy(), sensor.height // 8)
+        from oracle import oracle as O
+
+        cpu = {"value": nr / el, "unit": "rays/s", "cores": O.get_threads(), "kind": "port",
+               "sample": f"{nr} rays (the frame's frustum at 1/8 of its rows, the grid build included) in {el:.1f} s "
+                         "(fp32 restatement of the reference's march, full query at every sample, OpenMP)"}
+    clocks = clk.summary()
+    line = {
+        "metric": "rays/s", "value": value, "unit": "rays/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": best / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "particles": n, "rays": rays, "desc": w["desc"],
+                   "grid_dims": [128, 128, 128], "graph": gtotal <= total,
+                   "l2": "flushed (256 MiB write) before every timed step, outside the timed interval"},
+        "phase_ms_per_step": {"build": build_ms / args.steps, "march": t_march * 1e3},
+        "hits": int((depth > 0).sum()), "misses": int((depth < 0).sum()),
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": {"value": rays * e2e_steps / (e2e * 1e-3), "unit": "rays/s", "h2d_bytes_per_step": 24 * n,
+                "d2h_bytes_per_step": 4 * rays, "steps": e2e_steps,
+                "how": "pinned upload of x (and v), SensorRaycast.update, download of the depth image, every frame; "
+                       "independent frames pipelined on upload / compute / download streams"},
+        "gpu_launches": (grid.last_launches + 3) * args.steps,  # per timed update: build, gather, march, clamp
+        "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_raycast_reference(args):
+    """The fp32 CPU restatement of the reference's particle raycast (its own
+    grid build, the full query at every march sample) on the same scene and
+    camera, all host threads; each step a row subset of the frame."""
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    w = WORKLOADS[args.workload]
+    model = make_contact_scene(w, "cpu")
+    sensor = make_raycast_sensor(model, w)
+    x = model.particle_q.numpy()
+    rays = 0
+    el = 0.0
+    for _ in range(args.steps):
+        nr, t = raycast_cpu(model, sensor, x, sensor.height // 16)
+        rays += nr
+        el += t
+    value = rays / el
+    from oracle import oracle as O
+
+    line = {
+        "impl": "reference", "metric": "rays/s", "value": value, "unit": "rays/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "particles": model.particle_count, "desc": w["desc"]},
+        "cpu_baseline": {"value": value, "unit": "rays/s", "cores": O.get_threads(), "kind": "port",
+                         "sample": f"{args.steps} x {sensor.width * (sensor.height // 16)} rays (the frame's "
+                                   "frustum at 1/16 of its rows)"},
+        "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -1244,11 +1435,15 @@ def main(argv=None):
         ap.error("--warmup must be >= 3")
     grad = "grad" in WORKLOADS[args.workload]
     if args.impl == "reference":
+        if "raycast" in WORKLOADS[args.workload]:
+            return run_raycast_reference(args)
         if "contact" in WORKLOADS[args.workload]:
             return run_contact_reference(args)
         return run_grad_reference(args) if grad else run_reference(args)
     if "surrogate" in WORKLOADS[args.workload]:
         return run_surrogate(args)
+    if "raycast" in WORKLOADS[args.workload]:
+        return run_raycast(args)
     if "contact" in WORKLOADS[args.workload]:
         return run_contact(args)
     return run_grad(args) if grad else run_gpu(args)

@@ -318,6 +318,44 @@ NSPH_API int nsph_sph_segment_adjoint(nsph_sph* solver, const nsph_sph_params* p
                                       const float* gravity, int world_count,
                                       float* x_adj, float* v_adj, float* f_ext_adj, float* eos_b_adj, void* stream);
 
+/* ---- particle raycast (depth camera) on the HashGrid ----------------------
+ * Replaces, for particles, SensorRaycast.update(state, include_particles=True)
+ * (newton/_src/sensors/sensor_raycast.py:185-263, 272-320): the launch of
+ * sensor_raycast_particles_kernel (newton/_src/geometry/raycast.py:1090-1180)
+ * with ray_for_pixel (:727-775) and ray_intersect_particle_sphere
+ * (:123-156), and clamp_no_hits_kernel (sensor_raycast.py:18-23).
+ *
+ * nsph_raycast_particles: `grid` must have been built on x (n points) with
+ *   the cell width search_radius (the reference builds its
+ *   HashGrid(128, 128, 128) with radius = max particle radius + 1e-6). For
+ *   pixel (px, py) the ray from camera->position through the pixel centre
+ *   is marched in steps of march_step, at most max_steps samples, while
+ *   t <= max_distance and t <= the nearest hit so far; at each sample the
+ *   candidates of the grid query (search_radius) with radius > 0 are
+ *   intersected as spheres. depth (height x width, row-major) is read as the
+ *   initial nearest hit (a negative value means max_distance) and receives
+ *   the nearer particle hit, if any.
+ *   max_steps is at most NSPH_RAYCAST_MAX_STEPS (the reference's cap on the
+ *   samples of one ray, sensor_raycast.py:28).
+ * nsph_raycast_clamp_no_hits: depth[i] >= max_distance becomes -1. */
+#define NSPH_RAYCAST_MAX_STEPS (1 << 20)
+
+typedef struct nsph_raycast_camera {
+    float position[3];
+    float direction[3]; /* unit forward */
+    float up[3];        /* unit, orthogonal to direction */
+    float right[3];     /* unit, direction x up */
+    float fov_scale;    /* tan(vertical field of view / 2) */
+    float aspect_ratio; /* width / height */
+    int width, height;
+    float max_distance;
+} nsph_raycast_camera;
+
+NSPH_API int nsph_raycast_particles(nsph_grid* grid, const float* x, const float* radius, int n,
+                                    const nsph_raycast_camera* camera, float search_radius, float march_step,
+                                    int max_steps, float* depth, void* stream);
+NSPH_API int nsph_raycast_clamp_no_hits(float* depth, int count, float max_distance, void* stream);
+
 /* ---- particle-particle contact on the HashGrid ------------------------------
  * The reference's other consumers of the grid, rebuilt on nsph_grid (same
  * query: the candidates of hash_grid_query(grid, x_i, r_i + max_radius +

@@ -6,17 +6,18 @@ Drop-in for the particle part of NVIDIA Newton's API:
 - ``HashGrid`` (the ``wp.HashGrid`` build/query semantics),
 - ``solvers.SolverBase`` (``integrate_particles``) and ``solvers.SolverSPH``
   (weakly-compressible SPH: hash-grid neighbour search, density/EOS,
-  pressure + XSPH forces, integration).
+  pressure + XSPH forces, integration),
+- ``sensors.SensorRaycast`` (the depth camera's particle raycast on the grid).
 
 All compute runs in libnsph.so (hand-written CUDA for sm_100a, C ABI in
 include/nsph.h); there is no CPU fallback.
 """
 
-from . import solvers
+from . import sensors, solvers
 from .geometry import ParticleFlags
 from .hashgrid import HashGrid
 from .sim import Control, Model, ModelBuilder, State
 
 __version__ = "0.1.0"
 
-__all__ = ["Control", "HashGrid", "Model", "ModelBuilder", "ParticleFlags", "State", "solvers"]
+__all__ = ["Control", "HashGrid", "Model", "ModelBuilder", "ParticleFlags", "State", "sensors", "solvers"]

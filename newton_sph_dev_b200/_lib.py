@@ -85,6 +85,22 @@ class NsphContactParams(ctypes.Structure):
     ]
 
 
+class NsphRaycastCamera(ctypes.Structure):
+    """Layout of nsph_raycast_camera (include/nsph.h)."""
+
+    _fields_ = [
+        ("position", ctypes.c_float * 3),
+        ("direction", ctypes.c_float * 3),
+        ("up", ctypes.c_float * 3),
+        ("right", ctypes.c_float * 3),
+        ("fov_scale", ctypes.c_float),
+        ("aspect_ratio", ctypes.c_float),
+        ("width", ctypes.c_int),
+        ("height", ctypes.c_int),
+        ("max_distance", ctypes.c_float),
+    ]
+
+
 # (name, restype, argtypes) of every exported entry point, in header order.
 SIGNATURES = [
     ("nsph_version", ctypes.c_int, []),
@@ -167,6 +183,13 @@ SIGNATURES = [
         + [c_void_p] * 4
         + [c_void_p],
     ),
+    (
+        "nsph_raycast_particles",
+        ctypes.c_int,
+        [c_void_p, c_void_p, c_void_p, ctypes.c_int, ctypes.POINTER(NsphRaycastCamera), ctypes.c_float,
+         ctypes.c_float, ctypes.c_int, c_void_p, c_void_p],
+    ),
+    ("nsph_raycast_clamp_no_hits", ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_float, c_void_p]),
     (
         "nsph_particle_contact_forces",
         ctypes.c_int,

@@ -122,6 +122,16 @@ int oracle_particle_contact_deltas(float grid_radius, const int* dims, int n, co
 void oracle_set_threads(int n);
 int  oracle_get_threads(void);
 
+/* ---- particle raycast depth camera (raycast.c), fp32 --------------------
+ * The grid is built on x with cell width search_radius and dims; depth
+ * (height x width) holds the initial nearest hits (negative = none) and
+ * receives the nearer particle hits. oracle_raycast_clamp_no_hits turns
+ * values >= max_distance into -1. */
+int oracle_raycast_particles(const float* x, const float* radius, int n, const int* dims,
+                             const nsph_raycast_camera* cam, float search_radius, float march_step, int max_steps,
+                             float* depth);
+void oracle_raycast_clamp_no_hits(float* depth, int count, float max_distance);
+
 #ifdef __cplusplus
 }
 #endif

@@ -148,6 +148,11 @@ def lib() -> ctypes.CDLL:
     L.oracle_particle_contact_deltas.restype = ctypes.c_int
     L.oracle_particle_contact_deltas.argtypes = [ctypes.c_float, _i32p, ctypes.c_int] + [ctypes.c_void_p] * 5 + \
         [ctypes.c_float] * 5 + [ctypes.c_void_p]
+    L.oracle_raycast_particles.restype = ctypes.c_int
+    L.oracle_raycast_particles.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, _i32p, ctypes.c_void_p,
+                                           ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_void_p]
+    L.oracle_raycast_clamp_no_hits.restype = None
+    L.oracle_raycast_clamp_no_hits.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_float]
     L.oracle_set_threads.restype = None
     L.oracle_set_threads.argtypes = [ctypes.c_int]
     L.oracle_get_threads.restype = ctypes.c_int
@@ -526,6 +531,118 @@ def particle_contact_deltas(x, v, inv_mass, radius, flags, grid_radius: float, d
     if st != 0:
         raise RuntimeError(f"oracle_particle_contact_deltas status {st}")
     return d
+
+
+# ---------------------------------------------------------------------------
+# particle raycast depth camera (raycast.c)
+# ---------------------------------------------------------------------------
+class RaycastCamera(ctypes.Structure):
+    """Layout of nsph_raycast_camera (include/nsph.h)."""
+
+    _fields_ = [("position", ctypes.c_float * 3), ("direction", ctypes.c_float * 3), ("up", ctypes.c_float * 3),
+                ("right", ctypes.c_float * 3), ("fov_scale", ctypes.c_float), ("aspect_ratio", ctypes.c_float),
+                ("width", ctypes.c_int), ("height", ctypes.c_int), ("max_distance", ctypes.c_float)]
+
+
+def raycast_camera(position, direction, up, right, fov_scale, aspect_ratio, width, height, max_distance):
+    c = RaycastCamera()
+    for name, v in (("position", position), ("direction", direction), ("up", up), ("right", right)):
+        getattr(c, name)[:] = [float(np.float32(t)) for t in v]
+    c.fov_scale, c.aspect_ratio = float(np.float32(fov_scale)), float(np.float32(aspect_ratio))
+    c.width, c.height, c.max_distance = int(width), int(height), float(np.float32(max_distance))
+    return c
+
+
+def raycast_particles(x, radius, dims, cam: RaycastCamera, search_radius, march_step, max_steps, depth_init=None,
+                      clamp=True):
+    """The particle path of SensorRaycast.update restated (fp32): depth
+    (height, width) from depth_init (max_distance everywhere by default),
+    then the no-hit clamp to -1 when `clamp`."""
+    x, r = _f32(x), _f32(radius)
+    n = x.shape[0]
+    depth = np.array(depth_init if depth_init is not None else
+                     np.full((cam.height, cam.width), cam.max_distance), dtype=np.float32)
+    st = lib().oracle_raycast_particles(_p(x), _p(r), n, _i32(dims), ctypes.byref(cam),
+                                        float(np.float32(search_radius)), float(np.float32(march_step)),
+                                        int(max_steps), _p(depth))
+    if st != 0:
+        raise RuntimeError(f"oracle_raycast_particles status {st}")
+    if clamp:
+        lib().oracle_raycast_clamp_no_hits(_p(depth), depth.size, cam.max_distance)
+    return depth
+
+
+def raycast_particles_py(x, radius, dims, cam: RaycastCamera, search_radius, march_step, max_steps):
+    """The same loop in pure Python with numpy float32 scalars (small cases):
+    a check of raycast.c. Returns the clamped depth image."""
+    f = np.float32
+    x, radius = np.asarray(x, np.float32), np.asarray(radius, np.float32)
+    grid = grid_build_py(x, search_radius, dims)
+    inv = f(1.0) / f(search_radius)
+
+    def dot(a, b):
+        return f(f(f(a[0] * b[0]) + f(a[1] * b[1])) + f(a[2] * b[2]))
+
+    def query(p, rad):
+        out = []
+        lo, hi = [], []
+        for a in range(3):
+            s0 = trunc_sat_py(f(f(p[a] - f(rad)) * inv))
+            e0 = trunc_sat_py(f(f(p[a] + f(rad)) * inv))
+            e0 = min(e0, s0 + dims[a] - 1)
+            lo.append(s0)
+            hi.append(max(e0, s0))
+        for z in range(lo[2], hi[2] + 1):
+            for y in range(lo[1], hi[1] + 1):
+                for xx in range(lo[0], hi[0] + 1):
+                    c = [max(v + (1 << 20), 0) % dims[a] for a, v in enumerate((xx, y, z))]
+                    cell = c[2] * dims[0] * dims[1] + c[1] * dims[0] + c[0]
+                    out.extend(grid["point_ids"][grid["cell_starts"][cell]:grid["cell_ends"][cell]].tolist())
+        return out
+
+    w, h = cam.width, cam.height
+    maxd = f(cam.max_distance)
+    depth = np.full((h, w), maxd, np.float32)
+    o = [f(v) for v in cam.position]
+    for py in range(h):
+        for px in range(w):
+            ndc_x = f(f(f(f(2.0) * f(px)) + f(1.0)) / f(w)) - f(1.0)
+            ndc_y = f(1.0) - f(f(f(f(2.0) * f(py)) + f(1.0)) / f(h))
+            cx = f(f(ndc_x * f(cam.fov_scale)) * f(cam.aspect_ratio))
+            cy = f(ndc_y * f(cam.fov_scale))
+            d = [f(f(f(cam.right[k]) * cx) + f(f(cam.up[k]) * cy)) + f(cam.direction[k]) for k in range(3)]
+            d = [f(v) for v in d]
+            ln = f(np.sqrt(dot(d, d)))
+            d = [f(v / ln) if ln > 0 else f(0.0) for v in d]
+            best = depth[py, px]
+            if best < 0:
+                best = maxd
+            s, t = 0, f(0.0)
+            while s < max_steps and t <= maxd and t <= best:
+                p = [f(o[k] + f(d[k] * t)) for k in range(3)]
+                for j in query(p, search_radius):
+                    rad = radius[j]
+                    if rad <= 0:
+                        continue
+                    oc = [f(o[k] - x[j, k]) for k in range(3)]
+                    proj = dot(d, oc)
+                    cc = f(dot(oc, oc) - f(rad * rad))
+                    disc = f(f(proj * proj) - cc)
+                    if disc < 0:
+                        continue
+                    sq = f(np.sqrt(disc))
+                    th = f(-proj - sq)
+                    if th < 0:
+                        th = f(-proj + sq)
+                    if th < 0 or th > maxd:
+                        continue
+                    if th < best:
+                        best = th
+                        depth[py, px] = th
+                s += 1
+                t = f(t + f(march_step))
+    depth[depth >= maxd] = f(-1.0)
+    return depth
 
 
 # ---------------------------------------------------------------------------

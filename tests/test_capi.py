@@ -68,7 +68,8 @@ def _c_layout(struct: str, fields: list[str]) -> list[int]:
 
 
 @pytest.mark.parametrize("pyname,cname", [("NsphSphParams", "nsph_sph_params"), ("NsphGridView", "nsph_grid_view"),
-                                          ("NsphContactParams", "nsph_contact_params")])
+                                          ("NsphContactParams", "nsph_contact_params"),
+                                          ("NsphRaycastCamera", "nsph_raycast_camera")])
 def test_struct_layouts_match_header(pyname, cname):
     from newton_sph_dev_b200 import _lib
 
@@ -77,6 +78,15 @@ def test_struct_layouts_match_header(pyname, cname):
     c = _c_layout(cname, fields)
     assert c[0] == ctypes.sizeof(cls)
     assert c[1:] == [getattr(cls, f).offset for f in fields]
+
+
+def test_oracle_camera_layout_matches_header():
+    from oracle.oracle import RaycastCamera
+
+    fields = [f for f, _ in RaycastCamera._fields_]
+    c = _c_layout("nsph_raycast_camera", fields)
+    assert c[0] == ctypes.sizeof(RaycastCamera)
+    assert c[1:] == [getattr(RaycastCamera, f).offset for f in fields]
 
 
 def test_oracle_params_layout_matches_header():
