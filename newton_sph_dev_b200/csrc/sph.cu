@@ -414,7 +414,7 @@ __global__ void __launch_bounds__(kSphThreads, 3) k_density_worlds(const WorldCe
             continue;
         }
         const int w = attr >> kAttrGravShift;
-        const nsph_sph_params& p = wp[w];
+        const nsph_sph_params p = wp[w];  // a copy: its fields stay in registers across the candidate loop
         const GridDev g = world_grid(wc[w], ranges, ids);
         int nc = 0;
         const float rho = density_single(g, xs, p, xi, mask, n, k, nc);
