@@ -359,7 +359,10 @@ __device__ __forceinline__ void integrate_out(size_t i, float4 xi, float4 vi, in
 }
 
 // ---- pass 2: pressure force + XSPH + integrate --------------------------------
-__global__ void __launch_bounds__(kSphThreads, 3) k_force(GridDev g, const float4* __restrict__ xs,
+// Bounded to 64 registers (32 resident warps per SM instead of 24 at its
+// unbounded 77): the few spills sit outside the neighbour loop, and the extra
+// warps hide the neighbour loads' latency.
+__global__ void __launch_bounds__(kSphThreads, 4) k_force(GridDev g, const float4* __restrict__ xs,
                                                           const float4* __restrict__ vs,
                                                           const float2* __restrict__ aux,
                                                           const float2* __restrict__ rp, int n,
