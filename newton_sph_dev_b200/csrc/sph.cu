@@ -397,7 +397,7 @@ __device__ __forceinline__ GridDev world_grid(const WorldCells& c, const int2* _
     return GridDev{c.dx, c.dy, c.dz, c.inv, ranges + c.off, ids};
 }
 
-__global__ void __launch_bounds__(kSphThreads, 3) k_density_worlds(const WorldCells* __restrict__ wc,
+__global__ void __launch_bounds__(kSphThreads, 4) k_density_worlds(const WorldCells* __restrict__ wc,
                                                                    const nsph_sph_params* __restrict__ wp,
                                                                    const int2* __restrict__ ranges,
                                                                    const int* __restrict__ ids,
@@ -426,7 +426,7 @@ __global__ void __launch_bounds__(kSphThreads, 3) k_density_worlds(const WorldCe
     }
 }
 
-__global__ void __launch_bounds__(kSphThreads, 2) k_force_worlds(const WorldCells* __restrict__ wc,
+__global__ void __launch_bounds__(kSphThreads, 3) k_force_worlds(const WorldCells* __restrict__ wc,
                                                                  const nsph_sph_params* __restrict__ wp,
                                                                  const int2* __restrict__ ranges,
                                                                  const int* __restrict__ ids,
