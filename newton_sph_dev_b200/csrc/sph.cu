@@ -195,7 +195,9 @@ __device__ __forceinline__ void density_finish(int k, float m, float rho, const 
     rp[k] = make_float2(rho, pr);
 }
 
-__global__ void __launch_bounds__(kSphThreads, 3) k_density(GridDev g, const float4* __restrict__ xs,
+// Bounded to 48 registers (no spills): 40 resident warps per SM instead of
+// 32 at its unbounded 62.
+__global__ void __launch_bounds__(kSphThreads, 5) k_density(GridDev g, const float4* __restrict__ xs,
                                                             const float4* __restrict__ vs, int n,
                                                             const __grid_constant__ nsph_sph_params p,
                                                             float2* __restrict__ aux, float2* __restrict__ rp,
