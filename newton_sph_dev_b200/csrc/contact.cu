@@ -71,7 +71,8 @@ __global__ void k_contact_gather(const int* __restrict__ ids, int n, const float
     m1[k] = make_float4(v[3 * i], v[3 * i + 1], v[3 * i + 2], inv_mass ? inv_mass[i] : 0.f);
 }
 
-__global__ void k_contact_forces(GridDev g, int n, const float4* __restrict__ m0, const float4* __restrict__ m1,
+// bounded to 48 registers (from 64): 40 resident warps per SM
+__global__ void __launch_bounds__(128, 10) k_contact_forces(GridDev g, int n, const float4* __restrict__ m0, const float4* __restrict__ m1,
                                  const nsph_contact_params p, float* __restrict__ f_out)
 {
     const int kk = blockIdx.x * blockDim.x + threadIdx.x;
