@@ -896,7 +896,7 @@ __device__ __forceinline__ void force_features_single(const GridDev& g, const fl
 
 // per sorted particle k: feat[16 k ..] and sacc[2k] = (a, 0), sacc[2k+1] =
 // (dv, 0); per block: (sum of max(0, rho/rho0 - 1), active count)
-__global__ void __launch_bounds__(kSphThreads, 3) k_force_features(GridDev g, const float4* __restrict__ xs,
+__global__ void __launch_bounds__(kSphThreads, 4) k_force_features(GridDev g, const float4* __restrict__ xs,
                                                                    const float4* __restrict__ vs,
                                                                    const float2* __restrict__ aux,
                                                                    const float2* __restrict__ rp, int n,
