@@ -866,7 +866,7 @@ def run_grad_reference(args):
 
 
 # ---------------------------------------------------------------------------
-# learned surrogate step (4 x dt per step, plain step as fallback and judge)
+# learned surrogate step (4 x dt per step, plain step as fallback and yardstick)
 # ---------------------------------------------------------------------------
 # algorithmic bytes per particle: feature pass (read x, v, m/rho p/rho^2, rho p;
 # write 16 features, a, dv) and MLP + integrate (read them back with x, v,

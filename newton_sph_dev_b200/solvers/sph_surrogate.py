@@ -16,7 +16,7 @@ builds on the plain step. Pieces:
   (``nsph_mlp_gradient`` / ``nsph_mlp_adam``).
 - :class:`SurrogateSPH`: the stepper. Each call advances ``substeps * dt``:
   one surrogate step, or ``substeps`` plain steps when the surrogate is
-  suspended. The plain step is the fallback and the judge: the mean
+  suspended. The plain step is the fallback and the yardstick: the mean
   compression error e = mean_i max(0, rho_i/rho0 - 1) of every surrogate step
   is accumulated on the device; every ``window`` calls the host reads the
   window's worst value (one copy) and, above ``threshold``, runs plain steps
