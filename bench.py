@@ -148,25 +148,78 @@ def make_scene(name: str, device: str):
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
+    """SM clocks and clock-event reasons sampled during a timed region.
+
+    NVML (pynvml) is polled from a thread every 2 ms, with one sample taken
+    on entry and one on exit, so even a timed region of a few milliseconds
+    carries a record. Without NVML, nvidia-smi's 20 ms loop is used."""
+
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, period_s: float = 0.002):
         self.gpu_index = gpu_index
+        self.period_s = period_s
         self.proc = None
+        self.samples = []  # (sm_mhz, max_mhz, reason bits)
+        self.lines = []
+        self._nvml = None
+        self._thread = None
+        self._stop = None
+
+    def _nvml_handle(self):
+        try:
+            import pynvml
+            import torch
+
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(self.gpu_index).uuid)
+            uuid = uuid if uuid.startswith("GPU-") else "GPU-" + uuid
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid)
+        except Exception:
+            return None
+
+    def _sample(self):
+        nv, hdl = self._nvml
+        try:
+            sm = nv.nvmlDeviceGetClockInfo(hdl, nv.NVML_CLOCK_SM)
+            mx = nv.nvmlDeviceGetMaxClockInfo(hdl, nv.NVML_CLOCK_SM)
+            reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(hdl)
+            self.samples.append((float(sm), float(mx), int(reasons)))
+        except Exception:
+            pass
 
     def __enter__(self):
+        import threading
+
+        self._nvml = self._nvml_handle()
+        if self._nvml is not None:
+            self._sample()
+            self._stop = threading.Event()
+
+            def loop():
+                while not self._stop.wait(self.period_s):
+                    self._sample()
+
+            self._thread = threading.Thread(target=loop, daemon=True)
+            self._thread.start()
+            return self
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu_index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join()
+            self._sample()
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -178,8 +231,14 @@ class ClockSampler:
 
     def summary(self) -> dict:
         sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in getattr(self, "lines", []):
+        for s, m, bits in self.samples:
+            sm.append(s)
+            mx = m
+            for nm, bit in self.REASONS:
+                if bits & bit:
+                    reasons.add(nm)
+        names = [nm for nm, _ in self.REASONS]
+        for ln in self.lines:
             parts = [p.strip() for p in ln.split(",")]
             if len(parts) < 9:
                 continue
@@ -191,9 +250,11 @@ class ClockSampler:
             for nm, val in zip(names, parts[5:9]):
                 if val.lower().startswith("active"):
                     reasons.add(nm)
+        src = "nvml" if self.samples else "nvidia-smi"
         if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+            return {"sm_mhz": None, "sm_max_mhz": mx, "reasons": [], "samples": 0, "source": src}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm),
+                "source": src}
 
 
 # ---------------------------------------------------------------------------
@@ -418,6 +479,52 @@ def load_traffic(kernel: str):
         return None
 
 
+def load_kernel_counts(kernel: str) -> dict:
+    """ncu figures of a kernel at the bench workload (profiles/ncu_traffic.json)."""
+    p = REPO / "profiles" / "ncu_traffic.json"
+    if not p.exists():
+        return {}
+    try:
+        return dict(json.loads(p.read_text()).get(kernel, {}))
+    except (ValueError, OSError):
+        return {}
+
+
+def measure_fp32_peak(device) -> dict:
+    """FP32 FMA / warp-instruction issue peak of this GPU (nsph_fp32_peak)."""
+    import ctypes
+
+    import torch
+
+    from newton_sph_dev_b200 import _lib
+
+    tf, wi, ms = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+    st = _lib.load().nsph_fp32_peak(device.index or 0, 4096, ctypes.byref(tf), ctypes.byref(wi), ctypes.byref(ms),
+                                    torch.cuda.current_stream(device).cuda_stream)
+    _lib.check(st, "nsph_fp32_peak")
+    return {"fp32_tflops": tf.value, "warp_inst_per_s": wi.value, "ms": ms.value}
+
+
+def issue_roofline(kname: str, t_launch_s: float, n: int, peak: dict) -> dict:
+    """Issue roofline of a neighbour pass: warp instructions per launch (ncu,
+    the same workload) over its CUDA-event duration, against the measured
+    warp-instruction issue peak."""
+    c = load_kernel_counts(kname)
+    wi = c.get("warp_inst_per_launch")
+    ti = c.get("thread_inst_per_launch")
+    out = {"bound": "issue", "kernel": kname, "unit": "warp inst/s", "peak": peak["warp_inst_per_s"],
+           "peak_kind": "measured (nsph_fp32_peak: FFMA chains, 64 warps per SM)",
+           "fp32_peak_tflops": peak["fp32_tflops"], "warp_inst_per_launch": wi,
+           "thread_inst_per_particle": (ti / n) if ti else None, "simt_efficiency": (ti / wi / 32.0) if ti and wi else None,
+           "source": c.get("source")}
+    if wi:
+        out["achieved"] = wi / t_launch_s
+        out["frac"] = out["achieved"] / peak["warp_inst_per_s"]
+    else:
+        out["achieved"] = out["frac"] = None
+    return out
+
+
 def load_peak():
     p = REPO / "MEASURED_PEAKS.json"
     if p.exists():
@@ -482,6 +589,17 @@ def run_gpu(args):
             use_graph = False
             torch.cuda.synchronize()
 
+    # relaxation: the jittered lattice settles over its first ~100 steps, and
+    # the timed steps run on the settled state (untimed, an even count so
+    # the ping-pong order is unchanged)
+    relax = args.relax + (args.relax % 2)
+    for i in range(relax):
+        if graphs is not None:
+            graphs[i % 2].replay()
+        else:
+            step(s0, s1) if i % 2 == 0 else step(s1, s0)
+    torch.cuda.synchronize()
+
     phase = {"build": 0.0, "density": 0.0, "force": 0.0}
     total_ms = 0.0
     barrier(device)
@@ -502,14 +620,16 @@ def run_gpu(args):
     barrier(device)
     total_ms_max = max_over_ranks(total_ms, device)
     status = solver.status()
+    timed_state = s1 if args.steps % 2 == 1 else s0  # the last timed step's output
 
     value = world * n * args.steps / (total_ms_max * 1e-3)
     ms_per_step = total_ms_max / args.steps
 
     # ---- end to end through the public API with host buffers ----
     e2e_steps = min(args.steps, 100)
-    hx = model.particle_q.cpu().pin_memory()
-    hv = model.particle_qd.cpu().pin_memory()
+    # the host copy of the timed run's last state (not the initial lattice)
+    hx = timed_state.particle_q.cpu().pin_memory()
+    hv = timed_state.particle_qd.cpu().pin_memory()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     # (a) pipelined: every step uploads its inputs from pinned host memory,
@@ -546,7 +666,7 @@ def run_gpu(args):
     b_alg = (B_ALG_FORCE if dom == "force" else B_ALG_DENSITY) * n
     t_launch = phase[dom] / args.steps * 1e-3
     achieved = b_alg / t_launch / 1e9
-    kname = "k_force" if dom == "force" else "k_density"
+    kname = "k_force_list" if dom == "force" else "k_density_list"
     traffic = load_traffic(kname)
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                 "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
@@ -554,6 +674,9 @@ def run_gpu(args):
     step_achieved = B_ALG_STEP * n / (ms_per_step * 1e-3) / 1e9
     roofline_step = {"bound": "hbm", "achieved": step_achieved, "peak": peak, "unit": "GB/s",
                      "frac": step_achieved / peak, "alg_bytes_per_particle_step": B_ALG_STEP}
+
+    fp32 = measure_fp32_peak(device)
+    roof_issue = issue_roofline(kname, t_launch, n, fp32)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -591,21 +714,24 @@ def run_gpu(args):
                 "launch": {"threads": solver.launch[0], "blocks_per_sm": solver.launch[1],
                            "autotuned": tuned is not None} if hasattr(solver, "launch") else "default",
                 "l2": "flushed (256 MiB write) before every timed step, outside the timed interval",
+                "relaxation_steps": relax,
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             },
             "phase_ms_per_step": {k: v / args.steps for k, v in phase.items()},
             "roofline": roofline,
             "roofline_step": roofline_step,
+            "roofline_issue": roof_issue,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes, "steps": e2e_steps,
                     "how": "each step uploads x, v from pinned host memory, runs SolverSPH.step and downloads x, v; "
-                           "independent steps from the same host state, uploads and downloads overlapping other "
-                           "steps' compute on separate streams (double-buffered device states)",
+                           "independent steps from the same host state (the timed run's last state), uploads and "
+                           "downloads overlapping other steps' compute on separate streams (double-buffered device "
+                           "states)",
                     "serial_round_trip": {"value": e2e_serial, "how": "upload, step, download, next step from the "
                                                                       "downloaded state, no overlap"}},
             "gpu_launches": launches_per_step * args.steps,
-            "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+            "clocks": clocks,
             "status": status,
         }
         print(json.dumps(line), flush=True)
@@ -811,7 +937,7 @@ def run_grad(args):
             "e2e": {"value": e2e_value, "unit": "differentiable particle-steps/s",
                     "h2d_bytes_per_step": 2 * n * 12, "d2h_bytes_per_step": 2 * n * 12 + 8, "steps": e2e_iters},
             "gpu_launches": launches,
-            "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+            "clocks": clocks,
             "grads_finite": grads_finite,
             "loss": float(loss.item()),
         }
@@ -1056,7 +1182,7 @@ def run_surrogate(args):
                                               "independent calls pipelined on upload / compute / download streams",
                     "state": "the timed run's first state, fallback rule reset", "fallback_calls": e2e_fallbacks},
             "gpu_launches": stepper.launches_per_step * n_sur + fallbacks * sub * solver.last_launches,
-            "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+            "clocks": clocks,
             "status": status,
             "finite": finite,
         }
@@ -1197,7 +1323,7 @@ def run_contact(args):
                 "how": "pinned upload of x, v, grid build + contact forces, download of f, every step; independent "
                        "steps pipelined on upload / compute / download streams"},
         "gpu_launches": (grid.last_launches + 2) * args.steps,  # grid build + mirror gather + contact
-        "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+        "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -1380,7 +1506,7 @@ def run_raycast(args):
                 "how": "pinned upload of x (and v), SensorRaycast.update, download of the depth image, every frame; "
                        "independent frames pipelined on upload / compute / download streams"},
         "gpu_launches": (grid.last_launches + 3) * args.steps,  # per timed update: build, gather, march, clamp
-        "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+        "clocks": clocks,
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -1428,6 +1554,8 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=[k for k in WORKLOADS if not k.startswith("_")], default="tank_1m")
     ap.add_argument("--no-graph", action="store_true", help="time eager steps instead of graph replays")
+    ap.add_argument("--relax", type=int, default=200,
+                    help="untimed steps after the warm-up, so the timed steps run on a settled state")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shape")
     args = ap.parse_args(argv)

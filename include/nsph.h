@@ -129,13 +129,14 @@ NSPH_API int nsph_grid_query(const nsph_grid* grid, const float* queries, int nu
  *   point_cells, point_ids: num_points ints (sorted cell ids / original ids)
  *   cell_starts, cell_ends: dim_x*dim_y*dim_z ints each (cleared by the call,
  *                           then the [start,end) of every occupied cell)
- * The sort scratch is a fixed device array of the library (about 4 MiB,
- * held by every GPU that loads the library until the process exits), so
+ * The sort scratch is a fixed device array of the library (4.5 MiB, held
+ * by every GPU that loads the library until the process exits), so
  * num_points may not exceed NSPH_NOALLOC_MAX_POINTS (NSPH_ERR_CAPACITY).
  * All calls share that scratch: calls that overlap on the GPU (concurrent
  * streams, other host threads) race and must be serialised by the caller.
- * The first call on a device looks up the scratch's device address (a
- * runtime call, once per device); make that first call before any stream
+ * The first call on a device (of any size, num_points == 0 included) looks
+ * up the scratch's device address and loads every kernel a build launches
+ * (runtime calls, once per device); make that first call before any stream
  * capture. The call calls neither cudaMalloc nor cudaFree. */
 #define NSPH_NOALLOC_MAX_POINTS (1 << 18)
 NSPH_API int nsph_grid_build_noalloc(const float* points, int num_points, float radius, int dim_x, int dim_y,
@@ -395,6 +396,110 @@ NSPH_API int nsph_particle_contact_deltas(const nsph_grid* grid, int n, const fl
                                           const float* inv_mass, const float* radius, const int* flags, float k_mu,
                                           float k_cohesion, float max_radius, float dt, float relaxation,
                                           float* deltas, void* stream);
+
+/* ---- measurement helper (no counterpart in the reference) -----------------
+ * The device's FP32 / instruction-issue peak, the denominator of the issue
+ * roofline that bounds the neighbour passes: 64 resident warps per SM, each
+ * thread running 8 independent FMA chains of `iters` x 16 FFMA (one warp
+ * instruction per FFMA). Writes the FP32 rate (TFLOP/s), the warp
+ * instructions issued per second over the device and the timed launch's
+ * duration (ms, CUDA events on `stream` after one warm-up launch).
+ * Allocates a small sink buffer and synchronises: not for use in a step. */
+NSPH_API int nsph_fp32_peak(int device, int iters, float* tflops, float* warp_inst_per_s, float* ms, void* stream);
+
+/* ---- particles against static analytic shapes; the XPBD particle update --
+ * Shapes without a body (body -1: ground planes, world-fixed spheres and
+ * boxes), as ModelBuilder.add_shape_plane / add_ground_plane /
+ * add_shape_sphere / add_shape_box make them (newton/_src/sim/builder.py:
+ * 5611-5891). `type` takes the reference's GeoType values. The world
+ * transform is (pos, rot) with rot an (x, y, z, w) unit quaternion; scale is
+ * (radius, -, -) for a sphere, the half extents for a box and (width,
+ * length, -) for a plane (0 = infinite). ke/kd/kf/mu are the shape's
+ * material (ShapeConfig). */
+#define NSPH_GEO_PLANE 1
+#define NSPH_GEO_SPHERE 3
+#define NSPH_GEO_BOX 7
+typedef struct nsph_shape {
+    int   type;      /* GeoType: PLANE 1, SPHERE 3, BOX 7 (others never make contacts) */
+    int   flags;     /* ShapeFlags; COLLIDE_PARTICLES (1 << 2) enables particle contacts */
+    int   world;     /* shape_world; -1 = every world */
+    int   reserved;
+    float pos[3];
+    float rot[4];
+    float scale[3];
+    float ke, kd, kf, mu;
+} nsph_shape;
+
+/* Soft contacts (Contacts.soft_contact_*): device arrays owned by the
+ * caller; count is one int, the others hold `max` entries (vec3 arrays
+ * 3*max floats). */
+typedef struct nsph_soft_contacts {
+    int*   count;     /* soft_contact_count[0]: contacts found (may exceed max) */
+    int*   particle;  /* soft_contact_particle */
+    int*   shape;     /* soft_contact_shape */
+    float* body_pos;  /* soft_contact_body_pos (shape-body frame = world for static shapes) */
+    float* body_vel;  /* soft_contact_body_vel */
+    float* normal;    /* soft_contact_normal (world) */
+    int    max;       /* soft_contact_max */
+} nsph_soft_contacts;
+
+/* The particle side of the soft-contact material and the solver knobs. */
+typedef struct nsph_soft_contact_params {
+    float ke, kd, kf, mu;  /* Model.soft_contact_ke / kd / kf / mu */
+    float adhesion;        /* Model.particle_adhesion (the reference's particle_ka) */
+    float restitution;     /* Model.soft_contact_restitution */
+    float relaxation;      /* SolverXPBD.soft_contact_relaxation */
+    float dt;
+} nsph_soft_contact_params;
+
+/* Ints of scratch nsph_soft_contacts_create needs for n particles. */
+NSPH_API int nsph_soft_contacts_scratch_ints(int num_particles);
+/* Replaces create_soft_contacts (newton/_src/geometry/kernels.py:1001-1140,
+ * launched by the collision pipeline, newton/_src/sim/collide.py:1194-1228)
+ * for static shapes: a contact for every active particle p and shape s with
+ * COLLIDE_PARTICLES, a compatible world and sdf(x_p) < margin + r_p, with
+ * the shape-frame contact point x - n d mapped to world and the world
+ * normal. The reference appends with an atomic counter; here the contacts
+ * come in (particle, shape) order, so each particle's contacts are
+ * consecutive (the accumulating calls below rely on it). count[0] gets the
+ * number found; entries beyond max are dropped. `shapes` is a device array;
+ * `world` may be NULL (all -1). At most 1024 shapes. */
+NSPH_API int nsph_soft_contacts_create(const nsph_shape* shapes, int shape_count, int num_particles,
+                                       const float* x, const float* radius, const int* flags, const int* world,
+                                       float margin, nsph_soft_contacts* contacts, int* scratch, void* stream);
+/* Replaces eval_particle_body_contact for static shapes
+ * (newton/_src/solvers/semi_implicit/kernels_contact.py:143-262, launched
+ * by eval_particle_body_contact_forces :644-690): for each contact with
+ * c = n.(x - p) - r <= adhesion, f[particle] -= fn + (fd + ft), material
+ * averaged between params and the shape. */
+NSPH_API int nsph_particle_shape_contact_forces(const nsph_shape* shapes, int shape_count,
+                                                const nsph_soft_contacts* contacts,
+                                                const nsph_soft_contact_params* params, const float* x,
+                                                const float* v, const float* radius, const int* flags, float* f,
+                                                void* stream);
+/* Replaces solve_particle_shape_contacts for static shapes
+ * (newton/_src/solvers/xpbd/kernels.py:115-222, launched at
+ * solver_xpbd.py:386-412): deltas[particle] += w * delta_total. */
+NSPH_API int nsph_particle_shape_contact_deltas(const nsph_shape* shapes, int shape_count,
+                                                const nsph_soft_contacts* contacts,
+                                                const nsph_soft_contact_params* params, const float* x,
+                                                const float* v, const float* inv_mass, const float* radius,
+                                                const int* flags, float* deltas, void* stream);
+/* Replaces apply_particle_shape_restitution for static shapes
+ * (newton/_src/solvers/xpbd/kernels.py:34-112, launched at
+ * solver_xpbd.py:686-714): v_out[particle] += n (-v_new.n + max(-e v_old.n,
+ * 0)) for contacts that were approaching (v_old.n < 0); x_old / v_old are
+ * the step's input state. v_new may alias v_out. */
+NSPH_API int nsph_particle_shape_restitution(const nsph_soft_contacts* contacts,
+                                             const nsph_soft_contact_params* params, const float* v_new,
+                                             const float* x_old, const float* v_old, const float* radius,
+                                             const int* flags, float* v_out, void* stream);
+/* Replaces apply_particle_deltas (newton/_src/solvers/xpbd/kernels.py:
+ * 777-808): for active particles x_out = x_pred + delta, v_out = (x_out -
+ * x_orig)/dt clamped to |v| <= v_max; inactive particles are not written. */
+NSPH_API int nsph_apply_particle_deltas(int num_particles, const float* x_orig, const float* x_pred,
+                                        const int* flags, const float* deltas, float dt, float v_max, float* x_out,
+                                        float* v_out, void* stream);
 
 /* ---- learned surrogate step (no counterpart in the reference) -------------
  * A WCSPH step with a larger dt whose acceleration is corrected per particle

@@ -7,6 +7,9 @@ Drop-in for the particle part of NVIDIA Newton's API:
 - ``solvers.SolverBase`` (``integrate_particles``) and ``solvers.SolverSPH``
   (weakly-compressible SPH: hash-grid neighbour search, density/EOS,
   pressure + XSPH forces, integration),
+- ``solvers.SolverXPBD`` / ``solvers.SolverSemiImplicit`` (their particle
+  paths: particle-particle contacts on the grid, particle contacts with
+  static planes, spheres and boxes through ``Model.collide``),
 - ``sensors.SensorRaycast`` (the depth camera's particle raycast on the grid).
 
 All compute runs in libnsph.so (hand-written CUDA for sm_100a, C ABI in
@@ -14,10 +17,11 @@ include/nsph.h); there is no CPU fallback.
 """
 
 from . import sensors, solvers
-from .geometry import ParticleFlags
+from .geometry import GeoType, ParticleFlags, ShapeFlags
 from .hashgrid import HashGrid
-from .sim import Control, Model, ModelBuilder, State
+from .sim import Contacts, Control, Model, ModelBuilder, State
 
 __version__ = "0.1.0"
 
-__all__ = ["Control", "HashGrid", "Model", "ModelBuilder", "ParticleFlags", "State", "sensors", "solvers"]
+__all__ = ["Contacts", "Control", "GeoType", "HashGrid", "Model", "ModelBuilder", "ParticleFlags", "ShapeFlags", "State",
+           "sensors", "solvers"]

@@ -85,6 +85,53 @@ class NsphContactParams(ctypes.Structure):
     ]
 
 
+class NsphShape(ctypes.Structure):
+    """Layout of nsph_shape (include/nsph.h): one static analytic shape."""
+
+    _fields_ = [
+        ("type", ctypes.c_int),
+        ("flags", ctypes.c_int),
+        ("world", ctypes.c_int),
+        ("reserved", ctypes.c_int),
+        ("pos", ctypes.c_float * 3),
+        ("rot", ctypes.c_float * 4),
+        ("scale", ctypes.c_float * 3),
+        ("ke", ctypes.c_float),
+        ("kd", ctypes.c_float),
+        ("kf", ctypes.c_float),
+        ("mu", ctypes.c_float),
+    ]
+
+
+class NsphSoftContacts(ctypes.Structure):
+    """Layout of nsph_soft_contacts (include/nsph.h): device array pointers."""
+
+    _fields_ = [
+        ("count", c_void_p),
+        ("particle", c_void_p),
+        ("shape", c_void_p),
+        ("body_pos", c_void_p),
+        ("body_vel", c_void_p),
+        ("normal", c_void_p),
+        ("max", ctypes.c_int),
+    ]
+
+
+class NsphSoftContactParams(ctypes.Structure):
+    """Layout of nsph_soft_contact_params (include/nsph.h)."""
+
+    _fields_ = [
+        ("ke", ctypes.c_float),
+        ("kd", ctypes.c_float),
+        ("kf", ctypes.c_float),
+        ("mu", ctypes.c_float),
+        ("adhesion", ctypes.c_float),
+        ("restitution", ctypes.c_float),
+        ("relaxation", ctypes.c_float),
+        ("dt", ctypes.c_float),
+    ]
+
+
 class NsphRaycastCamera(ctypes.Structure):
     """Layout of nsph_raycast_camera (include/nsph.h)."""
 
@@ -199,6 +246,41 @@ SIGNATURES = [
         "nsph_particle_contact_deltas",
         ctypes.c_int,
         [c_void_p, ctypes.c_int] + [c_void_p] * 5 + [ctypes.c_float] * 5 + [c_void_p, c_void_p],
+    ),
+    (
+        "nsph_fp32_peak",
+        ctypes.c_int,
+        [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+         ctypes.POINTER(ctypes.c_float), c_void_p],
+    ),
+    ("nsph_soft_contacts_scratch_ints", ctypes.c_int, [ctypes.c_int]),
+    (
+        "nsph_soft_contacts_create",
+        ctypes.c_int,
+        [c_void_p, ctypes.c_int, ctypes.c_int] + [c_void_p] * 4
+        + [ctypes.c_float, ctypes.POINTER(NsphSoftContacts), c_void_p, c_void_p],
+    ),
+    (
+        "nsph_particle_shape_contact_forces",
+        ctypes.c_int,
+        [c_void_p, ctypes.c_int, ctypes.POINTER(NsphSoftContacts), ctypes.POINTER(NsphSoftContactParams)]
+        + [c_void_p] * 5 + [c_void_p],
+    ),
+    (
+        "nsph_particle_shape_contact_deltas",
+        ctypes.c_int,
+        [c_void_p, ctypes.c_int, ctypes.POINTER(NsphSoftContacts), ctypes.POINTER(NsphSoftContactParams)]
+        + [c_void_p] * 6 + [c_void_p],
+    ),
+    (
+        "nsph_particle_shape_restitution",
+        ctypes.c_int,
+        [ctypes.POINTER(NsphSoftContacts), ctypes.POINTER(NsphSoftContactParams)] + [c_void_p] * 6 + [c_void_p],
+    ),
+    (
+        "nsph_apply_particle_deltas",
+        ctypes.c_int,
+        [ctypes.c_int] + [c_void_p] * 4 + [ctypes.c_float, ctypes.c_float, c_void_p, c_void_p, c_void_p],
     ),
     ("nsph_sph_enable_surrogate", ctypes.c_int, [c_void_p]),
     (

@@ -665,7 +665,12 @@ extern "C" int nsph_grid_query(const nsph_grid* grid, const float* queries, int 
 namespace nsph {
 namespace {
 
-constexpr int kNoAllocTiles = (NSPH_NOALLOC_MAX_POINTS + kSortTile - 1) / kSortTile;
+// Every accepted size is a small build, so the sort uses the small builds'
+// 512-key tiles, like nsph_grid_build does for the same point count.
+static_assert(NSPH_NOALLOC_MAX_POINTS <= kSmallBuildPoints, "allocation-free builds are small builds");
+constexpr int kNoAllocItems = kSmallItems;
+constexpr int kNoAllocTiles = (NSPH_NOALLOC_MAX_POINTS + kSortThreads * kNoAllocItems - 1) /
+                              (kSortThreads * kNoAllocItems);
 // keys_a, vals_a, keys_b, vals_b (NSPH_NOALLOC_MAX_POINTS ints each), then
 // the per-tile digit histograms and the kRadix digit totals
 constexpr size_t kNoAllocSortInts = 4 * (size_t)NSPH_NOALLOC_MAX_POINTS;
@@ -676,6 +681,16 @@ constexpr size_t kNoAllocBytes = sizeof(int) * kNoAllocSortInts + sizeof(unsigne
 // all calls: the last call's contents stay behind, and calls that overlap on
 // the GPU race on it.
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+// start / end of each cell into two caller arrays (Warp's layout)
+__global__ void k_ranges_split(const int* __restrict__ cells, int n, int* __restrict__ starts, int* __restrict__ ends)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int c = cells[k];
+    if (k == 0 || cells[k - 1] != c) starts[c] = k;
+    if (k == n - 1 || cells[k + 1] != c) ends[c] = k + 1;
+}
 
 constexpr int kNoAllocMaxDevices = 64;
 unsigned char* g_noalloc_ptr[kNoAllocMaxDevices] = {};  // device address per device
@@ -691,20 +706,17 @@ int noalloc_scratch(int device, unsigned char** out)
     if (!g_noalloc_ptr[device]) {
         void* ptr = nullptr;
         NSPH_CUDA_TRY(cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+        // load every kernel a build may launch now, so that no later call
+        // (whatever its size, even the first one inside a stream capture)
+        // triggers lazy module loading
+        cudaFuncAttributes fa;
+        NSPH_CUDA_TRY(load_sort_kernels<kNoAllocItems>());
+        NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_scan_rows));
+        NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_ranges_split));
         g_noalloc_ptr[device] = static_cast<unsigned char*>(ptr);
     }
     *out = g_noalloc_ptr[device];
     return NSPH_OK;
-}
-
-// start / end of each cell into two caller arrays (Warp's layout)
-__global__ void k_ranges_split(const int* __restrict__ cells, int n, int* __restrict__ starts, int* __restrict__ ends)
-{
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const int c = cells[k];
-    if (k == 0 || cells[k - 1] != c) starts[c] = k;
-    if (k == n - 1 || cells[k + 1] != c) ends[c] = k + 1;
 }
 
 }  // namespace
@@ -746,9 +758,9 @@ extern "C" int nsph_grid_build_noalloc(const float* points, int num_points, floa
     while ((1LL << bits) < ncells) ++bits;
     const int passes = (bits + kRadixBits - 1) / kRadixBits;
     auto mask_of = [&](int p) { return (1 << std::min(kRadixBits, bits - p * kRadixBits)) - 1; };
-    const int ntiles = ntiles_of(n);
+    const int ntiles = ntiles_of(n, kNoAllocItems);
     const float inv = 1.0f / radius;
-    k_hash_hist<kSortItems><<<ntiles, kSortThreads, 0, cs>>>(points, n, inv, dim_x, dim_y, dim_z, keys_a, vals_a,
+    k_hash_hist<kNoAllocItems><<<ntiles, kSortThreads, 0, cs>>>(points, n, inv, dim_x, dim_y, dim_z, keys_a, vals_a,
                                                              hist, ntiles, mask_of(0), nullptr, 0, nullptr, nullptr,
                                                              nullptr, nullptr, 0);
     NSPH_LAUNCH_CHECK("k_hash_hist");
@@ -760,12 +772,12 @@ extern "C" int nsph_grid_build_noalloc(const float* points, int num_points, floa
         int* vout = last ? point_ids : ((p & 1) ? vals_a : vals_b);
         const int shift = p * kRadixBits;
         if (p > 0) {
-            k_upsweep<kSortItems><<<ntiles, kSortThreads, 0, cs>>>(kin, n, shift, mask_of(p), hist, ntiles);
+            k_upsweep<kNoAllocItems><<<ntiles, kSortThreads, 0, cs>>>(kin, n, shift, mask_of(p), hist, ntiles);
             NSPH_LAUNCH_CHECK("k_upsweep");
         }
         k_scan_rows<<<kRadix, kScanThreads, 0, cs>>>(hist, ntiles, digit_tot);
         NSPH_LAUNCH_CHECK("k_scan_rows");
-        k_downsweep<false, kSortItems><<<ntiles, kSortThreads, sizeof(DownsweepSmem<kSortItems>), cs>>>(
+        k_downsweep<false, kNoAllocItems><<<ntiles, kSortThreads, sizeof(DownsweepSmem<kNoAllocItems>), cs>>>(
             kin, vin, kout, vout, n, shift, mask_of(p), hist, ntiles, digit_tot, GatherArgs{});
         NSPH_LAUNCH_CHECK("k_downsweep");
         kin = kout;

@@ -219,6 +219,79 @@ __global__ void __launch_bounds__(kSphThreads, 5) k_density(GridDev g, const flo
     }
 }
 
+// ---- neighbour lists (the plain step) -----------------------------------------
+// The density pass of the plain step first tests every candidate (in query
+// order) and appends the sorted index of each neighbour to the particle's
+// list: slot t at nbr[t * n + k] (slot-major, so that a warp reading slot t
+// of 32 consecutive particles reads one contiguous 128-byte line), for the
+// first kNbrSlots neighbours, and their number in ncnt[k]. The cubic-spline
+// terms are then evaluated by a second loop over the list, in the same
+// order, so every lane of a warp runs the term code only for its own
+// neighbours (evaluated inside the candidate loop, a warp runs it for every
+// candidate slot at which any of its 32 lanes has a hit, which at a ~15% hit
+// rate is nearly all of them). The force pass walks the same list with one
+// uniform loop and no grid traversal. A particle with more than kNbrSlots
+// neighbours (dense clusters) is summed by re-testing its candidates, in the
+// same order. Sums, their order and every rounding are those of the fp32
+// oracle, as with the masks.
+constexpr int kNbrSlots = 64;
+
+__device__ __forceinline__ int neighbor_list(const GridDev& g, const float4* __restrict__ xs,
+                                             const nsph_sph_params& p, float4 xi, int* __restrict__ nbr, int n,
+                                             int k)
+{
+    int cnt = 0;
+    auto hit = [&](int j) {
+        if (cnt < kNbrSlots) nbr[(size_t)cnt * n + k] = j;
+        ++cnt;
+    };
+    for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
+        int j = lo;
+        for (; j + 4 <= hi; j += 4) {
+            float4 xj[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) xj[u] = __ldg(xs + j + u);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                float dx, dy, dz;
+                if (dist2(xi, xj[u], dx, dy, dz) < p.h2) hit(j + u);
+            }
+        }
+        for (; j < hi; ++j) {
+            float dx, dy, dz;
+            if (dist2(xi, __ldg(xs + j), dx, dy, dz) < p.h2) hit(j);
+        }
+    });
+    return cnt;
+}
+
+// rho of particle k from its list (read back by the thread that wrote it,
+// with plain loads), or by re-testing its candidates when the list overflowed
+__device__ __forceinline__ float density_from_list(const GridDev& g, const float4* __restrict__ xs,
+                                                   const nsph_sph_params& p, float4 xi, const int* nbr, int cnt,
+                                                   int n, int k)
+{
+    float rho = 0.f;
+    if (cnt <= kNbrSlots) {
+        int jn = cnt > 0 ? nbr[k] : 0;
+        for (int t = 0; t < cnt; ++t) {
+            const int j = jn;
+            if (t + 1 < cnt) jn = nbr[(size_t)(t + 1) * n + k];
+            const float4 xj = __ldg(xs + j);
+            float dx, dy, dz;
+            rho = __fmaf_rn(xj.w, wterm(dist2(xi, xj, dx, dy, dz), p), rho);
+        }
+    } else {
+        for_each_candidate(g, xi.x, xi.y, xi.z, p.h, [&](int j) {
+            const float4 xj = __ldg(xs + j);
+            float dx, dy, dz;
+            const float r2 = dist2(xi, xj, dx, dy, dz);
+            if (r2 < p.h2) rho = __fmaf_rn(xj.w, wterm(r2, p), rho);
+        });
+    }
+    return rho;
+}
+
 struct ForceAcc {
     float ax, ay, az, dvx, dvy, dvz;
 };
@@ -381,6 +454,83 @@ __global__ void __launch_bounds__(kSphThreads, 4) k_force(GridDev g, const float
             o.acc_sorted[2 * (size_t)k] = make_float4(acc.ax, acc.ay, acc.az, 0.f);
             o.acc_sorted[2 * (size_t)k + 1] = make_float4(acc.dvx, acc.dvy, acc.dvz, 0.f);
         }
+        integrate_out((size_t)g.ids[k], xi, vi, attr, rp[k], acc, p, p.dt, o);
+    }
+}
+
+// ---- the plain step's passes on neighbour lists ----------------------------------
+// Bounded to 48 registers, like the mask form: 40 resident warps per SM.
+__global__ void __launch_bounds__(kSphThreads, 5) k_density_list(GridDev g, const float4* __restrict__ xs,
+                                                                 const float4* __restrict__ vs, int n,
+                                                                 const __grid_constant__ nsph_sph_params p,
+                                                                 float2* __restrict__ aux, float2* __restrict__ rp,
+                                                                 int* __restrict__ nbr, int* __restrict__ ncnt,
+                                                                 unsigned* __restrict__ status)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float4 xi = xs[k];
+        if (!(__float_as_int(vs[k].w) & kAttrActive)) {
+            aux[k] = make_float2(0.f, 0.f);
+            rp[k] = make_float2(0.f, 0.f);
+            ncnt[k] = 0;
+            continue;
+        }
+        const int cnt = neighbor_list(g, xs, p, xi, nbr, n, k);
+        ncnt[k] = cnt;
+        const float rho = density_from_list(g, xs, p, xi, nbr, cnt, n, k);
+        density_finish(k, xi.w, rho, p, aux, rp, status);
+    }
+}
+
+// pressure and XSPH sums of particle k over its list, in order (loads of
+// neighbour t+1 issued before the terms of neighbour t), or by re-testing
+// its candidates when the list overflowed
+__device__ __forceinline__ void force_from_list(const GridDev& g, const float4* __restrict__ xs,
+                                                const float4* __restrict__ vs, const float2* __restrict__ aux,
+                                                const int* __restrict__ nbr, int cnt, int n, int k, float4 xi,
+                                                float4 vi, float pr2_i, const nsph_sph_params& p, ForceAcc& acc)
+{
+    if (cnt <= kNbrSlots) {
+        bool have = false;
+        float4 pxj = make_float4(0.f, 0.f, 0.f, 0.f), pvj = pxj;
+        float2 paj = make_float2(0.f, 0.f);
+        for (int t = 0; t < cnt; ++t) {
+            const int j = __ldg(nbr + (size_t)t * n + k);
+            if (j == k) continue;
+            const float4 nxj = __ldg(xs + j);
+            const float4 nvj = __ldg(vs + j);
+            const float2 naj = __ldg(aux + j);
+            if (have) force_term_data(pxj, pvj, paj, xi, vi, pr2_i, p, acc);
+            pxj = nxj;
+            pvj = nvj;
+            paj = naj;
+            have = true;
+        }
+        if (have) force_term_data(pxj, pvj, paj, xi, vi, pr2_i, p, acc);
+    } else {
+        for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
+            for (int j = lo; j < hi; ++j) {
+                float dx, dy, dz;
+                if (dist2(xi, __ldg(xs + j), dx, dy, dz) < p.h2 && j != k)
+                    force_term_data(__ldg(xs + j), __ldg(vs + j), __ldg(aux + j), xi, vi, pr2_i, p, acc);
+            }
+        });
+    }
+}
+
+__global__ void __launch_bounds__(kSphThreads, 4) k_force_list(GridDev g, const float4* __restrict__ xs,
+                                                               const float4* __restrict__ vs,
+                                                               const float2* __restrict__ aux,
+                                                               const float2* __restrict__ rp, int n,
+                                                               const __grid_constant__ nsph_sph_params p,
+                                                               const int* __restrict__ nbr,
+                                                               const int* __restrict__ ncnt, const StepOut o)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+        const float4 xi = xs[k], vi = vs[k];
+        const int attr = __float_as_int(vi.w);
+        ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        if (attr & kAttrActive) force_from_list(g, xs, vs, aux, nbr, ncnt[k], n, k, xi, vi, aux[k].y, p, acc);
         integrate_out((size_t)g.ids[k], xi, vi, attr, rp[k], acc, p, p.dt, o);
     }
 }
@@ -1089,6 +1239,8 @@ struct nsph_sph {
     float2* rp = nullptr;
     unsigned* mask = nullptr;  // kMaskWords x capacity neighbour bits (word-major)
     int* ncand = nullptr;      // candidates per particle
+    int* nbr = nullptr;        // plain step (single world): kNbrSlots x capacity neighbour lists (slot-major)
+    int* ncnt = nullptr;       //   neighbours per particle
     unsigned* status = nullptr;
     int last_n = 0;
     int last_launches = 0;
@@ -1217,6 +1369,8 @@ static void sph_free(nsph_sph* s)
     cudaFree(s->rp);
     cudaFree(s->mask);
     cudaFree(s->ncand);
+    cudaFree(s->nbr);
+    cudaFree(s->ncnt);
     cudaFree(s->wparams);
     cudaFree(s->status);
     cudaFree(s->adj_g);
@@ -1242,6 +1396,19 @@ extern "C" int nsph_sph_create(int device, int capacity, const int grid_dims[3],
     if (!s) return fail(NSPH_ERR_OUT_OF_MEMORY, "host allocation failed");
     int st = grid_init(s->grid, grid_dims[0], grid_dims[1], grid_dims[2], device);
     if (st == NSPH_OK) st = sph_create_common(s, device, capacity);
+    if (st == NSPH_OK) {  // the plain step's neighbour lists
+        DeviceGuard guard(device);
+        const size_t c = (size_t)(capacity > 0 ? capacity : 1);
+        cudaError_t e = cudaMalloc(&s->nbr, sizeof(int) * kNbrSlots * c);
+        if (e == cudaSuccess) e = cudaMalloc(&s->ncnt, sizeof(int) * c);
+        cudaFuncAttributes fa;
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_density_list);
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_force_list);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            st = fail(NSPH_ERR_OUT_OF_MEMORY, std::string("solver allocation: ") + cudaGetErrorString(e));
+        }
+    }
     if (st != NSPH_OK) {
         sph_free(s);
         delete s;
@@ -1370,14 +1537,14 @@ static int step_enqueue(nsph_sph* s, const nsph_sph_params* p, int n, const floa
         const GridDev g = s->grid.view();
         int blocks, threads;
         pass_launch(s, n, false, blocks, threads);
-        k_density<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->mask, s->ncand,
+        k_density_list<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->nbr, s->ncnt,
                                                    s->status);
-        NSPH_LAUNCH_CHECK("k_density");
+        NSPH_LAUNCH_CHECK("k_density_list");
         ++launches;
         if (s->ev[2]) NSPH_CUDA_TRY(record_mark(s->ev[2], cs));
         const StepOut o{f_ext, inv_mass, gravity, x_out, v_out, rho_out, p_out, a_out, s->status};
-        k_force<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->mask, s->ncand, o);
-        NSPH_LAUNCH_CHECK("k_force");
+        k_force_list<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->nbr, s->ncnt, o);
+        NSPH_LAUNCH_CHECK("k_force_list");
         ++launches;
     } else if (s->ev[2]) {
         NSPH_CUDA_TRY(record_mark(s->ev[2], cs));

@@ -2,7 +2,9 @@
 newton/_src/sim/builder.py: __init__ (:795), add_particle (:7186-7230),
 add_particles (:7232-7275), add_particle_grid (:8037-8130), begin_world /
 end_world (:2815-2909), add_custom_attribute (:1266) and the particle part of
-finalize (:9745, :9815-9855).
+finalize (:9745, :9815-9855); and static collision shapes for particle
+contacts: ShapeConfig (:231), add_shape_plane / add_ground_plane /
+add_shape_sphere / add_shape_box (:5611-5891) for shapes without a body.
 
 Particles are accumulated as numpy chunks instead of Python lists, so a
 million-particle lattice is built in well under a second; the values, their
@@ -17,8 +19,34 @@ from typing import Any
 import numpy as np
 import torch
 
-from ..geometry import ParticleFlags
+from ..geometry import GeoType, ParticleFlags, ShapeFlags
 from .model import Model
+
+_AXES = {"X": 0, "Y": 1, "Z": 2}
+
+
+def _axis_index(axis) -> int:
+    """0/1/2 from an int or "X"/"Y"/"Z" (newton's Axis)."""
+    if isinstance(axis, str):
+        return _AXES[axis.upper()]
+    return int(axis)
+
+
+def quat_between_vectors(a, b) -> tuple[float, float, float, float]:
+    """Unit quaternion (x, y, z, w) rotating unit vector a onto unit vector b:
+    axis a x b, half-angle from a.b (the half-vector construction); a
+    rotation by pi about an axis orthogonal to a when b = -a."""
+    a = np.asarray(a, dtype=np.float64) / np.linalg.norm(a)
+    b = np.asarray(b, dtype=np.float64) / np.linalg.norm(b)
+    c = float(np.dot(a, b))
+    if c < -1.0 + 1e-12:
+        helper = np.array([1.0, 0.0, 0.0]) if abs(a[0]) < 0.9 else np.array([0.0, 1.0, 0.0])
+        axis = np.cross(a, helper)
+        axis /= np.linalg.norm(axis)
+        return (float(axis[0]), float(axis[1]), float(axis[2]), 0.0)
+    axis = np.cross(a, b)
+    s = np.sqrt(2.0 * (1.0 + c))
+    return (float(axis[0] / s), float(axis[1] / s), float(axis[2] / s), float(0.5 * s))
 
 
 def quat_to_matrix(q) -> np.ndarray:
@@ -55,13 +83,44 @@ class ModelBuilder:
         def key(self) -> str:
             return f"{self.namespace}:{self.name}" if self.namespace else self.name
 
-    def __init__(self, up_axis: int = 2, gravity: float = -9.81):
+    class ShapeConfig:
+        """Physical and collision properties of a shape (builder.py:231-300):
+        the contact material ke / kd / kf / ka / mu, restitution, and whether
+        the shape collides with particles."""
+
+        def __init__(self, ke: float = 2.5e3, kd: float = 100.0, kf: float = 1000.0, ka: float = 0.0,
+                     mu: float = 1.0, restitution: float = 0.0, density: float = 1000.0,
+                     has_shape_collision: bool = True, has_particle_collision: bool = True,
+                     is_visible: bool = True, is_site: bool = False):
+            self.ke = ke
+            self.kd = kd
+            self.kf = kf
+            self.ka = ka
+            self.mu = mu
+            self.restitution = restitution
+            self.density = density
+            self.has_shape_collision = has_shape_collision
+            self.has_particle_collision = has_particle_collision
+            self.is_visible = is_visible
+            self.is_site = is_site
+
+        @property
+        def flags(self) -> int:
+            f = int(ShapeFlags.VISIBLE) if self.is_visible else 0
+            f |= int(ShapeFlags.COLLIDE_SHAPES) if self.has_shape_collision else 0
+            f |= int(ShapeFlags.COLLIDE_PARTICLES) if self.has_particle_collision else 0
+            f |= int(ShapeFlags.SITE) if self.is_site else 0
+            return f
+
+    def __init__(self, up_axis: int | str = 2, gravity: float = -9.81):
         """
         Args:
-            up_axis: 0 (x), 1 (y) or 2 (z, the default).
+            up_axis: 0 / "X", 1 / "Y" or 2 / "Z" (the default).
             gravity: magnitude of gravity along the up axis (default -9.81).
         """
-        self.up_axis = int(up_axis)
+        self.up_axis = _axis_index(up_axis)
+        self.default_shape_cfg = ModelBuilder.ShapeConfig()
+        self.shapes: list[dict] = []
         self.gravity: float = gravity
         self.world_count: int = 0
         self._current_world: int = -1
@@ -230,6 +289,62 @@ class ModelBuilder:
         self._append(points, velocity, masses, radii, fl)
 
     # ------------------------------------------------------------------
+    # static collision shapes (body -1)
+    def add_shape(self, body: int, type: int, xform=None, cfg: ShapeConfig | None = None, scale=(1.0, 1.0, 1.0),
+                  is_static: bool = True, label: str | None = None, **_ignored) -> int:
+        """Add a collision shape (builder.py add_shape). Only shapes without a
+        body (body == -1) are supported: rigid bodies are outside this
+        library."""
+        if int(body) != -1:
+            raise NotImplementedError("only static shapes (body=-1) are supported; rigid bodies are not part of the "
+                                      "particle path")
+        cfg = cfg if cfg is not None else self.default_shape_cfg
+        if xform is None:
+            xform = ((0.0, 0.0, 0.0), (0.0, 0.0, 0.0, 1.0))
+        pos, rot = xform
+        self.shapes.append(dict(type=int(type), flags=cfg.flags, world=self._current_world,
+                                pos=tuple(float(v) for v in pos), rot=tuple(float(v) for v in rot),
+                                scale=tuple(float(v) for v in scale), ke=cfg.ke, kd=cfg.kd, kf=cfg.kf, ka=cfg.ka,
+                                mu=cfg.mu, restitution=cfg.restitution, label=label or f"shape_{len(self.shapes)}"))
+        return len(self.shapes) - 1
+
+    def add_shape_plane(self, plane=(0.0, 0.0, 1.0, 0.0), xform=None, width: float = 10.0, length: float = 10.0,
+                        body: int = -1, cfg: ShapeConfig | None = None, color=None, label: str | None = None,
+                        custom_attributes=None) -> int:
+        """A plane (builder.py:5611-5674): with xform None it comes from the
+        plane equation a x + b y + c z + d = 0 (normal (a, b, c), offset
+        -d/|n| along it); the collision normal is the local +Z. width /
+        length 0 make it infinite for collision."""
+        if xform is None:
+            normal = np.asarray(plane[:3], dtype=np.float64)
+            norm = np.linalg.norm(normal)
+            normal = normal / norm
+            pos = -(plane[3] / norm) * normal
+            xform = (tuple(pos), quat_between_vectors((0.0, 0.0, 1.0), normal))
+        return self.add_shape(body, GeoType.PLANE, xform, cfg, (width, length, 0.0), label=label)
+
+    def add_ground_plane(self, height: float = 0.0, cfg: ShapeConfig | None = None, color=None,
+                         label: str | None = None) -> int:
+        """An infinite plane through height along the up axis (builder.py:5676-5701)."""
+        return self.add_shape_plane(plane=(*self.up_vector, -height), width=0.0, length=0.0, cfg=cfg,
+                                    label=label or "ground_plane")
+
+    def add_shape_sphere(self, body: int, xform=None, radius: float = 1.0, cfg: ShapeConfig | None = None,
+                         as_site: bool = False, color=None, label: str | None = None, custom_attributes=None) -> int:
+        """A sphere of the given radius centred at xform (builder.py:5703)."""
+        return self.add_shape(body, GeoType.SPHERE, xform, cfg, (radius, 0.0, 0.0), label=label)
+
+    def add_shape_box(self, body: int, xform=None, hx: float = 0.5, hy: float = 0.5, hz: float = 0.5,
+                      cfg: ShapeConfig | None = None, as_site: bool = False, color=None, label: str | None = None,
+                      custom_attributes=None) -> int:
+        """A box with half extents (hx, hy, hz) at xform (builder.py:5842)."""
+        return self.add_shape(body, GeoType.BOX, xform, cfg, (hx, hy, hz), label=label)
+
+    @property
+    def shape_count(self) -> int:
+        return len(self.shapes)
+
+    # ------------------------------------------------------------------
     def finalize(self, device: str | torch.device = "cuda:0", requires_grad: bool = False) -> Model:
         """Build the Model on `device` (particle part of builder.py:9745-9855
         and gravity :10655-10668)."""
@@ -272,6 +387,7 @@ class ModelBuilder:
                 attr.name, attr.namespace, attr.frequency, attr.assignment, attr.dtype, attr.width, attr.default
             )
         m._requested_state_attributes = set(self._requested_state_attributes)
+        m._set_shapes(self.shapes)
         if n > 1 and m.particle_max_radius > 0.0 and device.type == "cuda":
             from ..hashgrid import HashGrid
 
@@ -290,4 +406,4 @@ class ModelBuilder:
         return starts
 
 
-__all__ = ["ModelBuilder", "quat_to_matrix"]
+__all__ = ["ModelBuilder", "quat_between_vectors", "quat_to_matrix"]

@@ -141,10 +141,19 @@ int oracle_particle_contact_deltas(float grid_radius, const int* dims, int n, co
                                    const float* inv_mass, const float* radius, const int* flags, float k_mu,
                                    float k_cohesion, float max_radius, float dt, float relaxation, float* deltas)
 {
+    return oracle_particle_contact_deltas_grid(x, grid_radius, dims, n, x, v, inv_mass, radius, flags, k_mu,
+                                               k_cohesion, max_radius, dt, relaxation, deltas);
+}
+
+int oracle_particle_contact_deltas_grid(const float* grid_x, float grid_radius, const int* dims, int n,
+                                        const float* x, const float* v, const float* inv_mass, const float* radius,
+                                        const int* flags, float k_mu, float k_cohesion, float max_radius, float dt,
+                                        float relaxation, float* deltas)
+{
     if (!dims || n < 0 || !(grid_radius > 0.0f)) return NSPH_ERR_INVALID_ARG;
     if (n == 0) return NSPH_OK;
     contact_grid g;
-    int st = build(&g, x, n, grid_radius, dims);
+    int st = build(&g, grid_x, n, grid_radius, dims);
     if (st != NSPH_OK) {
         release(&g);
         return st;

@@ -117,6 +117,12 @@ int oracle_particle_contact_forces(const nsph_contact_params* p, float grid_radi
 int oracle_particle_contact_deltas(float grid_radius, const int* dims, int n, const float* x, const float* v,
                                    const float* inv_mass, const float* radius, const int* flags, float k_mu,
                                    float k_cohesion, float max_radius, float dt, float relaxation, float* deltas);
+/* The same with the grid built on grid_x while the particles sit at x (the
+ * XPBD iterations query the grid of the predicted positions). */
+int oracle_particle_contact_deltas_grid(const float* grid_x, float grid_radius, const int* dims, int n,
+                                        const float* x, const float* v, const float* inv_mass, const float* radius,
+                                        const int* flags, float k_mu, float k_cohesion, float max_radius, float dt,
+                                        float relaxation, float* deltas);
 
 /* Number of OpenMP threads the oracle uses (0 = OpenMP default). */
 void oracle_set_threads(int n);
@@ -131,6 +137,31 @@ int oracle_raycast_particles(const float* x, const float* radius, int n, const i
                              const nsph_raycast_camera* cam, float search_radius, float march_step, int max_steps,
                              float* depth);
 void oracle_raycast_clamp_no_hits(float* depth, int count, float max_distance);
+
+/* Particles against static analytic shapes and the XPBD particle update
+ * (shapes.c): soft contacts in (particle, shape) order, processed in contact
+ * order; fp32 restatements of create_soft_contacts,
+ * eval_particle_body_contact, solve_particle_shape_contacts,
+ * apply_particle_shape_restitution and apply_particle_deltas for shapes
+ * without a body. */
+int oracle_soft_contacts_create(const nsph_shape* shapes, int shape_count, int n, const float* x,
+                                const float* radius, const int* flags, const int* world, float margin, int max,
+                                int* count, int* particle, int* shape, float* body_pos, float* body_vel,
+                                float* normal);
+int oracle_shape_contact_forces(const nsph_shape* shapes, int count, const int* particle, const int* shape,
+                                const float* body_pos, const float* body_vel, const float* normal,
+                                const nsph_soft_contact_params* prm, const float* x, const float* v,
+                                const float* radius, const int* flags, float* f);
+int oracle_shape_contact_deltas(const nsph_shape* shapes, int count, const int* particle, const int* shape,
+                                const float* body_pos, const float* body_vel, const float* normal,
+                                const nsph_soft_contact_params* prm, const float* x, const float* v,
+                                const float* inv_mass, const float* radius, const int* flags, float* delta);
+int oracle_shape_restitution(int n, int count, const int* particle, const float* body_pos, const float* body_vel,
+                             const float* normal, const nsph_soft_contact_params* prm, const float* v_new,
+                             const float* x_old, const float* v_old, const float* radius, const int* flags,
+                             float* v_out);
+void oracle_apply_particle_deltas(int n, const float* x_orig, const float* x_pred, const int* flags,
+                                  const float* delta, float dt, float v_max, float* x_out, float* v_out);
 
 #ifdef __cplusplus
 }

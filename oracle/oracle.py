@@ -729,3 +729,205 @@ def cubic_spline_py(r: float, h: float) -> float:
     if q < 1.0:
         return s * 2.0 * (1.0 - q) ** 3
     return 0.0
+
+
+# ---------------------------------------------------------------------------
+# particles against static analytic shapes; the XPBD particle update (shapes.c)
+# ---------------------------------------------------------------------------
+class Shape(ctypes.Structure):
+    """Layout of nsph_shape (include/nsph.h)."""
+
+    _fields_ = [("type", ctypes.c_int), ("flags", ctypes.c_int), ("world", ctypes.c_int), ("reserved", ctypes.c_int),
+                ("pos", ctypes.c_float * 3), ("rot", ctypes.c_float * 4), ("scale", ctypes.c_float * 3),
+                ("ke", ctypes.c_float), ("kd", ctypes.c_float), ("kf", ctypes.c_float), ("mu", ctypes.c_float)]
+
+
+class SoftContactParams(ctypes.Structure):
+    """Layout of nsph_soft_contact_params (include/nsph.h)."""
+
+    _fields_ = [(k, ctypes.c_float) for k in ("ke", "kd", "kf", "mu", "adhesion", "restitution", "relaxation", "dt")]
+
+
+def shapes_array(shapes) -> ctypes.Array:
+    """ctypes array of Shape from dicts with the nsph_shape field names."""
+    arr = (Shape * max(1, len(shapes)))()
+    for i, s in enumerate(shapes):
+        arr[i].type = int(s["type"])
+        arr[i].flags = int(s.get("flags", 1 << 2))
+        arr[i].world = int(s.get("world", -1))
+        arr[i].pos[:] = [float(np.float32(t)) for t in s.get("pos", (0.0, 0.0, 0.0))]
+        arr[i].rot[:] = [float(np.float32(t)) for t in s.get("rot", (0.0, 0.0, 0.0, 1.0))]
+        arr[i].scale[:] = [float(np.float32(t)) for t in s.get("scale", (0.0, 0.0, 0.0))]
+        for k in ("ke", "kd", "kf", "mu"):
+            setattr(arr[i], k, float(np.float32(s.get(k, 0.0))))
+    return arr
+
+
+def soft_contact_params(ke, kd, kf, mu, adhesion, restitution, relaxation, dt) -> SoftContactParams:
+    return SoftContactParams(*[float(np.float32(t)) for t in (ke, kd, kf, mu, adhesion, restitution, relaxation, dt)])
+
+
+def _shape_lib():
+    L = lib()
+    if not getattr(L, "_shapes_declared", False):
+        L.oracle_soft_contacts_create.restype = ctypes.c_int
+        L.oracle_soft_contacts_create.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + \
+            [ctypes.c_void_p] * 4 + [ctypes.c_float, ctypes.c_int] + [ctypes.c_void_p] * 6
+        L.oracle_shape_contact_forces.restype = ctypes.c_int
+        L.oracle_shape_contact_forces.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 11
+        L.oracle_shape_contact_deltas.restype = ctypes.c_int
+        L.oracle_shape_contact_deltas.argtypes = [ctypes.c_void_p, ctypes.c_int] + [ctypes.c_void_p] * 12
+        L.oracle_shape_restitution.restype = ctypes.c_int
+        L.oracle_shape_restitution.argtypes = [ctypes.c_int, ctypes.c_int] + [ctypes.c_void_p] * 10
+        L.oracle_apply_particle_deltas.restype = None
+        L.oracle_apply_particle_deltas.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 4 + \
+            [ctypes.c_float, ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p]
+        L._shapes_declared = True
+    return L
+
+
+def soft_contacts_create(shapes, x, radius, flags, world=None, margin=0.01, max_contacts=None) -> dict:
+    """create_soft_contacts restated: contacts in (particle, shape) order."""
+    arr = shapes if isinstance(shapes, ctypes.Array) else shapes_array(shapes)
+    ns = len(shapes)
+    x, r, fl = _f32(x), _f32(radius), _i32(flags)
+    n = x.shape[0]
+    mx = n * ns if max_contacts is None else int(max_contacts)
+    out = {"count": np.zeros(1, np.int32), "particle": np.zeros(max(mx, 1), np.int32),
+           "shape": np.zeros(max(mx, 1), np.int32), "body_pos": np.zeros((max(mx, 1), 3), np.float32),
+           "body_vel": np.zeros((max(mx, 1), 3), np.float32), "normal": np.zeros((max(mx, 1), 3), np.float32)}
+    w = _i32(world) if world is not None else None
+    st = _shape_lib().oracle_soft_contacts_create(
+        ctypes.cast(arr, ctypes.c_void_p), ns, n, _p(x), _p(r), _p(fl), _p(w), float(np.float32(margin)), mx,
+        _p(out["count"]), _p(out["particle"]), _p(out["shape"]), _p(out["body_pos"]), _p(out["body_vel"]),
+        _p(out["normal"]))
+    if st != 0:
+        raise RuntimeError(f"oracle_soft_contacts_create status {st}")
+    out["max"] = mx
+    out["n"] = int(min(mx, out["count"][0]))
+    return out
+
+
+def _contact_args(c):
+    return [_p(c["particle"]), _p(c["shape"]), _p(c["body_pos"]), _p(c["body_vel"]), _p(c["normal"])]
+
+
+def shape_contact_forces(shapes, contacts, prm, x, v, radius, flags, f) -> np.ndarray:
+    """eval_particle_body_contact restated: returns f minus the contact forces."""
+    arr = shapes if isinstance(shapes, ctypes.Array) else shapes_array(shapes)
+    f = np.array(f, dtype=np.float32)
+    st = _shape_lib().oracle_shape_contact_forces(
+        ctypes.cast(arr, ctypes.c_void_p), contacts["n"], *_contact_args(contacts), ctypes.byref(prm), _p(_f32(x)),
+        _p(_f32(v)), _p(_f32(radius)), _p(_i32(flags)), _p(f))
+    if st != 0:
+        raise RuntimeError(f"oracle_shape_contact_forces status {st}")
+    return f
+
+
+def shape_contact_deltas(shapes, contacts, prm, x, v, inv_mass, radius, flags, delta) -> np.ndarray:
+    """solve_particle_shape_contacts restated: returns delta plus the corrections."""
+    arr = shapes if isinstance(shapes, ctypes.Array) else shapes_array(shapes)
+    d = np.array(delta, dtype=np.float32)
+    st = _shape_lib().oracle_shape_contact_deltas(
+        ctypes.cast(arr, ctypes.c_void_p), contacts["n"], *_contact_args(contacts), ctypes.byref(prm), _p(_f32(x)),
+        _p(_f32(v)), _p(_f32(inv_mass)), _p(_f32(radius)), _p(_i32(flags)), _p(d))
+    if st != 0:
+        raise RuntimeError(f"oracle_shape_contact_deltas status {st}")
+    return d
+
+
+def shape_restitution(contacts, prm, v_new, x_old, v_old, radius, flags, v_out) -> np.ndarray:
+    """apply_particle_shape_restitution restated: returns v_out plus the updates."""
+    vo = np.array(v_out, dtype=np.float32)
+    vn = _f32(v_new)
+    st = _shape_lib().oracle_shape_restitution(
+        vn.shape[0], contacts["n"], _p(contacts["particle"]), _p(contacts["body_pos"]), _p(contacts["body_vel"]),
+        _p(contacts["normal"]), ctypes.byref(prm), _p(vn), _p(_f32(x_old)), _p(_f32(v_old)), _p(_f32(radius)),
+        _p(_i32(flags)), _p(vo))
+    if st != 0:
+        raise RuntimeError(f"oracle_shape_restitution status {st}")
+    return vo
+
+
+def apply_particle_deltas(x_orig, x_pred, flags, delta, dt, v_max, x_out, v_out):
+    """apply_particle_deltas restated; x_out / v_out updated in place (active rows)."""
+    _shape_lib().oracle_apply_particle_deltas(_f32(x_orig).shape[0], _p(_f32(x_orig)), _p(_f32(x_pred)),
+                                              _p(_i32(flags)), _p(_f32(delta)), float(np.float32(dt)),
+                                              float(np.float32(v_max)), _p(x_out), _p(v_out))
+
+
+def xpbd_particle_step(m: dict, x_in, v_in, f_in, dt: float, iterations: int, relaxation: float,
+                       contacts=None, enable_restitution: bool = False, dims=(128, 128, 128), x_out_init=None,
+                       v_out_init=None):
+    """SolverXPBD.step for a particle model with static shapes
+    (newton/_src/solvers/xpbd/solver_xpbd.py:260-319, 362-440, 504, 638-714),
+    restated on the oracle's kernels, including the reference's buffer
+    ping-pong between the input and output states (_apply_particle_deltas,
+    :157-197).
+
+    m: dict of model arrays and scalars (inv_mass, radius, flags, world,
+    gravity, v_max, particle_mu, particle_cohesion, max_radius, shapes,
+    soft: the nsph_soft_contact_params values except relaxation and dt).
+    x_out_init / v_out_init: the output state's buffers before the step
+    (rows the step does not write keep them; zeros by default).
+    Returns (x_in_after, v_in_after, x_out, v_out): the reference also
+    writes intermediate iterates into the input state's buffers."""
+    n = x_in.shape[0]
+    xi, vi = np.array(x_in, np.float32), np.array(v_in, np.float32)
+    xo = np.array(x_out_init, np.float32) if x_out_init is not None else np.zeros_like(xi)
+    vo = np.array(v_out_init, np.float32) if v_out_init is not None else np.zeros_like(vi)
+    q_init, qd_init = xi.copy(), vi.copy()
+    integrate_particles(xi, vi, f_in, m["inv_mass"], m["flags"], m["world"], m["gravity"], dt, m["v_max"], xo, vo)
+    grid_r = float(np.float32(m["max_radius"] * 2.0 + m["particle_cohesion"]))
+    use_pp = n > 1 and m["max_radius"] > 0.0
+    prm = soft_contact_params(*m["soft"][:6], relaxation, dt)
+    bufs = {"in": (xi, vi), "out": (xo, vo)}
+    cur = "out"
+    counter = 0
+    grid_x = xo.copy()  # the grid is built once, on the predicted positions
+    for _ in range(iterations):
+        xq, vq = bufs[cur]
+        d = np.zeros((n, 3), np.float32)
+        if contacts is not None and len(m["shapes"]):
+            d = shape_contact_deltas(m["shapes"], contacts, prm, xq, vq, m["inv_mass"], m["radius"], m["flags"], d)
+        if use_pp:
+            d = particle_contact_deltas_on_grid(grid_x, xq, vq, m["inv_mass"], m["radius"], m["flags"], grid_r, dims,
+                                                m["particle_mu"], m["particle_cohesion"], m["max_radius"], dt,
+                                                relaxation, d)
+        # reference ping-pong: iteration 0 reads the output state and writes the input state's buffers
+        if counter == 0:
+            src, dst = "out", "in"
+        else:
+            src, dst = "in", "out"
+        counter = 1 - counter
+        apply_particle_deltas(q_init, bufs[src][0], m["flags"], d, dt, m["v_max"], bufs[dst][0], bufs[dst][1])
+        cur = dst
+    if cur != "out":
+        xo[...] = bufs[cur][0]
+        vo[...] = bufs[cur][1]
+    if enable_restitution and contacts is not None:
+        vo[...] = shape_restitution(contacts, prm, vo.copy(), q_init, qd_init, m["radius"], m["flags"], vo)
+    return xi, vi, xo, vo
+
+
+def particle_contact_deltas_on_grid(grid_x, x, v, inv_mass, radius, flags, grid_radius, dims, k_mu, k_cohesion,
+                                    max_radius, dt, relaxation, deltas_init):
+    """solve_particle_particle_contacts with the grid built on grid_x and the
+    particles at x (the XPBD iterations keep the grid of the predicted
+    positions while the particles move)."""
+    L = _shape_lib()
+    if not getattr(L, "_deltas_grid_declared", False):
+        L.oracle_particle_contact_deltas_grid.restype = ctypes.c_int
+        L.oracle_particle_contact_deltas_grid.argtypes = [ctypes.c_void_p, ctypes.c_float, _i32p, ctypes.c_int] + \
+            [ctypes.c_void_p] * 5 + [ctypes.c_float] * 5 + [ctypes.c_void_p]
+        L._deltas_grid_declared = True
+    gx, x32, v32 = _f32(grid_x), _f32(x), _f32(v)
+    w, r, fl = _f32(inv_mass), _f32(radius), _i32(flags)
+    d = np.array(deltas_init, dtype=np.float32)
+    st = L.oracle_particle_contact_deltas_grid(_p(gx), float(np.float32(grid_radius)), _i32(dims), x32.shape[0],
+                                               _p(x32), _p(v32), _p(w), _p(r), _p(fl),
+                                               *[float(np.float32(t)) for t in
+                                                 (k_mu, k_cohesion, max_radius, dt, relaxation)], _p(d))
+    if st != 0:
+        raise RuntimeError(f"oracle_particle_contact_deltas_grid status {st}")
+    return d

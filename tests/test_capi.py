@@ -69,7 +69,9 @@ def _c_layout(struct: str, fields: list[str]) -> list[int]:
 
 @pytest.mark.parametrize("pyname,cname", [("NsphSphParams", "nsph_sph_params"), ("NsphGridView", "nsph_grid_view"),
                                           ("NsphContactParams", "nsph_contact_params"),
-                                          ("NsphRaycastCamera", "nsph_raycast_camera")])
+                                          ("NsphRaycastCamera", "nsph_raycast_camera"),
+                                          ("NsphShape", "nsph_shape"), ("NsphSoftContacts", "nsph_soft_contacts"),
+                                          ("NsphSoftContactParams", "nsph_soft_contact_params")])
 def test_struct_layouts_match_header(pyname, cname):
     from newton_sph_dev_b200 import _lib
 

@@ -1,0 +1,185 @@
+"""Step parity at the benchmark's full size and on evolved states.
+
+The 1,048,576-particle tank (128x128x64 block at 0.005 m in a 2x1x1 m tank,
+velocities N(0, 0.01) from default_rng(2), h = 0.01, dt = 5e-5) is the
+workload the throughput figure is quoted on. These tests check its dynamics,
+not only its grid:
+
+  - one step from the initial lattice: grid, neighbour lists, rho, p, a, x, v
+    bit-exact against the fp32 oracle, and within the fp64 bars (density
+    1e-5 relative, positions 1e-5 of the domain, accelerations median 1e-5 /
+    max 1e-3 of the summed magnitudes);
+  - one step from a state the GPU solver reached after 600 steps (the dam
+    has started to fall: compressed layers, ragged cells), the oracle run on
+    that same input;
+  - a dense cluster whose particles see more than 256 candidates, so the
+    force pass re-tests candidates instead of reading its neighbour mask
+    (the overflow path), checked the same way.
+
+Reference semantics: integrate_particles (newton/_src/solvers/solver.py:10-47)
+and the lattice inputs of ModelBuilder.add_particle_grid
+(newton/_src/sim/builder.py:8083-8096).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import lattice_scene
+
+pytestmark = pytest.mark.gpu
+
+DEV = "cuda:0"
+DT = 5e-5
+
+
+def _tank():
+    return lattice_scene((128, 128, 64), spacing=0.005, vel_std=0.01, device=DEV, box_hi=(2.0, 1.0, 1.0),
+                         register=True)
+
+
+def _host(model, state):
+    return dict(
+        x=state.particle_q.cpu().numpy(),
+        v=state.particle_qd.cpu().numpy(),
+        f=state.particle_f.cpu().numpy(),
+        mass=model.particle_mass.cpu().numpy(),
+        inv_mass=model.particle_inv_mass.cpu().numpy(),
+        flags=model.particle_flags.cpu().numpy(),
+        world=model.particle_world.cpu().numpy(),
+        gravity=model.gravity.cpu().numpy(),
+    )
+
+
+def _check_step(O, solver, model, cfg, s0, s1, v_init, dt, check_grid=True):
+    """s1 = step(s0) on the device: compare with the oracles on s0's input."""
+    h = _host(model, s0)
+    consts = cfg.constants(dt, model.particle_max_velocity)
+    if check_grid:
+        g = solver.grid_arrays()
+        ref = O.grid_build(h["x"], float(consts["f32"]["cell_width"]), solver.grid_dims)
+        for k in ref:
+            np.testing.assert_array_equal(g[k].cpu().numpy(), ref[k], err_msg=k)
+        off, ids = solver.neighbors()
+        roff, rids = O.sph_neighbors(consts["f32"], solver.grid_dims, h["x"], h["flags"])
+        np.testing.assert_array_equal(off.cpu().numpy(), roff)
+        np.testing.assert_array_equal(ids.cpu().numpy(), rids)
+    args = (consts, solver.grid_dims, h["x"], h["v"], h["mass"], h["inv_mass"], h["flags"], h["world"], h["gravity"])
+    r32 = O.sph_step(*args, f_ext=h["f"], v_out_init=v_init, precision="f32")
+    rho = s1.sph.density.cpu().numpy()
+    np.testing.assert_array_equal(rho, r32["rho"])
+    np.testing.assert_array_equal(s1.sph.pressure.cpu().numpy(), r32["p"])
+    np.testing.assert_array_equal(s1.sph.acceleration.cpu().numpy(), r32["a"])
+    np.testing.assert_array_equal(s1.particle_q.cpu().numpy(), r32["x"])
+    np.testing.assert_array_equal(s1.particle_qd.cpu().numpy(), r32["v"])
+    r64 = O.sph_step(*args, f_ext=h["f"], v_out_init=v_init, precision="f64")
+    act = h["flags"] != 0
+    assert np.max(np.abs(rho[act].astype(np.float64) - r64["rho"][act]) / r64["rho"][act]) < 1e-5
+    x = s1.particle_q.cpu().numpy().astype(np.float64)
+    span = float(np.max(np.abs(r64["x"])))
+    assert np.max(np.abs(x - r64["x"])) < 1e-5 * span
+    a = s1.sph.acceleration.cpu().numpy().astype(np.float64)
+    abs_err = np.linalg.norm(a - r64["a"], axis=1)[act]
+    err = abs_err / np.maximum(r64["a_scale"][act], 1e-30)
+    assert np.median(err) < 1e-5 and np.percentile(err, 99.9) < 1e-4
+    # Per particle: within 1e-3 of its summed magnitudes, or within 1e-2 g in
+    # absolute terms. The second arm covers free-surface particles whose own
+    # pressure is clamped to 0: their small force is a sum of the neighbours'
+    # pressures, each carrying the fp32 EOS cancellation near rest density
+    # (an absolute error of about gamma * B * 2^-24 per pressure), which is
+    # large against their small summands (1.3e-2 relative, 0.03 m/s^2, on
+    # the 1M lattice; the fp32 oracle has the same error).
+    assert not np.any((err > 1e-3) & (abs_err > 1e-2 * 9.81))
+    return r32
+
+
+def test_tank_1m_step_from_lattice(oracle_mod):
+    from newton_sph_dev_b200.solvers import SolverSPH
+
+    model, cfg = _tank()
+    assert model.particle_count == 1048576
+    solver = SolverSPH(model, cfg)
+    s0, s1 = model.state(), model.state()
+    v_init = s1.particle_qd.cpu().numpy()
+    solver.step(s0, s1, None, None, DT)
+    torch.cuda.synchronize()
+    _check_step(oracle_mod, solver, model, cfg, s0, s1, v_init, DT)
+    assert solver.status() == 0
+
+
+def test_tank_1m_step_from_evolved_state(oracle_mod):
+    """600 graph-free device steps (0.03 s: the block starts to collapse),
+    then one step checked against the oracle run on the same input."""
+    from newton_sph_dev_b200.solvers import SolverSPH
+
+    model, cfg = _tank()
+    solver = SolverSPH(model, cfg)
+    s0, s1 = model.state(), model.state()
+    x0 = s0.particle_q.clone()
+    for _ in range(600):
+        solver.step(s0, s1, None, None, DT)
+        s0, s1 = s1, s0
+    torch.cuda.synchronize()
+    assert solver.status() == 0
+    # the state has moved well away from the lattice
+    moved = float(torch.linalg.norm(s0.particle_q - x0, dim=1).max())
+    assert moved > 0.2 * 0.005
+    v_init = s1.particle_qd.cpu().numpy()
+    solver.step(s0, s1, None, None, DT)
+    torch.cuda.synchronize()
+    _check_step(oracle_mod, solver, model, cfg, s0, s1, v_init, DT)
+    assert solver.status() == 0
+
+
+def _cluster_model(n_cluster=320, side=1.5, seed=9):
+    """A 12^3 lattice (spacing 0.01, h = 0.02) plus a dense cluster of
+    n_cluster particles in a cube of `side` x h away from it: every cluster
+    particle sees all n_cluster cluster particles as candidates (> 256)."""
+    import newton_sph_dev_b200 as nsph
+    from newton_sph_dev_b200.solvers import SolverSPH
+
+    s = 0.01
+    h = 2 * s
+    b = nsph.ModelBuilder()
+    SolverSPH.register_custom_attributes(b)
+    b.add_custom_attribute(nsph.ModelBuilder.CustomAttribute(
+        "acceleration", frequency=nsph.Model.AttributeFrequency.PARTICLE,
+        assignment=nsph.Model.AttributeAssignment.STATE, dtype=torch.float32, default=0.0, namespace="sph", width=3))
+    b.add_particle_grid(pos=(s / 2, s / 2, s / 2), rot=(0, 0, 0, 1), vel=(0, 0, 0), dim_x=12, dim_y=12, dim_z=12,
+                        cell_x=s, cell_y=s, cell_z=s, mass=1000.0 * s**3, jitter=0.2 * s)
+    rng = np.random.default_rng(seed)
+    c0 = np.array([0.30, 0.30, 0.30])
+    pts = c0 + rng.random((n_cluster, 3)) * side * h
+    b.add_particles(pos=pts, vel=rng.normal(0, 0.05, (n_cluster, 3)), mass=np.full(n_cluster, 1000.0 * s**3))
+    model = b.finalize(DEV)
+    cfg = SolverSPH.Config(smoothing_length=h, box_lo=(0.0, 0.0, 0.0), box_hi=(0.5, 0.5, 0.5))
+    return model, cfg
+
+
+def test_mask_overflow_dense_cluster(oracle_mod):
+    from newton_sph_dev_b200.solvers import SolverSPH
+
+    model, cfg = _cluster_model()
+    solver = SolverSPH(model, cfg)
+    s0, s1 = model.state(), model.state()
+    v_init = s1.particle_qd.cpu().numpy()
+    solver.step(s0, s1, None, None, 1e-6)
+    torch.cuda.synchronize()
+    # the cluster's particles have more candidates than the mask holds
+    h = _host(model, s0)
+    consts = cfg.constants(1e-6, model.particle_max_velocity)
+    grid = oracle_mod.grid_build(h["x"], float(consts["f32"]["cell_width"]), solver.grid_dims)
+    cand = [oracle_mod.grid_query(grid, solver.grid_dims, float(consts["f32"]["cell_inv"]), h["x"][i],
+                                  float(consts["f32"]["h"])).size for i in (model.particle_count - 1, 0)]
+    assert cand[0] > 256 and cand[1] <= 256
+    _check_step(oracle_mod, solver, model, cfg, s0, s1, v_init, 1e-6)
+    # and a few steps later, still bit-exact
+    for _ in range(3):
+        solver.step(s0, s1, None, None, 1e-6)
+        s0, s1 = s1, s0
+    v_init = s1.particle_qd.cpu().numpy()
+    solver.step(s0, s1, None, None, 1e-6)
+    torch.cuda.synchronize()
+    _check_step(oracle_mod, solver, model, cfg, s0, s1, v_init, 1e-6, check_grid=False)

@@ -72,3 +72,43 @@ def test_noalloc_build_refuses_more_points_than_its_scratch():
     st, *_ = _noalloc_build(lib, pts, 0.1, (8, 8, 8))
     assert st == _lib.NSPH_ERR_CAPACITY
     assert "NSPH_NOALLOC_MAX_POINTS" in _lib.last_error()
+
+
+def test_noalloc_build_inside_a_graph_capture():
+    """The reason the entry point exists: a build captured into a CUDA graph
+    (no allocation, no synchronisation during the capture), replayed on new
+    points copied into the captured input buffer."""
+    from newton_sph_dev_b200 import _lib
+
+    lib = _lib.load()
+    dims = (32, 32, 32)
+    radius = 0.04
+    n = 20_000
+    rng = np.random.default_rng(7)
+    pts = torch.zeros((n, 3), dtype=torch.float32, device=DEV)
+    cells = torch.zeros(n, dtype=torch.int32, device=DEV)
+    ids = torch.zeros(n, dtype=torch.int32, device=DEV)
+    starts = torch.zeros(dims[0] * dims[1] * dims[2], dtype=torch.int32, device=DEV)
+    ends = torch.zeros_like(starts)
+    # the warm-up call may be empty: it sets the device up all the same
+    st = lib.nsph_grid_build_noalloc(pts.data_ptr(), 0, radius, *dims, cells.data_ptr(), ids.data_ptr(),
+                                     starts.data_ptr(), ends.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert st == 0, _lib.last_error()
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    status = []
+    with torch.cuda.graph(graph):
+        status.append(lib.nsph_grid_build_noalloc(pts.data_ptr(), n, radius, *dims, cells.data_ptr(), ids.data_ptr(),
+                                                  starts.data_ptr(), ends.data_ptr(),
+                                                  torch.cuda.current_stream().cuda_stream))
+    assert status == [0], _lib.last_error()
+    for _ in range(2):
+        new = torch.from_numpy((rng.random((n, 3)) * 1.1 - 0.05).astype(np.float32)).to(DEV)
+        pts.copy_(new)
+        graph.replay()
+        torch.cuda.synchronize()
+        ref = _allocating_build(new, radius, dims)
+        for got, want, name in zip((cells, ids, starts, ends), ref, ("point_cells", "point_ids", "cell_starts",
+                                                                      "cell_ends")):
+            assert torch.equal(got.cpu(), want.cpu()), name
+    del graph
