@@ -39,6 +39,7 @@ def evaluate(model: SurrogateModel, shape=(32, 32, 32), spacing=0.01, dt=1e-4, s
     n = scene.particle_count
     out = {"particles": n, "macro_steps": macro_steps, "substeps": substeps, "dt": dt, "vel_std": vel_std}
     results = {}
+    diverged: dict = {}
     zero = SurrogateModel(device)
     zero.zero_correction()
     for name, m in (("plain", None), ("surrogate", model), ("uncorrected", zero)):
@@ -51,10 +52,13 @@ def evaluate(model: SurrogateModel, shape=(32, 32, 32), spacing=0.01, dt=1e-4, s
                 solver.step(s0, s1, None, None, dt)
                 s0, s1 = s1, s0
         else:
-            st = SurrogateSPH(solver, m, substeps=substeps, threshold=float("inf"), window=macro_steps)
-            for _ in range(macro_steps):
+            st = SurrogateSPH(solver, m, substeps=substeps, threshold=float("inf"), window=1)
+            for k in range(macro_steps):
                 st.step(s0, s1, dt)
                 s0, s1 = s1, s0
+                worst = st.window_worst[-1]
+                if not (worst < 1.0) and name not in diverged:  # compression above 100%, or not finite
+                    diverged[name] = k
             comp.append(st.mean_compression())
         solver.features_raw(s0.particle_q, s0.particle_qd, rho_out=rho, params=solver.step_params(dt))
         final_comp = float(torch.clamp(rho / 1000.0 - 1.0, min=0).mean())
@@ -65,7 +69,7 @@ def evaluate(model: SurrogateModel, shape=(32, 32, 32), spacing=0.01, dt=1e-4, s
         d = (x - ref).norm(dim=1) / h
         out[name] = {"rms_error_h": float(d.pow(2).mean().sqrt()), "max_error_h": float(d.max()),
                      "final_compression": fc, "mean_step_compression": mc,
-                     "finite": bool(torch.isfinite(x).all())}
+                     "finite": bool(torch.isfinite(x).all()), "diverged_at_step": diverged.get(name)}
     return out
 
 
@@ -74,17 +78,21 @@ def main(argv=None):
     ap.add_argument("--out", required=True)
     ap.add_argument("--report", default=None)
     ap.add_argument("--trajectories", type=int, default=200)
-    ap.add_argument("--samples", type=int, default=10, help="samples (of 4 plain steps) per trajectory")
+    ap.add_argument("--samples", type=int, default=10, help="samples (of `substeps` plain steps) per trajectory")
     ap.add_argument("--keep", type=float, default=0.125, help="fraction of particles kept per sample")
     ap.add_argument("--iters", type=int, default=3000)
     ap.add_argument("--batch", type=int, default=65536)
     ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--substeps", type=int, default=4,
+                    help="plain steps of 1e-4 s per surrogate step (4: dt c0/h = 0.4; 8: 0.8)")
+    ap.add_argument("--eval-steps", type=int, default=50, help="surrogate steps of the held-out rollout")
     ap.add_argument("--device", default="cuda:0")
     args = ap.parse_args(argv)
     t0 = time.time()
     feats, targs, info = generate_training_data(trajectories=args.trajectories, samples_per_trajectory=args.samples,
-                                                keep_fraction=args.keep, seed=args.seed, device=args.device)
+                                                keep_fraction=args.keep, seed=args.seed, device=args.device,
+                                                substeps=args.substeps)
     t_data = time.time() - t0
     model = SurrogateModel(args.device, seed=args.seed)
     t0 = time.time()
@@ -96,7 +104,7 @@ def main(argv=None):
                   "iters": args.iters, "batch": args.batch, "lr": args.lr}
     model.save(args.out)
     report = {"data": info, "data_seconds": t_data, "train_seconds": t_train, "train": res,
-              "eval": evaluate(model, device=args.device)}
+              "eval": evaluate(model, device=args.device, substeps=args.substeps, macro_steps=args.eval_steps)}
     text = json.dumps(report, indent=1)
     print(text)
     if args.report:
