@@ -593,6 +593,20 @@ NSPH_API int nsph_sph_adjoint_phase_times(nsph_sph* solver, float ms_out[5]);
  * durations of the last executed surrogate step in ms. */
 NSPH_API int nsph_sph_surrogate_phase_times(nsph_sph* solver, float ms_out[4]);
 
+/* Arithmetic of the plain single-world step's density and force passes.
+ * NSPH_ARITH_EXACT (the default): every fp32 operation correctly rounded in
+ * the fp32 oracle's order, so results are bit-exact with it.
+ * NSPH_ARITH_FAST: the kernel terms use the hardware reciprocal square root
+ * in place of the correctly rounded square root, reciprocal and division,
+ * and multiply-adds may contract; the neighbour test, and so the neighbour
+ * sets, are unchanged and sums keep the query order. Results then agree with
+ * the fp64 oracle to the same tolerances as the exact mode, not bit for bit
+ * with the fp32 oracle. Other steps (worlds, adjoint, surrogate) always use
+ * the exact arithmetic. */
+#define NSPH_ARITH_EXACT 0
+#define NSPH_ARITH_FAST 1
+NSPH_API int nsph_sph_set_arithmetic(nsph_sph* solver, int mode);
+
 /* Launch shape of the two neighbour passes (density, force): `threads` per
  * block (0 = default 256; else a multiple of 32 up to 256) and
  * `blocks_per_sm` (-1 = default: one thread per particle for a single world,

@@ -321,6 +321,7 @@ SIGNATURES = [
     ("nsph_sph_adjoint_phase_times", ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_float * 5)]),
     ("nsph_sph_surrogate_phase_times", ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_float * 4)]),
     ("nsph_sph_set_launch", ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int]),
+    ("nsph_sph_set_arithmetic", ctypes.c_int, [c_void_p, ctypes.c_int]),
     ("nsph_sph_last_launches", ctypes.c_int, [c_void_p]),
     ("nsph_sph_status", ctypes.c_int, [c_void_p, ctypes.POINTER(ctypes.c_uint), c_void_p]),
     ("nsph_sph_reset_status", ctypes.c_int, [c_void_p, c_void_p]),

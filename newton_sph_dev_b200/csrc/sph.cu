@@ -119,6 +119,26 @@ __device__ __forceinline__ float wterm(float r2, const nsph_sph_params& p)
     return kernel_w(__fmul_rn(__fsqrt_rn(r2), p.inv_h), p);
 }
 
+// ---- tolerance ("fast") arithmetic ---------------------------------------------
+// The same kernel values with the hardware reciprocal square root instead of
+// the correctly rounded square root, reciprocal and division, and with the
+// compiler free to contract multiply-adds: r = r2 * rsqrt(r2), 1/r = rsqrt(r2).
+// The neighbour test r2 < h2 is unchanged, so neighbour sets stay bit-exact;
+// sums keep the query order. Results are within the fp64 oracle's tolerance
+// (checked by the tests), not bit-exact with the fp32 oracle.
+__device__ __forceinline__ float kernel_w_fast(float q, const nsph_sph_params& p)
+{
+    const float t = 1.f - q;
+    const float v = q <= 0.5f ? fmaf(6.f * q * q, q - 1.f, 1.f) : (q < 1.f ? 2.f * t * t * t : 0.f);
+    return p.sigma * v;
+}
+
+__device__ __forceinline__ float wterm_fast(float r2, const nsph_sph_params& p)
+{
+    const float r = r2 > 0.f ? r2 * rsqrtf(r2) : 0.f;
+    return kernel_w_fast(r * p.inv_h, p);
+}
+
 // ---- pass 1: density + EOS --------------------------------------------------
 // Append `cnt` (<= 4) mask bits for the candidates at positions pos.. to the
 // particle's mask (word-major in global memory, the first kMaskWords words).
@@ -179,6 +199,7 @@ __device__ __forceinline__ float density_single(const GridDev& g, const float4* 
     return rho;
 }
 
+template <bool Fast = false>
 __device__ __forceinline__ void density_finish(int k, float m, float rho, const nsph_sph_params& p,
                                                float2* __restrict__ aux, float2* __restrict__ rp,
                                                unsigned* __restrict__ status)
@@ -186,8 +207,14 @@ __device__ __forceinline__ void density_finish(int k, float m, float rho, const 
     float pr = 0.f, mor = 0.f, pr2 = 0.f;
     if (rho > 0.f) {
         pr = eos(rho, p);
-        mor = __fdiv_rn(m, rho);
-        pr2 = __fdiv_rn(pr, __fmul_rn(rho, rho));
+        if (Fast) {
+            const float ir = __frcp_rn(rho);
+            mor = m * ir;
+            pr2 = pr * ir * ir;
+        } else {
+            mor = __fdiv_rn(m, rho);
+            pr2 = __fdiv_rn(pr, __fmul_rn(rho, rho));
+        }
     } else if (status) {
         atomicOr(status, (unsigned)NSPH_STATUS_ZERO_DENSITY);
     }
@@ -267,11 +294,13 @@ __device__ __forceinline__ int neighbor_list(const GridDev& g, const float4* __r
 
 // rho of particle k from its list (read back by the thread that wrote it,
 // with plain loads), or by re-testing its candidates when the list overflowed
+template <bool Fast>
 __device__ __forceinline__ float density_from_list(const GridDev& g, const float4* __restrict__ xs,
                                                    const nsph_sph_params& p, float4 xi, const int* nbr, int cnt,
                                                    int n, int k)
 {
     float rho = 0.f;
+    auto w = [&](float r2) { return Fast ? wterm_fast(r2, p) : wterm(r2, p); };
     if (cnt <= kNbrSlots) {
         int jn = cnt > 0 ? nbr[k] : 0;
         for (int t = 0; t < cnt; ++t) {
@@ -279,14 +308,14 @@ __device__ __forceinline__ float density_from_list(const GridDev& g, const float
             if (t + 1 < cnt) jn = nbr[(size_t)(t + 1) * n + k];
             const float4 xj = __ldg(xs + j);
             float dx, dy, dz;
-            rho = __fmaf_rn(xj.w, wterm(dist2(xi, xj, dx, dy, dz), p), rho);
+            rho = __fmaf_rn(xj.w, w(dist2(xi, xj, dx, dy, dz)), rho);
         }
     } else {
         for_each_candidate(g, xi.x, xi.y, xi.z, p.h, [&](int j) {
             const float4 xj = __ldg(xs + j);
             float dx, dy, dz;
             const float r2 = dist2(xi, xj, dx, dy, dz);
-            if (r2 < p.h2) rho = __fmaf_rn(xj.w, wterm(r2, p), rho);
+            if (r2 < p.h2) rho = __fmaf_rn(xj.w, w(r2), rho);
         });
     }
     return rho;
@@ -317,6 +346,31 @@ __device__ __forceinline__ void force_term_data(float4 xj, float4 vj, float2 aj,
     acc.dvx = __fmaf_rn(c, __fsub_rn(vj.x, vi.x), acc.dvx);
     acc.dvy = __fmaf_rn(c, __fsub_rn(vj.y, vi.y), acc.dvy);
     acc.dvz = __fmaf_rn(c, __fsub_rn(vj.z, vi.z), acc.dvz);
+}
+
+// force_term_data in the tolerance arithmetic (see kernel_w_fast)
+__device__ __forceinline__ void force_term_fast(float4 xj, float4 vj, float2 aj, float4 xi, float4 vi, float pr2_i,
+                                                const nsph_sph_params& p, ForceAcc& acc)
+{
+    if (!(__float_as_int(vj.w) & kAttrActive)) return;
+    const float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+    const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+    float w = p.sigma;
+    if (r2 > 0.f) {
+        const float ir = rsqrtf(r2);
+        const float q = r2 * ir * p.inv_h;
+        const float t = 1.f - q;
+        w = kernel_w_fast(q, p);
+        const float f = q <= 0.5f ? p.c_near * fmaf(3.f, q, -2.f) : (q < 1.f ? p.c_far * t * t * ir : 0.f);
+        const float s = xj.w * (pr2_i + aj.y) * f;
+        acc.ax -= s * dx;
+        acc.ay -= s * dy;
+        acc.az -= s * dz;
+    }
+    const float c = aj.x * w;
+    acc.dvx += c * (vj.x - vi.x);
+    acc.dvy += c * (vj.y - vi.y);
+    acc.dvz += c * (vj.z - vi.z);
 }
 
 // single particle: walk its neighbour mask (or re-test when the mask overflowed).
@@ -460,6 +514,7 @@ __global__ void __launch_bounds__(kSphThreads, 4) k_force(GridDev g, const float
 
 // ---- the plain step's passes on neighbour lists ----------------------------------
 // Bounded to 48 registers, like the mask form: 40 resident warps per SM.
+template <bool Fast>
 __global__ void __launch_bounds__(kSphThreads, 5) k_density_list(GridDev g, const float4* __restrict__ xs,
                                                                  const float4* __restrict__ vs, int n,
                                                                  const __grid_constant__ nsph_sph_params p,
@@ -477,14 +532,15 @@ __global__ void __launch_bounds__(kSphThreads, 5) k_density_list(GridDev g, cons
         }
         const int cnt = neighbor_list(g, xs, p, xi, nbr, n, k);
         ncnt[k] = cnt;
-        const float rho = density_from_list(g, xs, p, xi, nbr, cnt, n, k);
-        density_finish(k, xi.w, rho, p, aux, rp, status);
+        const float rho = density_from_list<Fast>(g, xs, p, xi, nbr, cnt, n, k);
+        density_finish<Fast>(k, xi.w, rho, p, aux, rp, status);
     }
 }
 
 // pressure and XSPH sums of particle k over its list, in order (loads of
 // neighbour t+1 issued before the terms of neighbour t), or by re-testing
 // its candidates when the list overflowed
+template <bool Fast>
 __device__ __forceinline__ void force_from_list(const GridDev& g, const float4* __restrict__ xs,
                                                 const float4* __restrict__ vs, const float2* __restrict__ aux,
                                                 const int* __restrict__ nbr, int cnt, int n, int k, float4 xi,
@@ -500,24 +556,39 @@ __device__ __forceinline__ void force_from_list(const GridDev& g, const float4* 
             const float4 nxj = __ldg(xs + j);
             const float4 nvj = __ldg(vs + j);
             const float2 naj = __ldg(aux + j);
-            if (have) force_term_data(pxj, pvj, paj, xi, vi, pr2_i, p, acc);
+            if (have) {
+                if (Fast)
+                    force_term_fast(pxj, pvj, paj, xi, vi, pr2_i, p, acc);
+                else
+                    force_term_data(pxj, pvj, paj, xi, vi, pr2_i, p, acc);
+            }
             pxj = nxj;
             pvj = nvj;
             paj = naj;
             have = true;
         }
-        if (have) force_term_data(pxj, pvj, paj, xi, vi, pr2_i, p, acc);
+        if (have) {
+            if (Fast)
+                force_term_fast(pxj, pvj, paj, xi, vi, pr2_i, p, acc);
+            else
+                force_term_data(pxj, pvj, paj, xi, vi, pr2_i, p, acc);
+        }
     } else {
         for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
             for (int j = lo; j < hi; ++j) {
                 float dx, dy, dz;
-                if (dist2(xi, __ldg(xs + j), dx, dy, dz) < p.h2 && j != k)
-                    force_term_data(__ldg(xs + j), __ldg(vs + j), __ldg(aux + j), xi, vi, pr2_i, p, acc);
+                if (dist2(xi, __ldg(xs + j), dx, dy, dz) < p.h2 && j != k) {
+                    if (Fast)
+                        force_term_fast(__ldg(xs + j), __ldg(vs + j), __ldg(aux + j), xi, vi, pr2_i, p, acc);
+                    else
+                        force_term_data(__ldg(xs + j), __ldg(vs + j), __ldg(aux + j), xi, vi, pr2_i, p, acc);
+                }
             }
         });
     }
 }
 
+template <bool Fast>
 __global__ void __launch_bounds__(kSphThreads, 4) k_force_list(GridDev g, const float4* __restrict__ xs,
                                                                const float4* __restrict__ vs,
                                                                const float2* __restrict__ aux,
@@ -530,7 +601,7 @@ __global__ void __launch_bounds__(kSphThreads, 4) k_force_list(GridDev g, const 
         const float4 xi = xs[k], vi = vs[k];
         const int attr = __float_as_int(vi.w);
         ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        if (attr & kAttrActive) force_from_list(g, xs, vs, aux, nbr, ncnt[k], n, k, xi, vi, aux[k].y, p, acc);
+        if (attr & kAttrActive) force_from_list<Fast>(g, xs, vs, aux, nbr, ncnt[k], n, k, xi, vi, aux[k].y, p, acc);
         integrate_out((size_t)g.ids[k], xi, vi, attr, rp[k], acc, p, p.dt, o);
     }
 }
@@ -1241,6 +1312,7 @@ struct nsph_sph {
     int* ncand = nullptr;      // candidates per particle
     int* nbr = nullptr;        // plain step (single world): kNbrSlots x capacity neighbour lists (slot-major)
     int* ncnt = nullptr;       //   neighbours per particle
+    int fast = 0;              // plain step: tolerance arithmetic (nsph_sph_set_arithmetic)
     unsigned* status = nullptr;
     int last_n = 0;
     int last_launches = 0;
@@ -1402,8 +1474,10 @@ extern "C" int nsph_sph_create(int device, int capacity, const int grid_dims[3],
         cudaError_t e = cudaMalloc(&s->nbr, sizeof(int) * kNbrSlots * c);
         if (e == cudaSuccess) e = cudaMalloc(&s->ncnt, sizeof(int) * c);
         cudaFuncAttributes fa;
-        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_density_list);
-        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_force_list);
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_density_list<false>);
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_force_list<false>);
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_density_list<true>);
+        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_force_list<true>);
         if (e != cudaSuccess) {
             cudaGetLastError();
             st = fail(NSPH_ERR_OUT_OF_MEMORY, std::string("solver allocation: ") + cudaGetErrorString(e));
@@ -1537,13 +1611,21 @@ static int step_enqueue(nsph_sph* s, const nsph_sph_params* p, int n, const floa
         const GridDev g = s->grid.view();
         int blocks, threads;
         pass_launch(s, n, false, blocks, threads);
-        k_density_list<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->nbr, s->ncnt,
-                                                   s->status);
+        if (s->fast)
+            k_density_list<true><<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->nbr, s->ncnt,
+                                                             s->status);
+        else
+            k_density_list<false><<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->nbr,
+                                                              s->ncnt, s->status);
         NSPH_LAUNCH_CHECK("k_density_list");
         ++launches;
         if (s->ev[2]) NSPH_CUDA_TRY(record_mark(s->ev[2], cs));
         const StepOut o{f_ext, inv_mass, gravity, x_out, v_out, rho_out, p_out, a_out, s->status};
-        k_force_list<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->nbr, s->ncnt, o);
+        if (s->fast)
+            k_force_list<true><<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->nbr, s->ncnt, o);
+        else
+            k_force_list<false><<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->nbr, s->ncnt,
+                                                            o);
         NSPH_LAUNCH_CHECK("k_force_list");
         ++launches;
     } else if (s->ev[2]) {
@@ -2243,6 +2325,15 @@ extern "C" int nsph_sph_step_surrogate(nsph_sph* s, const nsph_sph_params* p, co
     }
     if (s->eva[4]) NSPH_CUDA_TRY(record_mark(s->eva[4], cs));
     s->last_launches = launches;
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_set_arithmetic(nsph_sph* s, int mode)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    if (mode != NSPH_ARITH_EXACT && mode != NSPH_ARITH_FAST) return fail(NSPH_ERR_INVALID_ARG, "unknown arithmetic");
+    s->fast = mode == NSPH_ARITH_FAST;
     return NSPH_OK;
 }
 

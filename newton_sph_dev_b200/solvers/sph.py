@@ -72,6 +72,12 @@ class SPHConfig:
             each side (so no two box cells alias), else 128^3.
         apply_particle_f: add ``state_in.particle_f * inv_mass`` (external
             forces) to the acceleration, as integrate_particles does.
+        arithmetic: "exact" (default: every fp32 operation of the density
+            and force terms correctly rounded in the oracle's order, results
+            bit-exact with the fp32 oracle) or "fast" (hardware reciprocal
+            square root in the kernel terms; the same neighbour sets and
+            summation order, results within the fp64 oracle's tolerance).
+            Applies to the plain single-world step.
     """
 
     smoothing_length: float = 0.02
@@ -85,6 +91,7 @@ class SPHConfig:
     cell_width: float | None = None
     grid_dims: tuple[int, int, int] | None = None
     apply_particle_f: bool = True
+    arithmetic: str = "exact"
 
     # ---- derived constants ------------------------------------------
     def constants(self, dt: float, v_max: float) -> dict:
@@ -224,6 +231,15 @@ class SolverSPH(SolverBase):
             "SolverSPH()",
         )
         self._params = self.config.params(0.0, model.particle_max_velocity)
+        self.set_arithmetic(self.config.arithmetic)
+
+    def set_arithmetic(self, mode: str) -> None:
+        """"exact" or "fast" arithmetic of the plain step (see SPHConfig)."""
+        modes = {"exact": 0, "fast": 1}
+        if mode not in modes:
+            raise ValueError(f"arithmetic must be one of {sorted(modes)}, got {mode!r}")
+        _lib.check(self._lib.nsph_sph_set_arithmetic(self._handle, modes[mode]), "SolverSPH.set_arithmetic")
+        self.arithmetic = mode
 
     def _init_worlds(self, model: Model, configs: list[SPHConfig]) -> None:
         if len(configs) != model.world_count:
