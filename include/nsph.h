@@ -525,13 +525,24 @@ NSPH_API int nsph_apply_particle_deltas(int num_particles, const float* x_orig, 
  *   stats[1] = max(stats[1], stats[0]), stats[2] += 1 and
  *   stats[3] += stats[0], so a host that zeroes stats[1..2] reads a
  *   window's worst compression and step count with one copy. Kernels: grid
- *   build, density, feature pass, compression reduction, MLP + integrate. */
+ *   build, density (neighbour lists), then one kernel that gathers each
+ *   particle's force sums and features, stages them into the MLP's input
+ *   tile in shared memory, runs the MLP and integrates (the features never
+ *   go through HBM), then the compression reduction. If a tensor-core
+ *   completion wait gives up, the remaining particles are integrated without
+ *   the correction and NSPH_STATUS_SURROGATE_TIMEOUT is set.
+ * nsph_sph_set_surrogate_wait_limit: polls of each tensor-core completion
+ *   wait of the surrogate step (-1 = the default, about 4M polls). 0 makes
+ *   every wait give up before it polls, to exercise the timeout path; the
+ *   CTA then still waits, with the default limit, for the completion it
+ *   left outstanding before it frees its TMEM. */
 NSPH_API int nsph_sph_enable_surrogate(nsph_sph* solver);
 NSPH_API int nsph_sph_features(nsph_sph* solver, const nsph_sph_params* params, int n,
                                const float* x_in, const float* v_in,
                                const float* mass, const float* inv_mass, const int* flags, const int* world,
                                const float* gravity, int world_count,
                                float* feat_out, float* acc_out, float* rho_out, void* stream);
+NSPH_API int nsph_sph_set_surrogate_wait_limit(nsph_sph* solver, int polls);
 NSPH_API int nsph_sph_step_surrogate(nsph_sph* solver, const nsph_sph_params* params, const float* model,
                                      float acc_scale, int n,
                                      const float* x_in, const float* v_in, const float* f_ext,
@@ -588,9 +599,9 @@ NSPH_API int nsph_sph_phase_times(nsph_sph* solver, float ms_out[3]);
  * adjoint step in ms. */
 NSPH_API int nsph_sph_adjoint_phase_times(nsph_sph* solver, float ms_out[5]);
 /* With phase timing enabled, every surrogate step records five events:
- * start, after the grid build, after the density pass, after the feature
- * pass, end (compression reduction and MLP + integrate). Returns the four
- * durations of the last executed surrogate step in ms. */
+ * start, after the grid build, after the density pass, after the fused
+ * feature + MLP + integrate kernel, end (compression reduction). Returns the
+ * four durations of the last executed surrogate step in ms. */
 NSPH_API int nsph_sph_surrogate_phase_times(nsph_sph* solver, float ms_out[4]);
 
 /* Arithmetic of the plain single-world step's density and force passes.

@@ -292,6 +292,7 @@ SIGNATURES = [
         + [c_void_p] * 3
         + [c_void_p],
     ),
+    ("nsph_sph_set_surrogate_wait_limit", ctypes.c_int, [c_void_p, ctypes.c_int]),
     (
         "nsph_sph_step_surrogate",
         ctypes.c_int,

@@ -157,9 +157,9 @@ __device__ __forceinline__ void mlp_hidden_epilogue(uint32_t tmem_row, uint32_t 
 // at the completion still outstanding, which the caller waits for (bounded)
 // before it frees TMEM.
 template <class S>
-__device__ __forceinline__ bool mlp_wait(S& s, uint32_t& phase)
+__device__ __forceinline__ bool mlp_wait(S& s, uint32_t& phase, int limit = kMlpWaitLimit)
 {
-    const bool ok = __syncthreads_and(umma::mbar_wait(&s.bar, phase, kMlpWaitLimit)) != 0;
+    const bool ok = __syncthreads_and(umma::mbar_wait(&s.bar, phase, limit)) != 0;
     if (ok) phase ^= 1u;
     umma::fence_after_sync();
     return ok;
@@ -170,10 +170,10 @@ __device__ __forceinline__ bool mlp_wait(S& s, uint32_t& phase)
 // the output at c3 (each without bias); c2 may equal c1 and c3 may equal
 // either, since each accumulator is read out before the next MMA is issued. Returns false if an MMA wait gave up
 // (then no further MMA is issued). `phase` is the parity of the next
-// completion of s.bar.
+// completion of s.bar. `wait_limit` bounds each completion wait (polls).
 template <class S>
 __device__ bool mlp_forward_tile(S& s, uint32_t tmem, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t& phase,
-                                 float (&y)[kMlpOut])
+                                 float (&y)[kMlpOut], int wait_limit = kMlpWaitLimit)
 {
     using namespace umma;
     const int row = threadIdx.x;
@@ -185,7 +185,7 @@ __device__ bool mlp_forward_tile(S& s, uint32_t tmem, uint32_t c1, uint32_t c2, 
         mma_bf16(tmem + c1, smem_desc(xa, 128, 256), smem_desc(w1a, 128, 256), idesc_bf16_f32(128, kMlpHid), 0);
         mma_commit(&s.bar);
     }
-    if (!mlp_wait(s, phase)) return false;
+    if (!mlp_wait(s, phase, wait_limit)) return false;
     mlp_hidden_epilogue(tmem_row, c1, s.b1, s.h1, row);
     mlp_sync();
     // layer 2: z2 = h1 W2 (K = 64, four MMAs)
@@ -196,7 +196,7 @@ __device__ bool mlp_forward_tile(S& s, uint32_t tmem, uint32_t c1, uint32_t c2, 
                      idesc_bf16_f32(128, kMlpHid), k > 0);
         mma_commit(&s.bar);
     }
-    if (!mlp_wait(s, phase)) return false;
+    if (!mlp_wait(s, phase, wait_limit)) return false;
     mlp_hidden_epilogue(tmem_row, c2, s.b2, hidden2(s), row);
     mlp_sync();
     // layer 3: out = h2 W3 (K = 64, N = 16 of which 3 are used)
@@ -207,7 +207,7 @@ __device__ bool mlp_forward_tile(S& s, uint32_t tmem, uint32_t c1, uint32_t c2, 
                      idesc_bf16_f32(128, kMlpOutPad), k > 0);
         mma_commit(&s.bar);
     }
-    if (!mlp_wait(s, phase)) return false;
+    if (!mlp_wait(s, phase, wait_limit)) return false;
     float v[16];
     tmem_ld16(tmem_row + c3, v);
 #pragma unroll

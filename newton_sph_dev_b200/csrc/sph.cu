@@ -1027,10 +1027,11 @@ __global__ void k_adj_b_reduce(const float* __restrict__ bpart, int blocks, floa
 }
 
 // ==========================================================================
-// Surrogate step: the plain step's build and density pass, a force pass that
-// also gathers 16 neighbour features per particle (k_force_features), and
-// one kernel that evaluates the MLP on the tensor cores (mlp.cuh) and
-// integrates with the corrected acceleration a + da (k_surrogate). The
+// Surrogate step: the plain step's build and density pass (neighbour lists),
+// then one kernel (k_surrogate_fused) that gathers each particle's force
+// sums and 16 neighbour features, evaluates the MLP on the tensor cores
+// (mlp.cuh) and integrates with the corrected acceleration a + da. The
+// feature pass alone (k_force_features_list) serves the training data. The
 // features are dimensionless (lengths / h, velocities / c0, accelerations
 // h / c0^2, with c0^2 = B gamma / rho0):
 //   0 rho/rho0   1 rho/rho0 - 1   2-4 sum V_j W (x_j - x_i) / h
@@ -1078,31 +1079,31 @@ __device__ __forceinline__ void force_feature_term(float4 xj, float4 vj, float2 
     fa.dvg += aj.x * f * (rvx * dx + rvy * dy + rvz * dz);
 }
 
-__device__ __forceinline__ void force_features_single(const GridDev& g, const float4* __restrict__ xs,
-                                                      const float4* __restrict__ vs, const float2* __restrict__ aux,
-                                                      const unsigned* __restrict__ mask, int nc, int n, int k,
-                                                      float4 xi, float4 vi, float pr2_i, const nsph_sph_params& p,
-                                                      ForceAcc& acc, FeatAcc& fa)
+// pressure and XSPH sums (the statements of force_term_data, so the same
+// rounding) and the feature sums of particle k over its neighbour list, in
+// order
+__device__ __forceinline__ void force_features_from_list(const GridDev& g, const float4* __restrict__ xs,
+                                                         const float4* __restrict__ vs,
+                                                         const float2* __restrict__ aux, const int* __restrict__ nbr,
+                                                         int cnt, int n, int k, float4 xi, float4 vi, float pr2_i,
+                                                         const nsph_sph_params& p, ForceAcc& acc, FeatAcc& fa)
 {
-    if (nc <= kMaskBits) {
-        // one-deep software pipeline, as in force_single: the loads of
-        // neighbour t+1 are issued before the terms of neighbour t
+    if (cnt <= kNbrSlots) {
         bool have = false;
         float4 pxj = make_float4(0.f, 0.f, 0.f, 0.f), pvj = pxj;
         float2 paj = make_float2(0.f, 0.f);
-        for_each_masked(
-            g, xi, p.h, [&](int w) { return __ldg(mask + (size_t)w * n + k); },
-            [&](int j) {
-                if (j == k) return;
-                const float4 nxj = __ldg(xs + j);
-                const float4 nvj = __ldg(vs + j);
-                const float2 naj = __ldg(aux + j);
-                if (have) force_feature_term(pxj, pvj, paj, xi, vi, pr2_i, p, acc, fa);
-                pxj = nxj;
-                pvj = nvj;
-                paj = naj;
-                have = true;
-            });
+        for (int t = 0; t < cnt; ++t) {
+            const int j = __ldg(nbr + (size_t)t * n + k);
+            if (j == k) continue;
+            const float4 nxj = __ldg(xs + j);
+            const float4 nvj = __ldg(vs + j);
+            const float2 naj = __ldg(aux + j);
+            if (have) force_feature_term(pxj, pvj, paj, xi, vi, pr2_i, p, acc, fa);
+            pxj = nxj;
+            pvj = nvj;
+            paj = naj;
+            have = true;
+        }
         if (have) force_feature_term(pxj, pvj, paj, xi, vi, pr2_i, p, acc, fa);
     } else {
         for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
@@ -1115,54 +1116,70 @@ __device__ __forceinline__ void force_features_single(const GridDev& g, const fl
     }
 }
 
-// per sorted particle k: feat[16 k ..] and sacc[2k] = (a, 0), sacc[2k+1] =
-// (dv, 0); per block: (sum of max(0, rho/rho0 - 1), active count)
-__global__ void __launch_bounds__(kSphThreads, 4) k_force_features(GridDev g, const float4* __restrict__ xs,
-                                                                   const float4* __restrict__ vs,
-                                                                   const float2* __restrict__ aux,
-                                                                   const float2* __restrict__ rp, int n,
-                                                                   const __grid_constant__ nsph_sph_params p,
-                                                                   const unsigned* __restrict__ mask,
-                                                                   const int* __restrict__ ncand,
-                                                                   float* __restrict__ feat, float4* __restrict__ sacc,
-                                                                   float* __restrict__ cpart)
+// The 16 features of sorted particle k (all zero for an inactive one) and
+// its force sums; adds the particle's compression max(0, rho/rho0 - 1) and
+// 1 to (csum, ccount) when it is active.
+__device__ __forceinline__ void particle_features(const GridDev& g, const float4* __restrict__ xs,
+                                                  const float4* __restrict__ vs, const float2* __restrict__ aux,
+                                                  const float2* __restrict__ rp, const int* __restrict__ nbr,
+                                                  const int* __restrict__ ncnt, int n, int k, float4 xi, float4 vi,
+                                                  const nsph_sph_params& p, float (&f)[kFeat], ForceAcc& acc,
+                                                  float& csum, float& ccount)
 {
-    float csum = 0.f, ccount = 0.f;
+    acc = ForceAcc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (!(__float_as_int(vi.w) & kAttrActive)) {
+#pragma unroll
+        for (int j = 0; j < kFeat; ++j) f[j] = 0.f;
+        return;
+    }
     const float c0sq = fmaxf(p.eos_b * (float)p.eos_gamma * p.inv_rho0, 1e-30f);
     const float inv_c0 = rsqrtf(c0sq);
     const float ascale = p.h / c0sq;
+    const float2 ak = aux[k];
+    FeatAcc fa{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    force_features_from_list(g, xs, vs, aux, nbr, ncnt[k], n, k, xi, vi, ak.y, p, acc, fa);
+    const float2 rpk = rp[k];
+    const float ratio = rpk.x * p.inv_rho0;
+    f[0] = ratio;
+    f[1] = ratio - 1.f;
+    f[2] = fa.mx * p.inv_h;
+    f[3] = fa.my * p.inv_h;
+    f[4] = fa.mz * p.inv_h;
+    f[5] = acc.dvx * inv_c0;
+    f[6] = acc.dvy * inv_c0;
+    f[7] = acc.dvz * inv_c0;
+    f[8] = acc.ax * ascale;
+    f[9] = acc.ay * ascale;
+    f[10] = acc.az * ascale;
+    f[11] = fa.m2 * p.inv_h * p.inv_h;
+    f[12] = fa.sw + ak.x * p.sigma;
+    f[13] = fa.dvg * p.h * inv_c0;
+    f[14] = rpk.y * p.inv_rho0 / c0sq;
+    f[15] = sqrtf(f[8] * f[8] + f[9] * f[9] + f[10] * f[10]);
+    csum += fmaxf(ratio - 1.f, 0.f);
+    ccount += 1.f;
+}
+
+// per sorted particle k: feat[16 k ..] and sacc[2k] = (a, 0), sacc[2k+1] =
+// (dv, 0), from the neighbour lists; per block: (sum of max(0, rho/rho0 - 1),
+// active count)
+__global__ void __launch_bounds__(kSphThreads, 4) k_force_features_list(GridDev g, const float4* __restrict__ xs,
+                                                                        const float4* __restrict__ vs,
+                                                                        const float2* __restrict__ aux,
+                                                                        const float2* __restrict__ rp, int n,
+                                                                        const __grid_constant__ nsph_sph_params p,
+                                                                        const int* __restrict__ nbr,
+                                                                        const int* __restrict__ ncnt,
+                                                                        float* __restrict__ feat,
+                                                                        float4* __restrict__ sacc,
+                                                                        float* __restrict__ cpart)
+{
+    float csum = 0.f, ccount = 0.f;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const float4 xi = xs[k], vi = vs[k];
         float f[kFeat];
-        ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        if (__float_as_int(vi.w) & kAttrActive) {
-            const float2 ak = aux[k];
-            FeatAcc fa{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-            force_features_single(g, xs, vs, aux, mask, ncand[k], n, k, xi, vi, ak.y, p, acc, fa);
-            const float2 rpk = rp[k];
-            const float ratio = rpk.x * p.inv_rho0;
-            f[0] = ratio;
-            f[1] = ratio - 1.f;
-            f[2] = fa.mx * p.inv_h;
-            f[3] = fa.my * p.inv_h;
-            f[4] = fa.mz * p.inv_h;
-            f[5] = acc.dvx * inv_c0;
-            f[6] = acc.dvy * inv_c0;
-            f[7] = acc.dvz * inv_c0;
-            f[8] = acc.ax * ascale;
-            f[9] = acc.ay * ascale;
-            f[10] = acc.az * ascale;
-            f[11] = fa.m2 * p.inv_h * p.inv_h;
-            f[12] = fa.sw + ak.x * p.sigma;
-            f[13] = fa.dvg * p.h * inv_c0;
-            f[14] = rpk.y * p.inv_rho0 / c0sq;
-            f[15] = sqrtf(f[8] * f[8] + f[9] * f[9] + f[10] * f[10]);
-            csum += fmaxf(ratio - 1.f, 0.f);
-            ccount += 1.f;
-        } else {
-#pragma unroll
-            for (int j = 0; j < kFeat; ++j) f[j] = 0.f;
-        }
+        ForceAcc acc;
+        particle_features(g, xs, vs, aux, rp, nbr, ncnt, n, k, xi, vi, p, f, acc, csum, ccount);
         float4* fo = reinterpret_cast<float4*>(feat + (size_t)k * kFeat);
 #pragma unroll
         for (int j = 0; j < kFeat; j += 4) fo[j / 4] = make_float4(f[j], f[j + 1], f[j + 2], f[j + 3]);
@@ -1199,69 +1216,73 @@ __global__ void k_compression_reduce(const float* __restrict__ cpart, int blocks
     }
 }
 
-__device__ __forceinline__ void load_features(const float* __restrict__ feat, int k, int n, float (&f)[kFeat])
-{
-    if (k < n) {
-        const float4* fi = reinterpret_cast<const float4*>(feat + (size_t)k * kFeat);
-#pragma unroll
-        for (int j = 0; j < kFeat; j += 4) {
-            const float4 q4 = __ldg(fi + j / 4);
-            f[j] = q4.x;
-            f[j + 1] = q4.y;
-            f[j + 2] = q4.z;
-            f[j + 3] = q4.w;
-        }
-    } else {
-#pragma unroll
-        for (int j = 0; j < kFeat; ++j) f[j] = 0.f;
-    }
-}
-
-// the MLP on the tensor cores, then integrate with a + da (dynamic
-// particles). Loads are issued ahead of the MMA chain that hides them: the
-// current tile's integrate inputs and the next tile's features.
-__global__ void __launch_bounds__(kMlpTile, 1) k_surrogate(const float* __restrict__ model, float acc_scale,
-                                                           GridDev g, const float4* __restrict__ xs,
-                                                           const float4* __restrict__ vs,
-                                                           const float2* __restrict__ rp, int n,
-                                                           const __grid_constant__ nsph_sph_params p,
-                                                           const float* __restrict__ feat,
-                                                           const float4* __restrict__ sacc, const StepOut o)
+// The surrogate step's force pass fused with the MLP: each CTA takes tiles
+// of 128 consecutive sorted particles; every thread gathers its particle's
+// pressure / XSPH sums and 16 features from the neighbour list, stages the
+// normalised bf16 feature row straight into the A tile of layer 1 in shared
+// memory, the tcgen05 chain runs (accumulators in TMEM), and the thread
+// integrates with a + da. Features and force sums never leave the SM.
+// While one CTA waits on its MMAs, the other resident CTAs gather. If an
+// MMA-completion wait gives up (after wait_limit polls), the CTA issues no
+// further MMAs, integrates its remaining particles without the correction
+// (the plain step at this dt) and flags NSPH_STATUS_SURROGATE_TIMEOUT. Per
+// CTA: (sum of max(0, rho/rho0 - 1), active count) into cpart.
+__global__ void __launch_bounds__(kMlpTile, 6) k_surrogate_fused(const float* __restrict__ model, float acc_scale,
+                                                                 int wait_limit, GridDev g,
+                                                                 const float4* __restrict__ xs,
+                                                                 const float4* __restrict__ vs,
+                                                                 const float2* __restrict__ aux,
+                                                                 const float2* __restrict__ rp, int n,
+                                                                 const __grid_constant__ nsph_sph_params p,
+                                                                 const int* __restrict__ nbr,
+                                                                 const int* __restrict__ ncnt, const StepOut o,
+                                                                 float* __restrict__ cpart)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     MlpFwdSmem& s = *reinterpret_cast<MlpFwdSmem*>(smem_raw);
     const uint32_t tmem = mlp_cta_begin(model, s, kMlpFwdCols);
     uint32_t phase = 0;
     bool ok = true;
+    float csum = 0.f, ccount = 0.f;
     const int tiles = (n + kMlpTile - 1) / kMlpTile;
-    float f[kFeat];
-    load_features(feat, (int)blockIdx.x * kMlpTile + (int)threadIdx.x, n, f);
-    for (int t = blockIdx.x; t < tiles && ok; t += gridDim.x) {
+    for (int t = blockIdx.x; t < tiles; t += gridDim.x) {
         const int k = t * kMlpTile + threadIdx.x;
-        mlp_stage_input(s, f);
-        mlp_sync();
-        // in flight during the MMA chain
         const int kk = k < n ? k : 0;
-        const float4 xi = __ldg(xs + kk), vi = __ldg(vs + kk);
-        const float4 a = __ldg(sacc + 2 * (size_t)kk), dv = __ldg(sacc + 2 * (size_t)kk + 1);
-        const float2 rpk = __ldg(rp + kk);
-        const int ik = __ldg(g.ids + kk);
-        load_features(feat, k + (int)gridDim.x * kMlpTile, n, f);
-        float y[kMlpOut];
-        ok = mlp_forward_tile(s, tmem, 0, 0, 0, phase, y);
-        if (ok && k < n) {
+        const float4 xi = xs[kk], vi = vs[kk];
+        float f[kFeat];
+        ForceAcc acc;
+        if (k < n) {
+            particle_features(g, xs, vs, aux, rp, nbr, ncnt, n, k, xi, vi, p, f, acc, csum, ccount);
+        } else {
+            acc = ForceAcc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int j = 0; j < kFeat; ++j) f[j] = 0.f;
+        }
+        float y[kMlpOut] = {0.f, 0.f, 0.f};
+        if (ok) {  // uniform across the CTA (mlp_wait makes the outcome uniform)
+            mlp_stage_input(s, f);
+            mlp_sync();
+            ok = mlp_forward_tile(s, tmem, 0, 0, 0, phase, y, wait_limit);
+        }
+        if (k < n) {
             const int attr = __float_as_int(vi.w);
-            ForceAcc acc{a.x, a.y, a.z, dv.x, dv.y, dv.z};
-            if (attr & kAttrDynamic) {
+            if (ok && (attr & kAttrDynamic)) {
                 acc.ax = __fadd_rn(acc.ax, acc_scale * mlp_denorm(s, y, 0));
                 acc.ay = __fadd_rn(acc.ay, acc_scale * mlp_denorm(s, y, 1));
                 acc.az = __fadd_rn(acc.az, acc_scale * mlp_denorm(s, y, 2));
             }
-            integrate_out((size_t)ik, xi, vi, attr, rpk, acc, p, p.dt, o);
+            integrate_out((size_t)g.ids[k], xi, vi, attr, rp[k], acc, p, p.dt, o);
         }
         __syncthreads();
     }
     if (!ok && o.status && threadIdx.x == 0) atomicOr(o.status, (unsigned)NSPH_STATUS_SURROGATE_TIMEOUT);
+    csum = block_sum(csum);
+    __syncthreads();
+    ccount = block_sum(ccount);
+    if (threadIdx.x == 0) {
+        cpart[2 * blockIdx.x] = csum;
+        cpart[2 * blockIdx.x + 1] = ccount;
+    }
     mlp_cta_end(s, tmem, kMlpFwdCols, !ok, phase);
 }
 
@@ -1332,7 +1353,8 @@ struct nsph_sph {
     float* sfeat = nullptr;              // surrogate scratch (nsph_sph_enable_surrogate), sorted: 16 features
     float4* sacc = nullptr;              //   (a, 0), (dv, 0)
     float* cpart = nullptr;              //   per-block (compression sum, active count)
-    int surr_ctas = 0;                   //   resident CTAs of k_surrogate (its grid)
+    int surr_ctas = 0;                   //   resident CTAs of k_surrogate_fused (its grid)
+    int surr_wait_limit = -1;            //   polls of an MMA-completion wait (-1: kMlpWaitLimit)
     char* tape = nullptr;                // segment tape (nsph_sph_segment_adjoint): per step of a segment,
     int tape_steps = 0;                  //   the build and density outputs the step's reverse reads,
     size_t tape_step_bytes = 0;          //   tape_steps slots of tape_step_bytes, then two states
@@ -2193,18 +2215,20 @@ extern "C" int nsph_sph_enable_surrogate(nsph_sph* s)
     DeviceGuard guard(s->grid.device);
     if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
     const size_t c = (size_t)(s->capacity > 0 ? s->capacity : 1);
-    const size_t blocks = (c + 31) / 32 + 1;
+    const size_t blocks = std::max((c + 31) / 32 + 1, (size_t)4096);  // per-block partials of either pass
     cudaError_t e = cudaMalloc(&s->sfeat, sizeof(float) * kFeat * c);
     if (e == cudaSuccess) e = cudaMalloc(&s->sacc, sizeof(float4) * 2 * c);
     if (e == cudaSuccess) e = cudaMalloc(&s->cpart, sizeof(float) * 2 * blocks);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_surrogate, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpFwdSmem));
+        e = cudaFuncSetAttribute(k_surrogate_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(MlpFwdSmem));
     if (e == cudaSuccess) {
-        s->surr_ctas = mlp_resident_grid(k_surrogate, sizeof(MlpFwdSmem), s->grid.device);
+        s->surr_ctas = mlp_resident_grid(k_surrogate_fused, sizeof(MlpFwdSmem), s->grid.device);
         if (s->surr_ctas <= 0) e = cudaErrorUnknown;
     }
+    if (e == cudaSuccess && s->surr_ctas + 1 > (int)blocks) e = cudaErrorInvalidValue;
     cudaFuncAttributes fa;
-    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_force_features);
+    if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_force_features_list);
     if (e != cudaSuccess) {
         cudaGetLastError();
         cudaFree(s->sfeat);
@@ -2217,12 +2241,13 @@ extern "C" int nsph_sph_enable_surrogate(nsph_sph* s)
     return NSPH_OK;
 }
 
-// grid build, density pass and feature pass into the sorted scratch
-// (with `mark`, records phase events 0-3 when phase timing is enabled:
-// start, built, after the density pass, after the feature pass)
+// grid build, density pass and (with `features`) the feature pass into the
+// sorted scratch (with `mark`, records phase events 0-2 when phase timing is
+// enabled: start, built, after the density pass)
 static int features_enqueue(nsph_sph* s, const nsph_sph_params* p, int n, const float* x_in, const float* v_in,
                             const float* mass, const float* inv_mass, const int* flags, const int* world,
-                            int world_count, cudaStream_t cs, int& launches, int& blocks, bool mark = false)
+                            int world_count, cudaStream_t cs, int& launches, int& blocks, bool mark = false,
+                            bool features = true)
 {
     GatherArgs ga{x_in, v_in, mass, inv_mass, flags, world, world_count, s->xs, s->vs};
     if (mark && s->eva[0]) NSPH_CUDA_TRY(record_mark(s->eva[0], cs));
@@ -2235,18 +2260,20 @@ static int features_enqueue(nsph_sph* s, const nsph_sph_params* p, int n, const 
         const GridDev g = s->grid.view();
         int threads;
         pass_launch(s, n, false, blocks, threads);
-        k_density<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->mask, s->ncand,
-                                                   s->status);
-        NSPH_LAUNCH_CHECK("k_density");
+        k_density_list<false><<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->nbr, s->ncnt,
+                                                          s->status);
+        NSPH_LAUNCH_CHECK("k_density_list");
+        ++launches;
         if (mark && s->eva[2]) NSPH_CUDA_TRY(record_mark(s->eva[2], cs));
-        k_force_features<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->mask, s->ncand,
-                                                          s->sfeat, s->sacc, s->cpart);
-        NSPH_LAUNCH_CHECK("k_force_features");
-        launches += 2;
+        if (features) {
+            k_force_features_list<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, s->aux, s->rp, n, *p, s->nbr,
+                                                              s->ncnt, s->sfeat, s->sacc, s->cpart);
+            NSPH_LAUNCH_CHECK("k_force_features_list");
+            ++launches;
+        }
     } else if (mark && s->eva[2]) {
         NSPH_CUDA_TRY(record_mark(s->eva[2], cs));
     }
-    if (mark && s->eva[3]) NSPH_CUDA_TRY(record_mark(s->eva[3], cs));
     return NSPH_OK;
 }
 
@@ -2310,21 +2337,35 @@ extern "C" int nsph_sph_step_surrogate(nsph_sph* s, const nsph_sph_params* p, co
     cudaStream_t cs = (cudaStream_t)stream;
     int launches = 0, blocks = 0;
     st = features_enqueue(s, p, n, x_in, v_in, mass, inv_mass, flags, world, world_count, cs, launches, blocks,
-                          true);
+                          true, false);
     if (st != NSPH_OK) return st;
     if (n > 0) {
-        k_compression_reduce<<<1, 256, 0, cs>>>(s->cpart, blocks, stats);
-        NSPH_LAUNCH_CHECK("k_compression_reduce");
         const int tiles = (n + kMlpTile - 1) / kMlpTile;
         const int grid = std::min(tiles, std::max(1, s->surr_ctas));
+        const int wait_limit = s->surr_wait_limit >= 0 ? s->surr_wait_limit : kMlpWaitLimit;
         const StepOut o{f_ext, inv_mass, gravity, x_out, v_out, rho_out, p_out, nullptr, s->status};
-        k_surrogate<<<grid, kMlpTile, sizeof(MlpFwdSmem), cs>>>(model, acc_scale, s->grid.view(), s->xs, s->vs,
-                                                                    s->rp, n, *p, s->sfeat, s->sacc, o);
-        NSPH_LAUNCH_CHECK("k_surrogate");
+        k_surrogate_fused<<<grid, kMlpTile, sizeof(MlpFwdSmem), cs>>>(model, acc_scale, wait_limit, s->grid.view(),
+                                                                      s->xs, s->vs, s->aux, s->rp, n, *p, s->nbr,
+                                                                      s->ncnt, o, s->cpart);
+        NSPH_LAUNCH_CHECK("k_surrogate_fused");
+        if (s->eva[3]) NSPH_CUDA_TRY(record_mark(s->eva[3], cs));
+        k_compression_reduce<<<1, 256, 0, cs>>>(s->cpart, grid, stats);
+        NSPH_LAUNCH_CHECK("k_compression_reduce");
         launches += 2;
+    } else if (s->eva[3]) {
+        NSPH_CUDA_TRY(record_mark(s->eva[3], cs));
     }
     if (s->eva[4]) NSPH_CUDA_TRY(record_mark(s->eva[4], cs));
     s->last_launches = launches;
+    return NSPH_OK;
+}
+
+extern "C" int nsph_sph_set_surrogate_wait_limit(nsph_sph* s, int polls)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    if (polls < -1) return fail(NSPH_ERR_INVALID_ARG, "poll count below -1");
+    s->surr_wait_limit = polls;
     return NSPH_OK;
 }
 

@@ -83,9 +83,9 @@ class SensorRaycast:
     def __init__(self, model, camera_position, camera_direction, camera_up, fov_radians: float, width: int,
                  height: int, *, max_distance: float = 1000.0):
         warnings.warn(DEPRECATION_MESSAGE, DeprecationWarning, stacklevel=2)
-        if len(getattr(model, "shape_body", ()) or ()) > 0:
-            raise NotImplementedError("shape raycasts need the collision geometry pipeline, which this package "
-                                      "does not provide; only particles are raycast")
+        if int(getattr(model, "shape_count", 0) or 0) > 0:
+            raise NotImplementedError("the sensor raycasts particles only: shape raycasts (the model has "
+                                      f"{model.shape_count} shapes) are not provided by this package")
         self.model = model
         self.device = model.device
         self.width = int(width)

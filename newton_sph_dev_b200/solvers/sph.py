@@ -699,10 +699,18 @@ class SolverSPH(SolverBase):
                    "SolverSPH.adjoint_phase_times")
         return tuple(float(v) for v in ms)
 
+    def set_surrogate_wait_limit(self, polls: int = -1) -> None:
+        """Polls of each tensor-core completion wait of the surrogate step (-1:
+        the library default). 0 makes the waits give up at once, which
+        exercises the timeout path (uncorrected integration, status bit)."""
+        self.enable_surrogate()
+        _lib.check(self._lib.nsph_sph_set_surrogate_wait_limit(self._handle, int(polls)),
+                   "SolverSPH.set_surrogate_wait_limit")
+
     def surrogate_phase_times(self) -> tuple[float, float, float, float]:
-        """(build, density, feature pass, MLP + integrate) milliseconds of the
-        last executed surrogate step; waits for it. Needs
-        :meth:`enable_phase_timing`."""
+        """(build, density, fused features + MLP + integrate, compression
+        reduction) milliseconds of the last executed surrogate step; waits for
+        it. Needs :meth:`enable_phase_timing`."""
         ms = (ctypes.c_float * 4)()
         _lib.check(self._lib.nsph_sph_surrogate_phase_times(self._handle, ctypes.byref(ms)),
                    "SolverSPH.surrogate_phase_times")

@@ -361,7 +361,9 @@ class FallbackMonitor:
 class SurrogateSPH:
     """Advance a SolverSPH model by substeps x dt per call: one surrogate step
     of dt_big = substeps x dt, or substeps plain steps while the surrogate is
-    suspended by the fallback rule (see the module docstring)."""
+    suspended by the fallback rule (see the module docstring). A window in
+    which a tensor-core wait gave up (NSPH_STATUS_SURROGATE_TIMEOUT) counts as
+    failed, like one above the threshold."""
 
     def __init__(self, solver: SolverSPH, model: SurrogateModel, substeps: int = 4, threshold: float = 0.01,
                  window: int = 10, cooldown: int = 1, graphs: bool = False):
@@ -378,6 +380,7 @@ class SurrogateSPH:
         self.calls = 0
         self.surrogate_steps = 0
         self.fallback_calls = 0
+        self.timeouts = 0
         self.window_worst: list[float] = []
         self._window_mode = True
         self.acc_scale = accel_scale(solver.config)
@@ -433,6 +436,12 @@ class SurrogateSPH:
     def _end_window(self) -> None:
         if self._window_mode:
             worst = float(self.stats[1].item())
+            # a tensor-core wait that gave up integrated part of a step
+            # without the correction: count the window as failed
+            if self.solver.status() & _lib.NSPH_STATUS_SURROGATE_TIMEOUT:
+                self.timeouts += 1
+                self.solver.reset_status()
+                worst = float("nan")
             self.window_worst.append(worst)
             self.monitor.end_window(worst)
             self.stats[1:3].zero_()

@@ -224,3 +224,68 @@ def test_stepper_fallback_runs_plain_substeps():
     st.step(s1, s0, dt)
     st.step(s0, s1, dt)  # window 3: surrogate again (cooldown over)
     assert st.surrogate_steps == 3 and st.fallback_calls == 2
+
+
+def test_fallback_trips_on_corrupted_weights():
+    """Weights corrupted on the host (an output offset that drives every
+    particle down at about 500 g) compress the block against the floor: the
+    real 1% threshold trips the monitor, and the next window runs plain
+    substeps."""
+    from newton_sph_dev_b200.solvers.sph_surrogate import OUT_MEAN, SurrogateModel, SurrogateSPH, accel_scale
+
+    from newton_sph_dev_b200.solvers import SolverSPH
+
+    model, cfg, x, v, flags = _scene(seed=10)
+    solver = SolverSPH(model, cfg)
+    m = SurrogateModel(DEV, seed=0)
+    m.zero_correction()
+    m.buf[OUT_MEAN + 2] = -500.0 * 9.81 / accel_scale(cfg)  # the injected fault
+    st = SurrogateSPH(solver, m, substeps=4, threshold=0.01, window=4, cooldown=1)
+    s0, s1 = model.state(), model.state()
+    dt = 1e-4
+    for _ in range(4):
+        st.step(s0, s1, dt)
+        s0, s1 = s1, s0
+    assert st.monitor.trips == 1 and st.window_worst[-1] > 0.01
+    st.step(s0, s1, dt)
+    assert st.fallback_calls == 1
+
+
+def test_surrogate_wait_timeout_falls_back():
+    """MMA-completion waits that give up at once (wait limit 0): the step
+    integrates without the correction (the plain step at this dt, bit for
+    bit), sets NSPH_STATUS_SURROGATE_TIMEOUT, and the stepper counts the
+    window as failed and falls back."""
+    from newton_sph_dev_b200.solvers.sph_surrogate import SurrogateSPH
+
+    from newton_sph_dev_b200.solvers import SolverSPH
+
+    model, cfg, x, v, flags = _scene(seed=11)
+    solver = SolverSPH(model, cfg)
+    m = random_model(5)
+    solver.set_surrogate_wait_limit(0)
+    dt = 1e-4
+    p = solver.step_params(4 * dt)
+    stats = torch.zeros(4, device=DEV)
+    xs, vs = torch.empty_like(model.particle_q), model.particle_qd.clone()
+    solver.step_surrogate_raw(model.particle_q, model.particle_qd, xs, vs, p, m, 1.0, stats)
+    xp, vp = torch.empty_like(model.particle_q), model.particle_qd.clone()
+    solver.step_raw(model.particle_q, model.particle_qd, xp, vp, p)
+    torch.cuda.synchronize()
+    assert solver.status() & 8  # NSPH_STATUS_SURROGATE_TIMEOUT
+    assert torch.equal(xs, xp) and torch.equal(vs, vp)
+    solver.reset_status()
+    st = SurrogateSPH(solver, m, substeps=4, threshold=0.01, window=2, cooldown=1)
+    s0, s1 = model.state(), model.state()
+    for _ in range(2):
+        st.step(s0, s1, dt)
+        s0, s1 = s1, s0
+    assert st.timeouts == 1 and st.monitor.trips == 1
+    st.step(s0, s1, dt)
+    assert st.fallback_calls == 1
+    solver.set_surrogate_wait_limit(-1)  # the default again: the corrected step runs
+    solver.reset_status()
+    solver.step_surrogate_raw(model.particle_q, model.particle_qd, xs, vs, p, m, 1.0, stats)
+    torch.cuda.synchronize()
+    assert solver.status() == 0
+    assert not torch.equal(xs, xp)
