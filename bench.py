@@ -64,6 +64,13 @@ WORKLOADS = {
                               desc="learned surrogate on the 1,048,576-particle tank: one step of 4 x 5e-5 s with "
                                    "the MLP acceleration correction (tcgen05) per call, plain steps as fallback when "
                                    "the window's mean compression error exceeds 1%"),
+    "tank_1m_surrogate_8x": dict(shape=(128, 128, 64), spacing=0.005, box=(2.0, 1.0, 1.0), dt=5e-5, vel_std=0.01,
+                                 surrogate=dict(substeps=8, threshold=0.01, window=10,
+                                                weights="surrogate_weights_8x.npz"),
+                                 metric="effective particle-steps/s",
+                                 desc="learned surrogate on the 1,048,576-particle tank at dt = 4e-4 s: one step of "
+                                      "8 x 5e-5 s (dt c0 / h = 0.8) with the MLP correction per call, plain steps "
+                                      "as fallback when the window's compression error exceeds 1%"),
     "contact_1m": dict(shape=(128, 128, 64), spacing=0.0095, radius=0.005, vel_std=0.1, contact=True,
                        metric="particle-steps/s",
                        desc="particle-particle contact (eval_particle_contact): 1,048,576 spheres of radius 0.005 m "
@@ -678,6 +685,13 @@ def run_gpu(args):
     fp32 = measure_fp32_peak(device)
     roof_issue = issue_roofline(kname, t_launch, n, fp32)
 
+    # the learned surrogate beside the plain step, from the timed state (the
+    # three arms of surrogate_eval; not part of the headline value)
+    surrogate = None
+    if not isinstance(cfg, list) and args.surrogate_calls > 0:
+        surrogate = surrogate_eval(solver, model, 4, dt, args.surrogate_calls, timed_state.particle_q.clone(),
+                                   timed_state.particle_qd.clone(), device)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         model_cpu, cfg_cpu, w_cpu = make_scene(args.workload, "cpu")
@@ -721,6 +735,7 @@ def run_gpu(args):
             "roofline": roofline,
             "roofline_step": roofline_step,
             "roofline_issue": roof_issue,
+            "surrogate": surrogate,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes, "steps": e2e_steps,
@@ -997,8 +1012,9 @@ def run_grad_reference(args):
 # algorithmic bytes per particle: feature pass (read x, v, m/rho p/rho^2, rho p;
 # write 16 features, a, dv) and MLP + integrate (read them back with x, v,
 # rho p and the sort permutation; write x, v)
-B_ALG_FEATURES = 16 + 16 + 8 + 8 + 64 + 32
-B_ALG_MLP = 64 + 32 + 16 + 16 + 8 + 4 + 24
+# algorithmic bytes per particle of the fused surrogate kernel: read x, v (sorted mirrors, 32), the density
+# scratch (16), the neighbour-list count (4); write x, v (24)
+B_ALG_FUSED = 32 + 16 + 4 + 24
 MLP_FLOPS = 2 * (16 * 64 + 64 * 64 + 64 * 16)  # per particle, as issued (layer 3 padded to N = 16)
 
 
@@ -1012,7 +1028,110 @@ def load_tensor_peak():
     return 1590.0, "fallback"
 
 
+def surrogate_eval(solver, model, sub: int, dt: float, calls: int, start_q, start_qd, device, net=None,
+                   threshold: float = 0.01, window: int = 10, phase_timing: bool = True) -> dict:
+    """Three arms from the same state, each over the same span of simulated
+    time (calls x sub x dt), each call replayed from a CUDA graph with L2
+    flushed before it:
+
+    - surrogate: SurrogateSPH (one corrected step of sub x dt per call, plain
+      fallback under the compression rule);
+    - uncorrected: the same large step with a zero network (the plain WCSPH
+      step at sub x dt), no fallback;
+    - plain: sub x calls plain steps of dt.
+
+    Rates are particles x plain-dt steps of simulated time per second."""
+    import torch
+
+    from newton_sph_dev_b200.solvers.sph_surrogate import SurrogateModel, SurrogateSPH
+
+    n = model.particle_count
+    stream = torch.cuda.current_stream(device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {"calls": calls, "substeps": sub, "dt_plain": dt, "dt_large": sub * dt}
+
+    def arm(network, thr):
+        a, b = model.state(), model.state()
+        a.particle_q.copy_(start_q)
+        a.particle_qd.copy_(start_qd)
+        st = SurrogateSPH(solver, network, substeps=sub, threshold=thr, window=window, graphs=True)
+        # capture both ping-pong directions with two untimed calls, then start over
+        st.step(a, b, dt)
+        st.step(b, a, dt)
+        a.particle_q.copy_(start_q)
+        a.particle_qd.copy_(start_qd)
+        st.stats.zero_()
+        st.calls = 0
+        st.surrogate_steps = st.fallback_calls = st.timeouts = 0
+        st.window_worst = []
+        st.monitor.suspended = st.monitor.trips = 0
+        ms = fused_ms = 0.0
+        cur, nxt = a, b
+        torch.cuda.synchronize()
+        for _ in range(calls):
+            flush.zero_()
+            before = st.surrogate_steps
+            e0.record(stream)
+            st.step(cur, nxt, dt)
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+            if phase_timing and st.surrogate_steps > before:
+                fused_ms += solver.surrogate_phase_times()[2]
+            cur, nxt = nxt, cur
+        s = st.stats.cpu()
+        finite = bool(torch.isfinite(cur.particle_q).all() and torch.isfinite(cur.particle_qd).all())
+        res = {"value": n * sub * calls / (ms * 1e-3), "ms_per_call": ms / calls,
+               "mean_compression": float(s[3]) / max(1, st.surrogate_steps),
+               "max_window_compression": float(max(st.window_worst or [0.0])),
+               "surrogate_steps": st.surrogate_steps, "fallback_calls": st.fallback_calls,
+               "timeouts": st.timeouts, "finite": finite,
+               "fused_kernel_ms": fused_ms / max(1, st.surrogate_steps) if phase_timing else None,
+               "launches_per_call": st.launches_per_step}
+        st._graphs.clear()
+        return res
+
+    net = net if net is not None else SurrogateModel.pretrained(device)
+    out["surrogate"] = arm(net, threshold)
+    zero = SurrogateModel(device)
+    zero.zero_correction()
+    out["uncorrected"] = arm(zero, float("inf"))
+
+    # plain: sub x calls steps of dt from the same state
+    p0, p1 = model.state(), model.state()
+    for t in (p0, p1):
+        t.particle_q.copy_(start_q)
+        t.particle_qd.copy_(start_qd)
+    solver.step(p0, p1, None, None, dt)
+    ga, gb = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+    with torch.cuda.graph(ga):
+        solver.step(p0, p1, None, None, dt)
+    with torch.cuda.graph(gb):
+        solver.step(p1, p0, None, None, dt)
+    p0.particle_q.copy_(start_q)
+    p0.particle_qd.copy_(start_qd)
+    plain_ms = 0.0
+    torch.cuda.synchronize()
+    for i in range(sub * calls):
+        flush.zero_()
+        e0.record(stream)
+        (ga if i % 2 == 0 else gb).replay()
+        e1.record(stream)
+        e1.synchronize()
+        plain_ms += e0.elapsed_time(e1)
+    del ga, gb
+    out["plain"] = {"value": n * sub * calls / (plain_ms * 1e-3), "ms_per_step": plain_ms / (sub * calls)}
+    out["speedup_vs_plain"] = out["surrogate"]["value"] / out["plain"]["value"]
+    out["speedup_vs_uncorrected"] = out["surrogate"]["value"] / out["uncorrected"]["value"]
+    out["compression_definition"] = "mean over active particles of max(0, rho/rho0 - 1) at each large step's input"
+    return out
+
+
 def run_surrogate(args):
+    """The learned surrogate on the tank: the three arms of surrogate_eval
+    (surrogate, uncorrected large step, plain steps) over args.steps calls
+    from the relaxed state; the headline value is the surrogate's."""
     import torch
     import torch.distributed as dist
 
@@ -1034,103 +1153,57 @@ def run_surrogate(args):
     s0, s1 = model.state(), model.state()
     tuned = solver.autotune(s0, s1, dt) if not args.no_autotune else None
     solver.enable_phase_timing(True)
-    net = SurrogateModel.pretrained(device)
-    stepper = SurrogateSPH(solver, net, substeps=sub, threshold=sw["threshold"], window=sw["window"], graphs=True)
-    stream = torch.cuda.current_stream(device)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-
-    # surrogate run: warm-up calls (graph capture of both directions), then timed calls
-    for i in range(max(args.warmup, 3)):
-        stepper.step(s0, s1, dt) if i % 2 == 0 else stepper.step(s1, s0, dt)
-    cur, nxt = (s1, s0) if max(args.warmup, 3) % 2 == 1 else (s0, s1)
-    start_q, start_qd = cur.particle_q.clone(), cur.particle_qd.clone()
-    stepper.stats.zero_()
-    sur0, fb0 = stepper.surrogate_steps, stepper.fallback_calls
-    total_ms = 0.0
-    feat_ms = mlp_ms = 0.0
-    timed_sur = 0
-    barrier(device)
+    # relaxation with plain steps, then every arm starts from that state
+    relax = max(args.warmup, 3) + args.relax
+    relax += relax % 2
+    for i in range(relax):
+        solver.step(s0, s1, None, None, dt) if i % 2 == 0 else solver.step(s1, s0, None, None, dt)
     torch.cuda.synchronize()
+    start_q, start_qd = s0.particle_q.clone(), s0.particle_qd.clone()
+    weights = args.weights or sw.get("weights")
+    if weights:
+        path = Path(weights)
+        if not path.is_absolute() and not path.exists():
+            path = REPO / "newton_sph_dev_b200" / weights
+        net = SurrogateModel.load(path, device)
+    else:
+        net = SurrogateModel.pretrained(device)
+    barrier(device)
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
-            flush.zero_()
-            before = stepper.surrogate_steps
-            e0.record(stream)
-            stepper.step(cur, nxt, dt)
-            e1.record(stream)
-            e1.synchronize()
-            total_ms += e0.elapsed_time(e1)
-            if stepper.surrogate_steps > before:
-                ph = solver.surrogate_phase_times()
-                feat_ms += ph[2]
-                mlp_ms += ph[3]
-                timed_sur += 1
-            cur, nxt = nxt, cur
-    torch.cuda.synchronize()
-
-    # the plain step over the same span of simulated time from the same
-    # state (sub x steps plain steps, graph-replayed, L2 flushed before each)
-    p0, p1 = model.state(), model.state()
-    p0.particle_q.copy_(start_q)
-    p0.particle_qd.copy_(start_qd)
-    p1.particle_q.copy_(start_q)
-    p1.particle_qd.copy_(start_qd)
-    solver.step(p0, p1, None, None, dt)  # warm-up of the plain path; p1 is scratch
-    ga, gb = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
-    with torch.cuda.graph(ga):
-        solver.step(p0, p1, None, None, dt)
-    with torch.cuda.graph(gb):
-        solver.step(p1, p0, None, None, dt)
-    plain_steps = sub * args.steps
-    plain_ms = 0.0
-    for i in range(plain_steps):
-        flush.zero_()
-        e0.record(stream)
-        (ga if i % 2 == 0 else gb).replay()
-        e1.record(stream)
-        e1.synchronize()
-        plain_ms += e0.elapsed_time(e1)
-    del ga, gb
-    plain_value = n * plain_steps / (plain_ms * 1e-3)
-    barrier(device)
-    total_ms = max_over_ranks(total_ms, device)
+        ev = surrogate_eval(solver, model, sub, dt, args.steps, start_q, start_qd, device, net=net,
+                            threshold=sw["threshold"], window=sw["window"])
+    sur = ev["surrogate"]
+    total_ms = max_over_ranks(sur["ms_per_call"] * args.steps, device)
     value = world * n * sub * args.steps / (total_ms * 1e-3)
-    st = stepper.stats.cpu()
-    n_sur = stepper.surrogate_steps - sur0
-    mean_comp = float(st[3]) / max(1, n_sur)
-    fallbacks = stepper.fallback_calls - fb0
     status = solver.status()
-    finite = bool(torch.isfinite(cur.particle_q).all() and torch.isfinite(cur.particle_qd).all())
 
     # end to end through the public API: host state in, one call, host state
-    # out, every call (pipelined over independent calls, as for tank_1m). The
-    # calls all start from the timed run's first state, with the fallback
-    # rule reset: repeating one state repeats its compression, so a state
-    # whose surrogate step trips the rule would make every other window plain
+    # out, every call (pipelined over independent calls, as for tank_1m), all
+    # from the relaxed state with the fallback rule reset
     e2e_steps = min(args.steps, 50)
     hx, hv = start_q.cpu().pin_memory(), start_qd.cpu().pin_memory()
+    stepper = SurrogateSPH(solver, net, substeps=sub, threshold=sw["threshold"], window=sw["window"], graphs=True)
     stepper.monitor = FallbackMonitor(sw["threshold"])
-    stepper.calls = 0
-    fb_e2e0 = stepper.fallback_calls
     e2e_ms = pipelined_e2e(model, lambda a, b: stepper.step(a, b, dt), hx, hv, e2e_steps, device)
     e2e_ms = max_over_ranks(e2e_ms, device)
     e2e_value = world * n * sub * e2e_steps / (e2e_ms * 1e-3)
-    e2e_fallbacks = stepper.fallback_calls - fb_e2e0
+    e2e_fallbacks = stepper.fallback_calls
+    stepper._graphs.clear()
 
     peak, peak_kind = load_peak()
     tpeak, tpeak_kind = load_tensor_peak()
-    t_feat = feat_ms / max(1, timed_sur) * 1e-3
-    t_mlp = mlp_ms / max(1, timed_sur) * 1e-3
-    ach = B_ALG_FEATURES * n / t_feat / 1e9 if t_feat > 0 else None
-    roofline = {"bound": "hbm", "kernel": "k_force_features", "achieved": ach, "peak": peak, "peak_kind": peak_kind,
-                "unit": "GB/s", "frac": ach / peak if ach else None, "traffic": None,
-                "alg_bytes_per_launch": B_ALG_FEATURES * n, "ms_per_launch": t_feat * 1e3}
-    tflops = MLP_FLOPS * n / t_mlp / 1e12 if t_mlp > 0 else None
-    roofline_mlp = {"bound": "tensor", "kernel": "k_surrogate (MLP + integrate)", "achieved": tflops, "peak": tpeak,
-                    "peak_kind": tpeak_kind, "unit": "TFLOP/s", "frac": tflops / tpeak if tflops else None,
-                    "flops_per_particle": MLP_FLOPS, "ms_per_launch": t_mlp * 1e3,
-                    "hbm_achieved_gbs": B_ALG_MLP * n / t_mlp / 1e9 if t_mlp > 0 else None}
+    t_fused = (sur["fused_kernel_ms"] or 0.0) * 1e-3
+    ach = B_ALG_FUSED * n / t_fused / 1e9 if t_fused > 0 else None
+    roofline = {"bound": "hbm", "kernel": "k_surrogate_fused (features + MLP + integrate)", "achieved": ach,
+                "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": ach / peak if ach else None,
+                "traffic": load_traffic("k_surrogate_fused"), "alg_bytes_per_launch": B_ALG_FUSED * n,
+                "ms_per_launch": t_fused * 1e3}
+    tflops = MLP_FLOPS * n / t_fused / 1e12 if t_fused > 0 else None
+    roofline_mlp = {"bound": "tensor", "kernel": "k_surrogate_fused (its MLP share)", "achieved": tflops,
+                    "peak": tpeak, "peak_kind": tpeak_kind, "unit": "TFLOP/s",
+                    "frac": tflops / tpeak if tflops else None, "flops_per_particle": MLP_FLOPS,
+                    "note": "MLP flops as issued over the fused kernel's whole duration (the neighbour gather "
+                            "dominates it)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1140,7 +1213,6 @@ def run_surrogate(args):
                "sample": f"{steps_done} plain fp32 oracle steps (dt = {dt} s) of the full {n}-particle scene in "
                          f"{el:.1f} s (OpenMP); the CPU has no surrogate, one plain step is one dt of simulated time"}
     if rank == 0:
-        clocks = clk.summary()
         line = {
             "metric": w["metric"],
             "value": value,
@@ -1159,35 +1231,31 @@ def run_surrogate(args):
                 "step": f"one bench step = one call advancing {sub} x {dt} s of simulated time; value counts "
                         f"particles x plain-dt steps of simulated time",
                 "substeps": sub, "dt_plain": dt, "dt_surrogate": sub * dt, "fallback_threshold": sw["threshold"],
-                "window": sw["window"], "graph": True,
+                "window": sw["window"], "graph": True, "relaxation_steps": relax,
                 "launch": {"threads": solver.launch[0], "blocks_per_sm": solver.launch[1],
                            "autotuned": tuned is not None} if hasattr(solver, "launch") else "default",
-                "l2": "flushed (256 MiB write) before every timed step, outside the timed interval",
+                "l2": "flushed (256 MiB write) before every timed call, outside the timed interval",
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             },
-            "plain": {"value": plain_value, "unit": "particle-steps/s", "steps": plain_steps,
-                      "ms_per_step": plain_ms / plain_steps,
-                      "span": "the same simulated time as the timed surrogate calls, from the same state"},
-            "speedup_vs_plain": value / plain_value,
-            "compression_error": {"mean": mean_comp, "max_window": float(max(stepper.window_worst or [0.0])),
-                                  "definition": "mean over active particles of max(0, rho/rho0 - 1), per surrogate "
-                                                "step, averaged over the timed surrogate steps"},
-            "surrogate_steps": n_sur, "fallback_calls": fallbacks,
-            "phase_ms_per_surrogate_step": {"feature_pass": t_feat * 1e3, "mlp_integrate": t_mlp * 1e3},
+            "arms": ev,
+            "speedup_vs_plain": ev["speedup_vs_plain"],
+            "speedup_vs_uncorrected": ev["speedup_vs_uncorrected"],
+            "compression_error": {"mean": sur["mean_compression"], "max_window": sur["max_window_compression"],
+                                  "definition": ev["compression_definition"]},
             "roofline": roofline,
             "roofline_mlp": roofline_mlp,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": w["metric"], "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n,
                     "steps": e2e_steps, "how": "pinned upload, one SurrogateSPH.step call, download, every call; "
                                               "independent calls pipelined on upload / compute / download streams",
-                    "state": "the timed run's first state, fallback rule reset", "fallback_calls": e2e_fallbacks},
-            "gpu_launches": stepper.launches_per_step * n_sur + fallbacks * sub * solver.last_launches,
-            "clocks": clocks,
+                    "state": "the relaxed state, fallback rule reset", "fallback_calls": e2e_fallbacks},
+            "gpu_launches": sur["launches_per_call"] * sur["surrogate_steps"]
+            + sur["fallback_calls"] * sub * solver.last_launches,
+            "clocks": clk.summary(),
             "status": status,
-            "finite": finite,
+            "finite": sur["finite"],
         }
         print(json.dumps(line), flush=True)
-    stepper._graphs.clear()
     if world > 1:
         dist.destroy_process_group()
     return 0
@@ -1554,6 +1622,9 @@ def main(argv=None):
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=[k for k in WORKLOADS if not k.startswith("_")], default="tank_1m")
     ap.add_argument("--no-graph", action="store_true", help="time eager steps instead of graph replays")
+    ap.add_argument("--weights", default=None, help="surrogate weights (.npz) for the surrogate workloads")
+    ap.add_argument("--surrogate-calls", type=int, default=100,
+                    help="calls of the surrogate / uncorrected / plain comparison added to the plain step's line")
     ap.add_argument("--relax", type=int, default=200,
                     help="untimed steps after the warm-up, so the timed steps run on a settled state")
     ap.add_argument("--no-cpu-baseline", action="store_true")
