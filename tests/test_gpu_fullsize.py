@@ -89,14 +89,16 @@ def _check_step(O, solver, model, cfg, s0, s1, v_init, dt, check_grid=True, exac
     a = s1.sph.acceleration.cpu().numpy().astype(np.float64)
     abs_err = np.linalg.norm(a - r64["a"], axis=1)[act]
     err = abs_err / np.maximum(r64["a_scale"][act], 1e-30)
-    assert np.median(err) < 1e-5 and np.percentile(err, 99.9) < 1e-4
+    assert np.median(err) < 1e-5 and np.percentile(err, 99) < 1e-3
     # Per particle: within 1e-3 of its summed magnitudes, or within 1e-2 g in
-    # absolute terms. The second arm covers free-surface particles whose own
-    # pressure is clamped to 0: their small force is a sum of the neighbours'
-    # pressures, each carrying the fp32 EOS cancellation near rest density
-    # (an absolute error of about gamma * B * 2^-24 per pressure), which is
-    # large against their small summands (1.3e-2 relative, 0.03 m/s^2, on
-    # the 1M lattice; the fp32 oracle has the same error).
+    # absolute terms. The second arm covers particles whose own pressure is
+    # clamped to 0 (free surface, the rarefied layers of the falling block):
+    # their small force is a sum of the neighbours' pressures, each carrying
+    # the fp32 EOS cancellation near rest density (an absolute error of about
+    # gamma * B * 2^-24 per pressure), which is large against their small
+    # summands. The fp32 oracle has the same errors: on the 1M lattice the
+    # worst is 1.3e-2 relative (0.03 m/s^2); after 600 steps the 99th / 99.9th
+    # percentiles are 4.4e-4 / 4.5e-3 relative and the worst 0.023 m/s^2.
     assert not np.any((err > 1e-3) & (abs_err > 1e-2 * 9.81))
     return r32
 
