@@ -212,6 +212,10 @@ struct Grid {
     unsigned int* hist = nullptr;  // kRadix * ntiles(capacity)
     // cell table (ncells entries of {start, end})
     int2* cell_ranges = nullptr;
+    // counting build (single world, at most kCountMaxCells cells): per-cell
+    // counts (all zero between builds) and per-tile sums of the cell scan
+    int* cell_count = nullptr;
+    int* tile_sums = nullptr;
 
     GridDev view() const { return GridDev{dx, dy, dz, cell_inv, cell_ranges, point_ids}; }
 };

@@ -143,3 +143,25 @@ def test_model_grid_is_128_cubed():
     model.particle_grid.build(model.particle_q, 0.2)
     ids = model.particle_grid.point_ids.cpu().numpy()
     assert sorted(ids.tolist()) == list(range(model.particle_count))
+
+
+def test_counting_and_radix_builds_alternate(oracle_mod):
+    """Single-world grids build by cell counts when the table holds at most 16
+    cells per point, else by the radix sort. Builds that alternate between
+    the two on one grid, and repeated counting builds (whose per-cell counts
+    must return to zero), all match the oracle."""
+    from newton_sph_dev_b200 import HashGrid
+
+    dims = (64, 64, 64)  # 262,144 cells
+    grid = HashGrid(*dims, device=DEV)
+    for n, seed in ((20000, 1), (25000, 2), (10000, 3), (30000, 4), (5000, 5), (20000, 6)):
+        pts = _points(n, seed)
+        grid.build(torch.from_numpy(pts).to(DEV), 0.02)
+        torch.cuda.synchronize()
+        got = _grid_arrays(grid)
+        ref = oracle_mod.grid_build(pts, 0.02, dims)
+        for k in ref:
+            np.testing.assert_array_equal(got[k], ref[k], err_msg=f"n={n}: {k}")
+        counting = dims[0] * dims[1] * dims[2] <= 16 * n
+        launches = grid.last_launches() if callable(grid.last_launches) else grid.last_launches
+        assert (launches == 6) == counting, (n, launches)
