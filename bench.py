@@ -76,6 +76,12 @@ WORKLOADS = {
                        desc="particle-particle contact (eval_particle_contact): 1,048,576 spheres of radius 0.005 m "
                             "on a jittered 0.0095 m lattice (touching neighbours), v ~ N(0, 0.1 m/s); one step = "
                             "HashGrid build at 2 r_max + cohesion + contact forces"),
+    "xpbd_1m": dict(shape=(128, 128, 64), spacing=0.0095, radius=0.005, vel_std=0.1, xpbd=dict(iterations=4, dt=1e-3),
+                    metric="particle-steps/s",
+                    desc="XPBD particle step (SolverXPBD): 1,048,576 spheres of radius 0.005 m on a jittered 0.0095 m "
+                         "lattice resting on a ground plane, v ~ N(0, 0.1 m/s), gravity; one step = Model.collide "
+                         "(soft contacts with the plane) + integrate + HashGrid build at 2 r_max + 4 iterations of "
+                         "shape and particle corrections and apply_particle_deltas, dt = 1e-3 s"),
     "raycast_1m": dict(shape=(128, 128, 64), spacing=0.0095, radius=0.005, vel_std=0.0,
                        raycast=dict(width=640, height=480, fov=1.0, position=(2.2, -1.0, 1.6), target=(0.6, 0.6, 0.3),
                                     max_distance=4.0),
@@ -1425,6 +1431,156 @@ def run_contact(args):
     return 0
 
 
+def make_xpbd_scene(w, device):
+    import newton_sph_dev_b200 as nsph
+    import torch
+
+    s = w["spacing"]
+    b = nsph.ModelBuilder()
+    b.add_particle_grid(pos=(s / 2, s / 2, w["radius"]), rot=(0, 0, 0, 1), vel=(0, 0, 0), dim_x=w["shape"][0],
+                        dim_y=w["shape"][1], dim_z=w["shape"][2], cell_x=s, cell_y=s, cell_z=s, mass=1.0,
+                        jitter=0.2 * s, radius_mean=w["radius"])
+    b.add_ground_plane()
+    model = b.finalize(device)
+    rng = np.random.default_rng(seed=2)
+    model.particle_qd.copy_(torch.from_numpy(rng.normal(0.0, w["vel_std"], (model.particle_count, 3))
+                                             .astype(np.float32)))
+    model.particle_cohesion = 0.0
+    return model
+
+
+def run_xpbd(args):
+    """SolverXPBD on the sphere pile: Model.collide + step per bench step,
+    replayed from a CUDA graph per ping-pong direction."""
+    import torch
+
+    from newton_sph_dev_b200.solvers import SolverXPBD
+
+    world, rank, local = dist_env()
+    if world > 1:
+        raise SystemExit("xpbd_1m runs on one GPU (replicas are not wired for it)")
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    w = WORKLOADS[args.workload]
+    model = make_xpbd_scene(w, str(device))
+    n = model.particle_count
+    it, dt = w["xpbd"]["iterations"], w["xpbd"]["dt"]
+    solver = SolverXPBD(model, iterations=it)
+    s0, s1 = model.state(), model.state()
+    contacts = model.contacts()
+    stream = torch.cuda.current_stream(device)
+
+    def step(a, b):
+        model.collide(a, contacts)
+        solver.step(a, b, None, contacts, dt)
+
+    for i in range(max(args.warmup, 3) + args.relax // 10):
+        step(s0, s1) if i % 2 == 0 else step(s1, s0)
+    ga, gb = torch.cuda.CUDAGraph(), torch.cuda.CUDAGraph()
+    with torch.cuda.graph(ga):
+        step(s0, s1)
+    with torch.cuda.graph(gb):
+        step(s1, s0)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    total = 0.0
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            e0.record(stream)
+            (ga if i % 2 == 0 else gb).replay()
+            e1.record(stream)
+            e1.synchronize()
+            total += e0.elapsed_time(e1)
+    del ga, gb
+    value = n * args.steps / (total * 1e-3)
+    last = s1 if args.steps % 2 == 1 else s0
+    finite = bool(torch.isfinite(last.particle_q).all())
+    ncont = int(contacts.soft_contact_count.item())
+    # end to end: host state in, one step, host state out, every step
+    hx, hv = last.particle_q.cpu().pin_memory(), last.particle_qd.cpu().pin_memory()
+    e2e_steps = min(args.steps, 50)
+    e2e = pipelined_e2e(model, step, hx, hv, e2e_steps, device)
+    cpu = None
+    if not args.no_cpu_baseline:
+        rate, reps, el, threads = xpbd_oracle_rate(model, w, last.particle_q.cpu().numpy(),
+                                                   last.particle_qd.cpu().numpy(), budget_s=10.0)
+        cpu = {"value": rate, "unit": METRIC, "cores": threads, "kind": "port",
+               "sample": f"{reps} full steps of the {n}-particle scene in {el:.1f} s (the oracle's restatement of "
+                         "SolverXPBD.step: soft contacts, integrate, grid, iterations; OpenMP)"}
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "particles": n, "desc": w["desc"], "iterations": it, "dt": dt,
+                   "grid_dims": [128, 128, 128], "graph": True, "soft_contacts": ncont,
+                   "l2": "flushed (256 MiB write) before every timed step, outside the timed interval"},
+        "cpu_baseline": cpu,
+        "e2e": {"value": n * e2e_steps / (e2e * 1e-3), "unit": METRIC, "h2d_bytes_per_step": 24 * n,
+                "d2h_bytes_per_step": 24 * n, "steps": e2e_steps,
+                "how": "pinned upload of x, v, Model.collide + SolverXPBD.step, download of x, v, every step; "
+                       "independent steps pipelined on upload / compute / download streams"},
+        "gpu_launches": None,
+        "clocks": clk.summary(),
+        "finite": finite,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def xpbd_oracle_rate(model, w, x, v, budget_s: float):
+    """particle-steps/s of the oracle's XPBD step on the host cores."""
+    from oracle import oracle as O
+
+    O.build()
+    md = dict(inv_mass=model.particle_inv_mass.cpu().numpy(), radius=model.particle_radius.cpu().numpy(),
+              flags=model.particle_flags.cpu().numpy(), world=model.particle_world.cpu().numpy(),
+              gravity=model.gravity.cpu().numpy(), v_max=model.particle_max_velocity, particle_mu=model.particle_mu,
+              particle_cohesion=model.particle_cohesion, max_radius=model.particle_max_radius,
+              shapes=[dict(type=sh["type"], flags=sh["flags"], world=sh["world"], pos=sh["pos"], rot=sh["rot"],
+                           scale=sh["scale"], ke=sh["ke"], kd=sh["kd"], kf=sh["kf"], mu=sh["mu"])
+                      for sh in model._shapes],
+              soft=(model.soft_contact_ke, model.soft_contact_kd, model.soft_contact_kf, model.soft_contact_mu,
+                    model.particle_adhesion, model.soft_contact_restitution))
+    it, dt = w["xpbd"]["iterations"], w["xpbd"]["dt"]
+    f = np.zeros_like(x)
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        c = O.soft_contacts_create(md["shapes"], x, md["radius"], md["flags"], world=md["world"], margin=0.01)
+        xi, vi, x, v = O.xpbd_particle_step(md, x, v, f, dt, it, 0.9, contacts=c)
+        reps += 1
+        el = time.perf_counter() - t0
+        if el > budget_s or reps >= 5:
+            break
+    return model.particle_count * reps / el, reps, el, O.get_threads()
+
+
+def run_xpbd_reference(args):
+    """The oracle's restatement of SolverXPBD.step on the same scene, all host
+    threads."""
+    world, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    w = WORKLOADS[args.workload]
+    model = make_xpbd_scene(w, "cpu")
+    n = model.particle_count
+    rate, reps, el, threads = xpbd_oracle_rate(model, w, model.particle_q.numpy().copy(),
+                                               model.particle_qd.numpy().copy(), budget_s=60.0)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": reps, "warmup": 0, "ms_per_step": 1e3 * el / reps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": args.workload, "particles": n, "desc": w["desc"]},
+        "cpu_baseline": {"value": rate, "unit": METRIC, "cores": threads, "kind": "port",
+                         "sample": f"{reps} full steps (oracle restatement of SolverXPBD.step, OpenMP)"},
+        "e2e": {"value": rate, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_contact_reference(args):
     """The fp32 CPU restatement of eval_particle_contact (with its grid
     build) on the same scene, all host threads."""
@@ -1666,6 +1822,8 @@ def main(argv=None):
             return run_raycast_reference(args)
         if "contact" in WORKLOADS[args.workload]:
             return run_contact_reference(args)
+        if "xpbd" in WORKLOADS[args.workload]:
+            return run_xpbd_reference(args)
         return run_grad_reference(args) if grad else run_reference(args)
     if "surrogate" in WORKLOADS[args.workload]:
         return run_surrogate(args)
@@ -1673,6 +1831,8 @@ def main(argv=None):
         return run_raycast(args)
     if "contact" in WORKLOADS[args.workload]:
         return run_contact(args)
+    if "xpbd" in WORKLOADS[args.workload]:
+        return run_xpbd(args)
     return run_grad(args) if grad else run_gpu(args)
 
 
