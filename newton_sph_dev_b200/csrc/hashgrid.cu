@@ -303,9 +303,10 @@ __global__ void k_ranges(const int* __restrict__ cells, int n, int2* __restrict_
 //                 writes the cell table ({start, end}, {0, 0} when empty) and
 //                 turns count into start for the scatter
 //   k_cc_scatter  point -> start + slot (the arbitrary order)
-//   k_cc_rank     point -> start + (points of its cell with a smaller index):
-//                 the stable order; writes point_cells / point_ids, gathers
-//                 the sorted mirrors in SPH mode, and zeroes the cell's count
+//   k_cc_rank     per cell-ordered position: its point goes to start + (points
+//                 of its cell with a smaller index), the stable order; writes
+//                 point_cells / point_ids, gathers the sorted mirrors in SPH
+//                 mode, and zeroes the cell's count
 // The result is identical to the stable radix sort's.
 // --------------------------------------------------------------------------
 constexpr int kCcThreads = 1024;
@@ -412,17 +413,22 @@ __global__ void __launch_bounds__(256) k_cc_scatter(const int* __restrict__ cell
     tmp[start[cells[i]] + slots[i]] = i;
 }
 
+// one thread per position q of the cell-ordered (not yet stable) array: its
+// point i, the rank of i among its cell's points, and the stable position
+// start + rank, which lies in the same cell's range, so neighbouring threads
+// write neighbouring positions
 __global__ void __launch_bounds__(256) k_cc_rank(const int* __restrict__ cells, const int2* __restrict__ ranges,
                                                  const int* __restrict__ tmp, int n, int* __restrict__ count,
                                                  int* __restrict__ point_cells, int* __restrict__ point_ids,
                                                  GatherArgs gather, bool do_gather)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const int i = tmp[q];
     const int c = cells[i];
     const int2 se = ranges[c];
     int rank = 0;
-    for (int q = se.x; q < se.y; ++q) rank += tmp[q] < i;
+    for (int t = se.x; t < se.y; ++t) rank += tmp[t] < i;
     if (rank == 0) count[c] = 0;  // the counts start at zero for the next build
     const int g = se.x + rank;
     point_cells[g] = c;

@@ -249,64 +249,119 @@ __global__ void __launch_bounds__(kSphThreads, 5) k_density(GridDev g, const flo
 // ---- neighbour lists (the plain step) -----------------------------------------
 // The density pass of the plain step first tests every candidate (in query
 // order) and appends the sorted index of each neighbour to the particle's
-// list: slot t at nbr[t * n + k] (slot-major, so that a warp reading slot t
-// of 32 consecutive particles reads one contiguous 128-byte line), for the
-// first kNbrSlots neighbours, and their number in ncnt[k]. The cubic-spline
-// terms are then evaluated by a second loop over the list, in the same
-// order, so every lane of a warp runs the term code only for its own
-// neighbours (evaluated inside the candidate loop, a warp runs it for every
-// candidate slot at which any of its 32 lanes has a hit, which at a ~15% hit
-// rate is nearly all of them). The force pass walks the same list with one
-// uniform loop and no grid traversal. A particle with more than kNbrSlots
-// neighbours (dense clusters) is summed by re-testing its candidates, in the
-// same order. Sums, their order and every rounding are those of the fp32
-// oracle, as with the masks.
+// list, in groups of four: group g (slots 4g .. 4g+3) at nbr[g * n + k] as
+// one int4 (group-major, so that a warp reading group g of 32 consecutive
+// particles reads one contiguous 512-byte span), for the first kNbrSlots
+// neighbours, and their number in ncnt[k]. A thread keeps the last four hits
+// in registers and stores a full group at once (a store per four neighbours
+// instead of one per neighbour). The cubic-spline terms are then evaluated
+// by a second loop over the list, in the same order, so every lane of a warp
+// runs the term code only for its own neighbours (evaluated inside the
+// candidate loop, a warp runs it for every candidate slot at which any of
+// its 32 lanes has a hit, which at a ~15% hit rate is nearly all of them).
+// Readers load a whole group ahead of its use. The force pass walks the same
+// list with one uniform loop and no grid traversal. A particle with more
+// than kNbrSlots neighbours (dense clusters) is summed by re-testing its
+// candidates, in the same order. Sums, their order and every rounding are
+// those of the fp32 oracle, as with the masks.
 constexpr int kNbrSlots = 64;
+constexpr int kNbrGroups = kNbrSlots / 4;
 
 __device__ __forceinline__ int neighbor_list(const GridDev& g, const float4* __restrict__ xs,
-                                             const nsph_sph_params& p, float4 xi, int* __restrict__ nbr, int n,
+                                             const nsph_sph_params& p, float4 xi, int4* __restrict__ nbr, int n,
                                              int k)
 {
     int cnt = 0;
-    auto hit = [&](int j) {
-        if (cnt < kNbrSlots) nbr[(size_t)cnt * n + k] = j;
+    int b0 = 0, b1 = 0, b2 = 0, b3 = 0;
+    auto append = [&](int j) {
+        b0 = b1;
+        b1 = b2;
+        b2 = b3;
+        b3 = j;
         ++cnt;
+        if ((cnt & 3) == 0 && cnt <= kNbrSlots) nbr[(size_t)((cnt >> 2) - 1) * n + k] = make_int4(b0, b1, b2, b3);
     };
+    // Candidates are tested branch-free into a bit mask per chunk of up to 32
+    // of a run; the hits are appended after the chunk, so the append code runs
+    // once per neighbour (a warp iterates over its lanes' largest hit count of
+    // the chunk) instead of at every candidate where any lane has a hit.
     for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
-        int j = lo;
-        for (; j + 4 <= hi; j += 4) {
-            float4 xj[4];
+        for (int c0 = lo; c0 < hi; c0 += 32) {
+            const int m = min(32, hi - c0);
+            unsigned bits = 0u;
+            int j = 0;
+            for (; j + 4 <= m; j += 4) {
+                float4 xj[4];
 #pragma unroll
-            for (int u = 0; u < 4; ++u) xj[u] = __ldg(xs + j + u);
+                for (int u = 0; u < 4; ++u) xj[u] = __ldg(xs + c0 + j + u);
 #pragma unroll
-            for (int u = 0; u < 4; ++u) {
+                for (int u = 0; u < 4; ++u) {
+                    float dx, dy, dz;
+                    bits |= (unsigned)(dist2(xi, xj[u], dx, dy, dz) < p.h2) << (j + u);
+                }
+            }
+            for (; j < m; ++j) {
                 float dx, dy, dz;
-                if (dist2(xi, xj[u], dx, dy, dz) < p.h2) hit(j + u);
+                bits |= (unsigned)(dist2(xi, __ldg(xs + c0 + j), dx, dy, dz) < p.h2) << j;
+            }
+            while (bits) {
+                append(c0 + __ffs(bits) - 1);
+                bits &= bits - 1u;
             }
         }
-        for (; j < hi; ++j) {
-            float dx, dy, dz;
-            if (dist2(xi, __ldg(xs + j), dx, dy, dz) < p.h2) hit(j);
-        }
     });
+    const int r = cnt & 3;  // the last, partial group: its r hits are b(4-r) .. b3
+    if (r && cnt <= kNbrSlots)
+        nbr[(size_t)(cnt >> 2) * n + k] = r == 1 ? make_int4(b3, 0, 0, 0)
+                                                 : (r == 2 ? make_int4(b2, b3, 0, 0) : make_int4(b1, b2, b3, 0));
     return cnt;
 }
+
+// Sequential reader of a particle's list: get(t) for t = 0, 1, ... in order.
+// The group after the current one is loaded when the current one starts.
+// kReadOnly: the list was written by an earlier kernel (read-only path);
+// otherwise it is read back by the thread that wrote it (plain loads).
+template <bool kReadOnly>
+struct NbrReader {
+    const int4* base;
+    size_t stride;
+    int cnt;
+    int4 cur, nxt;
+    __device__ __forceinline__ int4 load(int g) const
+    {
+        const int4* a = base + (size_t)g * stride;
+        return kReadOnly ? __ldg(a) : *a;
+    }
+    __device__ __forceinline__ NbrReader(const int4* nbr, int n, int k, int count)
+        : base(nbr + k), stride((size_t)n), cnt(count)
+    {
+        cur = count > 0 ? load(0) : make_int4(0, 0, 0, 0);
+        nxt = count > 4 ? load(1) : make_int4(0, 0, 0, 0);
+    }
+    __device__ __forceinline__ int get(int t)
+    {
+        const int u = t & 3;
+        if (u == 0 && t > 0) {
+            cur = nxt;
+            if (t + 4 < cnt) nxt = load((t >> 2) + 1);
+        }
+        return u == 0 ? cur.x : (u == 1 ? cur.y : (u == 2 ? cur.z : cur.w));
+    }
+};
 
 // rho of particle k from its list (read back by the thread that wrote it,
 // with plain loads), or by re-testing its candidates when the list overflowed
 template <bool Fast>
 __device__ __forceinline__ float density_from_list(const GridDev& g, const float4* __restrict__ xs,
-                                                   const nsph_sph_params& p, float4 xi, const int* nbr, int cnt,
+                                                   const nsph_sph_params& p, float4 xi, const int4* nbr, int cnt,
                                                    int n, int k)
 {
     float rho = 0.f;
     auto w = [&](float r2) { return Fast ? wterm_fast(r2, p) : wterm(r2, p); };
     if (cnt <= kNbrSlots) {
-        int jn = cnt > 0 ? nbr[k] : 0;
+        NbrReader<false> rd(nbr, n, k, cnt);
         for (int t = 0; t < cnt; ++t) {
-            const int j = jn;
-            if (t + 1 < cnt) jn = nbr[(size_t)(t + 1) * n + k];
-            const float4 xj = __ldg(xs + j);
+            const float4 xj = __ldg(xs + rd.get(t));
             float dx, dy, dz;
             rho = __fmaf_rn(xj.w, w(dist2(xi, xj, dx, dy, dz)), rho);
         }
@@ -519,7 +574,7 @@ __global__ void __launch_bounds__(kSphThreads, 5) k_density_list(GridDev g, cons
                                                                  const float4* __restrict__ vs, int n,
                                                                  const __grid_constant__ nsph_sph_params p,
                                                                  float2* __restrict__ aux, float2* __restrict__ rp,
-                                                                 int* __restrict__ nbr, int* __restrict__ ncnt,
+                                                                 int4* __restrict__ nbr, int* __restrict__ ncnt,
                                                                  unsigned* __restrict__ status)
 {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -543,15 +598,16 @@ __global__ void __launch_bounds__(kSphThreads, 5) k_density_list(GridDev g, cons
 template <bool Fast>
 __device__ __forceinline__ void force_from_list(const GridDev& g, const float4* __restrict__ xs,
                                                 const float4* __restrict__ vs, const float2* __restrict__ aux,
-                                                const int* __restrict__ nbr, int cnt, int n, int k, float4 xi,
+                                                const int4* __restrict__ nbr, int cnt, int n, int k, float4 xi,
                                                 float4 vi, float pr2_i, const nsph_sph_params& p, ForceAcc& acc)
 {
     if (cnt <= kNbrSlots) {
         bool have = false;
         float4 pxj = make_float4(0.f, 0.f, 0.f, 0.f), pvj = pxj;
         float2 paj = make_float2(0.f, 0.f);
+        NbrReader<true> rd(nbr, n, k, cnt);
         for (int t = 0; t < cnt; ++t) {
-            const int j = __ldg(nbr + (size_t)t * n + k);
+            const int j = rd.get(t);
             if (j == k) continue;
             const float4 nxj = __ldg(xs + j);
             const float4 nvj = __ldg(vs + j);
@@ -594,7 +650,7 @@ __global__ void __launch_bounds__(kSphThreads, 4) k_force_list(GridDev g, const 
                                                                const float2* __restrict__ aux,
                                                                const float2* __restrict__ rp, int n,
                                                                const __grid_constant__ nsph_sph_params p,
-                                                               const int* __restrict__ nbr,
+                                                               const int4* __restrict__ nbr,
                                                                const int* __restrict__ ncnt, const StepOut o)
 {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -1084,7 +1140,7 @@ __device__ __forceinline__ void force_feature_term(float4 xj, float4 vj, float2 
 // order
 __device__ __forceinline__ void force_features_from_list(const GridDev& g, const float4* __restrict__ xs,
                                                          const float4* __restrict__ vs,
-                                                         const float2* __restrict__ aux, const int* __restrict__ nbr,
+                                                         const float2* __restrict__ aux, const int4* __restrict__ nbr,
                                                          int cnt, int n, int k, float4 xi, float4 vi, float pr2_i,
                                                          const nsph_sph_params& p, ForceAcc& acc, FeatAcc& fa)
 {
@@ -1092,8 +1148,9 @@ __device__ __forceinline__ void force_features_from_list(const GridDev& g, const
         bool have = false;
         float4 pxj = make_float4(0.f, 0.f, 0.f, 0.f), pvj = pxj;
         float2 paj = make_float2(0.f, 0.f);
+        NbrReader<true> rd(nbr, n, k, cnt);
         for (int t = 0; t < cnt; ++t) {
-            const int j = __ldg(nbr + (size_t)t * n + k);
+            const int j = rd.get(t);
             if (j == k) continue;
             const float4 nxj = __ldg(xs + j);
             const float4 nvj = __ldg(vs + j);
@@ -1121,7 +1178,7 @@ __device__ __forceinline__ void force_features_from_list(const GridDev& g, const
 // 1 to (csum, ccount) when it is active.
 __device__ __forceinline__ void particle_features(const GridDev& g, const float4* __restrict__ xs,
                                                   const float4* __restrict__ vs, const float2* __restrict__ aux,
-                                                  const float2* __restrict__ rp, const int* __restrict__ nbr,
+                                                  const float2* __restrict__ rp, const int4* __restrict__ nbr,
                                                   const int* __restrict__ ncnt, int n, int k, float4 xi, float4 vi,
                                                   const nsph_sph_params& p, float (&f)[kFeat], ForceAcc& acc,
                                                   float& csum, float& ccount)
@@ -1168,7 +1225,7 @@ __global__ void __launch_bounds__(kSphThreads, 4) k_force_features_list(GridDev 
                                                                         const float2* __restrict__ aux,
                                                                         const float2* __restrict__ rp, int n,
                                                                         const __grid_constant__ nsph_sph_params p,
-                                                                        const int* __restrict__ nbr,
+                                                                        const int4* __restrict__ nbr,
                                                                         const int* __restrict__ ncnt,
                                                                         float* __restrict__ feat,
                                                                         float4* __restrict__ sacc,
@@ -1234,7 +1291,7 @@ __global__ void __launch_bounds__(kMlpTile, 6) k_surrogate_fused(const float* __
                                                                  const float2* __restrict__ aux,
                                                                  const float2* __restrict__ rp, int n,
                                                                  const __grid_constant__ nsph_sph_params p,
-                                                                 const int* __restrict__ nbr,
+                                                                 const int4* __restrict__ nbr,
                                                                  const int* __restrict__ ncnt, const StepOut o,
                                                                  float* __restrict__ cpart)
 {
@@ -1331,7 +1388,7 @@ struct nsph_sph {
     float2* rp = nullptr;
     unsigned* mask = nullptr;  // kMaskWords x capacity neighbour bits (word-major)
     int* ncand = nullptr;      // candidates per particle
-    int* nbr = nullptr;        // plain step (single world): kNbrSlots x capacity neighbour lists (slot-major)
+    int4* nbr = nullptr;       // plain step (single world): kNbrGroups x capacity neighbour lists (group-major)
     int* ncnt = nullptr;       //   neighbours per particle
     int fast = 0;              // plain step: tolerance arithmetic (nsph_sph_set_arithmetic)
     unsigned* status = nullptr;
@@ -1493,7 +1550,7 @@ extern "C" int nsph_sph_create(int device, int capacity, const int grid_dims[3],
     if (st == NSPH_OK) {  // the plain step's neighbour lists
         DeviceGuard guard(device);
         const size_t c = (size_t)(capacity > 0 ? capacity : 1);
-        cudaError_t e = cudaMalloc(&s->nbr, sizeof(int) * kNbrSlots * c);
+        cudaError_t e = cudaMalloc(&s->nbr, sizeof(int4) * kNbrGroups * c);
         if (e == cudaSuccess) e = cudaMalloc(&s->ncnt, sizeof(int) * c);
         cudaFuncAttributes fa;
         if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_density_list<false>);
