@@ -62,15 +62,17 @@ WORKLOADS = {
                               surrogate=dict(substeps=4, threshold=0.01, window=10),
                               metric="effective particle-steps/s",
                               desc="learned surrogate on the 1,048,576-particle tank: one step of 4 x 5e-5 s with "
-                                   "the MLP acceleration correction (tcgen05) per call, plain steps as fallback when "
-                                   "the window's mean compression error exceeds 1%"),
+                                   "the MLP acceleration correction (tcgen05) per call; a window of 10 calls whose "
+                                   "compression error exceeds 1% is replaced by plain steps from its start, and the "
+                                   "next window(s) run plain steps"),
     "tank_1m_surrogate_8x": dict(shape=(128, 128, 64), spacing=0.005, box=(2.0, 1.0, 1.0), dt=5e-5, vel_std=0.01,
                                  surrogate=dict(substeps=8, threshold=0.01, window=10,
                                                 weights="surrogate_weights_8x.npz"),
                                  metric="effective particle-steps/s",
                                  desc="learned surrogate on the 1,048,576-particle tank at dt = 4e-4 s: one step of "
-                                      "8 x 5e-5 s (dt c0 / h = 0.8) with the MLP correction per call, plain steps "
-                                      "as fallback when the window's compression error exceeds 1%"),
+                                      "8 x 5e-5 s (dt c0 / h = 0.8) with the MLP correction per call; a window of 10 "
+                                      "calls whose compression error exceeds 1% is replaced by plain steps from its "
+                                      "start, and the next window(s) run plain steps (longer after failures in a row)"),
     "contact_1m": dict(shape=(128, 128, 64), spacing=0.0095, radius=0.005, vel_std=0.1, contact=True,
                        metric="particle-steps/s",
                        desc="particle-particle contact (eval_particle_contact): 1,048,576 spheres of radius 0.005 m "
@@ -481,26 +483,21 @@ def pipelined_e2e(model, step, hx, hv, steps: int, device, outputs=None) -> floa
     end.synchronize()
     return start.elapsed_time(end)
 
-def load_traffic(kernel: str):
-    p = REPO / "profiles" / "ncu_traffic.json"
-    if not p.exists():
-        return None
-    try:
-        d = json.loads(p.read_text())
-        return d.get(kernel, {}).get("traffic_bytes_per_launch")
-    except (ValueError, OSError):
-        return None
-
-
-def load_kernel_counts(kernel: str) -> dict:
-    """ncu figures of a kernel at the bench workload (profiles/ncu_traffic.json)."""
+def load_kernel_counts(kernel: str, workload: str) -> dict:
+    """ncu figures of a kernel (profiles/ncu_traffic.json), only when they
+    were captured on this workload (its name starts the entry's `workload`)."""
     p = REPO / "profiles" / "ncu_traffic.json"
     if not p.exists():
         return {}
     try:
-        return dict(json.loads(p.read_text()).get(kernel, {}))
+        c = dict(json.loads(p.read_text()).get(kernel, {}))
     except (ValueError, OSError):
         return {}
+    return c if str(c.get("workload", "")).split(" ")[0] == workload else {}
+
+
+def load_traffic(kernel: str, workload: str):
+    return load_kernel_counts(kernel, workload).get("traffic_bytes_per_launch")
 
 
 def measure_fp32_peak(device) -> dict:
@@ -518,11 +515,11 @@ def measure_fp32_peak(device) -> dict:
     return {"fp32_tflops": tf.value, "warp_inst_per_s": wi.value, "ms": ms.value}
 
 
-def issue_roofline(kname: str, t_launch_s: float, n: int, peak: dict) -> dict:
+def issue_roofline(kname: str, t_launch_s: float, n: int, peak: dict, workload: str) -> dict:
     """Issue roofline of a neighbour pass: warp instructions per launch (ncu,
     the same workload) over its CUDA-event duration, against the measured
     warp-instruction issue peak."""
-    c = load_kernel_counts(kname)
+    c = load_kernel_counts(kname, workload)
     wi = c.get("warp_inst_per_launch")
     ti = c.get("thread_inst_per_launch")
     out = {"bound": "issue", "kernel": kname, "unit": "warp inst/s", "peak": peak["warp_inst_per_s"],
@@ -680,7 +677,7 @@ def run_gpu(args):
     t_launch = phase[dom] / args.steps * 1e-3
     achieved = b_alg / t_launch / 1e9
     kname = "k_force_list" if dom == "force" else "k_density_list"
-    traffic = load_traffic(kname)
+    traffic = load_traffic(kname, args.workload)
     roofline = {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                 "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                 "alg_bytes_per_launch": b_alg}
@@ -689,7 +686,7 @@ def run_gpu(args):
                      "frac": step_achieved / peak, "alg_bytes_per_particle_step": B_ALG_STEP}
 
     fp32 = measure_fp32_peak(device)
-    roof_issue = issue_roofline(kname, t_launch, n, fp32)
+    roof_issue = issue_roofline(kname, t_launch, n, fp32, args.workload)
 
     # the same timed steps in the tolerance arithmetic (graph-replayed, L2
     # flushed, from the timed state); the headline stays the exact arithmetic
@@ -1095,15 +1092,14 @@ def surrogate_eval(solver, model, sub: int, dt: float, calls: int, start_q, star
         st.step(b, a, dt)
         a.particle_q.copy_(start_q)
         a.particle_qd.copy_(start_qd)
-        st.stats.zero_()
-        st.calls = 0
-        st.surrogate_steps = st.fallback_calls = st.timeouts = 0
-        st.window_worst = []
-        st.monitor.suspended = st.monitor.trips = 0
+        st.reset_counters()
+        solver.reset_status()
         ms = fused_ms = 0.0
         cur, nxt = a, b
+        diverged_at = None
+        done = 0
         torch.cuda.synchronize()
-        for _ in range(calls):
+        for c in range(calls):
             flush.zero_()
             before = st.surrogate_steps
             e0.record(stream)
@@ -1114,13 +1110,20 @@ def surrogate_eval(solver, model, sub: int, dt: float, calls: int, start_q, star
             if phase_timing and st.surrogate_steps > before:
                 fused_ms += solver.surrogate_phase_times()[2]
             cur, nxt = nxt, cur
-        s = st.stats.cpu()
+            done += 1
+            # an arm whose state has blown up is stopped (its neighbour
+            # counts explode and each further call only gets slower)
+            if (c + 1) % window == 0 and not bool(torch.isfinite(cur.particle_q).all()):
+                diverged_at = c + 1
+                break
         finite = bool(torch.isfinite(cur.particle_q).all() and torch.isfinite(cur.particle_qd).all())
-        res = {"value": n * sub * calls / (ms * 1e-3), "ms_per_call": ms / calls,
-               "mean_compression": float(s[3]) / max(1, st.surrogate_steps),
-               "max_window_compression": float(max(st.window_worst or [0.0])),
+        res = {"value": n * sub * done / (ms * 1e-3), "ms_per_call": ms / done, "calls_run": done,
+               "diverged_at_call": diverged_at,
+               "mean_compression": st.mean_compression(),
+               "max_window_compression": st.committed_window_worst(),
                "surrogate_steps": st.surrogate_steps, "fallback_calls": st.fallback_calls,
-               "timeouts": st.timeouts, "finite": finite,
+               "rollbacks": st.rollbacks, "rejected_window_worst": float(max(st.rejected_worst or [0.0])),
+               "timeouts": st.timeouts, "finite": finite, "status": solver.status(),
                "fused_kernel_ms": fused_ms / max(1, st.surrogate_steps) if phase_timing else None,
                "launches_per_call": st.launches_per_step}
         st._graphs.clear()
@@ -1209,7 +1212,7 @@ def run_surrogate(args):
     sur = ev["surrogate"]
     total_ms = max_over_ranks(sur["ms_per_call"] * args.steps, device)
     value = world * n * sub * args.steps / (total_ms * 1e-3)
-    status = solver.status()
+    status = sur["status"]  # the surrogate arm's (the uncorrected arm may blow up by design)
 
     # end to end through the public API: host state in, one call, host state
     # out, every call (pipelined over independent calls, as for tank_1m), all
@@ -1230,7 +1233,7 @@ def run_surrogate(args):
     ach = B_ALG_FUSED * n / t_fused / 1e9 if t_fused > 0 else None
     roofline = {"bound": "hbm", "kernel": "k_surrogate_fused (features + MLP + integrate)", "achieved": ach,
                 "peak": peak, "peak_kind": peak_kind, "unit": "GB/s", "frac": ach / peak if ach else None,
-                "traffic": load_traffic("k_surrogate_fused"), "alg_bytes_per_launch": B_ALG_FUSED * n,
+                "traffic": load_traffic("k_surrogate_fused", args.workload), "alg_bytes_per_launch": B_ALG_FUSED * n,
                 "ms_per_launch": t_fused * 1e3}
     tflops = MLP_FLOPS * n / t_fused / 1e12 if t_fused > 0 else None
     roofline_mlp = {"bound": "tensor", "kernel": "k_surrogate_fused (its MLP share)", "achieved": tflops,
@@ -1283,7 +1286,7 @@ def run_surrogate(args):
                     "steps": e2e_steps, "how": "pinned upload, one SurrogateSPH.step call, download, every call; "
                                               "independent calls pipelined on upload / compute / download streams",
                     "state": "the relaxed state, fallback rule reset", "fallback_calls": e2e_fallbacks},
-            "gpu_launches": sur["launches_per_call"] * sur["surrogate_steps"]
+            "gpu_launches": sur["launches_per_call"] * (sur["surrogate_steps"] + sur["rollbacks"] * sw["window"])
             + sur["fallback_calls"] * sub * solver.last_launches,
             "clocks": clk.summary(),
             "status": status,

@@ -21,8 +21,9 @@
 //   k_ranges      cell_starts / cell_ends from the sorted cell ids.
 // Single-world grids whose table holds at most kCountCellsPerPoint cells per
 // point (the SPH solver's grids) build by cell counts instead (count_build:
-// atomic counts, a scan of the cell table that writes the ranges, scatter,
-// stable rank within each cell): 6 launches instead of 10, the same result.
+// atomic counts, a single-pass scan of the cell table that writes the
+// ranges, scatter, stable rank within each cell): 4 launches instead of 10,
+// the same result.
 #include <algorithm>
 #include <cstdio>
 #include <mutex>
@@ -295,129 +296,231 @@ __global__ void k_ranges(const int* __restrict__ cells, int n, int2* __restrict_
 // Counting build (single-world grids whose cell table is at most a few times
 // the point count): the stable (cell, index) order from cell counts instead
 // of three radix passes.
-//   k_cc_count    cell of each point (original order), its slot in the cell
-//                 from an atomic counter (an arbitrary order within a cell)
-//   k_cc_tiles    per tile of kCcTile cells: the sum of the counts
-//   k_cc_scan     one CTA: exclusive scan of the tile sums
-//   k_cc_ranges   per cell: start = tile offset + exclusive scan in the tile;
-//                 writes the cell table ({start, end}, {0, 0} when empty) and
-//                 turns count into start for the scatter
-//   k_cc_scatter  point -> start + slot (the arbitrary order)
-//   k_cc_rank     per cell-ordered position: its point goes to start + (points
-//                 of its cell with a smaller index), the stable order; writes
-//                 point_cells / point_ids, gathers the sorted mirrors in SPH
-//                 mode, and zeroes the cell's count
+//   k_cc_count        cell of each point (original order), its slot in the
+//                     cell from an atomic counter (an arbitrary order within a
+//                     cell); clears the ranges of the previous build's cells
+//                     and the scan's look-back words
+//   k_cc_scan_ranges  single-pass exclusive scan of the counts in tiles of
+//                     kCsTile cells, each tile's offset found by decoupled
+//                     look-back over its predecessors; writes the ranges of
+//                     the occupied cells (the counts stay as they are, so a
+//                     tile can always sum the counts in front of it itself)
+//   k_cc_scatter      point -> start + slot (the arbitrary order), with its cell
+//   k_cc_rank         per cell-ordered position: its point goes to start +
+//                     (points of its cell with a smaller index), the stable
+//                     order; writes point_cells / point_ids, gathers the
+//                     sorted mirrors in SPH mode, and zeroes the cell's count
 // The result is identical to the stable radix sort's.
 // --------------------------------------------------------------------------
-constexpr int kCcThreads = 1024;
-constexpr int kCcPerThread = 4;
-constexpr int kCcTile = kCcThreads * kCcPerThread;  // cells per scan tile
+constexpr int kCcPoints = 4;     // points per thread of k_cc_count / k_cc_scatter
+constexpr int kCsThreads = 256;  // k_cc_scan_ranges
+constexpr int kCsPer = 32;       // cells per thread (eight int4 loads)
+constexpr int kCsTile = kCsThreads * kCsPer;
+// look-back word of a tile: flag in bits 32-33, value in bits 0-31
+constexpr unsigned long long kTileAggregate = 1ull << 32;  // the tile's own sum
+constexpr unsigned long long kTileInclusive = 2ull << 32;  // the sum of all tiles up to and including it
+constexpr unsigned long long kTileFlags = 3ull << 32;
+// Polls of a predecessor that has not published yet before the tile sums
+// the counts in front of it by itself. Tiles are taken in order from a
+// counter, so a predecessor is always running and publishes within
+// microseconds; the limit only bounds the wait. A limit of 0 skips the
+// look-back (every tile sums its prefix itself: the same result, slower).
+constexpr int kLookbackPolls = 1 << 14;
+
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
 
 __global__ void __launch_bounds__(256) k_cc_count(const float* __restrict__ points, int n, float inv, int dx, int dy,
                                                   int dz, int* __restrict__ count, int* __restrict__ cells,
-                                                  int* __restrict__ slots, unsigned* __restrict__ status)
+                                                  int* __restrict__ slots, const int* __restrict__ prev_cells,
+                                                  int prev_n, int2* __restrict__ ranges,
+                                                  unsigned long long* __restrict__ tile_state, int tiles,
+                                                  unsigned* __restrict__ status)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float x = points[3 * (size_t)i + 0];
-    const float y = points[3 * (size_t)i + 1];
-    const float z = points[3 * (size_t)i + 2];
-    if (status && !(isfinite(x) && isfinite(y) && isfinite(z))) atomicOr(status, (unsigned)NSPH_STATUS_NONFINITE_INPUT);
-    const int c = point_cell(x, y, z, inv, dx, dy, dz);
-    cells[i] = c;
-    slots[i] = atomicAdd(count + c, 1);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int stride = gridDim.x * blockDim.x;
+    if (t <= tiles) tile_state[t] = 0ull;  // look-back words, then the tile counter
+    // the previous build's cells: the first sorted entry of each clears its range
+    for (int k = t; k < prev_n; k += stride) {
+        const int c = prev_cells[k];
+        if (k == 0 || prev_cells[k - 1] != c) ranges[c] = make_int2(0, 0);
+    }
+    bool bad = false;
+    int c[kCcPoints];
+#pragma unroll
+    for (int u = 0; u < kCcPoints; ++u) {
+        const int i = t + u * stride;
+        c[u] = 0;
+        if (i < n) {
+            const float x = points[3 * (size_t)i + 0];
+            const float y = points[3 * (size_t)i + 1];
+            const float z = points[3 * (size_t)i + 2];
+            bad |= !(isfinite(x) && isfinite(y) && isfinite(z));
+            c[u] = point_cell(x, y, z, inv, dx, dy, dz);
+            cells[i] = c[u];
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < kCcPoints; ++u) {
+        const int i = t + u * stride;
+        if (i < n) slots[i] = atomicAdd(count + c[u], 1);
+    }
+    if (bad && status) atomicOr(status, (unsigned)NSPH_STATUS_NONFINITE_INPUT);
 }
 
-__device__ __forceinline__ int cc_block_scan(int v, int& total)
+__global__ void __launch_bounds__(kCsThreads) k_cc_scan_ranges(const int* __restrict__ count, long long ncells,
+                                                               int2* __restrict__ ranges,
+                                                               unsigned long long* __restrict__ tile_state, int tiles,
+                                                               int max_polls)
 {
-    __shared__ int ws[kCcThreads / 32];
+    __shared__ int s_tile, s_base;
+    __shared__ int ws[kCsThreads / 32];
+    __shared__ long long s_part[kCsThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int inc = v;
+    if (threadIdx.x == 0) s_tile = atomicAdd(reinterpret_cast<int*>(tile_state + tiles), 1);
+    __syncthreads();
+    const int tile = s_tile;
+    const long long c0 = (long long)tile * kCsTile + (long long)threadIdx.x * kCsPer;
+    int v[kCsPer];
+    if (c0 + kCsPer <= ncells) {  // count is 256-byte aligned and c0 a multiple of 16
+        const int4* p4 = reinterpret_cast<const int4*>(count + c0);
+#pragma unroll
+        for (int q = 0; q < kCsPer / 4; ++q) {
+            const int4 a = p4[q];
+            v[4 * q + 0] = a.x;
+            v[4 * q + 1] = a.y;
+            v[4 * q + 2] = a.z;
+            v[4 * q + 3] = a.w;
+        }
+    } else {
+#pragma unroll
+        for (int u = 0; u < kCsPer; ++u) v[u] = c0 + u < ncells ? count[c0 + u] : 0;
+    }
+    int sum = 0;
+#pragma unroll
+    for (int u = 0; u < kCsPer; ++u) sum += v[u];
+    int inc = sum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const int t = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += t;
+        const int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += y;
     }
     if (lane == 31) ws[warp] = inc;
     __syncthreads();
     if (warp == 0) {
-        int w = ws[lane];
+        int w = lane < kCsThreads / 32 ? ws[lane] : 0;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int t = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += t;
+        for (int o = 1; o < kCsThreads / 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += y;
         }
-        ws[lane] = w;
+        if (lane < kCsThreads / 32) ws[lane] = w;  // inclusive warp totals
+        const int total = __shfl_sync(0xffffffffu, w, kCsThreads / 32 - 1);
+        // warp-wide look-back: lane l reads the word of tile t - l; the window
+        // moves back 32 tiles while all of it holds aggregates only, and ends
+        // at the nearest inclusive prefix (tiles before 0 count as an
+        // inclusive 0)
+        int base = 0;
+        if (tile == 0) {
+            if (lane == 0) st_relaxed_u64(tile_state, kTileInclusive | (unsigned)total);
+        } else if (max_polls == 0) {
+            base = -1;
+        } else {
+            if (lane == 0) st_relaxed_u64(tile_state + tile, kTileAggregate | (unsigned)total);
+            int t = tile - 1, polls = 0;
+            while (true) {
+                const int idx = t - lane;
+                const unsigned long long word = idx >= 0 ? ld_relaxed_u64(tile_state + idx) : kTileInclusive;
+                const unsigned long long f = word & kTileFlags;
+                const unsigned incl = __ballot_sync(0xffffffffu, f == kTileInclusive);
+                const unsigned none = __ballot_sync(0xffffffffu, f == 0ull);
+                const int first = incl ? __ffs(incl) - 1 : 31;  // the lanes that count: 0 .. first
+                const unsigned need = first == 31 ? 0xffffffffu : ((2u << first) - 1u);
+                if (none & need) {  // a tile in the window has not published yet: poll again
+                    if (++polls > max_polls) {
+                        base = -1;  // sum the counts in front of the tile instead
+                        break;
+                    }
+                    __nanosleep(64);
+                    continue;
+                }
+                int val = lane <= first ? (int)(unsigned)word : 0;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+                base += val;
+                if (incl) break;
+                t -= 32;
+                polls = 0;
+            }
+            if (base >= 0 && lane == 0) st_relaxed_u64(tile_state + tile, kTileInclusive | (unsigned)(base + total));
+        }
+        if (lane == 0) s_base = base;
     }
     __syncthreads();
-    total = ws[kCcThreads / 32 - 1];
-    const int base = warp > 0 ? ws[warp - 1] : 0;
-    __syncthreads();
-    return base + inc - v;
-}
-
-__global__ void __launch_bounds__(kCcThreads) k_cc_tiles(const int* __restrict__ count, long long ncells,
-                                                         int* __restrict__ tile_sums)
-{
-    const long long c0 = (long long)blockIdx.x * kCcTile + (long long)threadIdx.x * kCcPerThread;
-    int s = 0;
+    int base = s_base;
+    if (base < 0) {  // only after kLookbackPolls unanswered polls
+        long long part = 0;
+        for (long long c = threadIdx.x; c < (long long)tile * kCsTile; c += kCsThreads) part += count[c];
 #pragma unroll
-    for (int u = 0; u < kCcPerThread; ++u)
-        if (c0 + u < ncells) s += count[c0 + u];
-    int total = 0;
-    cc_block_scan(s, total);
-    if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
-}
-
-__global__ void __launch_bounds__(kCcThreads) k_cc_scan(int* __restrict__ tile_sums, int tiles)
-{
-    int carry = 0;
-    for (int base = 0; base < tiles; base += kCcThreads) {
-        const int t = base + threadIdx.x;
-        const int v = t < tiles ? tile_sums[t] : 0;
-        int total = 0;
-        const int ex = cc_block_scan(v, total);
-        if (t < tiles) tile_sums[t] = carry + ex;
-        carry += total;
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        if (lane == 0) s_part[warp] = part;
+        __syncthreads();
+        long long b = 0;
+#pragma unroll
+        for (int k = 0; k < kCsThreads / 32; ++k) b += s_part[k];
+        base = (int)b;
+        if (threadIdx.x == 0) st_relaxed_u64(tile_state + tile, kTileInclusive | (unsigned)(base + ws[kCsThreads / 32 - 1]));
     }
-}
-
-__global__ void __launch_bounds__(kCcThreads) k_cc_ranges(int* __restrict__ count, long long ncells,
-                                                          const int* __restrict__ tile_off, int2* __restrict__ ranges)
-{
-    const long long c0 = (long long)blockIdx.x * kCcTile + (long long)threadIdx.x * kCcPerThread;
-    int v[kCcPerThread];
-    int s = 0;
+    int start = base + (warp > 0 ? ws[warp - 1] : 0) + inc - sum;
 #pragma unroll
-    for (int u = 0; u < kCcPerThread; ++u) {
-        v[u] = c0 + u < ncells ? count[c0 + u] : 0;
-        s += v[u];
-    }
-    int total = 0;
-    int start = tile_off[blockIdx.x] + cc_block_scan(s, total);
-#pragma unroll
-    for (int u = 0; u < kCcPerThread; ++u) {
-        if (c0 + u < ncells) {
-            ranges[c0 + u] = v[u] ? make_int2(start, start + v[u]) : make_int2(0, 0);
-            count[c0 + u] = v[u] ? start : 0;  // empty cells keep their zero count
-        }
+    for (int u = 0; u < kCsPer; ++u) {
+        if (v[u]) ranges[c0 + u] = make_int2(start, start + v[u]);  // empty cells keep {0, 0}
         start += v[u];
     }
 }
 
 __global__ void __launch_bounds__(256) k_cc_scatter(const int* __restrict__ cells, const int* __restrict__ slots,
-                                                    const int* __restrict__ start, int n, int* __restrict__ tmp)
+                                                    const int2* __restrict__ ranges, int n, int* __restrict__ tmp,
+                                                    int* __restrict__ tmp_cells)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    tmp[start[cells[i]] + slots[i]] = i;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int stride = gridDim.x * blockDim.x;
+    int c[kCcPoints], s[kCcPoints];
+#pragma unroll
+    for (int u = 0; u < kCcPoints; ++u) {
+        const int i = t + u * stride;
+        c[u] = i < n ? cells[i] : 0;
+        s[u] = i < n ? slots[i] : 0;
+    }
+#pragma unroll
+    for (int u = 0; u < kCcPoints; ++u) {
+        const int i = t + u * stride;
+        if (i < n) s[u] += ranges[c[u]].x;
+    }
+#pragma unroll
+    for (int u = 0; u < kCcPoints; ++u) {
+        const int i = t + u * stride;
+        if (i < n) {
+            tmp[s[u]] = i;
+            tmp_cells[s[u]] = c[u];
+        }
+    }
 }
 
 // one thread per position q of the cell-ordered (not yet stable) array: its
 // point i, the rank of i among its cell's points, and the stable position
 // start + rank, which lies in the same cell's range, so neighbouring threads
 // write neighbouring positions
-__global__ void __launch_bounds__(256) k_cc_rank(const int* __restrict__ cells, const int2* __restrict__ ranges,
+__global__ void __launch_bounds__(256) k_cc_rank(const int* __restrict__ tmp_cells, const int2* __restrict__ ranges,
                                                  const int* __restrict__ tmp, int n, int* __restrict__ count,
                                                  int* __restrict__ point_cells, int* __restrict__ point_ids,
                                                  GatherArgs gather, bool do_gather)
@@ -425,15 +528,9 @@ __global__ void __launch_bounds__(256) k_cc_rank(const int* __restrict__ cells, 
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n) return;
     const int i = tmp[q];
-    const int c = cells[i];
-    const int2 se = ranges[c];
-    int rank = 0;
-    for (int t = se.x; t < se.y; ++t) rank += tmp[t] < i;
-    if (rank == 0) count[c] = 0;  // the counts start at zero for the next build
-    const int g = se.x + rank;
-    point_cells[g] = c;
-    point_ids[g] = i;
-    if (do_gather) {
+    const int c = tmp_cells[q];
+    float4 xs, vs;
+    if (do_gather) {  // the gathered loads go out before the rank loop
         const size_t ii = (size_t)i;
         const float x = gather.x[3 * ii + 0], y = gather.x[3 * ii + 1], z = gather.x[3 * ii + 2];
         const float vx = gather.v[3 * ii + 0], vy = gather.v[3 * ii + 1], vz = gather.v[3 * ii + 2];
@@ -444,8 +541,19 @@ __global__ void __launch_bounds__(256) k_cc_rank(const int* __restrict__ cells, 
         int gw = gather.world ? gather.world[ii] : 0;
         gw = gw < 0 ? 0 : (gw >= gather.world_count ? gather.world_count - 1 : gw);
         const int attr = (active ? kAttrActive : 0) | (w > 0.f ? kAttrDynamic : 0) | (gw << kAttrGravShift);
-        gather.xs[g] = make_float4(x, y, z, active ? m : 0.f);
-        gather.vs[g] = make_float4(vx, vy, vz, __int_as_float(attr));
+        xs = make_float4(x, y, z, active ? m : 0.f);
+        vs = make_float4(vx, vy, vz, __int_as_float(attr));
+    }
+    const int2 se = ranges[c];
+    int rank = 0;
+    for (int t = se.x; t < se.y; ++t) rank += tmp[t] < i;
+    if (rank == 0) count[c] = 0;  // the counts start at zero for the next build
+    const int g = se.x + rank;
+    point_cells[g] = c;
+    point_ids[g] = i;
+    if (do_gather) {
+        gather.xs[g] = xs;
+        gather.vs[g] = vs;
     }
 }
 
@@ -529,15 +637,14 @@ int grid_init(Grid& g, int dx, int dy, int dz, int device)
     if (nc <= kCountMaxCells) {  // the counting build's per-cell counts
         NSPH_CUDA_TRY(cudaMalloc(&g.cell_count, sizeof(int) * nc));
         NSPH_CUDA_TRY(cudaMemset(g.cell_count, 0, sizeof(int) * nc));
-        NSPH_CUDA_TRY(cudaMalloc(&g.tile_sums, sizeof(int) * (size_t)((nc + kCcTile - 1) / kCcTile + 1)));
+        NSPH_CUDA_TRY(cudaMalloc(&g.tile_state,
+                                 sizeof(unsigned long long) * (size_t)((nc + kCsTile - 1) / kCsTile + 1)));
     }
     // load every kernel now, so that a later stream capture never triggers
     // lazy module loading
     cudaFuncAttributes fa;
     NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_cc_count));
-    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_cc_tiles));
-    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_cc_scan));
-    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_cc_ranges));
+    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_cc_scan_ranges));
     NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_cc_scatter));
     NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_cc_rank));
     NSPH_CUDA_TRY(load_sort_kernels<kSortItems>());
@@ -629,7 +736,7 @@ void grid_free(Grid& g)
     cudaFree(g.hist);
     cudaFree(g.cell_ranges);
     cudaFree(g.cell_count);
-    cudaFree(g.tile_sums);
+    cudaFree(g.tile_state);
     cudaFree(g.worlds);
     g = Grid();
 }
@@ -694,27 +801,26 @@ int build_passes(Grid& g, const float* points, int n, float cell_inv, const Gath
     return NSPH_OK;
 }
 
-// the counting build (see k_cc_count): 6 launches
+// the counting build (see k_cc_count): 4 launches
 int count_build(Grid& g, const float* points, int n, float cell_inv, const GatherArgs* gather, unsigned int* status,
-                cudaStream_t stream, int& nl)
+                cudaStream_t stream, int& nl, int prev_n)
 {
-    const int blocks = (n + 255) / 256;
-    const int tiles = (int)((g.ncells + kCcTile - 1) / kCcTile);
+    const int tiles = (int)((g.ncells + kCsTile - 1) / kCsTile);
+    const int per_block = 256 * kCcPoints;
+    const int blocks = std::max((n + per_block - 1) / per_block, (tiles + 1 + 255) / 256);
     k_cc_count<<<blocks, 256, 0, stream>>>(points, n, cell_inv, g.dx, g.dy, g.dz, g.cell_count, g.keys_a, g.vals_a,
-                                           status);
+                                           g.point_cells, prev_n, g.cell_ranges, g.tile_state, tiles, status);
     NSPH_LAUNCH_CHECK("k_cc_count");
-    k_cc_tiles<<<tiles, kCcThreads, 0, stream>>>(g.cell_count, g.ncells, g.tile_sums);
-    NSPH_LAUNCH_CHECK("k_cc_tiles");
-    k_cc_scan<<<1, kCcThreads, 0, stream>>>(g.tile_sums, tiles);
-    NSPH_LAUNCH_CHECK("k_cc_scan");
-    k_cc_ranges<<<tiles, kCcThreads, 0, stream>>>(g.cell_count, g.ncells, g.tile_sums, g.cell_ranges);
-    NSPH_LAUNCH_CHECK("k_cc_ranges");
-    k_cc_scatter<<<blocks, 256, 0, stream>>>(g.keys_a, g.vals_a, g.cell_count, n, g.keys_b);
+    k_cc_scan_ranges<<<tiles, kCsThreads, 0, stream>>>(g.cell_count, g.ncells, g.cell_ranges, g.tile_state, tiles,
+                                                       g.scan_polls < 0 ? kLookbackPolls : g.scan_polls);
+    NSPH_LAUNCH_CHECK("k_cc_scan_ranges");
+    k_cc_scatter<<<(n + per_block - 1) / per_block, 256, 0, stream>>>(g.keys_a, g.vals_a, g.cell_ranges, n, g.keys_b,
+                                                                       g.vals_b);
     NSPH_LAUNCH_CHECK("k_cc_scatter");
-    k_cc_rank<<<blocks, 256, 0, stream>>>(g.keys_a, g.cell_ranges, g.keys_b, n, g.cell_count, g.point_cells,
-                                          g.point_ids, gather ? *gather : GatherArgs{}, gather != nullptr);
+    k_cc_rank<<<(n + 255) / 256, 256, 0, stream>>>(g.vals_b, g.cell_ranges, g.keys_b, n, g.cell_count, g.point_cells,
+                                                   g.point_ids, gather ? *gather : GatherArgs{}, gather != nullptr);
     NSPH_LAUNCH_CHECK("k_cc_rank");
-    nl += 6;
+    nl += 4;
     return NSPH_OK;
 }
 
@@ -730,7 +836,7 @@ int grid_build(Grid& g, const float* points, int n, float cell_width, float cell
     if (n > 0 && !points) return fail(NSPH_ERR_INVALID_ARG, "build: null points");
     const int prev_n = g.built ? g.num_points : 0;
     if (g.world_count == 0 && g.cell_count && n > 0 && g.ncells <= (long long)kCountCellsPerPoint * n) {
-        const int st = count_build(g, points, n, cell_inv, gather, status, stream, nl);
+        const int st = count_build(g, points, n, cell_inv, gather, status, stream, nl, prev_n);
         if (st != NSPH_OK) return st;
         g.num_points = n;
         g.cell_width = cell_width;
@@ -806,6 +912,13 @@ extern "C" int nsph_grid_reserve(nsph_grid* grid, int num_points)
         return fail(NSPH_ERR_OUT_OF_MEMORY, "grid reserve: contact mirror allocation failed");
     }
     grid->mirror_cap = grid->g.capacity;
+    return NSPH_OK;
+}
+
+extern "C" int nsph_grid_set_scan_polls(nsph_grid* grid, int polls)
+{
+    if (!grid) return fail(NSPH_ERR_INVALID_ARG, "null grid");
+    grid->g.scan_polls = polls < 0 ? -1 : polls;
     return NSPH_OK;
 }
 

@@ -213,9 +213,11 @@ struct Grid {
     // cell table (ncells entries of {start, end})
     int2* cell_ranges = nullptr;
     // counting build (single world, at most kCountMaxCells cells): per-cell
-    // counts (all zero between builds) and per-tile sums of the cell scan
+    // counts (all zero between builds), and the cell scan's per-tile look-back
+    // words followed by its tile counter
     int* cell_count = nullptr;
-    int* tile_sums = nullptr;
+    unsigned long long* tile_state = nullptr;
+    int scan_polls = -1;  // the cell scan's look-back wait (-1: the default limit)
 
     GridDev view() const { return GridDev{dx, dy, dz, cell_inv, cell_ranges, point_ids}; }
 };

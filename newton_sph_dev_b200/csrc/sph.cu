@@ -676,14 +676,14 @@ __device__ __forceinline__ GridDev world_grid(const WorldCells& c, const int2* _
     return GridDev{c.dx, c.dy, c.dz, c.inv, ranges + c.off, ids};
 }
 
-__global__ void __launch_bounds__(kSphThreads, 4) k_density_worlds(const WorldCells* __restrict__ wc,
+__global__ void __launch_bounds__(kSphThreads, 3) k_density_worlds(const WorldCells* __restrict__ wc,
                                                                    const nsph_sph_params* __restrict__ wp,
                                                                    const int2* __restrict__ ranges,
                                                                    const int* __restrict__ ids,
                                                                    const float4* __restrict__ xs,
                                                                    const float4* __restrict__ vs, int n,
                                                                    float2* __restrict__ aux, float2* __restrict__ rp,
-                                                                   unsigned* __restrict__ mask, int* __restrict__ ncand,
+                                                                   int4* __restrict__ nbr, int* __restrict__ ncnt,
                                                                    unsigned* __restrict__ status)
 {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -692,15 +692,15 @@ __global__ void __launch_bounds__(kSphThreads, 4) k_density_worlds(const WorldCe
         if (!(attr & kAttrActive)) {
             aux[k] = make_float2(0.f, 0.f);
             rp[k] = make_float2(0.f, 0.f);
-            ncand[k] = 0;
+            ncnt[k] = 0;
             continue;
         }
         const int w = attr >> kAttrGravShift;
         const nsph_sph_params p = wp[w];  // a copy: its fields stay in registers across the candidate loop
         const GridDev g = world_grid(wc[w], ranges, ids);
-        int nc = 0;
-        const float rho = density_single(g, xs, p, xi, mask, n, k, nc);
-        ncand[k] = nc;
+        const int cnt = neighbor_list(g, xs, p, xi, nbr, n, k);
+        ncnt[k] = cnt;
+        const float rho = density_from_list<false>(g, xs, p, xi, nbr, cnt, n, k);
         density_finish(k, xi.w, rho, p, aux, rp, status);
     }
 }
@@ -713,8 +713,8 @@ __global__ void __launch_bounds__(kSphThreads, 3) k_force_worlds(const WorldCell
                                                                  const float4* __restrict__ vs,
                                                                  const float2* __restrict__ aux,
                                                                  const float2* __restrict__ rp, int n, float dt,
-                                                                 const unsigned* __restrict__ mask,
-                                                                 const int* __restrict__ ncand, const StepOut o)
+                                                                 const int4* __restrict__ nbr,
+                                                                 const int* __restrict__ ncnt, const StepOut o)
 {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const float4 xi = xs[k], vi = vs[k];
@@ -723,7 +723,7 @@ __global__ void __launch_bounds__(kSphThreads, 3) k_force_worlds(const WorldCell
         const nsph_sph_params& p = wp[w];
         const GridDev g = world_grid(wc[w], ranges, ids);
         ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        if (attr & kAttrActive) force_single(g, xs, vs, aux, mask, ncand[k], n, k, xi, vi, aux[k].y, p, acc);
+        if (attr & kAttrActive) force_from_list<false>(g, xs, vs, aux, nbr, ncnt[k], n, k, xi, vi, aux[k].y, p, acc);
         integrate_out((size_t)ids[k], xi, vi, attr, rp[k], acc, p, dt, o);
     }
 }
@@ -1388,7 +1388,7 @@ struct nsph_sph {
     float2* rp = nullptr;
     unsigned* mask = nullptr;  // kMaskWords x capacity neighbour bits (word-major)
     int* ncand = nullptr;      // candidates per particle
-    int4* nbr = nullptr;       // plain step (single world): kNbrGroups x capacity neighbour lists (group-major)
+    int4* nbr = nullptr;       // plain and worlds steps: kNbrGroups x capacity neighbour lists (group-major)
     int* ncnt = nullptr;       //   neighbours per particle
     int fast = 0;              // plain step: tolerance arithmetic (nsph_sph_set_arithmetic)
     unsigned* status = nullptr;
@@ -1547,11 +1547,9 @@ extern "C" int nsph_sph_create(int device, int capacity, const int grid_dims[3],
     if (!s) return fail(NSPH_ERR_OUT_OF_MEMORY, "host allocation failed");
     int st = grid_init(s->grid, grid_dims[0], grid_dims[1], grid_dims[2], device);
     if (st == NSPH_OK) st = sph_create_common(s, device, capacity);
-    if (st == NSPH_OK) {  // the plain step's neighbour lists
+    if (st == NSPH_OK) {  // the plain step's kernels
         DeviceGuard guard(device);
-        const size_t c = (size_t)(capacity > 0 ? capacity : 1);
-        cudaError_t e = cudaMalloc(&s->nbr, sizeof(int4) * kNbrGroups * c);
-        if (e == cudaSuccess) e = cudaMalloc(&s->ncnt, sizeof(int) * c);
+        cudaError_t e = cudaSuccess;
         cudaFuncAttributes fa;
         if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_density_list<false>);
         if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_force_list<false>);
@@ -1623,6 +1621,8 @@ static int sph_create_common(nsph_sph* s, int device, int capacity)
         if (e == cudaSuccess) e = cudaMalloc(&s->rp, sizeof(float2) * c);
         if (e == cudaSuccess) e = cudaMalloc(&s->mask, sizeof(unsigned) * kMaskWords * c);
         if (e == cudaSuccess) e = cudaMalloc(&s->ncand, sizeof(int) * c);
+        if (e == cudaSuccess) e = cudaMalloc(&s->nbr, sizeof(int4) * kNbrGroups * c);
+        if (e == cudaSuccess) e = cudaMalloc(&s->ncnt, sizeof(int) * c);
         if (e == cudaSuccess) e = cudaMalloc(&s->status, sizeof(unsigned));
         if (e == cudaSuccess) e = cudaMemset(s->status, 0, sizeof(unsigned));
         cudaFuncAttributes fa;
@@ -1833,15 +1833,15 @@ extern "C" int nsph_sph_step_worlds(nsph_sph* s, float dt, int n, const float* x
         int blocks, threads;
         pass_launch(s, n, true, blocks, threads);
         k_density_worlds<<<blocks, threads, 0, cs>>>(s->grid.worlds, s->wparams, s->grid.cell_ranges,
-                                                         s->grid.point_ids, s->xs, s->vs, n, s->aux, s->rp, s->mask,
-                                                         s->ncand, s->status);
+                                                         s->grid.point_ids, s->xs, s->vs, n, s->aux, s->rp, s->nbr,
+                                                         s->ncnt, s->status);
         NSPH_LAUNCH_CHECK("k_density_worlds");
         ++launches;
         if (s->ev[2]) NSPH_CUDA_TRY(record_mark(s->ev[2], cs));
         const StepOut o{f_ext, inv_mass, gravity, x_out, v_out, rho_out, p_out, a_out, s->status};
         k_force_worlds<<<blocks, threads, 0, cs>>>(s->grid.worlds, s->wparams, s->grid.cell_ranges,
-                                                       s->grid.point_ids, s->xs, s->vs, s->aux, s->rp, n, dt, s->mask,
-                                                       s->ncand, o);
+                                                       s->grid.point_ids, s->xs, s->vs, s->aux, s->rp, n, dt, s->nbr,
+                                                       s->ncnt, o);
         NSPH_LAUNCH_CHECK("k_force_worlds");
         ++launches;
     } else if (s->ev[2]) {
@@ -2263,6 +2263,32 @@ extern "C" int nsph_sph_adjoint_phase_times(nsph_sph* s, float ms_out[5])
 // ==========================================================================
 // C ABI: surrogate step
 // ==========================================================================
+// Resident CTAs per SM of k_surrogate_fused by default. Six fit (shared
+// memory, TMEM columns, registers), but six leave about 28 KB of L1 for the
+// neighbour gathers; five (the rest of the SM's storage as L1) measured
+// 0.29 ms per launch on the 1M tank against 0.39 ms at six (0.32 at four).
+constexpr int kSurrogateCtasPerSm = 5;
+
+static int set_surrogate_ctas(nsph_sph* s, int ctas_per_sm)
+{
+    DeviceGuard guard(s->grid.device);
+    if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
+    const int most = mlp_resident_grid(k_surrogate_fused, sizeof(MlpFwdSmem), s->grid.device);
+    int sms = 0, smem_sm = 0, reserved = 0;
+    NSPH_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->grid.device));
+    NSPH_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, s->grid.device));
+    NSPH_CUDA_TRY(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, s->grid.device));
+    if (most <= 0 || sms <= 0 || smem_sm <= 0) return fail(NSPH_ERR_CUDA, "cannot size the surrogate grid");
+    const int per_sm = std::max(1, std::min(ctas_per_sm == 0 ? kSurrogateCtasPerSm : ctas_per_sm, most / sms));
+    // the shared-memory carveout that holds per_sm CTAs, so that the rest of
+    // the SM's unified L1 / shared storage serves the neighbour gathers
+    const int need = per_sm * (int)(sizeof(MlpFwdSmem) + reserved);
+    const int pct = std::min(100, (need * 100 + smem_sm - 1) / smem_sm);
+    NSPH_CUDA_TRY(cudaFuncSetAttribute(k_surrogate_fused, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+    s->surr_ctas = sms * per_sm;
+    return NSPH_OK;
+}
+
 extern "C" int nsph_sph_enable_surrogate(nsph_sph* s)
 {
     clear_error();
@@ -2295,7 +2321,7 @@ extern "C" int nsph_sph_enable_surrogate(nsph_sph* s)
         s->sacc = nullptr;
         return fail(NSPH_ERR_OUT_OF_MEMORY, std::string("surrogate allocation: ") + cudaGetErrorString(e));
     }
-    return NSPH_OK;
+    return set_surrogate_ctas(s, 0);  // the default resident CTAs per SM and their carveout
 }
 
 // grid build, density pass and (with `features`) the feature pass into the
@@ -2415,6 +2441,15 @@ extern "C" int nsph_sph_step_surrogate(nsph_sph* s, const nsph_sph_params* p, co
     if (s->eva[4]) NSPH_CUDA_TRY(record_mark(s->eva[4], cs));
     s->last_launches = launches;
     return NSPH_OK;
+}
+
+extern "C" int nsph_sph_set_surrogate_launch(nsph_sph* s, int ctas_per_sm)
+{
+    clear_error();
+    if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
+    if (ctas_per_sm < 0 || ctas_per_sm > 64) return fail(NSPH_ERR_INVALID_ARG, "ctas_per_sm out of [0, 64]");
+    if (!s->sfeat) return fail(NSPH_ERR_INVALID_ARG, "surrogate not enabled (nsph_sph_enable_surrogate)");
+    return set_surrogate_ctas(s, ctas_per_sm);
 }
 
 extern "C" int nsph_sph_set_surrogate_wait_limit(nsph_sph* s, int polls)

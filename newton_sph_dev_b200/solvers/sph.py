@@ -10,9 +10,10 @@ positions (solver_xpbd.py:315-319), per-particle neighbour gathers through
 the grid (kernels_contact.py:35-84) and integrate_particles semantics
 (solver.py:10-47).
 
-One step = one ``nsph_sph_step`` call into libnsph.so: grid build (hash +
-LSD radix sort + cell ranges + sorted gather), density/EOS pass,
-pressure/XSPH/integrate pass. Stream-ordered on the current torch stream,
+One step = one ``nsph_sph_step`` call into libnsph.so: grid build (cell
+counts, a single-pass scan of the cell table, stable ranking within each
+cell and the sorted gather; the LSD radix sort for sparse cell tables),
+density/EOS pass (neighbour lists), pressure/XSPH/integrate pass. Stream-ordered on the current torch stream,
 no allocation and no host sync, so a step (or a loop of steps) can be
 captured with ``torch.cuda.graph``. Gravity is read from ``model.gravity``
 on the device, so ``model.set_gravity`` reaches replayed graphs; scalar
@@ -706,6 +707,15 @@ class SolverSPH(SolverBase):
         self.enable_surrogate()
         _lib.check(self._lib.nsph_sph_set_surrogate_wait_limit(self._handle, int(polls)),
                    "SolverSPH.set_surrogate_wait_limit")
+
+    def set_surrogate_launch(self, ctas_per_sm: int = 0) -> None:
+        """Resident CTAs per SM of the surrogate step's fused kernel (0: the
+        default, 5 on a B200). Fewer CTAs leave more of the SM's L1 to the
+        neighbour gathers (see nsph_sph_set_surrogate_launch); results do
+        not change."""
+        self.enable_surrogate()
+        _lib.check(self._lib.nsph_sph_set_surrogate_launch(self._handle, int(ctas_per_sm)),
+                   "SolverSPH.set_surrogate_launch")
 
     def surrogate_phase_times(self) -> tuple[float, float, float, float]:
         """(build, density, fused features + MLP + integrate, compression

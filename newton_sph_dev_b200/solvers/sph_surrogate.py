@@ -19,8 +19,11 @@ builds on the plain step. Pieces:
   suspended. The plain step is the fallback and the yardstick: the mean
   compression error e = mean_i max(0, rho_i/rho0 - 1) of every surrogate step
   is accumulated on the device; every ``window`` calls the host reads the
-  window's worst value (one copy) and, above ``threshold``, runs plain steps
-  for the next window(s) before trying the surrogate again.
+  window's worst value (one copy). Above ``threshold`` (or NaN) the window is
+  rejected: with ``rollback`` (the default) the state saved at the window's
+  start is restored and the window is run again with plain steps, so every
+  committed surrogate window stays within the threshold; the surrogate is
+  then suspended for the next window(s), longer after consecutive failures.
 
 Every quantity the network sees or predicts is dimensionless (lengths / h,
 velocities / c0, accelerations h / c0^2 with c0^2 = B gamma / rho0), so a
@@ -338,24 +341,36 @@ class FallbackMonitor:
     """Host side of the fallback rule (no device access): given the worst
     compression error of each window of surrogate steps, decide whether the
     next window runs the surrogate or the plain step. A window above the
-    threshold suspends the surrogate for `cooldown` windows."""
+    threshold suspends the surrogate for `cooldown` windows; with `backoff`,
+    each further failure in a row doubles that (up to `max_cooldown`), and a
+    window that passes resets it."""
 
-    def __init__(self, threshold: float = 0.01, cooldown: int = 1):
+    def __init__(self, threshold: float = 0.01, cooldown: int = 1, backoff: bool = False, max_cooldown: int = 64):
         self.threshold = threshold
         self.cooldown = cooldown
+        self.backoff = bool(backoff)
+        self.max_cooldown = int(max_cooldown)
         self.suspended = 0
         self.trips = 0
+        self.in_a_row = 0
 
     def use_surrogate(self) -> bool:
         return self.suspended == 0
 
-    def end_window(self, worst: float | None) -> None:
-        """worst: the window's max compression error (None for a plain window)."""
+    def end_window(self, worst: float | None) -> bool:
+        """worst: the window's max compression error (None for a plain
+        window). Returns True when a surrogate window failed (trip)."""
         if worst is None:
             self.suspended = max(0, self.suspended - 1)
-        elif not (worst <= self.threshold):  # NaN counts as a trip
+            return False
+        if not (worst <= self.threshold):  # NaN counts as a trip
             self.trips += 1
-            self.suspended = self.cooldown
+            self.in_a_row += 1
+            c = self.cooldown * (2 ** (self.in_a_row - 1) if self.backoff else 1)
+            self.suspended = min(c, max(self.max_cooldown, self.cooldown))
+            return True
+        self.in_a_row = 0
+        return False
 
 
 class SurrogateSPH:
@@ -363,17 +378,32 @@ class SurrogateSPH:
     of dt_big = substeps x dt, or substeps plain steps while the surrogate is
     suspended by the fallback rule (see the module docstring). A window in
     which a tensor-core wait gave up (NSPH_STATUS_SURROGATE_TIMEOUT) counts as
-    failed, like one above the threshold."""
+    failed, like one above the threshold.
+
+    With ``rollback`` (default) a failed window is replaced: the call that
+    ends it restores the state saved when the window began (two device
+    copies per window) and runs the window's calls again as plain steps, so
+    the state it returns is the plain trajectory's; states returned by the
+    window's earlier calls were speculative. Without it, a failed window is
+    kept and only the next window(s) run plain steps. ``backoff`` doubles the
+    suspension after each further failure in a row (see FallbackMonitor)."""
 
     def __init__(self, solver: SolverSPH, model: SurrogateModel, substeps: int = 4, threshold: float = 0.01,
-                 window: int = 10, cooldown: int = 1, graphs: bool = False):
+                 window: int = 10, cooldown: int = 1, graphs: bool = False, rollback: bool = True,
+                 backoff: bool = True):
         if solver.batched:
             raise ValueError("the surrogate needs a single-world solver")
         self.solver = solver
         self.model = model
         self.substeps = int(substeps)
         self.window = int(window)
-        self.monitor = FallbackMonitor(threshold, cooldown)
+        self.monitor = FallbackMonitor(threshold, cooldown, backoff=backoff)
+        self.rollback = bool(rollback)
+        self._ckpt = None
+        self.rollbacks = 0
+        self.committed_compression = 0.0  # sum of e over the surrogate steps kept
+        self.rejected_worst: list[float] = []
+        self._stats_at_window = 0.0
         solver.enable_surrogate()
         self.stats = torch.zeros(4, dtype=torch.float32, device=solver.model.device)
         self._traj = None
@@ -392,23 +422,65 @@ class SurrogateSPH:
         """Advance state_in by substeps x dt into state_out."""
         if self.calls % self.window == 0:
             self._window_mode = self.monitor.use_surrogate()
+            if self._window_mode and self.rollback:  # the state the window may return to
+                if self._ckpt is None:
+                    self._ckpt = (torch.empty_like(state_in.particle_q), torch.empty_like(state_in.particle_qd))
+                self._ckpt[0].copy_(state_in.particle_q)
+                self._ckpt[1].copy_(state_in.particle_qd)
         if self._window_mode:
             self._surrogate_step(state_in, state_out, dt)
             self.surrogate_steps += 1
         else:
-            n = self.solver.model.particle_count
-            if self._traj is None:
-                dev = self.solver.model.device
-                self._traj = (torch.empty((self.substeps, n, 3), dtype=torch.float32, device=dev),
-                              torch.empty((self.substeps, n, 3), dtype=torch.float32, device=dev))
-            tx, tv = self._traj
-            self.solver.rollout_raw(state_in.particle_q, state_in.particle_qd, tx, tv, self.solver.step_params(dt))
-            state_out.particle_q.copy_(tx[-1])
-            state_out.particle_qd.copy_(tv[-1])
+            self._plain_call(state_in.particle_q, state_in.particle_qd, state_out, dt)
             self.fallback_calls += 1
         self.calls += 1
         if self.calls % self.window == 0:
-            self._end_window()
+            self._end_window(state_out, dt)
+
+    def reset_counters(self) -> None:
+        """Start the counters, the statistics and the fallback rule afresh
+        (captured graphs are kept)."""
+        self.stats.zero_()
+        self.calls = self.surrogate_steps = self.fallback_calls = self.timeouts = self.rollbacks = 0
+        self.window_worst = []
+        self.rejected_worst = []
+        self.committed_compression = 0.0
+        self._stats_at_window = 0.0
+        self.monitor.suspended = self.monitor.trips = self.monitor.in_a_row = 0
+
+    def _plain_steps(self, q, qd, state_out, dt):
+        """substeps plain steps of dt from (q, qd) into state_out, through two
+        scratch states (each step's velocity output starts as its input, so
+        inactive particles keep their velocity, as in nsph_sph_rollout)."""
+        if self._traj is None:
+            self._traj = tuple(torch.empty_like(q) for _ in range(4))
+        p = self.solver.step_params(dt)
+        cur_q, cur_qd = q, qd
+        for i in range(self.substeps):
+            last = i == self.substeps - 1
+            oq, oqd = (state_out.particle_q, state_out.particle_qd) if last else self._traj[2 * (i % 2):2 * (i % 2) + 2]
+            oqd.copy_(cur_qd)
+            self.solver.step_raw(cur_q, cur_qd, oq, oqd, p)
+            cur_q, cur_qd = oq, oqd
+
+    def _plain_call(self, q, qd, state_out, dt):
+        """substeps plain steps of dt from (q, qd) into state_out (replayed
+        from a CUDA graph per (buffers, dt) with ``graphs``)."""
+        if not self.graphs:
+            self._plain_steps(q, qd, state_out, dt)
+            return
+        key = ("plain", q.data_ptr(), qd.data_ptr(), state_out.particle_q.data_ptr(),
+               state_out.particle_qd.data_ptr(), float(dt))
+        g = self._graphs.get(key)
+        if g is None:  # run eagerly this time, then capture for the next calls
+            self._plain_steps(q, qd, state_out, dt)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                self._plain_steps(q, qd, state_out, dt)
+            self._graphs[key] = g
+            # the capture ran nothing: state_out holds the eager result
+            return
+        g.replay()
 
     def _surrogate_call(self, state_in, state_out, dt):
         self.solver.step_surrogate_raw(state_in.particle_q, state_in.particle_qd, state_out.particle_q,
@@ -433,25 +505,49 @@ class SurrogateSPH:
             return
         g.replay()
 
-    def _end_window(self) -> None:
-        if self._window_mode:
-            worst = float(self.stats[1].item())
-            # a tensor-core wait that gave up integrated part of a step
-            # without the correction: count the window as failed
-            if self.solver.status() & _lib.NSPH_STATUS_SURROGATE_TIMEOUT:
-                self.timeouts += 1
-                self.solver.reset_status()
-                worst = float("nan")
-            self.window_worst.append(worst)
-            self.monitor.end_window(worst)
-            self.stats[1:3].zero_()
-        else:
+    def _end_window(self, state_out, dt: float) -> None:
+        if not self._window_mode:
             self.monitor.end_window(None)
+            return
+        s = self.stats.cpu()  # one copy: worst, steps, running sum
+        worst = float(s[1])
+        window_sum = float(s[3]) - self._stats_at_window
+        self._stats_at_window = float(s[3])
+        # a tensor-core wait that gave up integrated part of a step
+        # without the correction: count the window as failed
+        if self.solver.status() & _lib.NSPH_STATUS_SURROGATE_TIMEOUT:
+            self.timeouts += 1
+            self.solver.reset_status()
+            worst = float("nan")
+        self.window_worst.append(worst)
+        failed = self.monitor.end_window(worst)
+        self.stats[1:3].zero_()
+        if failed and self.rollback:
+            # replace the window: plain steps from the state it began with
+            self.rollbacks += 1
+            self.rejected_worst.append(worst)
+            self.surrogate_steps -= self.window
+            self.fallback_calls += self.window
+            q, qd = self._ckpt
+            for i in range(self.window):
+                self._plain_call(q, qd, state_out, dt)
+                if i + 1 < self.window:  # the next call starts from this one's result
+                    q.copy_(state_out.particle_q)
+                    qd.copy_(state_out.particle_qd)
+        else:
+            self.committed_compression += window_sum
+
+    def committed_window_worst(self) -> float:
+        """Worst step compression over the kept surrogate windows."""
+        kept = [w for w in self.window_worst if w == w and w <= self.monitor.threshold] if self.rollback \
+            else self.window_worst
+        return float(max(kept or [0.0]))
 
     def mean_compression(self) -> float:
-        """Mean compression error over all surrogate steps so far (syncs)."""
-        s = self.stats.cpu()
-        return float(s[3] / max(1, self.surrogate_steps))
+        """Mean compression error over the surrogate steps kept so far, as of
+        the last completed window."""
+        return self.committed_compression / max(1, self.surrogate_steps - (self.calls % self.window
+                                                                              if self._window_mode else 0))
 
 
 __all__ = ["FEATURES", "FallbackMonitor", "SurrogateModel", "SurrogateSPH", "SurrogateTrainer", "accel_scale",

@@ -195,9 +195,9 @@ def test_zero_correction_is_the_plain_step_and_monitor():
 
 
 def test_stepper_fallback_runs_plain_substeps():
-    """A threshold below any possible error trips the monitor after the first
-    window: the next window runs plain substeps, bit-identical to a rollout of
-    plain steps."""
+    """Without rollback, a threshold below any possible error trips the
+    monitor after the first window, which is kept: the next window runs plain
+    substeps, bit-identical to a rollout of plain steps."""
     from newton_sph_dev_b200.solvers.sph_surrogate import SurrogateModel, SurrogateSPH
 
     from newton_sph_dev_b200.solvers import SolverSPH
@@ -206,7 +206,7 @@ def test_stepper_fallback_runs_plain_substeps():
     solver = SolverSPH(model, cfg)
     m = SurrogateModel(DEV, seed=0)
     m.zero_correction()
-    st = SurrogateSPH(solver, m, substeps=4, threshold=-1.0, window=2, cooldown=1)
+    st = SurrogateSPH(solver, m, substeps=4, threshold=-1.0, window=2, cooldown=1, rollback=False, backoff=False)
     s0, s1 = model.state(), model.state()
     dt = 1e-4
     for _ in range(2):  # window 1: surrogate
@@ -224,6 +224,42 @@ def test_stepper_fallback_runs_plain_substeps():
     st.step(s1, s0, dt)
     st.step(s0, s1, dt)  # window 3: surrogate again (cooldown over)
     assert st.surrogate_steps == 3 and st.fallback_calls == 2
+
+
+def test_stepper_rollback_replaces_failed_window():
+    """With rollback (the default), a failed window is replaced: the call that
+    ends it returns the plain trajectory from the window's starting state,
+    bit for bit, the window's surrogate steps are not counted, and the
+    suspensions after consecutive failures grow (1, then 2 windows)."""
+    from newton_sph_dev_b200.solvers.sph_surrogate import SurrogateSPH
+
+    from newton_sph_dev_b200.solvers import SolverSPH
+
+    model, cfg, x, v, flags = _scene(seed=13)
+    solver = SolverSPH(model, cfg)
+    m = random_model(7)
+    st = SurrogateSPH(solver, m, substeps=4, threshold=-1.0, window=2, cooldown=1)
+    s0, s1 = model.state(), model.state()
+    dt = 1e-4
+    x0, v0 = s0.particle_q.clone(), s0.particle_qd.clone()
+    for _ in range(2):  # window 1: surrogate, rejected
+        st.step(s0, s1, dt)
+        s0, s1 = s1, s0
+    assert st.rollbacks == 1 and st.surrogate_steps == 0 and st.fallback_calls == 2
+    tx = torch.empty((8, model.particle_count, 3), device=DEV)
+    tv = torch.empty_like(tx)
+    solver.rollout_raw(x0, v0, tx, tv, solver.step_params(dt))
+    torch.cuda.synchronize()
+    assert torch.equal(s0.particle_q, tx[-1]) and torch.equal(s0.particle_qd, tv[-1])
+    modes = []
+    for _ in range(10):  # plain (1 window), surrogate (rejected), plain (2 windows), surrogate
+        before = st.surrogate_steps + st.rollbacks * 2
+        st.step(s0, s1, dt)
+        s0, s1 = s1, s0
+        modes.append("s" if st.surrogate_steps + st.rollbacks * 2 > before else "p")
+    assert "".join(modes) == "ppssppppss"
+    assert st.rollbacks == 3 and st.mean_compression() == 0.0
+    assert bool(torch.isfinite(s0.particle_q).all())
 
 
 def test_fallback_trips_on_corrupted_weights():
@@ -246,9 +282,14 @@ def test_fallback_trips_on_corrupted_weights():
     for _ in range(4):
         st.step(s0, s1, dt)
         s0, s1 = s1, s0
-    assert st.monitor.trips == 1 and st.window_worst[-1] > 0.01
+    # tripped, and the window was replaced by plain steps (no compression left)
+    assert st.monitor.trips == 1 and st.window_worst[-1] > 0.01 and st.rollbacks == 1
+    assert st.fallback_calls == 4 and st.surrogate_steps == 0
+    rho = torch.empty(model.particle_count, device=DEV)
+    solver.features_raw(s0.particle_q, s0.particle_qd, rho_out=rho, params=solver.step_params(dt))
+    assert float(torch.clamp(rho / 1000.0 - 1.0, min=0).mean()) < 0.01
     st.step(s0, s1, dt)
-    assert st.fallback_calls == 1
+    assert st.fallback_calls == 5
 
 
 def test_surrogate_wait_timeout_falls_back():
@@ -280,12 +321,38 @@ def test_surrogate_wait_timeout_falls_back():
     for _ in range(2):
         st.step(s0, s1, dt)
         s0, s1 = s1, s0
-    assert st.timeouts == 1 and st.monitor.trips == 1
+    assert st.timeouts == 1 and st.monitor.trips == 1 and st.rollbacks == 1
     st.step(s0, s1, dt)
-    assert st.fallback_calls == 1
+    assert st.fallback_calls == 3
     solver.set_surrogate_wait_limit(-1)  # the default again: the corrected step runs
     solver.reset_status()
     solver.step_surrogate_raw(model.particle_q, model.particle_qd, xs, vs, p, m, 1.0, stats)
     torch.cuda.synchronize()
     assert solver.status() == 0
     assert not torch.equal(xs, xp)
+
+
+@pytest.mark.parametrize("ctas_per_sm", [1, 2, 4])
+def test_surrogate_launch_shape_keeps_results(ctas_per_sm):
+    """Fewer resident CTAs per SM for the fused kernel (a larger L1 for its
+    neighbour gathers): the same positions and velocities, bit for bit, as
+    the default grid, and the same compression statistics up to the order of
+    the per-CTA partial sums."""
+    from newton_sph_dev_b200.solvers import SolverSPH
+
+    model, cfg, x, v, flags = _scene(seed=12)
+    solver = SolverSPH(model, cfg)
+    m = random_model(6)
+    p = solver.step_params(4e-4)
+    out = []
+    for k in (0, ctas_per_sm):
+        solver.set_surrogate_launch(k)
+        stats = torch.zeros(4, device=DEV)
+        xs, vs = torch.empty_like(model.particle_q), model.particle_qd.clone()
+        solver.step_surrogate_raw(model.particle_q, model.particle_qd, xs, vs, p, m, 1.0, stats)
+        torch.cuda.synchronize()
+        out.append((xs, vs, stats))
+    solver.set_surrogate_launch(0)
+    assert solver.status() == 0
+    assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
+    torch.testing.assert_close(out[0][2], out[1][2], rtol=1e-5, atol=0.0)

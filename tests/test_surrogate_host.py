@@ -91,3 +91,29 @@ def test_fallback_monitor():
     assert m.use_surrogate()
     m.end_window(math.nan)  # a non-finite monitor value trips too
     assert not m.use_surrogate() and m.trips == 2
+
+
+def test_fallback_monitor_backoff():
+    """With backoff, each failure in a row doubles the suspension (capped);
+    a window that passes resets it."""
+    m = FallbackMonitor(threshold=0.01, cooldown=1, backoff=True, max_cooldown=4)
+
+    def plain_windows():
+        k = 0
+        while not m.use_surrogate():
+            m.end_window(None)
+            k += 1
+        return k
+
+    assert m.end_window(0.5) is True
+    assert plain_windows() == 1
+    assert m.end_window(0.5) is True
+    assert plain_windows() == 2
+    assert m.end_window(math.nan) is True
+    assert plain_windows() == 4
+    assert m.end_window(0.5) is True
+    assert plain_windows() == 4  # capped
+    assert m.end_window(0.001) is False  # passes: the next failure starts over
+    assert m.end_window(0.5) is True
+    assert plain_windows() == 1
+    assert m.trips == 5
