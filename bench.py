@@ -113,7 +113,25 @@ def worlds_layout(w):
     return out
 
 
-def make_worlds_scene(name: str, device: str, max_worlds: int | None = None):
+def partition_worlds(sizes, parts: int) -> list[list[int]]:
+    """Split worlds over `parts` ranks by particle count: largest first, each
+    to the least-loaded rank (ties to the lowest rank); each rank keeps its
+    worlds in their original order. Deterministic, so every rank computes the
+    same split without communication."""
+    loads = [0] * parts
+    out = [[] for _ in range(parts)]
+    for k in sorted(range(len(sizes)), key=lambda i: (-int(sizes[i]), i)):
+        r = min(range(parts), key=lambda j: (loads[j], j))
+        out[r].append(k)
+        loads[r] += int(sizes[k])
+    return [sorted(o) for o in out]
+
+
+def world_sizes(layout) -> list[int]:
+    return [a * b * c for (a, b, c), _ in layout]
+
+
+def make_worlds_scene(name: str, device: str, max_worlds: int | None = None, subset: list[int] | None = None):
     import newton_sph_dev_b200 as nsph
     from newton_sph_dev_b200.solvers import SolverSPH
 
@@ -121,6 +139,8 @@ def make_worlds_scene(name: str, device: str, max_worlds: int | None = None):
     layout = worlds_layout(w)
     if max_worlds is not None:
         layout = layout[:max_worlds]
+    if subset is not None:  # this rank's share of the worlds
+        layout = [layout[k] for k in subset]
     b = nsph.ModelBuilder()
     cfgs = []
     for shape, s in layout:
@@ -135,11 +155,17 @@ def make_worlds_scene(name: str, device: str, max_worlds: int | None = None):
     return model, cfgs, w
 
 
-def make_scene(name: str, device: str):
+def make_scene(name: str, device: str, rank: int = 0, world: int = 1):
+    """The workload's scene; batched worlds are split over the ranks (each
+    rank builds its share, see partition_worlds), other workloads are
+    replicated."""
     import torch
 
     if "worlds" in WORKLOADS[name]:
-        return make_worlds_scene(name, device)
+        subset = None
+        if world > 1:
+            subset = partition_worlds(world_sizes(worlds_layout(WORKLOADS[name])), world)[rank]
+        return make_worlds_scene(name, device, subset=subset)
     import newton_sph_dev_b200 as nsph
     from newton_sph_dev_b200.solvers import SolverSPH
 
@@ -559,8 +585,10 @@ def run_gpu(args):
 
     from newton_sph_dev_b200.solvers import SolverSPH
 
-    model, cfg, w = make_scene(args.workload, str(device))
+    model, cfg, w = make_scene(args.workload, str(device), rank, world)
     n = model.particle_count
+    sharded = "worlds" in w and world > 1  # the worlds are split over the ranks, not replicated
+    n_job = sum(world_sizes(worlds_layout(w))) if sharded else world * n
     solver = SolverSPH(model, cfg)
     dt = w["dt"]
     s0, s1 = model.state(), model.state()
@@ -632,7 +660,7 @@ def run_gpu(args):
     status = solver.status()
     timed_state = s1 if args.steps % 2 == 1 else s0  # the last timed step's output
 
-    value = world * n * args.steps / (total_ms_max * 1e-3)
+    value = n_job * args.steps / (total_ms_max * 1e-3)
     ms_per_step = total_ms_max / args.steps
 
     # ---- end to end through the public API with host buffers ----
@@ -650,7 +678,7 @@ def run_gpu(args):
     e2e_ms = pipelined_e2e(model, lambda a, b: solver.step(a, b, None, None, dt), hx, hv, e2e_steps, device)
     barrier(device)
     e2e_ms_max = max_over_ranks(e2e_ms, device)
-    e2e_value = world * n * e2e_steps / (e2e_ms_max * 1e-3)
+    e2e_value = n_job * e2e_steps / (e2e_ms_max * 1e-3)
     # (b) serial host round trip: upload, step, download, and the next step
     # starts from the downloaded state
     serial_ms = 0.0
@@ -744,22 +772,24 @@ def run_gpu(args):
             "warmup": args.warmup,
             "ms_per_step": ms_per_step,
             "higher_is_better": True,
-            "scaling": "weak",
+            "scaling": "strong" if sharded else "weak",
             "vs_baseline": None,
             "dtype": "f32",
             "data": "synthetic",
             "config": {
                 "workload": args.workload,
-                "particles": n,
+                "particles": n_job if sharded else n,
                 "desc": w["desc"],
                 "grid_dims": list(solver.grid_dims) if solver.grid_dims is not None else "per world (tight)",
-                "worlds": model.world_count,
+                "worlds": w["worlds"] if sharded else model.world_count,
                 "graph": use_graph,
                 "launch": {"threads": solver.launch[0], "blocks_per_sm": solver.launch[1],
                            "autotuned": tuned is not None} if hasattr(solver, "launch") else "default",
                 "l2": "flushed (256 MiB write) before every timed step, outside the timed interval",
                 "relaxation_steps": relax,
-                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                "parallelism": (f"worlds split over {world} GPUs by particle count (rank 0: {model.world_count} "
+                                f"worlds, {n} particles); no collective in the step" if sharded
+                                else f"replicas x{world}" if world > 1 else "single GPU"),
             },
             "phase_ms_per_step": {k: v / args.steps for k, v in phase.items()},
             "roofline": roofline,

@@ -107,15 +107,6 @@ typedef struct nsph_grid_view {
 NSPH_API int nsph_grid_get_view(const nsph_grid* grid, nsph_grid_view* view);
 /* Number of kernels the last nsph_grid_build launched. */
 NSPH_API int nsph_grid_last_launches(const nsph_grid* grid);
-/* Builds whose cell table holds at most 16 cells per point (single world, at
- * most 2^26 cells) sort by cell counts, with a single-pass scan of the cell
- * table in tiles of 8192 cells: each tile finds its offset by polling its
- * predecessors' published sums (decoupled look-back) and, after `polls`
- * unanswered polls, sums the counts in front of it itself. The result does
- * not depend on the limit. polls = 0 skips the look-back (every tile sums
- * its prefix itself); polls < 0 restores the default (16384). A test hook:
- * the look-back never waits long, since tiles are taken in order. */
-NSPH_API int nsph_grid_set_scan_polls(nsph_grid* grid, int polls);
 
 /* Batched hash_grid_query(grid, pos, radius) + hash_grid_query_next:
  * enumerate, for each of num_queries positions (device, num_queries x 3
@@ -559,16 +550,20 @@ NSPH_API int nsph_sph_step_surrogate(nsph_sph* solver, const nsph_sph_params* pa
                                      const float* gravity, int world_count,
                                      float* x_out, float* v_out, float* rho_out, float* p_out, float* stats,
                                      void* stream);
-/* Resident CTAs per SM of the surrogate step's fused kernel (its grid is
- * SMs x ctas_per_sm persistent CTAs of 128 particles, about 34 KB of shared
- * memory each); at most as many as fit (6 on a B200). 0 = the default, 5:
- * the kernel's preferred shared-memory carveout is set to what those CTAs
- * need, so that the rest of each SM's unified L1 / shared storage caches the
- * neighbour gathers (at 6 only about 28 KB of L1 is left). The carveout is
- * a property of the kernel, so it applies to every solver of the process.
- * Results do not depend on the count. nsph_sph_enable_surrogate applies the
- * default; call this after it. */
-NSPH_API int nsph_sph_set_surrogate_launch(nsph_sph* solver, int ctas_per_sm);
+/* Launch shape of the surrogate step's fused kernel: persistent CTAs, each
+ * taking tiles of 128 particles. tiles_per_cta = 1: CTAs of 128 threads and
+ * about 34 KB of shared memory; 2: CTAs of 256 threads whose two tiles share
+ * one copy of the weights (about 53 KB) and run their MMA chains
+ * independently; 0 = the default (1). ctas_per_sm: resident CTAs per SM, at
+ * most as many as fit (6 of one tile, 4 of two on a B200); 0 = the default
+ * (5 of one tile, as many as fit of two). The kernel's preferred
+ * shared-memory carveout is set to what those CTAs need, so that the rest of
+ * each SM's unified L1 / shared storage caches the neighbour gathers (6 CTAs
+ * of one tile leave only about 28 KB of L1). The carveout is a property of
+ * the kernel, so it applies to every solver of the process. Results do not
+ * depend on the launch shape. nsph_sph_enable_surrogate applies the default;
+ * call this after it. */
+NSPH_API int nsph_sph_set_surrogate_launch(nsph_sph* solver, int ctas_per_sm, int tiles_per_cta);
 
 /* The MLP on its own (training and checks).
  * nsph_mlp_model_floats: size of the model buffer in floats.

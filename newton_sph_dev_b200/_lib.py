@@ -159,7 +159,6 @@ SIGNATURES = [
     ("nsph_grid_build", ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_float, c_void_p]),
     ("nsph_grid_get_view", ctypes.c_int, [c_void_p, ctypes.POINTER(NsphGridView)]),
     ("nsph_grid_last_launches", ctypes.c_int, [c_void_p]),
-    ("nsph_grid_set_scan_polls", ctypes.c_int, [c_void_p, ctypes.c_int]),
     ("nsph_grid_query", ctypes.c_int, [c_void_p, c_void_p, ctypes.c_int, ctypes.c_float, c_void_p, c_void_p, c_void_p, c_void_p]),
     (
         "nsph_grid_build_noalloc",
@@ -293,7 +292,7 @@ SIGNATURES = [
         + [c_void_p] * 3
         + [c_void_p],
     ),
-    ("nsph_sph_set_surrogate_launch", ctypes.c_int, [c_void_p, ctypes.c_int]),
+    ("nsph_sph_set_surrogate_launch", ctypes.c_int, [c_void_p, ctypes.c_int, ctypes.c_int]),
     ("nsph_sph_set_surrogate_wait_limit", ctypes.c_int, [c_void_p, ctypes.c_int]),
     (
         "nsph_sph_step_surrogate",

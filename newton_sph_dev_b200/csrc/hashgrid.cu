@@ -298,57 +298,37 @@ __global__ void k_ranges(const int* __restrict__ cells, int n, int2* __restrict_
 // of three radix passes.
 //   k_cc_count        cell of each point (original order), its slot in the
 //                     cell from an atomic counter (an arbitrary order within a
-//                     cell); clears the ranges of the previous build's cells
-//                     and the scan's look-back words
-//   k_cc_scan_ranges  single-pass exclusive scan of the counts in tiles of
-//                     kCsTile cells, each tile's offset found by decoupled
-//                     look-back over its predecessors; writes the ranges of
-//                     the occupied cells (the counts stay as they are, so a
-//                     tile can always sum the counts in front of it itself)
+//                     cell), and the point counts per tile of kCsTile cells;
+//                     both atomics warp-aggregated (one per distinct cell or
+//                     tile of a warp); clears the ranges of the previous
+//                     build's cells
+//   k_cc_scan_ranges  per tile: its offset (the sum of the earlier tiles'
+//                     counts), the exclusive scan of its cells' counts, the
+//                     ranges of its occupied cells
 //   k_cc_scatter      point -> start + slot (the arbitrary order), with its cell
 //   k_cc_rank         per cell-ordered position: its point goes to start +
 //                     (points of its cell with a smaller index), the stable
 //                     order; writes point_cells / point_ids, gathers the
 //                     sorted mirrors in SPH mode, and zeroes the cell's count
-// The result is identical to the stable radix sort's.
+//                     and the tile counts for the next build
+// No kernel waits on another block. The result is identical to the stable
+// radix sort's.
 // --------------------------------------------------------------------------
 constexpr int kCcPoints = 4;     // points per thread of k_cc_count / k_cc_scatter
 constexpr int kCsThreads = 256;  // k_cc_scan_ranges
 constexpr int kCsPer = 32;       // cells per thread (eight int4 loads)
 constexpr int kCsTile = kCsThreads * kCsPer;
-// look-back word of a tile: flag in bits 32-33, value in bits 0-31
-constexpr unsigned long long kTileAggregate = 1ull << 32;  // the tile's own sum
-constexpr unsigned long long kTileInclusive = 2ull << 32;  // the sum of all tiles up to and including it
-constexpr unsigned long long kTileFlags = 3ull << 32;
-// Polls of a predecessor that has not published yet before the tile sums
-// the counts in front of it by itself. Tiles are taken in order from a
-// counter, so a predecessor is always running and publishes within
-// microseconds; the limit only bounds the wait. A limit of 0 skips the
-// look-back (every tile sums its prefix itself: the same result, slower).
-constexpr int kLookbackPolls = 1 << 14;
-
-__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long* p)
-{
-    unsigned long long v;
-    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-
-__device__ __forceinline__ void st_relaxed_u64(unsigned long long* p, unsigned long long v)
-{
-    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
-}
 
 __global__ void __launch_bounds__(256) k_cc_count(const float* __restrict__ points, int n, float inv, int dx, int dy,
-                                                  int dz, int* __restrict__ count, int* __restrict__ cells,
-                                                  int* __restrict__ slots, const int* __restrict__ prev_cells,
-                                                  int prev_n, int2* __restrict__ ranges,
-                                                  unsigned long long* __restrict__ tile_state, int tiles,
-                                                  unsigned* __restrict__ status)
+                                                  int dz, int* __restrict__ count, int* __restrict__ tile_count,
+                                                  int* __restrict__ cells, int* __restrict__ slots,
+                                                  const int* __restrict__ prev_cells, int prev_n,
+                                                  int2* __restrict__ ranges, unsigned* __restrict__ status)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int stride = gridDim.x * blockDim.x;
-    if (t <= tiles) tile_state[t] = 0ull;  // look-back words, then the tile counter
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = lanemask_lt();
     // the previous build's cells: the first sorted entry of each clears its range
     for (int k = t; k < prev_n; k += stride) {
         const int c = prev_cells[k];
@@ -359,7 +339,7 @@ __global__ void __launch_bounds__(256) k_cc_count(const float* __restrict__ poin
 #pragma unroll
     for (int u = 0; u < kCcPoints; ++u) {
         const int i = t + u * stride;
-        c[u] = 0;
+        c[u] = -1;
         if (i < n) {
             const float x = points[3 * (size_t)i + 0];
             const float y = points[3 * (size_t)i + 1];
@@ -369,29 +349,41 @@ __global__ void __launch_bounds__(256) k_cc_count(const float* __restrict__ poin
             cells[i] = c[u];
         }
     }
+    // i = t + u * stride is uniform in u across the warp's lanes up to n, so
+    // the lanes with i < n are a prefix of the warp
 #pragma unroll
     for (int u = 0; u < kCcPoints; ++u) {
         const int i = t + u * stride;
-        if (i < n) slots[i] = atomicAdd(count + c[u], 1);
+        const unsigned active = __ballot_sync(0xffffffffu, i < n);
+        if (i < n) {
+            const unsigned same = __match_any_sync(active, c[u]);
+            const int leader = __ffs(same) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(count + c[u], __popc(same));
+            base = __shfl_sync(same, base, leader);
+            slots[i] = base + __popc(same & lt);
+            const int tl = c[u] / kCsTile;
+            const unsigned tile_same = __match_any_sync(active, tl);
+            if (lane == __ffs(tile_same) - 1) atomicAdd(tile_count + tl, __popc(tile_same));
+        }
     }
     if (bad && status) atomicOr(status, (unsigned)NSPH_STATUS_NONFINITE_INPUT);
 }
 
-__global__ void __launch_bounds__(kCsThreads) k_cc_scan_ranges(const int* __restrict__ count, long long ncells,
-                                                               int2* __restrict__ ranges,
-                                                               unsigned long long* __restrict__ tile_state, int tiles,
-                                                               int max_polls)
+__global__ void __launch_bounds__(kCsThreads) k_cc_scan_ranges(const int* __restrict__ count,
+                                                               const int* __restrict__ tile_count, long long ncells,
+                                                               int2* __restrict__ ranges)
 {
-    __shared__ int s_tile, s_base;
     __shared__ int ws[kCsThreads / 32];
-    __shared__ long long s_part[kCsThreads / 32];
+    __shared__ int s_base[kCsThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (threadIdx.x == 0) s_tile = atomicAdd(reinterpret_cast<int*>(tile_state + tiles), 1);
-    __syncthreads();
-    const int tile = s_tile;
+    const int tile = blockIdx.x;
+    // the tile's offset: the counts of the tiles before it
+    int before = 0;
+    for (int q = threadIdx.x; q < tile; q += kCsThreads) before += tile_count[q];
     const long long c0 = (long long)tile * kCsTile + (long long)threadIdx.x * kCsPer;
     int v[kCsPer];
-    if (c0 + kCsPer <= ncells) {  // count is 256-byte aligned and c0 a multiple of 16
+    if (c0 + kCsPer <= ncells) {  // count is 256-byte aligned and c0 a multiple of 32
         const int4* p4 = reinterpret_cast<const int4*>(count + c0);
 #pragma unroll
         for (int q = 0; q < kCsPer / 4; ++q) {
@@ -413,74 +405,18 @@ __global__ void __launch_bounds__(kCsThreads) k_cc_scan_ranges(const int* __rest
     for (int o = 1; o < 32; o <<= 1) {
         const int y = __shfl_up_sync(0xffffffffu, inc, o);
         if (lane >= o) inc += y;
+        before += __shfl_xor_sync(0xffffffffu, before, o);
     }
     if (lane == 31) ws[warp] = inc;
+    if (lane == 0) s_base[warp] = before;
     __syncthreads();
-    if (warp == 0) {
-        int w = lane < kCsThreads / 32 ? ws[lane] : 0;
+    int base = 0, warp_off = 0;
 #pragma unroll
-        for (int o = 1; o < kCsThreads / 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += y;
-        }
-        if (lane < kCsThreads / 32) ws[lane] = w;  // inclusive warp totals
-        const int total = __shfl_sync(0xffffffffu, w, kCsThreads / 32 - 1);
-        // warp-wide look-back: lane l reads the word of tile t - l; the window
-        // moves back 32 tiles while all of it holds aggregates only, and ends
-        // at the nearest inclusive prefix (tiles before 0 count as an
-        // inclusive 0)
-        int base = 0;
-        if (tile == 0) {
-            if (lane == 0) st_relaxed_u64(tile_state, kTileInclusive | (unsigned)total);
-        } else if (max_polls == 0) {
-            base = -1;
-        } else {
-            if (lane == 0) st_relaxed_u64(tile_state + tile, kTileAggregate | (unsigned)total);
-            int t = tile - 1, polls = 0;
-            while (true) {
-                const int idx = t - lane;
-                const unsigned long long word = idx >= 0 ? ld_relaxed_u64(tile_state + idx) : kTileInclusive;
-                const unsigned long long f = word & kTileFlags;
-                const unsigned incl = __ballot_sync(0xffffffffu, f == kTileInclusive);
-                const unsigned none = __ballot_sync(0xffffffffu, f == 0ull);
-                const int first = incl ? __ffs(incl) - 1 : 31;  // the lanes that count: 0 .. first
-                const unsigned need = first == 31 ? 0xffffffffu : ((2u << first) - 1u);
-                if (none & need) {  // a tile in the window has not published yet: poll again
-                    if (++polls > max_polls) {
-                        base = -1;  // sum the counts in front of the tile instead
-                        break;
-                    }
-                    __nanosleep(64);
-                    continue;
-                }
-                int val = lane <= first ? (int)(unsigned)word : 0;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
-                base += val;
-                if (incl) break;
-                t -= 32;
-                polls = 0;
-            }
-            if (base >= 0 && lane == 0) st_relaxed_u64(tile_state + tile, kTileInclusive | (unsigned)(base + total));
-        }
-        if (lane == 0) s_base = base;
+    for (int w = 0; w < kCsThreads / 32; ++w) {
+        base += s_base[w];
+        warp_off += w < warp ? ws[w] : 0;
     }
-    __syncthreads();
-    int base = s_base;
-    if (base < 0) {  // only after kLookbackPolls unanswered polls
-        long long part = 0;
-        for (long long c = threadIdx.x; c < (long long)tile * kCsTile; c += kCsThreads) part += count[c];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-        if (lane == 0) s_part[warp] = part;
-        __syncthreads();
-        long long b = 0;
-#pragma unroll
-        for (int k = 0; k < kCsThreads / 32; ++k) b += s_part[k];
-        base = (int)b;
-        if (threadIdx.x == 0) st_relaxed_u64(tile_state + tile, kTileInclusive | (unsigned)(base + ws[kCsThreads / 32 - 1]));
-    }
-    int start = base + (warp > 0 ? ws[warp - 1] : 0) + inc - sum;
+    int start = base + warp_off + inc - sum;
 #pragma unroll
     for (int u = 0; u < kCsPer; ++u) {
         if (v[u]) ranges[c0 + u] = make_int2(start, start + v[u]);  // empty cells keep {0, 0}
@@ -522,10 +458,12 @@ __global__ void __launch_bounds__(256) k_cc_scatter(const int* __restrict__ cell
 // write neighbouring positions
 __global__ void __launch_bounds__(256) k_cc_rank(const int* __restrict__ tmp_cells, const int2* __restrict__ ranges,
                                                  const int* __restrict__ tmp, int n, int* __restrict__ count,
+                                                 int* __restrict__ tile_count, int tiles,
                                                  int* __restrict__ point_cells, int* __restrict__ point_ids,
                                                  GatherArgs gather, bool do_gather)
 {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < tiles) tile_count[q] = 0;  // read by k_cc_scan_ranges, which has finished
     if (q >= n) return;
     const int i = tmp[q];
     const int c = tmp_cells[q];
@@ -637,8 +575,9 @@ int grid_init(Grid& g, int dx, int dy, int dz, int device)
     if (nc <= kCountMaxCells) {  // the counting build's per-cell counts
         NSPH_CUDA_TRY(cudaMalloc(&g.cell_count, sizeof(int) * nc));
         NSPH_CUDA_TRY(cudaMemset(g.cell_count, 0, sizeof(int) * nc));
-        NSPH_CUDA_TRY(cudaMalloc(&g.tile_state,
-                                 sizeof(unsigned long long) * (size_t)((nc + kCsTile - 1) / kCsTile + 1)));
+        const size_t tiles = (size_t)((nc + kCsTile - 1) / kCsTile);
+        NSPH_CUDA_TRY(cudaMalloc(&g.tile_count, sizeof(int) * tiles));
+        NSPH_CUDA_TRY(cudaMemset(g.tile_count, 0, sizeof(int) * tiles));
     }
     // load every kernel now, so that a later stream capture never triggers
     // lazy module loading
@@ -736,7 +675,7 @@ void grid_free(Grid& g)
     cudaFree(g.hist);
     cudaFree(g.cell_ranges);
     cudaFree(g.cell_count);
-    cudaFree(g.tile_state);
+    cudaFree(g.tile_count);
     cudaFree(g.worlds);
     g = Grid();
 }
@@ -807,18 +746,19 @@ int count_build(Grid& g, const float* points, int n, float cell_inv, const Gathe
 {
     const int tiles = (int)((g.ncells + kCsTile - 1) / kCsTile);
     const int per_block = 256 * kCcPoints;
-    const int blocks = std::max((n + per_block - 1) / per_block, (tiles + 1 + 255) / 256);
-    k_cc_count<<<blocks, 256, 0, stream>>>(points, n, cell_inv, g.dx, g.dy, g.dz, g.cell_count, g.keys_a, g.vals_a,
-                                           g.point_cells, prev_n, g.cell_ranges, g.tile_state, tiles, status);
+    const int blocks = (n + per_block - 1) / per_block;
+    k_cc_count<<<blocks, 256, 0, stream>>>(points, n, cell_inv, g.dx, g.dy, g.dz, g.cell_count, g.tile_count,
+                                           g.keys_a, g.vals_a, g.point_cells, prev_n, g.cell_ranges, status);
     NSPH_LAUNCH_CHECK("k_cc_count");
-    k_cc_scan_ranges<<<tiles, kCsThreads, 0, stream>>>(g.cell_count, g.ncells, g.cell_ranges, g.tile_state, tiles,
-                                                       g.scan_polls < 0 ? kLookbackPolls : g.scan_polls);
+    k_cc_scan_ranges<<<tiles, kCsThreads, 0, stream>>>(g.cell_count, g.tile_count, g.ncells, g.cell_ranges);
     NSPH_LAUNCH_CHECK("k_cc_scan_ranges");
-    k_cc_scatter<<<(n + per_block - 1) / per_block, 256, 0, stream>>>(g.keys_a, g.vals_a, g.cell_ranges, n, g.keys_b,
-                                                                       g.vals_b);
+    k_cc_scatter<<<blocks, 256, 0, stream>>>(g.keys_a, g.vals_a, g.cell_ranges, n, g.keys_b, g.vals_b);
     NSPH_LAUNCH_CHECK("k_cc_scatter");
-    k_cc_rank<<<(n + 255) / 256, 256, 0, stream>>>(g.vals_b, g.cell_ranges, g.keys_b, n, g.cell_count, g.point_cells,
-                                                   g.point_ids, gather ? *gather : GatherArgs{}, gather != nullptr);
+    // n >= tiles (the policy keeps the table at most 16 cells per point, and
+    // a tile holds 8192 cells), so the rank grid also covers the tile counts
+    k_cc_rank<<<(n + 255) / 256, 256, 0, stream>>>(g.vals_b, g.cell_ranges, g.keys_b, n, g.cell_count, g.tile_count,
+                                                   tiles, g.point_cells, g.point_ids, gather ? *gather : GatherArgs{},
+                                                   gather != nullptr);
     NSPH_LAUNCH_CHECK("k_cc_rank");
     nl += 4;
     return NSPH_OK;
@@ -912,13 +852,6 @@ extern "C" int nsph_grid_reserve(nsph_grid* grid, int num_points)
         return fail(NSPH_ERR_OUT_OF_MEMORY, "grid reserve: contact mirror allocation failed");
     }
     grid->mirror_cap = grid->g.capacity;
-    return NSPH_OK;
-}
-
-extern "C" int nsph_grid_set_scan_polls(nsph_grid* grid, int polls)
-{
-    if (!grid) return fail(NSPH_ERR_INVALID_ARG, "null grid");
-    grid->g.scan_polls = polls < 0 ? -1 : polls;
     return NSPH_OK;
 }
 

@@ -284,4 +284,130 @@ __device__ __forceinline__ float mlp_denorm(const S& s, const float (&y)[kMlpOut
     return fmaf(y[o], s.norm[kOutStd - kInMean + o], s.norm[kOutMean - kInMean + o]);
 }
 
+// ---- inference with several tiles per CTA ------------------------------------
+// kGroups groups of 128 threads share one copy of the weights; group g owns
+// its input and hidden tiles, its completion barrier and TMEM columns
+// [64 g, 64 g + 64). Groups synchronise on their own named barriers
+// (ids 1 .. kGroups), so one group's MMA round trips overlap the other
+// groups' work. TMEM lane quadrant q of a group is accessed by its warp
+// q (warp index mod 4), as tcgen05.ld requires.
+template <int kGroups>
+struct MlpFwdGroupSmem {
+    static_assert(kGroups == 2, "named barriers 1 and 2 serve two groups");
+    __nv_bfloat16 w1t[kMlpHid * kMlpIn];
+    __nv_bfloat16 w2t[kMlpHid * kMlpHid];
+    __nv_bfloat16 w3t[kMlpOutPad * kMlpHid];
+    __nv_bfloat16 x[kGroups][kMlpTile * kMlpIn];
+    __nv_bfloat16 h1[kGroups][kMlpTile * kMlpHid];  // silu(z1), then silu(z2)
+    float b1[kMlpHid], b2[kMlpHid], b3[kMlpOutPad];
+    float norm[kMlpModelFloats - kInMean];
+    uint64_t bar[kGroups];
+    uint32_t tmem;
+};
+
+// named barrier of group g (id 1 + g, 128 threads), ordering this thread's
+// shared-memory writes before the tensor core's reads and tcgen05 operations
+// across the barrier
+// (ids are immediates, so the kernel reserves only the barriers it names;
+// groups 0 and 1)
+__device__ __forceinline__ void mlp_group_sync(int g)
+{
+    umma::fence_smem_to_async();
+    umma::fence_before_sync();
+    if (g == 0)
+        asm volatile("barrier.cta.sync 1, 128;" ::: "memory");
+    else
+        asm volatile("barrier.cta.sync 2, 128;" ::: "memory");
+    umma::fence_after_sync();
+}
+
+// AND of v over group g's 128 threads (named barrier 1 + g)
+__device__ __forceinline__ bool mlp_group_and(bool v, int g)
+{
+    uint32_t r;
+    if (g == 0)
+        asm volatile(
+            "{\n.reg .pred p, q;\nsetp.ne.u32 q, %1, 0;\nbarrier.cta.red.and.pred p, 1, 128, q;\n"
+            "selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(r)
+            : "r"((uint32_t)v)
+            : "memory");
+    else
+        asm volatile(
+            "{\n.reg .pred p, q;\nsetp.ne.u32 q, %1, 0;\nbarrier.cta.red.and.pred p, 2, 128, q;\n"
+            "selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(r)
+            : "r"((uint32_t)v)
+            : "memory");
+    return r != 0;
+}
+
+// wait for the next completion of group g's barrier (the outcome is uniform
+// over the group); the phase advances on success
+template <int kGroups>
+__device__ __forceinline__ bool mlp_group_wait(MlpFwdGroupSmem<kGroups>& s, int g, uint32_t& phase, int limit)
+{
+    const bool ok = mlp_group_and(umma::mbar_wait(&s.bar[g], phase, limit), g);
+    if (ok) phase ^= 1u;
+    umma::fence_after_sync();
+    return ok;
+}
+
+// stage group g's inputs: row `row` of its tile
+template <int kGroups>
+__device__ __forceinline__ void mlp_group_stage_input(MlpFwdGroupSmem<kGroups>& s, int g, int row,
+                                                      const float (&feat)[kMlpIn])
+{
+    float v[kMlpIn];
+#pragma unroll
+    for (int j = 0; j < kMlpIn; ++j) v[j] = (feat[j] - s.norm[j]) * s.norm[kMlpIn + j];
+    store_row8(s.x[g], row, 0, kMlpIn, v);
+    store_row8(s.x[g], row, 8, kMlpIn, v + 8);
+}
+
+// forward of group g's tile (inputs staged and made visible with
+// mlp_group_sync): z1, z2 and the output take the group's TMEM columns in
+// turn; row 0 of the group issues the MMAs. Returns false if a wait gave up
+// (then the group issues no further MMA).
+template <int kGroups>
+__device__ bool mlp_group_forward_tile(MlpFwdGroupSmem<kGroups>& s, int g, int row, uint32_t tmem, uint32_t& phase,
+                                       float (&y)[kMlpOut], int wait_limit)
+{
+    using namespace umma;
+    const uint32_t col = (uint32_t)(kMlpFwdCols * g);
+    const uint32_t tmem_row = tmem + ((uint32_t)(((threadIdx.x >> 5) & 3) * 32) << 16);
+    const uint32_t xa = smem_addr(s.x[g]), ha = smem_addr(s.h1[g]);
+    const uint32_t w1a = smem_addr(s.w1t), w2a = smem_addr(s.w2t), w3a = smem_addr(s.w3t);
+    if (row == 0) {
+        mma_bf16(tmem + col, smem_desc(xa, 128, 256), smem_desc(w1a, 128, 256), idesc_bf16_f32(128, kMlpHid), 0);
+        mma_commit(&s.bar[g]);
+    }
+    if (!mlp_group_wait(s, g, phase, wait_limit)) return false;
+    mlp_hidden_epilogue(tmem_row, col, s.b1, s.h1[g], row);
+    mlp_group_sync(g);
+    if (row == 0) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            mma_bf16(tmem + col, smem_desc(ha + 256 * k, 128, 1024), smem_desc(w2a + 256 * k, 128, 1024),
+                     idesc_bf16_f32(128, kMlpHid), k > 0);
+        mma_commit(&s.bar[g]);
+    }
+    if (!mlp_group_wait(s, g, phase, wait_limit)) return false;
+    mlp_hidden_epilogue(tmem_row, col, s.b2, s.h1[g], row);
+    mlp_group_sync(g);
+    if (row == 0) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            mma_bf16(tmem + col, smem_desc(ha + 256 * k, 128, 1024), smem_desc(w3a + 256 * k, 128, 1024),
+                     idesc_bf16_f32(128, kMlpOutPad), k > 0);
+        mma_commit(&s.bar[g]);
+    }
+    if (!mlp_group_wait(s, g, phase, wait_limit)) return false;
+    float v[16];
+    tmem_ld16(tmem_row + col, v);
+#pragma unroll
+    for (int o = 0; o < kMlpOut; ++o) y[o] = v[o] + s.b3[o];
+    return true;
+}
+
 }  // namespace nsph

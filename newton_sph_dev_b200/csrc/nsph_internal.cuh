@@ -213,11 +213,9 @@ struct Grid {
     // cell table (ncells entries of {start, end})
     int2* cell_ranges = nullptr;
     // counting build (single world, at most kCountMaxCells cells): per-cell
-    // counts (all zero between builds), and the cell scan's per-tile look-back
-    // words followed by its tile counter
+    // counts and per-tile (8192 cells) counts, all zero between builds
     int* cell_count = nullptr;
-    unsigned long long* tile_state = nullptr;
-    int scan_polls = -1;  // the cell scan's look-back wait (-1: the default limit)
+    int* tile_count = nullptr;
 
     GridDev view() const { return GridDev{dx, dy, dz, cell_inv, cell_ranges, point_ids}; }
 };

@@ -1343,6 +1343,79 @@ __global__ void __launch_bounds__(kMlpTile, 6) k_surrogate_fused(const float* __
     mlp_cta_end(s, tmem, kMlpFwdCols, !ok, phase);
 }
 
+// k_surrogate_fused with kGroups tiles per CTA: groups of 128 threads share
+// one copy of the weights (12 KB) and run their tiles independently (own
+// input / hidden tiles, completion barrier, 64 TMEM columns, named barriers),
+// so one group's MMA round trips overlap the other groups' gathers, and a CTA
+// of 2 groups holds 53 KB of shared memory for 8 warps instead of 67 KB.
+// Same per-particle arithmetic as k_surrogate_fused; the timeout rule
+// applies per group.
+template <int kGroups>
+__global__ void __launch_bounds__(kGroups * kMlpTile, 6 / kGroups)
+    k_surrogate_fused_groups(const float* __restrict__ model, float acc_scale, int wait_limit, GridDev g,
+                             const float4* __restrict__ xs, const float4* __restrict__ vs,
+                             const float2* __restrict__ aux, const float2* __restrict__ rp, int n,
+                             const __grid_constant__ nsph_sph_params p, const int4* __restrict__ nbr,
+                             const int* __restrict__ ncnt, const StepOut o, float* __restrict__ cpart)
+{
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    auto& s = *reinterpret_cast<MlpFwdGroupSmem<kGroups>*>(smem_raw);
+    const int grp = threadIdx.x / kMlpTile, row = threadIdx.x % kMlpTile;
+    mlp_stage_weights(model, s);
+    if (threadIdx.x < kGroups) umma::mbar_init(&s.bar[threadIdx.x], 1);
+    if (threadIdx.x < 32) umma::tmem_alloc(&s.tmem, kGroups * kMlpFwdCols);
+    mlp_sync();
+    const uint32_t tmem = s.tmem;
+    uint32_t phase = 0;
+    bool ok = true;
+    float csum = 0.f, ccount = 0.f;
+    const int tiles = (n + kMlpTile - 1) / kMlpTile;
+    for (int t = blockIdx.x * kGroups + grp; t < tiles; t += gridDim.x * kGroups) {
+        const int k = t * kMlpTile + row;
+        const int kk = k < n ? k : 0;
+        const float4 xi = xs[kk], vi = vs[kk];
+        float f[kFeat];
+        ForceAcc acc;
+        if (k < n) {
+            particle_features(g, xs, vs, aux, rp, nbr, ncnt, n, k, xi, vi, p, f, acc, csum, ccount);
+        } else {
+            acc = ForceAcc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+            for (int j = 0; j < kFeat; ++j) f[j] = 0.f;
+        }
+        float y[kMlpOut] = {0.f, 0.f, 0.f};
+        if (ok) {  // uniform across the group (mlp_group_wait makes the outcome uniform)
+            mlp_group_stage_input(s, grp, row, f);
+            mlp_group_sync(grp);
+            ok = mlp_group_forward_tile(s, grp, row, tmem, phase, y, wait_limit);
+        }
+        if (k < n) {
+            const int attr = __float_as_int(vi.w);
+            if (ok && (attr & kAttrDynamic)) {
+                acc.ax = __fadd_rn(acc.ax, acc_scale * mlp_denorm(s, y, 0));
+                acc.ay = __fadd_rn(acc.ay, acc_scale * mlp_denorm(s, y, 1));
+                acc.az = __fadd_rn(acc.az, acc_scale * mlp_denorm(s, y, 2));
+            }
+            integrate_out((size_t)g.ids[k], xi, vi, attr, rp[k], acc, p, p.dt, o);
+        }
+    }
+    if (!ok && o.status && row == 0) atomicOr(o.status, (unsigned)NSPH_STATUS_SURROGATE_TIMEOUT);
+    // a group whose wait gave up waits once more (bounded) for the completion
+    // it left outstanding, before the CTA frees its TMEM
+    if (!ok) umma::mbar_wait(&s.bar[grp], phase, kMlpWaitLimit);
+    csum = block_sum(csum);
+    __syncthreads();
+    ccount = block_sum(ccount);
+    if (threadIdx.x == 0) {
+        cpart[2 * blockIdx.x] = csum;
+        cpart[2 * blockIdx.x + 1] = ccount;
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    if (threadIdx.x < 32) umma::tmem_dealloc(tmem, kGroups * kMlpFwdCols);
+}
+
 // sorted scratch -> original order: feat (n x 16), acc (n x 6: a, dv)
 __global__ void k_scatter_features(const int* __restrict__ ids, int n, const float* __restrict__ sfeat,
                                    const float4* __restrict__ sacc, float* __restrict__ feat_out,
@@ -1410,7 +1483,8 @@ struct nsph_sph {
     float* sfeat = nullptr;              // surrogate scratch (nsph_sph_enable_surrogate), sorted: 16 features
     float4* sacc = nullptr;              //   (a, 0), (dv, 0)
     float* cpart = nullptr;              //   per-block (compression sum, active count)
-    int surr_ctas = 0;                   //   resident CTAs of k_surrogate_fused (its grid)
+    int surr_ctas = 0;                   //   resident CTAs of the fused surrogate kernel (its grid)
+    int surr_groups = 1;                 //   tiles of 128 particles per CTA (1: k_surrogate_fused, 2: the grouped kernel)
     int surr_wait_limit = -1;            //   polls of an MMA-completion wait (-1: kMlpWaitLimit)
     char* tape = nullptr;                // segment tape (nsph_sph_segment_adjoint): per step of a segment,
     int tape_steps = 0;                  //   the build and density outputs the step's reverse reads,
@@ -2263,29 +2337,63 @@ extern "C" int nsph_sph_adjoint_phase_times(nsph_sph* s, float ms_out[5])
 // ==========================================================================
 // C ABI: surrogate step
 // ==========================================================================
-// Resident CTAs per SM of k_surrogate_fused by default. Six fit (shared
-// memory, TMEM columns, registers), but six leave about 28 KB of L1 for the
-// neighbour gathers; five (the rest of the SM's storage as L1) measured
-// 0.29 ms per launch on the 1M tank against 0.39 ms at six (0.32 at four).
+// Default launch of the fused surrogate kernel: 5 CTAs of one 128-particle
+// tile per SM. Six fit (shared memory, TMEM columns, registers), but six leave
+// about 28 KB of L1 for the neighbour gathers; five (the rest of the SM's
+// storage as L1) measured 0.29 ms per launch on the 1M tank against 0.39 ms
+// at six (0.32 at four).
 constexpr int kSurrogateCtasPerSm = 5;
+constexpr int kSurrogateGroups = 1;
 
-static int set_surrogate_ctas(nsph_sph* s, int ctas_per_sm)
+// resident CTAs per SM of a fused surrogate kernel: registers (allocated per
+// warp in units of 256), shared memory (plus the per-CTA reservation) and
+// the SM's 512 TMEM columns; 0 on a CUDA error
+template <class K>
+static int surrogate_per_sm(K kernel, int threads, size_t smem, int tmem_cols, int device)
+{
+    cudaFuncAttributes fa;
+    int smem_sm = 0, reserved = 0, regs_sm = 0;
+    if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, device) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    const int warp_regs = ((fa.numRegs * 32 + 255) / 256) * 256;
+    const int by_regs = regs_sm / (warp_regs * (threads / 32));
+    const int by_smem = smem_sm / (int)(smem + fa.sharedSizeBytes + reserved);
+    return std::min(std::min(by_regs, by_smem), kTmemCols / tmem_cols);
+}
+
+static int set_surrogate_ctas(nsph_sph* s, int ctas_per_sm, int groups)
 {
     DeviceGuard guard(s->grid.device);
     if (!guard.ok) return fail(NSPH_ERR_CUDA, "cannot select CUDA device");
-    const int most = mlp_resident_grid(k_surrogate_fused, sizeof(MlpFwdSmem), s->grid.device);
     int sms = 0, smem_sm = 0, reserved = 0;
     NSPH_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->grid.device));
     NSPH_CUDA_TRY(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, s->grid.device));
     NSPH_CUDA_TRY(cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, s->grid.device));
+    if (groups == 0) groups = kSurrogateGroups;
+    const size_t smem = groups == 2 ? sizeof(MlpFwdGroupSmem<2>) : sizeof(MlpFwdSmem);
+    const int most = groups == 2 ? surrogate_per_sm(k_surrogate_fused_groups<2>, 2 * kMlpTile, smem,
+                                                    2 * (int)kMlpFwdCols, s->grid.device)
+                                 : surrogate_per_sm(k_surrogate_fused, kMlpTile, smem, (int)kMlpFwdCols,
+                                                    s->grid.device);
     if (most <= 0 || sms <= 0 || smem_sm <= 0) return fail(NSPH_ERR_CUDA, "cannot size the surrogate grid");
-    const int per_sm = std::max(1, std::min(ctas_per_sm == 0 ? kSurrogateCtasPerSm : ctas_per_sm, most / sms));
+    const int def = groups == 2 ? most : kSurrogateCtasPerSm;
+    const int per_sm = std::max(1, std::min(ctas_per_sm == 0 ? def : ctas_per_sm, most));
     // the shared-memory carveout that holds per_sm CTAs, so that the rest of
     // the SM's unified L1 / shared storage serves the neighbour gathers
-    const int need = per_sm * (int)(sizeof(MlpFwdSmem) + reserved);
+    const int need = per_sm * (int)(smem + reserved);
     const int pct = std::min(100, (need * 100 + smem_sm - 1) / smem_sm);
-    NSPH_CUDA_TRY(cudaFuncSetAttribute(k_surrogate_fused, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+    if (groups == 2)
+        NSPH_CUDA_TRY(
+            cudaFuncSetAttribute(k_surrogate_fused_groups<2>, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
+    else
+        NSPH_CUDA_TRY(cudaFuncSetAttribute(k_surrogate_fused, cudaFuncAttributePreferredSharedMemoryCarveout, pct));
     s->surr_ctas = sms * per_sm;
+    s->surr_groups = groups;
     return NSPH_OK;
 }
 
@@ -2305,11 +2413,14 @@ extern "C" int nsph_sph_enable_surrogate(nsph_sph* s)
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_surrogate_fused, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)sizeof(MlpFwdSmem));
-    if (e == cudaSuccess) {
-        s->surr_ctas = mlp_resident_grid(k_surrogate_fused, sizeof(MlpFwdSmem), s->grid.device);
-        if (s->surr_ctas <= 0) e = cudaErrorUnknown;
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_surrogate_fused_groups<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(MlpFwdGroupSmem<2>));
+    if (e == cudaSuccess) {  // an upper bound on either kernel's grid, for the partials
+        const int most = mlp_resident_grid(k_surrogate_fused, sizeof(MlpFwdSmem), s->grid.device);
+        if (most <= 0) e = cudaErrorUnknown;
+        else if (most + 1 > (int)blocks) e = cudaErrorInvalidValue;
     }
-    if (e == cudaSuccess && s->surr_ctas + 1 > (int)blocks) e = cudaErrorInvalidValue;
     cudaFuncAttributes fa;
     if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_force_features_list);
     if (e != cudaSuccess) {
@@ -2321,7 +2432,7 @@ extern "C" int nsph_sph_enable_surrogate(nsph_sph* s)
         s->sacc = nullptr;
         return fail(NSPH_ERR_OUT_OF_MEMORY, std::string("surrogate allocation: ") + cudaGetErrorString(e));
     }
-    return set_surrogate_ctas(s, 0);  // the default resident CTAs per SM and their carveout
+    return set_surrogate_ctas(s, 0, 0);  // the default launch and its carveout
 }
 
 // grid build, density pass and (with `features`) the feature pass into the
@@ -2424,13 +2535,22 @@ extern "C" int nsph_sph_step_surrogate(nsph_sph* s, const nsph_sph_params* p, co
     if (st != NSPH_OK) return st;
     if (n > 0) {
         const int tiles = (n + kMlpTile - 1) / kMlpTile;
-        const int grid = std::min(tiles, std::max(1, s->surr_ctas));
         const int wait_limit = s->surr_wait_limit >= 0 ? s->surr_wait_limit : kMlpWaitLimit;
         const StepOut o{f_ext, inv_mass, gravity, x_out, v_out, rho_out, p_out, nullptr, s->status};
-        k_surrogate_fused<<<grid, kMlpTile, sizeof(MlpFwdSmem), cs>>>(model, acc_scale, wait_limit, s->grid.view(),
-                                                                      s->xs, s->vs, s->aux, s->rp, n, *p, s->nbr,
-                                                                      s->ncnt, o, s->cpart);
-        NSPH_LAUNCH_CHECK("k_surrogate_fused");
+        int grid;
+        if (s->surr_groups == 2) {
+            grid = std::min((tiles + 1) / 2, std::max(1, s->surr_ctas));
+            k_surrogate_fused_groups<2><<<grid, 2 * kMlpTile, sizeof(MlpFwdGroupSmem<2>), cs>>>(
+                model, acc_scale, wait_limit, s->grid.view(), s->xs, s->vs, s->aux, s->rp, n, *p, s->nbr, s->ncnt, o,
+                s->cpart);
+            NSPH_LAUNCH_CHECK("k_surrogate_fused_groups");
+        } else {
+            grid = std::min(tiles, std::max(1, s->surr_ctas));
+            k_surrogate_fused<<<grid, kMlpTile, sizeof(MlpFwdSmem), cs>>>(model, acc_scale, wait_limit,
+                                                                          s->grid.view(), s->xs, s->vs, s->aux, s->rp,
+                                                                          n, *p, s->nbr, s->ncnt, o, s->cpart);
+            NSPH_LAUNCH_CHECK("k_surrogate_fused");
+        }
         if (s->eva[3]) NSPH_CUDA_TRY(record_mark(s->eva[3], cs));
         k_compression_reduce<<<1, 256, 0, cs>>>(s->cpart, grid, stats);
         NSPH_LAUNCH_CHECK("k_compression_reduce");
@@ -2443,13 +2563,14 @@ extern "C" int nsph_sph_step_surrogate(nsph_sph* s, const nsph_sph_params* p, co
     return NSPH_OK;
 }
 
-extern "C" int nsph_sph_set_surrogate_launch(nsph_sph* s, int ctas_per_sm)
+extern "C" int nsph_sph_set_surrogate_launch(nsph_sph* s, int ctas_per_sm, int tiles_per_cta)
 {
     clear_error();
     if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
     if (ctas_per_sm < 0 || ctas_per_sm > 64) return fail(NSPH_ERR_INVALID_ARG, "ctas_per_sm out of [0, 64]");
+    if (tiles_per_cta < 0 || tiles_per_cta > 2) return fail(NSPH_ERR_INVALID_ARG, "tiles_per_cta out of [0, 2]");
     if (!s->sfeat) return fail(NSPH_ERR_INVALID_ARG, "surrogate not enabled (nsph_sph_enable_surrogate)");
-    return set_surrogate_ctas(s, ctas_per_sm);
+    return set_surrogate_ctas(s, ctas_per_sm, tiles_per_cta);
 }
 
 extern "C" int nsph_sph_set_surrogate_wait_limit(nsph_sph* s, int polls)

@@ -98,12 +98,6 @@ class HashGrid:
         """Kernels launched by the last build."""
         return int(self._lib.nsph_grid_last_launches(self._handle))
 
-    def set_scan_polls(self, polls: int) -> None:
-        """Look-back wait of the counting build's cell scan (polls of an
-        unpublished predecessor tile before a tile sums its prefix itself;
-        0: no look-back; negative: the default). The result is the same."""
-        _lib.check(self._lib.nsph_grid_set_scan_polls(self._handle, int(polls)), "HashGrid.set_scan_polls")
-
     # ---- host-visible views for tests and consumers --------------------
     def _view(self) -> _lib.NsphGridView:
         v = _lib.NsphGridView()

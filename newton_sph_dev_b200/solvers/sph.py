@@ -708,13 +708,12 @@ class SolverSPH(SolverBase):
         _lib.check(self._lib.nsph_sph_set_surrogate_wait_limit(self._handle, int(polls)),
                    "SolverSPH.set_surrogate_wait_limit")
 
-    def set_surrogate_launch(self, ctas_per_sm: int = 0) -> None:
-        """Resident CTAs per SM of the surrogate step's fused kernel (0: the
-        default, 5 on a B200). Fewer CTAs leave more of the SM's L1 to the
-        neighbour gathers (see nsph_sph_set_surrogate_launch); results do
-        not change."""
+    def set_surrogate_launch(self, ctas_per_sm: int = 0, tiles_per_cta: int = 0) -> None:
+        """Launch shape of the surrogate step's fused kernel: resident CTAs
+        per SM and 128-particle tiles per CTA (1 or 2; 0: the defaults). See
+        nsph_sph_set_surrogate_launch; results do not change."""
         self.enable_surrogate()
-        _lib.check(self._lib.nsph_sph_set_surrogate_launch(self._handle, int(ctas_per_sm)),
+        _lib.check(self._lib.nsph_sph_set_surrogate_launch(self._handle, int(ctas_per_sm), int(tiles_per_cta)),
                    "SolverSPH.set_surrogate_launch")
 
     def surrogate_phase_times(self) -> tuple[float, float, float, float]:

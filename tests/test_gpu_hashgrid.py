@@ -167,20 +167,16 @@ def test_counting_and_radix_builds_alternate(oracle_mod):
         assert (launches == 4) == counting, (n, launches)
 
 
-@pytest.mark.parametrize("polls", [-1, 0, 1])
-def test_counting_build_scan_lookback(oracle_mod, polls):
-    """The counting build's single-pass cell scan on a table whose size is
-    not a multiple of the scan tile (the last tile reads its counts one by
-    one), with the default look-back, with none (every tile sums the counts
-    in front of it: the path a tile takes when its predecessor does not
-    answer) and with a one-poll limit (a mix of both): the same grid as the
-    oracle's each time, over repeated builds."""
+def test_counting_build_partial_tile(oracle_mod):
+    """The counting build on a cell table whose size is not a multiple of the
+    scan's 8192-cell tile (the last tile reads its counts one by one), over
+    repeated builds (the per-cell and per-tile counts must return to zero):
+    the same grid as the oracle's each time."""
     from newton_sph_dev_b200 import HashGrid
 
-    dims = (61, 53, 47)  # 151,951 cells: 37 tiles of 4096, the last one partial
+    dims = (61, 53, 47)  # 151,951 cells: 19 tiles, the last one partial
     grid = HashGrid(*dims, device=DEV)
-    grid.set_scan_polls(polls)
-    for n, seed in ((12000, 11), (20000, 12), (15000, 13)):
+    for n, seed in ((12000, 11), (20000, 12), (15000, 13), (150000, 14)):
         pts = _points(n, seed)
         grid.build(torch.from_numpy(pts).to(DEV), 0.02)
         torch.cuda.synchronize()
@@ -188,4 +184,4 @@ def test_counting_build_scan_lookback(oracle_mod, polls):
         got = _grid_arrays(grid)
         ref = oracle_mod.grid_build(pts, 0.02, dims)
         for k in ref:
-            np.testing.assert_array_equal(got[k], ref[k], err_msg=f"n={n} polls={polls}: {k}")
+            np.testing.assert_array_equal(got[k], ref[k], err_msg=f"n={n}: {k}")

@@ -332,12 +332,13 @@ def test_surrogate_wait_timeout_falls_back():
     assert not torch.equal(xs, xp)
 
 
-@pytest.mark.parametrize("ctas_per_sm", [1, 2, 4])
-def test_surrogate_launch_shape_keeps_results(ctas_per_sm):
-    """Fewer resident CTAs per SM for the fused kernel (a larger L1 for its
-    neighbour gathers): the same positions and velocities, bit for bit, as
-    the default grid, and the same compression statistics up to the order of
-    the per-CTA partial sums."""
+@pytest.mark.parametrize("ctas_per_sm,tiles_per_cta", [(1, 1), (2, 1), (4, 1), (0, 2), (1, 2), (2, 2)])
+def test_surrogate_launch_shape_keeps_results(ctas_per_sm, tiles_per_cta):
+    """Other launch shapes of the fused kernel (fewer resident CTAs per SM, a
+    larger L1 for its gathers; two tiles per CTA sharing the weights): the
+    same positions and velocities, bit for bit, as the default launch, and
+    the same compression statistics up to the order of the per-CTA partial
+    sums."""
     from newton_sph_dev_b200.solvers import SolverSPH
 
     model, cfg, x, v, flags = _scene(seed=12)
@@ -345,8 +346,8 @@ def test_surrogate_launch_shape_keeps_results(ctas_per_sm):
     m = random_model(6)
     p = solver.step_params(4e-4)
     out = []
-    for k in (0, ctas_per_sm):
-        solver.set_surrogate_launch(k)
+    for k, t in ((0, 0), (ctas_per_sm, tiles_per_cta)):
+        solver.set_surrogate_launch(k, t)
         stats = torch.zeros(4, device=DEV)
         xs, vs = torch.empty_like(model.particle_q), model.particle_qd.clone()
         solver.step_surrogate_raw(model.particle_q, model.particle_qd, xs, vs, p, m, 1.0, stats)
@@ -356,3 +357,37 @@ def test_surrogate_launch_shape_keeps_results(ctas_per_sm):
     assert solver.status() == 0
     assert torch.equal(out[0][0], out[1][0]) and torch.equal(out[0][1], out[1][1])
     torch.testing.assert_close(out[0][2], out[1][2], rtol=1e-5, atol=0.0)
+
+
+def test_grouped_surrogate_wait_timeout_is_the_plain_step():
+    """Two tiles per CTA with waits that give up at once: each group
+    integrates without the correction (the plain step at this dt, bit for
+    bit) and the status bit is set; the default limit again gives the
+    corrected step, as the one-tile kernel does."""
+    from newton_sph_dev_b200.solvers import SolverSPH
+
+    model, cfg, x, v, flags = _scene(seed=14)
+    solver = SolverSPH(model, cfg)
+    m = random_model(8)
+    solver.set_surrogate_launch(0, 2)
+    solver.set_surrogate_wait_limit(0)
+    p = solver.step_params(4e-4)
+    stats = torch.zeros(4, device=DEV)
+    xs, vs = torch.empty_like(model.particle_q), model.particle_qd.clone()
+    solver.step_surrogate_raw(model.particle_q, model.particle_qd, xs, vs, p, m, 1.0, stats)
+    xp, vp = torch.empty_like(model.particle_q), model.particle_qd.clone()
+    solver.step_raw(model.particle_q, model.particle_qd, xp, vp, p)
+    torch.cuda.synchronize()
+    assert solver.status() & 8
+    assert torch.equal(xs, xp) and torch.equal(vs, vp)
+    solver.reset_status()
+    solver.set_surrogate_wait_limit(-1)
+    x1, v1 = torch.empty_like(model.particle_q), model.particle_qd.clone()
+    solver.step_surrogate_raw(model.particle_q, model.particle_qd, x1, v1, p, m, 1.0, stats)
+    solver.set_surrogate_launch(0, 1)
+    x2, v2 = torch.empty_like(model.particle_q), model.particle_qd.clone()
+    solver.step_surrogate_raw(model.particle_q, model.particle_qd, x2, v2, p, m, 1.0, stats)
+    solver.set_surrogate_launch(0, 0)
+    torch.cuda.synchronize()
+    assert solver.status() == 0
+    assert torch.equal(x1, x2) and torch.equal(v1, v2) and not torch.equal(x1, xp)
