@@ -1129,14 +1129,18 @@ def surrogate_eval(solver, model, sub: int, dt: float, calls: int, start_q, star
         diverged_at = None
         done = 0
         torch.cuda.synchronize()
+        by_kind = {"surrogate": 0.0, "plain": 0.0, "rollback": 0.0}
         for c in range(calls):
             flush.zero_()
             before = st.surrogate_steps
+            rb = st.rollbacks
             e0.record(stream)
             st.step(cur, nxt, dt)
             e1.record(stream)
             e1.synchronize()
-            ms += e0.elapsed_time(e1)
+            t_call = e0.elapsed_time(e1)
+            ms += t_call
+            by_kind["rollback" if st.rollbacks > rb else ("surrogate" if st.surrogate_steps > before else "plain")] += t_call
             if phase_timing and st.surrogate_steps > before:
                 fused_ms += solver.surrogate_phase_times()[2]
             cur, nxt = nxt, cur
@@ -1154,6 +1158,7 @@ def surrogate_eval(solver, model, sub: int, dt: float, calls: int, start_q, star
                "surrogate_steps": st.surrogate_steps, "fallback_calls": st.fallback_calls,
                "rollbacks": st.rollbacks, "rejected_window_worst": float(max(st.rejected_worst or [0.0])),
                "timeouts": st.timeouts, "finite": finite, "status": solver.status(),
+               "ms_by_call_kind": by_kind,
                "fused_kernel_ms": fused_ms / max(1, st.surrogate_steps) if phase_timing else None,
                "launches_per_call": st.launches_per_step}
         st._graphs.clear()

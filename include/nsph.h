@@ -554,8 +554,8 @@ NSPH_API int nsph_sph_step_surrogate(nsph_sph* solver, const nsph_sph_params* pa
  * taking tiles of 128 particles. tiles_per_cta = 1: CTAs of 128 threads and
  * about 34 KB of shared memory; 2: CTAs of 256 threads whose two tiles share
  * one copy of the weights (about 53 KB) and run their MMA chains
- * independently; 0 = the default (1). ctas_per_sm: resident CTAs per SM, at
- * most as many as fit (6 of one tile, 4 of two on a B200); 0 = the default
+ * independently; 0 = the default (2). ctas_per_sm: resident CTAs per SM, at
+ * most as many as fit (6 of one tile, 3 of two on a B200); 0 = the default
  * (5 of one tile, as many as fit of two). The kernel's preferred
  * shared-memory carveout is set to what those CTAs need, so that the rest of
  * each SM's unified L1 / shared storage caches the neighbour gathers (6 CTAs

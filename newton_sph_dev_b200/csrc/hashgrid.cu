@@ -298,10 +298,9 @@ __global__ void k_ranges(const int* __restrict__ cells, int n, int2* __restrict_
 // of three radix passes.
 //   k_cc_count        cell of each point (original order), its slot in the
 //                     cell from an atomic counter (an arbitrary order within a
-//                     cell), and the point counts per tile of kCsTile cells;
-//                     both atomics warp-aggregated (one per distinct cell or
-//                     tile of a warp); clears the ranges of the previous
-//                     build's cells
+//                     cell), and the point counts per tile of kCsTile cells
+//                     (one atomic per warp whose points share a tile); clears
+//                     the ranges of the previous build's cells
 //   k_cc_scan_ranges  per tile: its offset (the sum of the earlier tiles'
 //                     counts), the exclusive scan of its cells' counts, the
 //                     ranges of its occupied cells
@@ -328,7 +327,6 @@ __global__ void __launch_bounds__(256) k_cc_count(const float* __restrict__ poin
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int stride = gridDim.x * blockDim.x;
     const int lane = threadIdx.x & 31;
-    const unsigned lt = lanemask_lt();
     // the previous build's cells: the first sorted entry of each clears its range
     for (int k = t; k < prev_n; k += stride) {
         const int c = prev_cells[k];
@@ -349,22 +347,24 @@ __global__ void __launch_bounds__(256) k_cc_count(const float* __restrict__ poin
             cells[i] = c[u];
         }
     }
-    // i = t + u * stride is uniform in u across the warp's lanes up to n, so
-    // the lanes with i < n are a prefix of the warp
 #pragma unroll
     for (int u = 0; u < kCcPoints; ++u) {
         const int i = t + u * stride;
-        const unsigned active = __ballot_sync(0xffffffffu, i < n);
-        if (i < n) {
-            const unsigned same = __match_any_sync(active, c[u]);
-            const int leader = __ffs(same) - 1;
-            int base = 0;
-            if (lane == leader) base = atomicAdd(count + c[u], __popc(same));
-            base = __shfl_sync(same, base, leader);
-            slots[i] = base + __popc(same & lt);
-            const int tl = c[u] / kCsTile;
-            const unsigned tile_same = __match_any_sync(active, tl);
-            if (lane == __ffs(tile_same) - 1) atomicAdd(tile_count + tl, __popc(tile_same));
+        if (i < n) slots[i] = atomicAdd(count + c[u], 1);
+    }
+    // tile counts: the lanes with i < n are a prefix of the warp (i grows with
+    // the lane), and consecutive points mostly fall in one tile, so a warp
+    // whose points share a tile adds them with one atomic
+#pragma unroll
+    for (int u = 0; u < kCcPoints; ++u) {
+        const int i = t + u * stride;
+        const int tl = i < n ? c[u] / kCsTile : -1;
+        const int t0 = __shfl_sync(0xffffffffu, tl, 0);
+        const unsigned act = __ballot_sync(0xffffffffu, i < n);
+        if (__all_sync(0xffffffffu, tl == t0 || i >= n)) {
+            if (lane == 0 && t0 >= 0) atomicAdd(tile_count + t0, __popc(act));
+        } else if (i < n) {
+            atomicAdd(tile_count + tl, 1);
         }
     }
     if (bad && status) atomicOr(status, (unsigned)NSPH_STATUS_NONFINITE_INPUT);

@@ -2337,13 +2337,13 @@ extern "C" int nsph_sph_adjoint_phase_times(nsph_sph* s, float ms_out[5])
 // ==========================================================================
 // C ABI: surrogate step
 // ==========================================================================
-// Default launch of the fused surrogate kernel: 5 CTAs of one 128-particle
-// tile per SM. Six fit (shared memory, TMEM columns, registers), but six leave
-// about 28 KB of L1 for the neighbour gathers; five (the rest of the SM's
-// storage as L1) measured 0.29 ms per launch on the 1M tank against 0.39 ms
-// at six (0.32 at four).
-constexpr int kSurrogateCtasPerSm = 5;
-constexpr int kSurrogateGroups = 1;
+// Default launch of the fused surrogate kernel: CTAs of two 128-particle
+// tiles sharing the weights, as many per SM as fit (3: registers), with the
+// carveout they need. Measured on the relaxed 1M tank (same box, back to
+// back): 0.273 ms per launch; one tile per CTA: 0.292 ms at 5 CTAs per SM,
+// 0.319 at 4, 0.395 at 6 (which leaves about 28 KB of L1 for the gathers).
+constexpr int kSurrogateCtasPerSm = 5;  // CTAs per SM when tiles_per_cta = 1
+constexpr int kSurrogateGroups = 2;
 
 // resident CTAs per SM of a fused surrogate kernel: registers (allocated per
 // warp in units of 256), shared memory (plus the per-CTA reservation) and
