@@ -21,8 +21,8 @@
 //   k_ranges      cell_starts / cell_ends from the sorted cell ids.
 // Single-world grids whose table holds at most kCountCellsPerPoint cells per
 // point (the SPH solver's grids) build by cell counts instead (count_build:
-// atomic counts, a single-pass scan of the cell table that writes the
-// ranges, scatter, stable rank within each cell): 4 launches instead of 10,
+// atomic counts, per-tile sums and a scan of the cell table that writes the
+// ranges, scatter, stable rank within each cell): 5 launches instead of 10,
 // the same result.
 #include <algorithm>
 #include <cstdio>
@@ -298,9 +298,8 @@ __global__ void k_ranges(const int* __restrict__ cells, int n, int2* __restrict_
 // of three radix passes.
 //   k_cc_count        cell of each point (original order), its slot in the
 //                     cell from an atomic counter (an arbitrary order within a
-//                     cell), and the point counts per tile of kCsTile cells
-//                     (one atomic per warp whose points share a tile); clears
-//                     the ranges of the previous build's cells
+//                     cell); clears the ranges of the previous build's cells
+//   k_cc_tile_sums    the points of each tile of kCsTile cells
 //   k_cc_scan_ranges  per tile: its offset (the sum of the earlier tiles'
 //                     counts), the exclusive scan of its cells' counts, the
 //                     ranges of its occupied cells
@@ -309,7 +308,6 @@ __global__ void k_ranges(const int* __restrict__ cells, int n, int2* __restrict_
 //                     (points of its cell with a smaller index), the stable
 //                     order; writes point_cells / point_ids, gathers the
 //                     sorted mirrors in SPH mode, and zeroes the cell's count
-//                     and the tile counts for the next build
 // No kernel waits on another block. The result is identical to the stable
 // radix sort's.
 // --------------------------------------------------------------------------
@@ -319,14 +317,13 @@ constexpr int kCsPer = 32;       // cells per thread (eight int4 loads)
 constexpr int kCsTile = kCsThreads * kCsPer;
 
 __global__ void __launch_bounds__(256) k_cc_count(const float* __restrict__ points, int n, float inv, int dx, int dy,
-                                                  int dz, int* __restrict__ count, int* __restrict__ tile_count,
-                                                  int* __restrict__ cells, int* __restrict__ slots,
-                                                  const int* __restrict__ prev_cells, int prev_n,
-                                                  int2* __restrict__ ranges, unsigned* __restrict__ status)
+                                                  int dz, int* __restrict__ count, int* __restrict__ cells,
+                                                  int* __restrict__ slots, const int* __restrict__ prev_cells,
+                                                  int prev_n, int2* __restrict__ ranges,
+                                                  unsigned* __restrict__ status)
 {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int stride = gridDim.x * blockDim.x;
-    const int lane = threadIdx.x & 31;
     // the previous build's cells: the first sorted entry of each clears its range
     for (int k = t; k < prev_n; k += stride) {
         const int c = prev_cells[k];
@@ -352,22 +349,49 @@ __global__ void __launch_bounds__(256) k_cc_count(const float* __restrict__ poin
         const int i = t + u * stride;
         if (i < n) slots[i] = atomicAdd(count + c[u], 1);
     }
-    // tile counts: the lanes with i < n are a prefix of the warp (i grows with
-    // the lane), and consecutive points mostly fall in one tile, so a warp
-    // whose points share a tile adds them with one atomic
-#pragma unroll
-    for (int u = 0; u < kCcPoints; ++u) {
-        const int i = t + u * stride;
-        const int tl = i < n ? c[u] / kCsTile : -1;
-        const int t0 = __shfl_sync(0xffffffffu, tl, 0);
-        const unsigned act = __ballot_sync(0xffffffffu, i < n);
-        if (__all_sync(0xffffffffu, tl == t0 || i >= n)) {
-            if (lane == 0 && t0 >= 0) atomicAdd(tile_count + t0, __popc(act));
-        } else if (i < n) {
-            atomicAdd(tile_count + tl, 1);
-        }
-    }
     if (bad && status) atomicOr(status, (unsigned)NSPH_STATUS_NONFINITE_INPUT);
+}
+
+// this thread's kCsPer counts of the tile (int4 loads where the tile is whole)
+__device__ __forceinline__ void cc_load_counts(const int* __restrict__ count, long long ncells, long long c0,
+                                               int (&v)[kCsPer])
+{
+    if (c0 + kCsPer <= ncells) {  // count is 256-byte aligned and c0 a multiple of 32
+        const int4* p4 = reinterpret_cast<const int4*>(count + c0);
+#pragma unroll
+        for (int q = 0; q < kCsPer / 4; ++q) {
+            const int4 a = p4[q];
+            v[4 * q + 0] = a.x;
+            v[4 * q + 1] = a.y;
+            v[4 * q + 2] = a.z;
+            v[4 * q + 3] = a.w;
+        }
+    } else {
+#pragma unroll
+        for (int u = 0; u < kCsPer; ++u) v[u] = c0 + u < ncells ? count[c0 + u] : 0;
+    }
+}
+
+__global__ void __launch_bounds__(kCsThreads) k_cc_tile_sums(const int* __restrict__ count, long long ncells,
+                                                             int* __restrict__ tile_count)
+{
+    __shared__ int part[kCsThreads / 32];
+    const long long c0 = (long long)blockIdx.x * kCsTile + (long long)threadIdx.x * kCsPer;
+    int v[kCsPer];
+    cc_load_counts(count, ncells, c0, v);
+    int sum = 0;
+#pragma unroll
+    for (int u = 0; u < kCsPer; ++u) sum += v[u];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int total = 0;
+#pragma unroll
+        for (int w = 0; w < kCsThreads / 32; ++w) total += part[w];
+        tile_count[blockIdx.x] = total;
+    }
 }
 
 __global__ void __launch_bounds__(kCsThreads) k_cc_scan_ranges(const int* __restrict__ count,
@@ -383,20 +407,7 @@ __global__ void __launch_bounds__(kCsThreads) k_cc_scan_ranges(const int* __rest
     for (int q = threadIdx.x; q < tile; q += kCsThreads) before += tile_count[q];
     const long long c0 = (long long)tile * kCsTile + (long long)threadIdx.x * kCsPer;
     int v[kCsPer];
-    if (c0 + kCsPer <= ncells) {  // count is 256-byte aligned and c0 a multiple of 32
-        const int4* p4 = reinterpret_cast<const int4*>(count + c0);
-#pragma unroll
-        for (int q = 0; q < kCsPer / 4; ++q) {
-            const int4 a = p4[q];
-            v[4 * q + 0] = a.x;
-            v[4 * q + 1] = a.y;
-            v[4 * q + 2] = a.z;
-            v[4 * q + 3] = a.w;
-        }
-    } else {
-#pragma unroll
-        for (int u = 0; u < kCsPer; ++u) v[u] = c0 + u < ncells ? count[c0 + u] : 0;
-    }
+    cc_load_counts(count, ncells, c0, v);
     int sum = 0;
 #pragma unroll
     for (int u = 0; u < kCsPer; ++u) sum += v[u];
@@ -458,12 +469,10 @@ __global__ void __launch_bounds__(256) k_cc_scatter(const int* __restrict__ cell
 // write neighbouring positions
 __global__ void __launch_bounds__(256) k_cc_rank(const int* __restrict__ tmp_cells, const int2* __restrict__ ranges,
                                                  const int* __restrict__ tmp, int n, int* __restrict__ count,
-                                                 int* __restrict__ tile_count, int tiles,
                                                  int* __restrict__ point_cells, int* __restrict__ point_ids,
                                                  GatherArgs gather, bool do_gather)
 {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q < tiles) tile_count[q] = 0;  // read by k_cc_scan_ranges, which has finished
     if (q >= n) return;
     const int i = tmp[q];
     const int c = tmp_cells[q];
@@ -577,12 +586,12 @@ int grid_init(Grid& g, int dx, int dy, int dz, int device)
         NSPH_CUDA_TRY(cudaMemset(g.cell_count, 0, sizeof(int) * nc));
         const size_t tiles = (size_t)((nc + kCsTile - 1) / kCsTile);
         NSPH_CUDA_TRY(cudaMalloc(&g.tile_count, sizeof(int) * tiles));
-        NSPH_CUDA_TRY(cudaMemset(g.tile_count, 0, sizeof(int) * tiles));
     }
     // load every kernel now, so that a later stream capture never triggers
     // lazy module loading
     cudaFuncAttributes fa;
     NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_cc_count));
+    NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_cc_tile_sums));
     NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_cc_scan_ranges));
     NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_cc_scatter));
     NSPH_CUDA_TRY(cudaFuncGetAttributes(&fa, k_cc_rank));
@@ -740,27 +749,27 @@ int build_passes(Grid& g, const float* points, int n, float cell_inv, const Gath
     return NSPH_OK;
 }
 
-// the counting build (see k_cc_count): 4 launches
+// the counting build (see k_cc_count): 5 launches
 int count_build(Grid& g, const float* points, int n, float cell_inv, const GatherArgs* gather, unsigned int* status,
                 cudaStream_t stream, int& nl, int prev_n)
 {
     const int tiles = (int)((g.ncells + kCsTile - 1) / kCsTile);
     const int per_block = 256 * kCcPoints;
     const int blocks = (n + per_block - 1) / per_block;
-    k_cc_count<<<blocks, 256, 0, stream>>>(points, n, cell_inv, g.dx, g.dy, g.dz, g.cell_count, g.tile_count,
-                                           g.keys_a, g.vals_a, g.point_cells, prev_n, g.cell_ranges, status);
+    k_cc_count<<<blocks, 256, 0, stream>>>(points, n, cell_inv, g.dx, g.dy, g.dz, g.cell_count, g.keys_a, g.vals_a,
+                                           g.point_cells, prev_n, g.cell_ranges, status);
     NSPH_LAUNCH_CHECK("k_cc_count");
+    k_cc_tile_sums<<<tiles, kCsThreads, 0, stream>>>(g.cell_count, g.ncells, g.tile_count);
+    NSPH_LAUNCH_CHECK("k_cc_tile_sums");
     k_cc_scan_ranges<<<tiles, kCsThreads, 0, stream>>>(g.cell_count, g.tile_count, g.ncells, g.cell_ranges);
     NSPH_LAUNCH_CHECK("k_cc_scan_ranges");
     k_cc_scatter<<<blocks, 256, 0, stream>>>(g.keys_a, g.vals_a, g.cell_ranges, n, g.keys_b, g.vals_b);
     NSPH_LAUNCH_CHECK("k_cc_scatter");
-    // n >= tiles (the policy keeps the table at most 16 cells per point, and
-    // a tile holds 8192 cells), so the rank grid also covers the tile counts
-    k_cc_rank<<<(n + 255) / 256, 256, 0, stream>>>(g.vals_b, g.cell_ranges, g.keys_b, n, g.cell_count, g.tile_count,
-                                                   tiles, g.point_cells, g.point_ids, gather ? *gather : GatherArgs{},
+    k_cc_rank<<<(n + 255) / 256, 256, 0, stream>>>(g.vals_b, g.cell_ranges, g.keys_b, n, g.cell_count,
+                                                   g.point_cells, g.point_ids, gather ? *gather : GatherArgs{},
                                                    gather != nullptr);
     NSPH_LAUNCH_CHECK("k_cc_rank");
-    nl += 4;
+    nl += 5;
     return NSPH_OK;
 }
 

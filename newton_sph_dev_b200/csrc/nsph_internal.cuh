@@ -213,7 +213,7 @@ struct Grid {
     // cell table (ncells entries of {start, end})
     int2* cell_ranges = nullptr;
     // counting build (single world, at most kCountMaxCells cells): per-cell
-    // counts and per-tile (8192 cells) counts, all zero between builds
+    // counts (all zero between builds) and per-tile (8192 cells) counts
     int* cell_count = nullptr;
     int* tile_count = nullptr;
 

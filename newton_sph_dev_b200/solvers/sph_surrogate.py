@@ -249,14 +249,17 @@ def surrogate_targets(config: SPHConfig, dt_big: float, x0, v0, x1, acc, gravity
 
 def generate_training_data(trajectories: int = 200, shape=(32, 32, 32), spacing: float = 0.01, dt: float = 1e-4,
                            substeps: int = 4, samples_per_trajectory: int = 10, keep_fraction: float = 0.125,
-                           vel_scale=(0.0, 0.5), box=(1.0, 1.0, 1.0), seed: int = 0,
+                           vel_scale=(0.0, 0.5), box=(1.0, 1.0, 1.0), seed: int = 0, stride: int = 1,
                            device: str | torch.device = "cuda:0"):
     """Features (N, 16) and dimensionless targets (N, 3) from plain
     trajectories of jittered lattice blocks (32^3 = 32,768 particles by
     default, in a 1 m box, velocities N(0, s^2) per component with s uniform
-    in vel_scale). Each trajectory runs samples_per_trajectory x substeps
-    plain steps of dt; every substeps-th state is a sample, of which a random
-    keep_fraction of the particles is kept.
+    in vel_scale). Each trajectory runs samples_per_trajectory x stride x
+    substeps plain steps of dt; every (stride x substeps)-th state is a
+    sample (whose target spans the next substeps steps), of which a random
+    keep_fraction of the particles is kept. A stride above 1 spreads the
+    samples over a longer span of the flow (the block's collapse and
+    splash) at the same number of rows.
 
     Returns (features, targets, info)."""
     rng = np.random.default_rng(seed)
@@ -290,12 +293,15 @@ def generate_training_data(trajectories: int = 200, shape=(32, 32, 32), spacing:
             targs.append(target[sel].clone())
             kept += int(sel.sum())
             x, v = x1.clone(), tv[-1].clone()
+            for _ in range(stride - 1):  # unrecorded plain steps to the next sample
+                solver.rollout_raw(x, v, tx, tv, p_small)
+                x, v = tx[-1].clone(), tv[-1].clone()
     features = torch.cat(feats)
     targets = torch.cat(targs)
     info = {"trajectories": trajectories, "particles": int(np.prod(shape)), "spacing": spacing, "dt": dt,
             "substeps": substeps, "samples_per_trajectory": samples_per_trajectory,
-            "plain_steps_per_trajectory": samples_per_trajectory * substeps, "keep_fraction": keep_fraction,
-            "vel_scale": tuple(vel_scale), "rows": kept, "seed": seed}
+            "plain_steps_per_trajectory": samples_per_trajectory * stride * substeps, "stride": stride,
+            "keep_fraction": keep_fraction, "vel_scale": tuple(vel_scale), "rows": kept, "seed": seed}
     return features, targets, info
 
 

@@ -86,13 +86,16 @@ def main(argv=None):
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--substeps", type=int, default=4,
                     help="plain steps of 1e-4 s per surrogate step (4: dt c0/h = 0.4; 8: 0.8)")
+    ap.add_argument("--stride", type=int, default=1,
+                    help="surrogate steps between samples (1: consecutive; larger spreads a trajectory's samples "
+                         "over more of the flow)")
     ap.add_argument("--eval-steps", type=int, default=50, help="surrogate steps of the held-out rollout")
     ap.add_argument("--device", default="cuda:0")
     args = ap.parse_args(argv)
     t0 = time.time()
     feats, targs, info = generate_training_data(trajectories=args.trajectories, samples_per_trajectory=args.samples,
                                                 keep_fraction=args.keep, seed=args.seed, device=args.device,
-                                                substeps=args.substeps)
+                                                substeps=args.substeps, stride=args.stride)
     t_data = time.time() - t0
     model = SurrogateModel(args.device, seed=args.seed)
     t0 = time.time()
