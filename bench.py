@@ -745,10 +745,18 @@ def run_gpu(args):
 
     # the learned surrogate beside the plain step, from the timed state (the
     # three arms of surrogate_eval; not part of the headline value)
-    surrogate = None
+    surrogate = surrogate_8x = None
     if not isinstance(cfg, list) and args.surrogate_calls > 0:
         surrogate = surrogate_eval(solver, model, 4, dt, args.surrogate_calls, timed_state.particle_q.clone(),
                                    timed_state.particle_qd.clone(), device)
+        if args.workload.startswith("tank_"):  # dt = 5e-5: one step of 4e-4 s = 8 plain steps
+            from newton_sph_dev_b200.solvers.sph_surrogate import SurrogateModel
+
+            sw8 = WORKLOADS["tank_1m_surrogate_8x"]["surrogate"]
+            net8 = SurrogateModel.load(REPO / "newton_sph_dev_b200" / sw8["weights"], device)
+            surrogate_8x = surrogate_eval(solver, model, sw8["substeps"], dt, args.surrogate_calls,
+                                          timed_state.particle_q.clone(), timed_state.particle_qd.clone(), device,
+                                          net=net8, threshold=sw8["threshold"], window=sw8["window"])
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -797,6 +805,7 @@ def run_gpu(args):
             "roofline_issue": roof_issue,
             "fast_arithmetic": fast,
             "surrogate": surrogate,
+            "surrogate_8x": surrogate_8x,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": state_bytes,
                     "d2h_bytes_per_step": state_bytes, "steps": e2e_steps,
