@@ -709,7 +709,9 @@ __global__ void __launch_bounds__(kSphThreads, 4) k_density_worlds(const WorldCe
     }
 }
 
-__global__ void __launch_bounds__(kSphThreads, 3) k_force_worlds(const WorldCells* __restrict__ wc,
+// Bounded to 64 registers: 2.39 -> 2.11 ms per pass on worlds_4096 against
+// 80 at three blocks per SM (same box, back to back).
+__global__ void __launch_bounds__(kSphThreads, 4) k_force_worlds(const WorldCells* __restrict__ wc,
                                                                  const nsph_sph_params* __restrict__ wp,
                                                                  const int2* __restrict__ ranges,
                                                                  const int* __restrict__ ids,
