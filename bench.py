@@ -482,46 +482,45 @@ def graph_replayed(step):
     return run
 
 
-def pipelined_e2e(model, step, hx, hv, steps: int, device, outputs=None) -> float:
+def pipelined_e2e(model, step, hx, hv, steps: int, device, outputs=None, nbuf: int = 2) -> float:
     """Milliseconds for `steps` end-to-end steps through the public API:
     upload (x, v) from the pinned host tensors hx, hv, step(state_in,
     state_out), download outputs(state_out) (default: x, v) into pinned host
-    tensors. Three streams
-    (upload, compute, download) and two device state pairs let the upload of
-    step k+1 and the download of step k-1 run while step k computes; events
-    order every reuse of a buffer. Timed with CUDA events from a common start
-    to the last download."""
+    tensors. Three streams (upload, compute, download) and `nbuf` device
+    state pairs let the uploads of the next steps and the downloads of the
+    previous ones run while a step computes; events order every reuse of a
+    buffer. Timed with CUDA events from a common start to the last download."""
     import torch
 
     if outputs is None:
         outputs = lambda st: (st.particle_q, st.particle_qd)  # noqa: E731
     s_in, s_c, s_out = (torch.cuda.Stream(device) for _ in range(3))
-    ins = [model.state(), model.state()]
-    outs = [model.state(), model.state()]
-    host_out = [[torch.empty(t.shape, dtype=t.dtype).pin_memory() for t in outputs(outs[b])] for b in range(2)]
-    up = [torch.cuda.Event() for _ in range(2)]
-    done = [torch.cuda.Event() for _ in range(2)]
-    down = [torch.cuda.Event() for _ in range(2)]
+    ins = [model.state() for _ in range(nbuf)]
+    outs = [model.state() for _ in range(nbuf)]
+    host_out = [[torch.empty(t.shape, dtype=t.dtype).pin_memory() for t in outputs(outs[b])] for b in range(nbuf)]
+    up = [torch.cuda.Event() for _ in range(nbuf)]
+    done = [torch.cuda.Event() for _ in range(nbuf)]
+    down = [torch.cuda.Event() for _ in range(nbuf)]
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     cur = torch.cuda.current_stream(device)
-    # one untimed round to warm the streams' first launches
-    for k in range(steps + 2):
-        b = k % 2
-        if k == 2:
+    # one untimed round (each buffer once) to warm the streams' first launches
+    for k in range(steps + nbuf):
+        b = k % nbuf
+        if k == nbuf:
             torch.cuda.synchronize()
             start.record(cur)
             for st in (s_in, s_c, s_out):
                 st.wait_event(start)
         with torch.cuda.stream(s_in):
-            if k >= 2:
-                s_in.wait_event(done[b])  # step k-2 no longer reads ins[b]
+            if k >= nbuf:
+                s_in.wait_event(done[b])  # step k - nbuf no longer reads ins[b]
             ins[b].particle_q.copy_(hx, non_blocking=True)
             ins[b].particle_qd.copy_(hv, non_blocking=True)
             up[b].record(s_in)
         with torch.cuda.stream(s_c):
             s_c.wait_event(up[b])
-            if k >= 2:
-                s_c.wait_event(down[b])  # the download of step k-2 has read outs[b]
+            if k >= nbuf:
+                s_c.wait_event(down[b])  # the download of step k - nbuf has read outs[b]
             step(ins[b], outs[b])
             done[b].record(s_c)
         with torch.cuda.stream(s_out):
