@@ -1006,7 +1006,7 @@ def run_grad(args):
     t_dens = dens_ms / args.steps * 1e-3
     t_pair = pair_ms / args.steps * 1e-3
     achieved = B_ALG_DENSITY * n / t_dens / 1e9
-    roofline = {"bound": "hbm", "kernel": "k_density", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+    roofline = {"bound": "hbm", "kernel": "k_density_list", "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
                 "unit": "GB/s", "frac": achieved / peak, "traffic": None,
                 "alg_bytes_per_launch": B_ALG_DENSITY * n}
     pair_ach = B_ALG_ADJ_PAIR * n / t_pair / 1e9

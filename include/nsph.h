@@ -302,14 +302,14 @@ NSPH_API int nsph_sph_rollout_adjoint(nsph_sph* solver, const nsph_sph_params* p
  * nsph_sph_segment_adjoint: `steps` steps from (x0, v0). The forward keeps,
  *   per step, the grid build, density pass and force sums that the step's
  *   reverse reads (sorted mirrors, cell table, sorted ids, m/rho, p/rho^2,
- *   rho, p, neighbour masks, a and the XSPH sum), so the reverse skips the
+ *   rho, p, neighbour lists, a and the XSPH sum), so the reverse skips the
  *   rebuild, the density pass and the force recompute. x_adj / v_adj hold the adjoint of
  *   the state after `steps` steps on entry and of (x0, v0) on return (they
  *   must not overlap each other or x0 / v0); f_ext_adj and eos_b_adj
  *   accumulate as in nsph_sph_step_adjoint. Afterwards the solver's grid
  *   describes the last step's input.
  * nsph_sph_reserve_segment: allocates the tape for segments of up to
- *   `steps` steps (120 bytes per particle of capacity plus 8 bytes per grid
+ *   `steps` steps (344 bytes per particle of capacity plus 8 bytes per grid
  *   cell, per step, and two states); nsph_sph_segment_adjoint reserves on
  *   demand, so call this first where the call is captured in a graph. */
 NSPH_API int nsph_sph_reserve_segment(nsph_sph* solver, int steps);

@@ -75,45 +75,6 @@ __device__ __forceinline__ float eos(float rho, const nsph_sph_params& p)
     return pr;
 }
 
-// ---- neighbour masks ---------------------------------------------------------
-// The density pass and the force pass see the same positions x_n, so they
-// have the same candidate sequence (Warp query order) and the same
-// neighbours. The density pass records, for candidate number c of particle
-// k, whether it passed the distance test: bit (c & 31) of word
-// mask[(c >> 5) * n + k] (word-major, so a warp's stores coalesce), for the
-// first kMaskWords*32 candidates, and the candidate count in ncand[k]. The
-// force pass walks the same runs and visits only the set bits, in the same
-// order, so it skips ~85% of the candidates without changing any rounding.
-// A particle with more candidates than the mask holds (dense clusters or an
-// aliased grid) is re-tested candidate by candidate.
-constexpr int kMaskWords = 8;
-constexpr int kMaskBits = kMaskWords * 32;
-
-// Walk the set bits of a particle's neighbour mask over the same runs the
-// traversal produced: visit(j) for each neighbour, in query order. `word(w)`
-// returns mask word w of this particle.
-template <class W, class V>
-__device__ __forceinline__ void for_each_masked(const GridDev& g, float4 xi, float h, W&& word, V&& visit)
-{
-    int pos = 0;
-    for_each_run(g, xi.x, xi.y, xi.z, h, [&](int lo, int hi) {
-        const int end = pos + (hi - lo);
-        int c = pos;
-        while (c < end) {
-            const int nb = min(32 - (c & 31), end - c);
-            unsigned bits = word(c >> 5) >> (c & 31);
-            if (nb < 32) bits &= (1u << nb) - 1u;
-            const int base = lo + (c - pos);
-            while (bits) {
-                visit(base + __ffs(bits) - 1);
-                bits &= bits - 1u;
-            }
-            c += nb;
-        }
-        pos = end;
-    });
-}
-
 __device__ __forceinline__ float wterm(float r2, const nsph_sph_params& p)
 {
     return kernel_w(__fmul_rn(__fsqrt_rn(r2), p.inv_h), p);
@@ -139,66 +100,7 @@ __device__ __forceinline__ float wterm_fast(float r2, const nsph_sph_params& p)
     return kernel_w_fast(r * p.inv_h, p);
 }
 
-// ---- pass 1: density + EOS --------------------------------------------------
-// Append `cnt` (<= 4) mask bits for the candidates at positions pos.. to the
-// particle's mask (word-major in global memory, the first kMaskWords words).
-__device__ __forceinline__ void mask_append(unsigned bits, int cnt, int& pos, unsigned& word,
-                                            unsigned* __restrict__ mask, int n, int k)
-{
-    const int sh = pos & 31;
-    word |= bits << sh;
-    if (sh + cnt >= 32) {
-        const int w = pos >> 5;
-        if (w < kMaskWords) mask[(size_t)w * n + k] = word;
-        word = sh ? bits >> (32 - sh) : 0u;
-    }
-    pos += cnt;
-}
-
-// single particle: direct accumulation in query order (candidates tested four
-// at a time, terms added in order), neighbour mask built alongside
-__device__ __forceinline__ float density_single(const GridDev& g, const float4* __restrict__ xs,
-                                                const nsph_sph_params& p, float4 xi, unsigned* __restrict__ mask,
-                                                int n, int k, int& ncand)
-{
-    float rho = 0.f;
-    int pos = 0;
-    unsigned word = 0u;
-    for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
-        int j = lo;
-        for (; j + 4 <= hi; j += 4) {
-            float4 xj[4];
-            float r2[4];
-#pragma unroll
-            for (int u = 0; u < 4; ++u) xj[u] = __ldg(xs + j + u);
-            unsigned nib = 0u;
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                float dx, dy, dz;
-                r2[u] = dist2(xi, xj[u], dx, dy, dz);
-                nib |= (unsigned)(r2[u] < p.h2) << u;
-            }
-            if (nib) {
-#pragma unroll
-                for (int u = 0; u < 4; ++u)
-                    if (nib & (1u << u)) rho = __fmaf_rn(xj[u].w, wterm(r2[u], p), rho);
-            }
-            mask_append(nib, 4, pos, word, mask, n, k);
-        }
-        for (; j < hi; ++j) {
-            const float4 xj = __ldg(xs + j);
-            float dx, dy, dz;
-            const float r2 = dist2(xi, xj, dx, dy, dz);
-            const bool hit = r2 < p.h2;
-            if (hit) rho = __fmaf_rn(xj.w, wterm(r2, p), rho);
-            mask_append((unsigned)hit, 1, pos, word, mask, n, k);
-        }
-    });
-    if ((pos & 31) != 0 && (pos >> 5) < kMaskWords) mask[(size_t)(pos >> 5) * n + k] = word;
-    ncand = pos;
-    return rho;
-}
-
+// ---- density + EOS -----------------------------------------------------------
 template <bool Fast = false>
 __device__ __forceinline__ void density_finish(int k, float m, float rho, const nsph_sph_params& p,
                                                float2* __restrict__ aux, float2* __restrict__ rp,
@@ -222,30 +124,6 @@ __device__ __forceinline__ void density_finish(int k, float m, float rho, const 
     rp[k] = make_float2(rho, pr);
 }
 
-// Bounded to 48 registers (no spills): 40 resident warps per SM instead of
-// 32 at its unbounded 62.
-__global__ void __launch_bounds__(kSphThreads, 5) k_density(GridDev g, const float4* __restrict__ xs,
-                                                            const float4* __restrict__ vs, int n,
-                                                            const __grid_constant__ nsph_sph_params p,
-                                                            float2* __restrict__ aux, float2* __restrict__ rp,
-                                                            unsigned* __restrict__ mask, int* __restrict__ ncand,
-                                                            unsigned* __restrict__ status)
-{
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const float4 xi = xs[k];
-        if (!(__float_as_int(vs[k].w) & kAttrActive)) {
-            aux[k] = make_float2(0.f, 0.f);
-            rp[k] = make_float2(0.f, 0.f);
-            ncand[k] = 0;
-            continue;
-        }
-        int nc = 0;
-        const float rho = density_single(g, xs, p, xi, mask, n, k, nc);
-        ncand[k] = nc;
-        density_finish(k, xi.w, rho, p, aux, rp, status);
-    }
-}
-
 // ---- neighbour lists (the plain step) -----------------------------------------
 // The density pass of the plain step first tests every candidate (in query
 // order) and appends the sorted index of each neighbour to the particle's
@@ -263,7 +141,7 @@ __global__ void __launch_bounds__(kSphThreads, 5) k_density(GridDev g, const flo
 // list with one uniform loop and no grid traversal. A particle with more
 // than kNbrSlots neighbours (dense clusters) is summed by re-testing its
 // candidates, in the same order. Sums, their order and every rounding are
-// those of the fp32 oracle, as with the masks.
+// those of the fp32 oracle.
 constexpr int kNbrSlots = 64;
 constexpr int kNbrGroups = kNbrSlots / 4;
 
@@ -428,43 +306,6 @@ __device__ __forceinline__ void force_term_fast(float4 xj, float4 vj, float2 aj,
     acc.dvz += c * (vj.z - vi.z);
 }
 
-// single particle: walk its neighbour mask (or re-test when the mask overflowed).
-// One-deep software pipeline: the loads of neighbour t+1 are issued before the
-// terms of neighbour t are evaluated (order unchanged).
-__device__ __forceinline__ void force_single(const GridDev& g, const float4* __restrict__ xs,
-                                             const float4* __restrict__ vs, const float2* __restrict__ aux,
-                                             const unsigned* __restrict__ mask, int nc, int n, int k, float4 xi,
-                                             float4 vi, float pr2_i, const nsph_sph_params& p, ForceAcc& acc)
-{
-    if (nc <= kMaskBits) {
-        bool have = false;
-        float4 pxj = make_float4(0.f, 0.f, 0.f, 0.f), pvj = pxj;
-        float2 paj = make_float2(0.f, 0.f);
-        for_each_masked(
-            g, xi, p.h, [&](int w) { return __ldg(mask + (size_t)w * n + k); },
-            [&](int j) {
-                if (j == k) return;
-                const float4 nxj = __ldg(xs + j);
-                const float4 nvj = __ldg(vs + j);
-                const float2 naj = __ldg(aux + j);
-                if (have) force_term_data(pxj, pvj, paj, xi, vi, pr2_i, p, acc);
-                pxj = nxj;
-                pvj = nvj;
-                paj = naj;
-                have = true;
-            });
-        if (have) force_term_data(pxj, pvj, paj, xi, vi, pr2_i, p, acc);
-    } else {
-        for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
-            for (int j = lo; j < hi; ++j) {
-                float dx, dy, dz;
-                if (dist2(xi, __ldg(xs + j), dx, dy, dz) < p.h2 && j != k)
-                    force_term_data(__ldg(xs + j), __ldg(vs + j), __ldg(aux + j), xi, vi, pr2_i, p, acc);
-            }
-        });
-    }
-}
-
 struct StepOut {
     const float* f_ext;
     const float* inv_mass;
@@ -542,33 +383,8 @@ __device__ __forceinline__ void integrate_out(size_t i, float4 xi, float4 vi, in
     o.v_out[3 * i + 2] = v1z;
 }
 
-// ---- pass 2: pressure force + XSPH + integrate --------------------------------
-// Bounded to 64 registers (32 resident warps per SM instead of 24 at its
-// unbounded 77): the few spills sit outside the neighbour loop, and the extra
-// warps hide the neighbour loads' latency.
-__global__ void __launch_bounds__(kSphThreads, 4) k_force(GridDev g, const float4* __restrict__ xs,
-                                                          const float4* __restrict__ vs,
-                                                          const float2* __restrict__ aux,
-                                                          const float2* __restrict__ rp, int n,
-                                                          const __grid_constant__ nsph_sph_params p,
-                                                          const unsigned* __restrict__ mask,
-                                                          const int* __restrict__ ncand, const StepOut o)
-{
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-        const float4 xi = xs[k], vi = vs[k];
-        const int attr = __float_as_int(vi.w);
-        ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        if (attr & kAttrActive) force_single(g, xs, vs, aux, mask, ncand[k], n, k, xi, vi, aux[k].y, p, acc);
-        if (o.acc_sorted) {
-            o.acc_sorted[2 * (size_t)k] = make_float4(acc.ax, acc.ay, acc.az, 0.f);
-            o.acc_sorted[2 * (size_t)k + 1] = make_float4(acc.dvx, acc.dvy, acc.dvz, 0.f);
-        }
-        integrate_out((size_t)g.ids[k], xi, vi, attr, rp[k], acc, p, p.dt, o);
-    }
-}
-
 // ---- the plain step's passes on neighbour lists ----------------------------------
-// Bounded to 48 registers, like the mask form: 40 resident warps per SM.
+// Bounded to 48 registers (4 bytes of spills): 40 resident warps per SM.
 template <bool Fast>
 __global__ void __launch_bounds__(kSphThreads, 5) k_density_list(GridDev g, const float4* __restrict__ xs,
                                                                  const float4* __restrict__ vs, int n,
@@ -658,6 +474,10 @@ __global__ void __launch_bounds__(kSphThreads, 4) k_force_list(GridDev g, const 
         const int attr = __float_as_int(vi.w);
         ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (attr & kAttrActive) force_from_list<Fast>(g, xs, vs, aux, nbr, ncnt[k], n, k, xi, vi, aux[k].y, p, acc);
+        if (o.acc_sorted) {  // the force sums, for the adjoint's segment tape
+            o.acc_sorted[2 * (size_t)k] = make_float4(acc.ax, acc.ay, acc.az, 0.f);
+            o.acc_sorted[2 * (size_t)k + 1] = make_float4(acc.dvx, acc.dvy, acc.dvz, 0.f);
+        }
         integrate_out((size_t)g.ids[k], xi, vi, attr, rp[k], acc, p, p.dt, o);
     }
 }
@@ -822,18 +642,19 @@ __device__ __forceinline__ float kernel_df_over_r(float q, float inv_r, const ns
 }
 
 // visit(j) for every neighbour j != k of sorted particle k, in query order,
-// from the density pass's masks (re-testing when they overflowed)
+// from the density pass's neighbour list (re-testing its candidates when the
+// list overflowed)
 template <class V>
 __device__ __forceinline__ void for_each_neighbor(const GridDev& g, const float4* __restrict__ xs,
-                                                  const unsigned* __restrict__ mask, int nc, int n, int k, float4 xi,
+                                                  const int4* __restrict__ nbr, int cnt, int n, int k, float4 xi,
                                                   const nsph_sph_params& p, V&& visit)
 {
-    if (nc <= kMaskBits) {
-        for_each_masked(
-            g, xi, p.h, [&](int w) { return __ldg(mask + (size_t)w * n + k); },
-            [&](int j) {
-                if (j != k) visit(j);
-            });
+    if (cnt <= kNbrSlots) {
+        NbrReader<true> rd(nbr, n, k, cnt);
+        for (int t = 0; t < cnt; ++t) {
+            const int j = rd.get(t);
+            if (j != k) visit(j);
+        }
     } else {
         for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
             for (int j = lo; j < hi; ++j) {
@@ -868,8 +689,8 @@ __global__ void __launch_bounds__(kSphThreads, 2) k_adj_local(GridDev g, const f
                                                               const float4* __restrict__ vs,
                                                               const float2* __restrict__ aux, int n,
                                                               const __grid_constant__ nsph_sph_params p,
-                                                              const unsigned* __restrict__ mask,
-                                                              const int* __restrict__ ncand, const AdjIO io)
+                                                              const int4* __restrict__ nbr,
+                                                              const int* __restrict__ ncnt, const AdjIO io)
 {
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
         const float4 xi = xs[k], vi = vs[k];
@@ -890,7 +711,7 @@ __global__ void __launch_bounds__(kSphThreads, 2) k_adj_local(GridDev g, const f
                 const float4 a = io.acc[2 * (size_t)k], d = io.acc[2 * (size_t)k + 1];
                 acc = ForceAcc{a.x, a.y, a.z, d.x, d.y, d.z};
             } else {
-                force_single(g, xs, vs, aux, mask, ncand[k], n, k, xi, vi, aux[k].y, p, acc);
+                force_from_list<false>(g, xs, vs, aux, nbr, ncnt[k], n, k, xi, vi, aux[k].y, p, acc);
             }
             const bool dynamic = (attr & kAttrDynamic) != 0;
             float w = 0.f;
@@ -977,8 +798,8 @@ __global__ void __launch_bounds__(kSphThreads, 2) k_adj_pair(GridDev g, const fl
                                                              const float2* __restrict__ aux,
                                                              const float2* __restrict__ rp, int n,
                                                              const __grid_constant__ nsph_sph_params p,
-                                                             const unsigned* __restrict__ mask,
-                                                             const int* __restrict__ ncand, const AdjIO io)
+                                                             const int4* __restrict__ nbr,
+                                                             const int* __restrict__ ncnt, const AdjIO io)
 {
     float bsum = 0.f;
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
@@ -993,7 +814,7 @@ __global__ void __launch_bounds__(kSphThreads, 2) k_adj_pair(GridDev g, const fl
         const float mk = xi.w;
         float pr2b = 0.f, morb = 0.f;
         float xb[3] = {0.f, 0.f, 0.f}, vb[3] = {0.f, 0.f, 0.f};
-        for_each_neighbor(g, xs, mask, ncand[k], n, k, xi, p, [&](int j) {
+        for_each_neighbor(g, xs, nbr, ncnt[k], n, k, xi, p, [&](int j) {
             const float4 vj = __ldg(vs + j);
             if (!(__float_as_int(vj.w) & kAttrActive)) return;
             const float4 xj = __ldg(xs + j);
@@ -1053,8 +874,8 @@ __global__ void __launch_bounds__(kSphThreads, 2) k_adj_pair(GridDev g, const fl
 __global__ void __launch_bounds__(kSphThreads, 3) k_adj_density(GridDev g, const float4* __restrict__ xs,
                                                                 const float4* __restrict__ vs, int n,
                                                                 const __grid_constant__ nsph_sph_params p,
-                                                                const unsigned* __restrict__ mask,
-                                                                const int* __restrict__ ncand,
+                                                                const int4* __restrict__ nbr,
+                                                                const int* __restrict__ ncnt,
                                                                 const float* __restrict__ rho_adj,
                                                                 float* __restrict__ x_in_adj)
 {
@@ -1063,7 +884,7 @@ __global__ void __launch_bounds__(kSphThreads, 3) k_adj_density(GridDev g, const
         const float4 xi = xs[k];
         const float rbk = rho_adj[k], mk = xi.w;
         float xb[3] = {0.f, 0.f, 0.f};
-        for_each_neighbor(g, xs, mask, ncand[k], n, k, xi, p, [&](int j) {
+        for_each_neighbor(g, xs, nbr, ncnt[k], n, k, xi, p, [&](int j) {
             const float4 xj = __ldg(xs + j);
             float dx, dy, dz;
             const float r2 = dist2(xi, xj, dx, dy, dz);
@@ -1465,9 +1286,7 @@ struct nsph_sph {
     float4* vs = nullptr;
     float2* aux = nullptr;
     float2* rp = nullptr;
-    unsigned* mask = nullptr;  // kMaskWords x capacity neighbour bits (word-major)
-    int* ncand = nullptr;      // candidates per particle
-    int4* nbr = nullptr;       // plain and worlds steps: kNbrGroups x capacity neighbour lists (group-major)
+    int4* nbr = nullptr;       // kNbrGroups x capacity neighbour lists (group-major), every step form
     int* ncnt = nullptr;       //   neighbours per particle
     int fast = 0;              // plain step: tolerance arithmetic (nsph_sph_set_arithmetic)
     unsigned* status = nullptr;
@@ -1498,15 +1317,15 @@ struct nsph_sph {
 };
 
 // One step's slot of the segment tape: the sorted mirrors, the density
-// pass's outputs and neighbour masks, the grid (sorted ids, cell table) and
+// pass's outputs and neighbour lists, the grid (sorted ids, cell table) and
 // the force pass's sums.
 struct TapeStep {
     float4* xs;
     float4* vs;
     float2* aux;
     float2* rp;
-    unsigned* mask;
-    int* ncand;
+    int4* nbr;
+    int* ncnt;
     int* ids;
     int2* ranges;
     float4* acc;  // the force pass's (a, 0), (dv, 0) per sorted particle
@@ -1517,7 +1336,7 @@ static size_t tape_align(size_t b) { return (b + 255) & ~(size_t)255; }
 static size_t tape_slot_bytes(size_t c, long long ncells)
 {
     return 2 * tape_align(sizeof(float4) * c) + 2 * tape_align(sizeof(float2) * c) +
-           tape_align(sizeof(unsigned) * kMaskWords * c) + 2 * tape_align(sizeof(int) * c) +
+           tape_align(sizeof(int4) * kNbrGroups * c) + 2 * tape_align(sizeof(int) * c) +
            tape_align(sizeof(int2) * (size_t)ncells) + tape_align(sizeof(float4) * 2 * c);
 }
 
@@ -1534,9 +1353,9 @@ static TapeStep tape_slot(const nsph_sph* s, int t)
     b += tape_align(sizeof(float2) * c);
     ts.rp = reinterpret_cast<float2*>(b);
     b += tape_align(sizeof(float2) * c);
-    ts.mask = reinterpret_cast<unsigned*>(b);
-    b += tape_align(sizeof(unsigned) * kMaskWords * c);
-    ts.ncand = reinterpret_cast<int*>(b);
+    ts.nbr = reinterpret_cast<int4*>(b);
+    b += tape_align(sizeof(int4) * kNbrGroups * c);
+    ts.ncnt = reinterpret_cast<int*>(b);
     b += tape_align(sizeof(int) * c);
     ts.ids = reinterpret_cast<int*>(b);
     b += tape_align(sizeof(int) * c);
@@ -1598,8 +1417,6 @@ static void sph_free(nsph_sph* s)
     cudaFree(s->vs);
     cudaFree(s->aux);
     cudaFree(s->rp);
-    cudaFree(s->mask);
-    cudaFree(s->ncand);
     cudaFree(s->nbr);
     cudaFree(s->ncnt);
     cudaFree(s->wparams);
@@ -1699,15 +1516,11 @@ static int sph_create_common(nsph_sph* s, int device, int capacity)
         if (e == cudaSuccess) e = cudaMalloc(&s->vs, sizeof(float4) * c);
         if (e == cudaSuccess) e = cudaMalloc(&s->aux, sizeof(float2) * c);
         if (e == cudaSuccess) e = cudaMalloc(&s->rp, sizeof(float2) * c);
-        if (e == cudaSuccess) e = cudaMalloc(&s->mask, sizeof(unsigned) * kMaskWords * c);
-        if (e == cudaSuccess) e = cudaMalloc(&s->ncand, sizeof(int) * c);
         if (e == cudaSuccess) e = cudaMalloc(&s->nbr, sizeof(int4) * kNbrGroups * c);
         if (e == cudaSuccess) e = cudaMalloc(&s->ncnt, sizeof(int) * c);
         if (e == cudaSuccess) e = cudaMalloc(&s->status, sizeof(unsigned));
         if (e == cudaSuccess) e = cudaMemset(s->status, 0, sizeof(unsigned));
         cudaFuncAttributes fa;
-        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_density);
-        if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_force);
         if (e == cudaSuccess) e = cudaFuncGetAttributes(&fa, k_neighbors);
         if (e == cudaSuccess) e = cudaDeviceSynchronize();
         if (e != cudaSuccess) {
@@ -2094,13 +1907,13 @@ static int adjoint_kernels(nsph_sph* s, const nsph_sph_params* p, int n, const G
 {
     int blocks, threads;
     pass_launch(s, n, false, blocks, threads);
-    k_adj_local<<<blocks, threads, 0, cs>>>(g, ts.xs, ts.vs, ts.aux, n, *p, ts.mask, ts.ncand, io);
+    k_adj_local<<<blocks, threads, 0, cs>>>(g, ts.xs, ts.vs, ts.aux, n, *p, ts.nbr, ts.ncnt, io);
     NSPH_LAUNCH_CHECK("k_adj_local");
     if (mark && s->eva[3]) NSPH_CUDA_TRY(record_mark(s->eva[3], cs));
-    k_adj_pair<<<blocks, threads, 0, cs>>>(g, ts.xs, ts.vs, ts.aux, ts.rp, n, *p, ts.mask, ts.ncand, io);
+    k_adj_pair<<<blocks, threads, 0, cs>>>(g, ts.xs, ts.vs, ts.aux, ts.rp, n, *p, ts.nbr, ts.ncnt, io);
     NSPH_LAUNCH_CHECK("k_adj_pair");
     if (mark && s->eva[4]) NSPH_CUDA_TRY(record_mark(s->eva[4], cs));
-    k_adj_density<<<blocks, threads, 0, cs>>>(g, ts.xs, ts.vs, n, *p, ts.mask, ts.ncand, io.rho, io.x_in_adj);
+    k_adj_density<<<blocks, threads, 0, cs>>>(g, ts.xs, ts.vs, n, *p, ts.nbr, ts.ncnt, io.rho, io.x_in_adj);
     NSPH_LAUNCH_CHECK("k_adj_density");
     launches += 3;
     if (eos_b_adj) {
@@ -2128,14 +1941,14 @@ static int adjoint_enqueue(nsph_sph* s, const nsph_sph_params* p, int n, const f
         const GridDev g = s->grid.view();
         int blocks, threads;
         pass_launch(s, n, false, blocks, threads);
-        k_density<<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->mask, s->ncand,
-                                                   s->status);
-        NSPH_LAUNCH_CHECK("k_density");
+        k_density_list<false><<<blocks, threads, 0, cs>>>(g, s->xs, s->vs, n, *p, s->aux, s->rp, s->nbr, s->ncnt,
+                                                          s->status);
+        NSPH_LAUNCH_CHECK("k_density_list");
         if (s->eva[2]) NSPH_CUDA_TRY(record_mark(s->eva[2], cs));
         ++launches;
         const AdjIO io{x_out_adj, v_out_adj, rho_out_adj, x_in_adj, v_in_adj, f_ext_adj, f_ext, inv_mass, gravity,
                        s->adj_g, s->adj_d, s->adj_rho, s->adj_bpart};
-        const TapeStep ts{s->xs, s->vs, s->aux, s->rp, s->mask, s->ncand, nullptr, nullptr, nullptr};
+        const TapeStep ts{s->xs, s->vs, s->aux, s->rp, s->nbr, s->ncnt, nullptr, nullptr, nullptr};
         st = adjoint_kernels(s, p, n, g, ts, io, eos_b_adj, cs, launches, true);
         if (st != NSPH_OK) return st;
     } else {
@@ -2290,16 +2103,17 @@ extern "C" int nsph_sph_segment_adjoint(nsph_sph* s, const nsph_sph_params* p, i
         GridDev g = s->grid.view();
         g.ranges = ts.ranges;
         g.ids = ts.ids;
-        k_density<<<blocks, threads, 0, cs>>>(g, ts.xs, ts.vs, n, *p, ts.aux, ts.rp, ts.mask, ts.ncand, s->status);
-        NSPH_LAUNCH_CHECK("k_density");
+        k_density_list<false><<<blocks, threads, 0, cs>>>(g, ts.xs, ts.vs, n, *p, ts.aux, ts.rp, ts.nbr, ts.ncnt,
+                                                          s->status);
+        NSPH_LAUNCH_CHECK("k_density_list");
         ++launches;
         float* xo = tape_state(s, (t + 1) & 1);
         float* vo = xo + len;
         // inactive particles keep their velocity (the step leaves it untouched)
         if (t + 1 < steps) NSPH_CUDA_TRY(cudaMemcpyAsync(vo, vi, sizeof(float) * len, cudaMemcpyDeviceToDevice, cs));
         const StepOut o{f_ext, inv_mass, gravity, xo, vo, nullptr, nullptr, nullptr, s->status, ts.acc};
-        k_force<<<blocks, threads, 0, cs>>>(g, ts.xs, ts.vs, ts.aux, ts.rp, n, *p, ts.mask, ts.ncand, o);
-        NSPH_LAUNCH_CHECK("k_force");
+        k_force_list<false><<<blocks, threads, 0, cs>>>(g, ts.xs, ts.vs, ts.aux, ts.rp, n, *p, ts.nbr, ts.ncnt, o);
+        NSPH_LAUNCH_CHECK("k_force_list");
         ++launches;
     }
     // the solver's mirrors describe its grid's last build (the last step's input)
