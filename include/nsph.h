@@ -62,6 +62,18 @@ NSPH_API const char* nsph_status_string(int status);
 /* Message of the last failed call on this host thread ("" if none). */
 NSPH_API const char* nsph_last_error(void);
 
+/* Build flags of this library: NSPH_BUILD_BOUNDS_CHECK when it was compiled
+ * with -DNSPH_BOUNDS_CHECK (python -m newton_sph_dev_b200._build
+ * --bounds-check, into libnsph_bounds.so). In that build every gather and
+ * scatter of the grid, neighbour and build kernels checks its index; a
+ * violation is counted and the access redirected or skipped, so the check
+ * never faults. */
+#define NSPH_BUILD_BOUNDS_CHECK 1
+NSPH_API int nsph_build_flags(void);
+/* Bounds-check violations counted on the current device since the last
+ * call (the counters are reset); always 0 in the release build. */
+NSPH_API int nsph_debug_bounds_violations(unsigned long long* count);
+
 /* ======================================================================== *
  *  HashGrid — replaces wp.HashGrid(dim_x, dim_y, dim_z)                    *
  *  (builder.py:9853; reserve solver_xpbd.py:139; build solver_xpbd.py:319) *

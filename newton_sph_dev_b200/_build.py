@@ -54,21 +54,32 @@ def needs_rebuild() -> bool:
     return any(p.stat().st_mtime > t for p in sources() + headers() + [Path(__file__)])
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    """Compile libnsph.so if any source is newer than the library."""
-    if not force and not needs_rebuild():
-        return LIB_PATH
-    tmp = LIB_PATH.with_suffix(".so.tmp")
+BOUNDS_LIB_PATH = PKG_DIR / "libnsph_bounds.so"
+
+
+def build(force: bool = False, verbose: bool = False, bounds_check: bool = False) -> Path:
+    """Compile libnsph.so if any source is newer than the library.
+
+    bounds_check: compile the bounds-checked build (-DNSPH_BOUNDS_CHECK) into
+    libnsph_bounds.so instead; load it by setting NSPH_LIBRARY to its path."""
+    out = BOUNDS_LIB_PATH if bounds_check else LIB_PATH
+    if not force and not bounds_check and not needs_rebuild():
+        return out
+    tmp = out.with_suffix(".so.tmp")
     cmd = [nvcc_path(), *NVCC_FLAGS, f"-I{REPO_DIR / 'include'}", "-shared", "-o", str(tmp)]
+    if bounds_check:
+        cmd.append("-DNSPH_BOUNDS_CHECK")
     cmd += [str(s) for s in sources()]
     if verbose:
         print(" ".join(cmd))
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"nvcc failed ({res.returncode}):\n{res.stdout}\n{res.stderr}")
-    os.replace(tmp, LIB_PATH)
-    return LIB_PATH
+    os.replace(tmp, out)
+    return out
 
 
 if __name__ == "__main__":
-    print(build(force=True, verbose=True))
+    import sys
+
+    print(build(force=True, verbose=True, bounds_check="--bounds-check" in sys.argv[1:]))

@@ -11,7 +11,10 @@ import ctypes
 import os
 from pathlib import Path
 
-_LIB_PATH = Path(__file__).resolve().parent / "libnsph.so"
+# NSPH_LIBRARY selects another build of the library (the bounds-checked
+# libnsph_bounds.so, for instance); by default the in-tree libnsph.so
+_LIB_PATH = Path(os.environ["NSPH_LIBRARY"]).resolve() if os.environ.get("NSPH_LIBRARY") else \
+    Path(__file__).resolve().parent / "libnsph.so"
 
 NSPH_OK = 0
 NSPH_ERR_INVALID_ARG = 1
@@ -153,6 +156,8 @@ SIGNATURES = [
     ("nsph_version", ctypes.c_int, []),
     ("nsph_status_string", ctypes.c_char_p, [ctypes.c_int]),
     ("nsph_last_error", ctypes.c_char_p, []),
+    ("nsph_build_flags", ctypes.c_int, []),
+    ("nsph_debug_bounds_violations", ctypes.c_int, [ctypes.POINTER(ctypes.c_ulonglong)]),
     ("nsph_grid_create", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(c_void_p)]),
     ("nsph_grid_destroy", ctypes.c_int, [c_void_p]),
     ("nsph_grid_reserve", ctypes.c_int, [c_void_p, ctypes.c_int]),
@@ -398,3 +403,19 @@ def stream_handle(device) -> int:
     import torch
 
     return torch.cuda.current_stream(device).cuda_stream
+
+
+NSPH_BUILD_BOUNDS_CHECK = 1
+
+
+def bounds_checked() -> bool:
+    """True when the loaded library is the bounds-checked build."""
+    return bool(load().nsph_build_flags() & NSPH_BUILD_BOUNDS_CHECK)
+
+
+def bounds_violations() -> int:
+    """Index violations the bounds-checked build counted on the current
+    device since the last call (0 in the release build)."""
+    v = ctypes.c_ulonglong(0)
+    check(load().nsph_debug_bounds_violations(ctypes.byref(v)), "bounds_violations")
+    return int(v.value)

@@ -41,3 +41,27 @@ extern "C" const char* nsph_status_string(int status)
 }
 
 extern "C" const char* nsph_last_error(void) { return nsph::g_last_error.c_str(); }
+
+extern "C" int nsph_build_flags(void)
+{
+#ifdef NSPH_BOUNDS_CHECK
+    return NSPH_BUILD_BOUNDS_CHECK;
+#else
+    return 0;
+#endif
+}
+
+extern "C" int nsph_debug_bounds_violations(unsigned long long* count)
+{
+    nsph::clear_error();
+    if (!count) return nsph::fail(NSPH_ERR_INVALID_ARG, "null count");
+    unsigned long long total = 0;
+    for (unsigned long long v : {nsph::nsph_bounds_read_hashgrid(), nsph::nsph_bounds_read_sph(),
+                                 nsph::nsph_bounds_read_contact(), nsph::nsph_bounds_read_shapes(),
+                                 nsph::nsph_bounds_read_raycast()}) {
+        if (v == ~0ull) return nsph::fail(NSPH_ERR_CUDA, "cannot read the bounds-check counters");
+        total += v;
+    }
+    *count = total;
+    return NSPH_OK;
+}

@@ -24,6 +24,8 @@
 #include "nsph_internal.cuh"
 
 namespace nsph {
+
+NSPH_BOUNDS_READER(contact)
 namespace {
 
 __device__ __forceinline__ float dot3(float ax, float ay, float az, float bx, float by, float bz)
@@ -192,6 +194,7 @@ extern "C" int nsph_particle_contact_forces(const nsph_grid* grid, const nsph_co
                                             float* f_out, void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_particle_contact_forces");
     int st = check_grid(grid, n);
     if (st != NSPH_OK) return st;
     if (!params) return fail(NSPH_ERR_INVALID_ARG, "null params");
@@ -215,6 +218,7 @@ extern "C" int nsph_particle_contact_deltas(const nsph_grid* grid, int n, const 
                                             float* deltas, void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_particle_contact_deltas");
     int st = check_grid(grid, n);
     if (st != NSPH_OK) return st;
     if (n == 0) return NSPH_OK;

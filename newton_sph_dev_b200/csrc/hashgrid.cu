@@ -34,6 +34,8 @@
 
 namespace nsph {
 
+NSPH_BOUNDS_READER(hashgrid)
+
 namespace {
 
 __device__ __forceinline__ unsigned lanemask_lt()
@@ -456,7 +458,7 @@ __global__ void __launch_bounds__(256) k_cc_scatter(const int* __restrict__ cell
 #pragma unroll
     for (int u = 0; u < kCcPoints; ++u) {
         const int i = t + u * stride;
-        if (i < n) {
+        if (i < n && in_bounds(s[u] >= 0 && s[u] < n)) {
             tmp[s[u]] = i;
             tmp_cells[s[u]] = c[u];
         }
@@ -476,6 +478,7 @@ __global__ void __launch_bounds__(256) k_cc_rank(const int* __restrict__ tmp_cel
     if (q >= n) return;
     const int i = tmp[q];
     const int c = tmp_cells[q];
+    if (!in_bounds(i >= 0 && i < n)) return;
     float4 xs, vs;
     if (do_gather) {  // the gathered loads go out before the rank loop
         const size_t ii = (size_t)i;
@@ -492,6 +495,7 @@ __global__ void __launch_bounds__(256) k_cc_rank(const int* __restrict__ tmp_cel
         vs = make_float4(vx, vy, vz, __int_as_float(attr));
     }
     const int2 se = ranges[c];
+    if (!in_bounds(se.x >= 0 && se.x <= q && q < se.y && se.y <= n)) return;
     int rank = 0;
     for (int t = se.x; t < se.y; ++t) rank += tmp[t] < i;
     if (rank == 0) count[c] = 0;  // the counts start at zero for the next build
@@ -867,6 +871,7 @@ extern "C" int nsph_grid_reserve(nsph_grid* grid, int num_points)
 extern "C" int nsph_grid_build(nsph_grid* grid, const float* points, int num_points, float radius, void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_grid_build");
     if (!grid) return fail(NSPH_ERR_INVALID_ARG, "null grid");
     if (!(radius > 0.f) || !isfinite(radius)) return fail(NSPH_ERR_INVALID_ARG, "radius must be positive and finite");
     DeviceGuard guard(grid->g.device);
@@ -905,6 +910,7 @@ extern "C" int nsph_grid_query(const nsph_grid* grid, const float* queries, int 
                                int* counts, const long long* offsets, int* out_ids, void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_grid_query");
     if (!grid) return fail(NSPH_ERR_INVALID_ARG, "null grid");
     if (!grid->g.built) return fail(NSPH_ERR_NOT_BUILT, "query before build");
     if (num_queries < 0) return fail(NSPH_ERR_INVALID_ARG, "negative query count");
@@ -995,6 +1001,7 @@ extern "C" int nsph_grid_build_noalloc(const float* points, int num_points, floa
                                        void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_grid_build_noalloc");
     if (num_points < 0) return fail(NSPH_ERR_INVALID_ARG, "negative point count");
     if (num_points > NSPH_NOALLOC_MAX_POINTS)
         return fail(NSPH_ERR_CAPACITY, "nsph_grid_build_noalloc: more than NSPH_NOALLOC_MAX_POINTS (" +

@@ -58,6 +58,7 @@ extern "C" int nsph_integrate_particles(const float* x, const float* v, const fl
                                         int num, float dt, float v_max, float* x_new, float* v_new, void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_integrate_particles");
     if (num < 0) return fail(NSPH_ERR_INVALID_ARG, "negative particle count");
     if (num == 0) return NSPH_OK;
     if (!x || !v || !f || !inv_mass || !flags || !gravity || !x_new || !v_new)

@@ -305,6 +305,7 @@ extern "C" int nsph_mlp_forward(int device, const float* model, const float* fea
                                 unsigned int* err, void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_mlp_forward");
     if (n < 0) return fail(NSPH_ERR_INVALID_ARG, "negative count");
     if (n == 0) return NSPH_OK;
     if (!model || !features || !out || !err) return fail(NSPH_ERR_INVALID_ARG, "null argument");
@@ -332,6 +333,7 @@ extern "C" int nsph_mlp_gradient(int device, const float* model, const float* fe
                                  unsigned int* err, void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_mlp_gradient");
     if (batch <= 0) return fail(NSPH_ERR_INVALID_ARG, "batch must be positive");
     if (!model || !features || !targets || !batch_idx || !partials || !grad || !err)
         return fail(NSPH_ERR_INVALID_ARG, "null argument");
@@ -354,6 +356,7 @@ extern "C" int nsph_mlp_adam(int device, float* model, const float* grad, float*
                              float beta2, float eps, int step, void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_mlp_adam");
     if (!model || !grad || !m || !v) return fail(NSPH_ERR_INVALID_ARG, "null argument");
     if (step < 1) return fail(NSPH_ERR_INVALID_ARG, "step counts from 1");
     DeviceGuard guard(device);

@@ -11,6 +11,8 @@
 
 #include <string>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "nsph.h"
 
 namespace nsph {
@@ -20,8 +22,62 @@ namespace nsph {
 // ---------------------------------------------------------------------------
 void set_error(const std::string& msg);
 void clear_error();
+
+// NVTX range over a public entry point (host side; a no-op unless a
+// profiler is attached): the enqueue of a step, build or query shows as one
+// named range on the timeline.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 int fail(int status, const std::string& msg);
 int cuda_fail(cudaError_t err, const char* what);
+
+// ---------------------------------------------------------------------------
+// bounds-checked build (-DNSPH_BOUNDS_CHECK): the kernels' gathers and
+// scatters check their indices; a violation is counted (one counter per
+// translation unit, read by nsph_debug_bounds_violations) and the access is
+// redirected to index 0 or skipped, so the check itself never faults. In the
+// release build in_bounds() is the constant true and the checks compile away.
+// ---------------------------------------------------------------------------
+#ifdef NSPH_BOUNDS_CHECK
+static __device__ unsigned long long g_bounds_violations;
+#endif
+
+__device__ __forceinline__ bool in_bounds(bool ok)
+{
+#ifdef NSPH_BOUNDS_CHECK
+    if (!ok) atomicAdd(&g_bounds_violations, 1ull);
+    return ok;
+#else
+    (void)ok;
+    return true;
+#endif
+}
+
+// defines unsigned long long nsph_bounds_read_<tag>(): this translation
+// unit's violation count on the current device, reset to zero (0 in the
+// release build)
+#ifdef NSPH_BOUNDS_CHECK
+#define NSPH_BOUNDS_READER(tag)                                                                    \
+    unsigned long long nsph_bounds_read_##tag()                                                    \
+    {                                                                                              \
+        unsigned long long v = 0, z = 0;                                                           \
+        if (cudaMemcpyFromSymbol(&v, g_bounds_violations, sizeof(v)) != cudaSuccess) v = ~0ull;    \
+        cudaMemcpyToSymbol(g_bounds_violations, &z, sizeof(z));                                    \
+        return v;                                                                                  \
+    }
+#else
+#define NSPH_BOUNDS_READER(tag) \
+    unsigned long long nsph_bounds_read_##tag() { return 0; }
+#endif
+unsigned long long nsph_bounds_read_hashgrid();
+unsigned long long nsph_bounds_read_sph();
+unsigned long long nsph_bounds_read_contact();
+unsigned long long nsph_bounds_read_shapes();
+unsigned long long nsph_bounds_read_raycast();
 
 #define NSPH_CUDA_TRY(expr)                                   \
     do {                                                      \
@@ -96,6 +152,7 @@ struct GridDev {
     float inv;
     const int2* __restrict__ ranges;  // per cell {start, end} in sorted order, {0,0} if empty
     const int* __restrict__ ids;      // sorted position -> original index
+    int n;                            // points of the build (read by the bounds-checked build only)
 };
 
 // Visit, in Warp's order, the sorted positions of the cells overlapping the
@@ -117,7 +174,9 @@ __device__ __forceinline__ void for_each_run(const GridDev& g, float px, float p
     query_bounds(pz, r, g.inv, g.dz, zs, ze);
     int lo = 0, hi = 0;
     auto visit = [&](int c) {
+        if (!in_bounds(c >= 0 && c < g.dx * g.dy * g.dz)) return;
         const int2 se = __ldg(g.ranges + c);
+        if (!in_bounds(se.x >= 0 && se.x <= se.y && se.y <= g.n)) return;
         if (se.y > se.x) {
             if (se.x == hi && hi > lo) {
                 hi = se.y;
@@ -217,7 +276,7 @@ struct Grid {
     int* cell_count = nullptr;
     int* tile_count = nullptr;
 
-    GridDev view() const { return GridDev{dx, dy, dz, cell_inv, cell_ranges, point_ids}; }
+    GridDev view() const { return GridDev{dx, dy, dz, cell_inv, cell_ranges, point_ids, num_points}; }
 };
 
 // Gather performed by the last radix pass (SPH mode): writes the sorted

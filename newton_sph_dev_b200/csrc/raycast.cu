@@ -32,6 +32,8 @@
 #include "nsph_internal.cuh"
 
 namespace nsph {
+
+NSPH_BOUNDS_READER(raycast)
 namespace {
 
 constexpr int kRayTileX = 32;  // a warp: 32 consecutive pixels of a row
@@ -207,6 +209,7 @@ extern "C" int nsph_raycast_particles(nsph_grid* grid, const float* x, const flo
                                       int max_steps, float* depth, void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_raycast_particles");
     if (!grid || !camera) return fail(NSPH_ERR_INVALID_ARG, "null grid or camera");
     const nsph_raycast_camera& c = *camera;
     if (c.width < 0 || c.height < 0) return fail(NSPH_ERR_INVALID_ARG, "negative image size");

@@ -30,6 +30,8 @@
 #include "nsph_internal.cuh"
 
 namespace nsph {
+
+NSPH_BOUNDS_READER(shapes)
 namespace {
 
 constexpr int kShapeThreads = 256;
@@ -459,6 +461,7 @@ extern "C" int nsph_soft_contacts_create(const nsph_shape* shapes, int shape_cou
                                          nsph_soft_contacts* contacts, int* scratch, void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_soft_contacts_create");
     int st = check_shapes(shapes, shape_count);
     if (st != NSPH_OK) return st;
     st = check_contacts(contacts);
@@ -547,6 +550,7 @@ extern "C" int nsph_apply_particle_deltas(int n, const float* x_orig, const floa
                                           void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_apply_particle_deltas");
     if (n < 0) return fail(NSPH_ERR_INVALID_ARG, "negative particle count");
     if (n == 0) return NSPH_OK;
     if (!x_orig || !x_pred || !flags || !deltas || !x_out || !v_out)

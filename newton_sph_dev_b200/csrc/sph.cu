@@ -28,6 +28,9 @@
 #include "nsph_internal.cuh"
 
 namespace nsph {
+
+NSPH_BOUNDS_READER(sph)
+
 namespace {
 
 constexpr int kSphThreads = 256;
@@ -213,6 +216,7 @@ struct NbrReader {
     __device__ __forceinline__ NbrReader(const int4* nbr, int n, int k, int count)
         : base(nbr + k), stride((size_t)n), cnt(count)
     {
+        in_bounds(count >= 0 && count <= kNbrSlots);
         cur = count > 0 ? load(0) : make_int4(0, 0, 0, 0);
         nxt = count > 4 ? load(1) : make_int4(0, 0, 0, 0);
     }
@@ -223,7 +227,8 @@ struct NbrReader {
             cur = nxt;
             if (t + 4 < cnt) nxt = load((t >> 2) + 1);
         }
-        return u == 0 ? cur.x : (u == 1 ? cur.y : (u == 2 ? cur.z : cur.w));
+        const int j = u == 0 ? cur.x : (u == 1 ? cur.y : (u == 2 ? cur.z : cur.w));
+        return in_bounds(j >= 0 && (size_t)j < stride) ? j : 0;
     }
 };
 
@@ -491,9 +496,9 @@ __global__ void __launch_bounds__(kSphThreads, 4) k_force_list(GridDev g, const 
 // neighbours are found and summed exactly as in the single-world kernels, in
 // its own world's query order.
 __device__ __forceinline__ GridDev world_grid(const WorldCells& c, const int2* __restrict__ ranges,
-                                              const int* __restrict__ ids)
+                                              const int* __restrict__ ids, int n)
 {
-    return GridDev{c.dx, c.dy, c.dz, c.inv, ranges + c.off, ids};
+    return GridDev{c.dx, c.dy, c.dz, c.inv, ranges + c.off, ids, n};
 }
 
 // Bounded to 64 registers (36 bytes of spills outside the candidate loop):
@@ -521,7 +526,7 @@ __global__ void __launch_bounds__(kSphThreads, 4) k_density_worlds(const WorldCe
         }
         const int w = attr >> kAttrGravShift;
         const nsph_sph_params p = wp[w];  // a copy: its fields stay in registers across the candidate loop
-        const GridDev g = world_grid(wc[w], ranges, ids);
+        const GridDev g = world_grid(wc[w], ranges, ids, n);
         const int cnt = neighbor_list(g, xs, p, xi, nbr, n, k);
         ncnt[k] = cnt;
         const float rho = density_from_list<false>(g, xs, p, xi, nbr, cnt, n, k);
@@ -547,7 +552,7 @@ __global__ void __launch_bounds__(kSphThreads, 4) k_force_worlds(const WorldCell
         const int attr = __float_as_int(vi.w);
         const int w = attr >> kAttrGravShift;
         const nsph_sph_params& p = wp[w];
-        const GridDev g = world_grid(wc[w], ranges, ids);
+        const GridDev g = world_grid(wc[w], ranges, ids, n);
         ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         if (attr & kAttrActive) force_from_list<false>(g, xs, vs, aux, nbr, ncnt[k], n, k, xi, vi, aux[k].y, p, acc);
         integrate_out((size_t)ids[k], xi, vi, attr, rp[k], acc, p, dt, o);
@@ -570,7 +575,7 @@ __global__ void k_neighbors_worlds(const WorldCells* __restrict__ wc, const nsph
     if (attr & kAttrActive) {
         const int w = attr >> kAttrGravShift;
         const float h = wp[w].h, h2 = wp[w].h2;
-        const GridDev g = world_grid(wc[w], ranges, ids);
+        const GridDev g = world_grid(wc[w], ranges, ids, n);
         for_each_candidate(g, xi.x, xi.y, xi.z, h, [&](int j) {
             float dx, dy, dz;
             if (dist2(xi, xs[j], dx, dy, dz) < h2 && (__float_as_int(vs[j].w) & kAttrActive)) {
@@ -1613,6 +1618,7 @@ extern "C" int nsph_sph_step(nsph_sph* s, const nsph_sph_params* p, int n, const
                              float* v_out, float* rho_out, float* p_out, float* a_out, void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_sph_step");
     if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
     int st = check_params(p);
     if (st == NSPH_OK) st = check_step_inputs(s, n, x_in, v_in, mass, inv_mass, flags, gravity, world_count);
@@ -1641,6 +1647,7 @@ extern "C" int nsph_sph_rollout(nsph_sph* s, const nsph_sph_params* p, int n, in
                                 float* x_traj, float* v_traj, void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_sph_rollout");
     if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
     int st = check_params(p);
     if (st == NSPH_OK) st = check_step_inputs(s, n, x0, v0, mass, inv_mass, flags, gravity, world_count);
@@ -1700,6 +1707,7 @@ extern "C" int nsph_sph_step_worlds(nsph_sph* s, float dt, int n, const float* x
                                     float* v_out, float* rho_out, float* p_out, float* a_out, void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_sph_step_worlds");
     if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
     if (s->grid.world_count <= 0) return fail(NSPH_ERR_INVALID_ARG, "solver was not created for batched worlds");
     if (!s->wparams_set) return fail(NSPH_ERR_INVALID_ARG, "world parameters not set (nsph_sph_set_world_params)");
@@ -1974,6 +1982,7 @@ extern "C" int nsph_sph_step_adjoint(nsph_sph* s, const nsph_sph_params* p, int 
                                      void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_sph_step_adjoint");
     if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
     int st = check_params(p);
     if (st == NSPH_OK) st = check_adjoint_ready(s);
@@ -2000,6 +2009,7 @@ extern "C" int nsph_sph_rollout_adjoint(nsph_sph* s, const nsph_sph_params* p, i
                                         float* f_ext_adj, float* eos_b_adj, void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_sph_rollout_adjoint");
     if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
     int st = check_params(p);
     if (st == NSPH_OK) st = check_adjoint_ready(s);
@@ -2062,6 +2072,7 @@ extern "C" int nsph_sph_segment_adjoint(nsph_sph* s, const nsph_sph_params* p, i
                                         float* f_ext_adj, float* eos_b_adj, void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_sph_segment_adjoint");
     if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
     int st = check_params(p);
     if (st == NSPH_OK) st = check_adjoint_ready(s);
@@ -2304,6 +2315,7 @@ extern "C" int nsph_sph_features(nsph_sph* s, const nsph_sph_params* p, int n, c
                                  float* rho_out, void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_sph_features");
     if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
     int st = check_params(p);
     if (st == NSPH_OK) st = check_surrogate_ready(s);
@@ -2337,6 +2349,7 @@ extern "C" int nsph_sph_step_surrogate(nsph_sph* s, const nsph_sph_params* p, co
                                        float* rho_out, float* p_out, float* stats, void* stream)
 {
     clear_error();
+    NvtxRange nvtx_range("nsph_sph_step_surrogate");
     if (!s) return fail(NSPH_ERR_INVALID_ARG, "null solver");
     int st = check_params(p);
     if (st == NSPH_OK) st = check_surrogate_ready(s);

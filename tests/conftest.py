@@ -17,6 +17,24 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200, sm_100a)")
 
 
+@pytest.fixture(autouse=True)
+def _no_bounds_violations(request):
+    """With the bounds-checked build loaded (NSPH_LIBRARY=.../libnsph_bounds.so),
+    every GPU test must end with no index violation counted by the kernels."""
+    import os
+
+    yield
+    if not os.environ.get("NSPH_LIBRARY") or request.node.get_closest_marker("gpu") is None:
+        return
+    from newton_sph_dev_b200 import _lib
+
+    if _lib.bounds_checked():
+        import torch
+
+        torch.cuda.synchronize()
+        assert _lib.bounds_violations() == 0, "the bounds-checked build counted index violations"
+
+
 @pytest.fixture(scope="session")
 def oracle_mod():
     from oracle import oracle
