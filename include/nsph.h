@@ -420,19 +420,27 @@ NSPH_API int nsph_particle_contact_deltas(const nsph_grid* grid, int n, const fl
 NSPH_API int nsph_fp32_peak(int device, int iters, float* tflops, float* warp_inst_per_s, float* ms, void* stream);
 
 /* ---- particles against static analytic shapes; the XPBD particle update --
- * Shapes without a body (body -1: ground planes, world-fixed spheres and
- * boxes), as ModelBuilder.add_shape_plane / add_ground_plane /
- * add_shape_sphere / add_shape_box make them (newton/_src/sim/builder.py:
- * 5611-5891). `type` takes the reference's GeoType values. The world
- * transform is (pos, rot) with rot an (x, y, z, w) unit quaternion; scale is
- * (radius, -, -) for a sphere, the half extents for a box and (width,
- * length, -) for a plane (0 = infinite). ke/kd/kf/mu are the shape's
- * material (ShapeConfig). */
+ * Shapes without a body (body -1: ground planes and world-fixed spheres,
+ * boxes, capsules, cylinders, cones and ellipsoids), as
+ * ModelBuilder.add_shape_plane / add_ground_plane / add_shape_sphere /
+ * add_shape_box / add_shape_capsule / add_shape_cylinder / add_shape_cone /
+ * add_shape_ellipsoid make them (newton/_src/sim/builder.py:5611-6050).
+ * `type` takes the reference's GeoType values. The world transform is (pos,
+ * rot) with rot an (x, y, z, w) unit quaternion; scale is (radius, -, -)
+ * for a sphere, the half extents for a box, (width, length, -) for a plane
+ * (0 = infinite), (radius, half_height, -) for a capsule, cylinder or cone
+ * (axis local +Z; a cone's apex at +half_height) and the semi-axes for an
+ * ellipsoid. ke/kd/kf/mu are the shape's material (ShapeConfig). */
 #define NSPH_GEO_PLANE 1
 #define NSPH_GEO_SPHERE 3
+#define NSPH_GEO_CAPSULE 4
+#define NSPH_GEO_ELLIPSOID 5
+#define NSPH_GEO_CYLINDER 6
 #define NSPH_GEO_BOX 7
+#define NSPH_GEO_CONE 9
 typedef struct nsph_shape {
-    int   type;      /* GeoType: PLANE 1, SPHERE 3, BOX 7 (others never make contacts) */
+    int   type;      /* GeoType: PLANE 1, SPHERE 3, CAPSULE 4, ELLIPSOID 5, CYLINDER 6, BOX 7, CONE 9
+                        (others never make contacts) */
     int   flags;     /* ShapeFlags; COLLIDE_PARTICLES (1 << 2) enables particle contacts */
     int   world;     /* shape_world; -1 = every world */
     int   reserved;

@@ -4,7 +4,8 @@
 //   nsph_soft_contacts_create            create_soft_contacts
 //       (newton/_src/geometry/kernels.py:1001-1140, launched by the
 //       collision pipeline, newton/_src/sim/collide.py:1194-1228) for
-//       shapes of type PLANE, SPHERE and BOX without a body
+//       shapes of type PLANE, SPHERE, BOX, CAPSULE, CYLINDER, CONE and
+//       ELLIPSOID without a body
 //   nsph_particle_shape_contact_forces   eval_particle_body_contact
 //       (newton/_src/solvers/semi_implicit/kernels_contact.py:143-262)
 //   nsph_particle_shape_contact_deltas   solve_particle_shape_contacts
@@ -102,10 +103,106 @@ __device__ __forceinline__ Xform xform_inverse(const Xform& X)
     return Xform{v3(-t.x, -t.y, -t.z), ui, X.w};
 }
 
+__device__ __forceinline__ float sgnf(float v) { return v < 0.f ? -1.f : 1.f; }
+__device__ __forceinline__ float len2(float a, float b) { return __fsqrt_rn(__fadd_rn(__fmul_rn(a, a), __fmul_rn(b, b))); }
+// v / |v| when |v| > 1e-8, else the fallback direction
+__device__ __forceinline__ V3 unit_or(V3 v, V3 fallback)
+{
+    const float l = length(v);
+    return l > 1.0e-8f ? divs(v, l) : fallback;
+}
+
+// signed distance of the capped cone about +Z with the given bottom (z =
+// -hh) and top (z = +hh) radii (_sdf_capped_cone_z,
+// newton/_src/geometry/kernels.py:141-161)
+__device__ __forceinline__ float capped_cone_z(float rb, float rt, float hh, V3 x)
+{
+    const float qx = len2(x.x, x.y), qy = x.z;
+    const float k1x = rt, k1y = hh;
+    const float k2x = __fsub_rn(rt, rb), k2y = __fmul_rn(2.f, hh);
+    const float cax = __fsub_rn(qx, fminf(qx, qy < 0.f ? rb : rt));
+    const float cay = __fsub_rn(fabsf(qy), hh);
+    const float denom = __fadd_rn(__fmul_rn(k2x, k2x), __fmul_rn(k2y, k2y));
+    float t = 0.f;
+    if (denom > 0.f) {
+        const float num = __fadd_rn(__fmul_rn(__fsub_rn(k1x, qx), k2x), __fmul_rn(__fsub_rn(k1y, qy), k2y));
+        t = fminf(fmaxf(__fdiv_rn(num, denom), 0.f), 1.f);
+    }
+    const float cbx = __fadd_rn(__fsub_rn(qx, k1x), __fmul_rn(k2x, t));
+    const float cby = __fadd_rn(__fsub_rn(qy, k1y), __fmul_rn(k2y, t));
+    const float sign = (cbx < 0.f && cay < 0.f) ? -1.f : 1.f;
+    const float da = __fadd_rn(__fmul_rn(cax, cax), __fmul_rn(cay, cay));
+    const float db = __fadd_rn(__fmul_rn(cbx, cbx), __fmul_rn(cby, cby));
+    return __fmul_rn(sign, __fsqrt_rn(fminf(da, db)));
+}
+
 // signed distance and outward direction of a shape in its local frame
-// (sdf_* / sdf_*_grad, newton/_src/geometry/kernels.py:165-250, 568-600)
+// (sdf_* / sdf_*_grad, newton/_src/geometry/kernels.py:165-600; capsules,
+// cylinders and cones along local +Z as create_soft_contacts uses them)
 __device__ __forceinline__ bool shape_sdf(const nsph_shape& s, V3 x, float& d, V3& n)
 {
+    if (s.type == NSPH_GEO_CAPSULE) {
+        const float r = s.scale[0], hh = s.scale[1];
+        if (x.z > hh) {
+            const V3 v = v3(x.x, x.y, __fsub_rn(x.z, hh));
+            d = __fsub_rn(length(v), r);
+            n = unit_or(v, v3(0.f, 0.f, 1.f));
+        } else if (x.z < -hh) {
+            const V3 v = v3(x.x, x.y, __fadd_rn(x.z, hh));
+            d = __fsub_rn(length(v), r);
+            n = unit_or(v, v3(0.f, 0.f, -1.f));
+        } else {
+            const V3 v = v3(x.x, x.y, 0.f);
+            d = __fsub_rn(length(v), r);
+            n = unit_or(v, v3(0.f, 0.f, 1.f));
+        }
+        return true;
+    }
+    if (s.type == NSPH_GEO_CYLINDER) {
+        const float r = s.scale[0], hh = s.scale[1];
+        const V3 v = v3(x.x, x.y, 0.f);
+        const float vl = length(v);
+        const float dx = __fsub_rn(vl, r), dy = __fsub_rn(fabsf(x.z), hh);
+        d = __fadd_rn(fminf(fmaxf(dx, dy), 0.f), len2(fmaxf(dx, 0.f), fmaxf(dy, 0.f)));
+        const V3 radial = vl > 1.0e-8f ? divs(v, vl) : v3(0.f, 0.f, 1.f);
+        const V3 axial = v3(0.f, 0.f, sgnf(x.z));
+        if (dx > 0.f && dy > 0.f)
+            n = unit_or(add(mul(radial, dx), mul(axial, dy)), radial);
+        else
+            n = dx > dy ? radial : axial;
+        return true;
+    }
+    if (s.type == NSPH_GEO_CONE) {
+        const float r = s.scale[0], hh = s.scale[1];
+        d = capped_cone_z(r, 0.f, hh, x);
+        if (hh <= 0.f) {
+            n = v3(0.f, 0.f, sgnf(x.z));
+            return true;
+        }
+        const float rl = length(v3(x.x, x.y, 0.f));
+        const float h2 = __fmul_rn(2.f, hh);
+        const float dx = __fsub_rn(rl, __fdiv_rn(__fmul_rn(r, __fsub_rn(hh, x.z)), h2));
+        const float dy = __fsub_rn(fabsf(x.z), hh);
+        if (dx > dy) {
+            n = rl > 0.f ? normalize(add(divs(v3(x.x, x.y, 0.f), rl), v3(0.f, 0.f, __fdiv_rn(r, h2))))
+                         : v3(0.f, 0.f, 1.f);
+        } else {
+            n = v3(0.f, 0.f, sgnf(x.z));
+        }
+        return true;
+    }
+    if (s.type == NSPH_GEO_ELLIPSOID) {
+        const float e = 1.0e-8f;
+        const V3 r = v3(fmaxf(fabsf(s.scale[0]), e), fmaxf(fabsf(s.scale[1]), e), fmaxf(fabsf(s.scale[2]), e));
+        const V3 ir = v3(__fdiv_rn(1.f, r.x), __fdiv_rn(1.f, r.y), __fdiv_rn(1.f, r.z));
+        const V3 ir2 = v3(__fmul_rn(ir.x, ir.x), __fmul_rn(ir.y, ir.y), __fmul_rn(ir.z, ir.z));
+        const V3 q0 = v3(__fmul_rn(x.x, ir.x), __fmul_rn(x.y, ir.y), __fmul_rn(x.z, ir.z));
+        const V3 q1 = v3(__fmul_rn(x.x, ir2.x), __fmul_rn(x.y, ir2.y), __fmul_rn(x.z, ir2.z));
+        const float k0 = length(q0), k1 = length(q1);
+        d = k1 > e ? __fdiv_rn(__fmul_rn(k0, __fsub_rn(k0, 1.f)), k1) : -fminf(fminf(r.x, r.y), r.z);
+        n = k1 < e ? v3(0.f, 0.f, 1.f) : unit_or(mul(q1, __fdiv_rn(k0, k1)), v3(0.f, 0.f, 1.f));
+        return true;
+    }
     if (s.type == NSPH_GEO_SPHERE) {
         const float l = length(x);
         d = __fsub_rn(l, s.scale[0]);

@@ -24,8 +24,9 @@ class ShapeFlags(IntEnum):
 
 
 class GeoType(IntEnum):
-    """Shape types. This library makes particle contacts with PLANE, SPHERE
-    and BOX shapes that belong to no body."""
+    """Shape types. This library makes particle contacts with PLANE, SPHERE,
+    BOX, CAPSULE, CYLINDER, CONE and ELLIPSOID shapes that belong to no
+    body."""
 
     NONE = 0
     PLANE = 1

@@ -104,6 +104,18 @@ class ModelBuilder:
             self.is_visible = is_visible
             self.is_site = is_site
 
+        def copy(self) -> "ModelBuilder.ShapeConfig":
+            c = ModelBuilder.ShapeConfig()
+            c.__dict__.update(self.__dict__)
+            return c
+
+        def mark_as_site(self) -> None:
+            """A site: no shape or particle collision, zero density (builder.py:389-403)."""
+            self.is_site = True
+            self.has_shape_collision = False
+            self.has_particle_collision = False
+            self.density = 0.0
+
         @property
         def flags(self) -> int:
             f = int(ShapeFlags.VISIBLE) if self.is_visible else 0
@@ -329,16 +341,58 @@ class ModelBuilder:
         return self.add_shape_plane(plane=(*self.up_vector, -height), width=0.0, length=0.0, cfg=cfg,
                                     label=label or "ground_plane")
 
+    def _shape_cfg(self, cfg, as_site: bool):
+        """The shape's config; a site gets a copy marked as one (as the
+        reference's add_shape_* do with as_site)."""
+        if not as_site:
+            return cfg
+        cfg = (cfg if cfg is not None else self.default_shape_cfg).copy()
+        cfg.mark_as_site()
+        return cfg
+
     def add_shape_sphere(self, body: int, xform=None, radius: float = 1.0, cfg: ShapeConfig | None = None,
                          as_site: bool = False, color=None, label: str | None = None, custom_attributes=None) -> int:
         """A sphere of the given radius centred at xform (builder.py:5703)."""
-        return self.add_shape(body, GeoType.SPHERE, xform, cfg, (radius, 0.0, 0.0), label=label)
+        return self.add_shape(body, GeoType.SPHERE, xform, self._shape_cfg(cfg, as_site), (radius, 0.0, 0.0),
+                              label=label)
 
     def add_shape_box(self, body: int, xform=None, hx: float = 0.5, hy: float = 0.5, hz: float = 0.5,
                       cfg: ShapeConfig | None = None, as_site: bool = False, color=None, label: str | None = None,
                       custom_attributes=None) -> int:
         """A box with half extents (hx, hy, hz) at xform (builder.py:5842)."""
-        return self.add_shape(body, GeoType.BOX, xform, cfg, (hx, hy, hz), label=label)
+        return self.add_shape(body, GeoType.BOX, xform, self._shape_cfg(cfg, as_site), (hx, hy, hz), label=label)
+
+    def add_shape_ellipsoid(self, body: int, xform=None, rx: float = 1.0, ry: float = 0.75, rz: float = 0.5,
+                            cfg: ShapeConfig | None = None, as_site: bool = False, color=None,
+                            label: str | None = None, custom_attributes=None, **kwargs) -> int:
+        """An ellipsoid with semi-axes (rx, ry, rz) along its local axes
+        (builder.py:5747-5790). Its particle contacts use the reference's
+        approximate SDF k0 (k0 - 1) / k1."""
+        return self.add_shape(body, GeoType.ELLIPSOID, xform, self._shape_cfg(cfg, as_site), (rx, ry, rz),
+                              label=label)
+
+    def add_shape_capsule(self, body: int, xform=None, radius: float = 1.0, half_height: float = 0.5,
+                          cfg: ShapeConfig | None = None, as_site: bool = False, color=None,
+                          label: str | None = None, custom_attributes=None) -> int:
+        """A capsule along its local Z axis: a cylinder of the given radius
+        and half height with hemispherical ends (builder.py:5892-5943)."""
+        return self.add_shape(body, GeoType.CAPSULE, xform, self._shape_cfg(cfg, as_site), (radius, half_height, 0.0),
+                              label=label)
+
+    def add_shape_cylinder(self, body: int, xform=None, radius: float = 1.0, half_height: float = 0.5,
+                           cfg: ShapeConfig | None = None, as_site: bool = False, color=None,
+                           label: str | None = None, custom_attributes=None) -> int:
+        """A cylinder along its local Z axis (builder.py:5945-5996)."""
+        return self.add_shape(body, GeoType.CYLINDER, xform, self._shape_cfg(cfg, as_site),
+                              (radius, half_height, 0.0), label=label)
+
+    def add_shape_cone(self, body: int, xform=None, radius: float = 1.0, half_height: float = 0.5,
+                       cfg: ShapeConfig | None = None, as_site: bool = False, color=None, label: str | None = None,
+                       custom_attributes=None) -> int:
+        """A cone along its local Z axis, base of the given radius at
+        -half_height and apex at +half_height (builder.py:5998-6050)."""
+        return self.add_shape(body, GeoType.CONE, xform, self._shape_cfg(cfg, as_site), (radius, half_height, 0.0),
+                              label=label)
 
     @property
     def shape_count(self) -> int:

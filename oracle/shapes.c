@@ -6,8 +6,10 @@
  * Restates, operation by operation, for shapes without a body (identity
  * body transform, zero body velocity):
  *   create_soft_contacts              newton/_src/geometry/kernels.py:1001-1140
- *     with sdf_sphere / sdf_box / sdf_plane and their gradients (:165-250,
- *     :568-600), contacts in (particle, shape) order
+ *     with sdf_sphere / sdf_box / sdf_capsule / sdf_cylinder / sdf_cone /
+ *     sdf_ellipsoid / sdf_plane and their gradients (:132-600; capsules,
+ *     cylinders and cones along local +Z), contacts in (particle, shape)
+ *     order
  *   eval_particle_body_contact        newton/_src/solvers/semi_implicit/kernels_contact.py:143-262
  *   solve_particle_shape_contacts     newton/_src/solvers/xpbd/kernels.py:115-222
  *   apply_particle_shape_restitution  newton/_src/solvers/xpbd/kernels.py:34-112
@@ -59,8 +61,90 @@ static inline v3 qrot(v3 u, float w, v3 v)
     return add(add(a, b), d);
 }
 
+static inline float sgn(float v) { return v < 0.0f ? -1.0f : 1.0f; }
+static inline float len2(float a, float b) { return sqrtf(a * a + b * b); }
+static inline v3 unit_or(v3 v, v3 fallback)
+{
+    const float l = len(v);
+    return l > 1.0e-8f ? divs(v, l) : fallback;
+}
+
+/* _sdf_capped_cone_z (kernels.py:141-161): bottom radius rb at z = -hh, top rt at +hh */
+static float capped_cone_z(float rb, float rt, float hh, v3 x)
+{
+    const float qx = len2(x.x, x.y), qy = x.z;
+    const float k1x = rt, k1y = hh, k2x = rt - rb, k2y = 2.0f * hh;
+    const float cax = qx - fminf(qx, qy < 0.0f ? rb : rt), cay = fabsf(qy) - hh;
+    const float denom = k2x * k2x + k2y * k2y;
+    float t = 0.0f;
+    if (denom > 0.0f) t = fminf(fmaxf(((k1x - qx) * k2x + (k1y - qy) * k2y) / denom, 0.0f), 1.0f);
+    const float cbx = (qx - k1x) + k2x * t, cby = (qy - k1y) + k2y * t;
+    const float sign = (cbx < 0.0f && cay < 0.0f) ? -1.0f : 1.0f;
+    return sign * sqrtf(fminf(cax * cax + cay * cay, cbx * cbx + cby * cby));
+}
+
 static int sdf(const nsph_shape* s, v3 x, float* d, v3* n)
 {
+    if (s->type == NSPH_GEO_CAPSULE) { /* sdf_capsule / _grad, kernels.py:262-329 */
+        const float r = s->scale[0], hh = s->scale[1];
+        v3 v, fb;
+        if (x.z > hh) {
+            v = mk(x.x, x.y, x.z - hh);
+            fb = mk(0.0f, 0.0f, 1.0f);
+        } else if (x.z < -hh) {
+            v = mk(x.x, x.y, x.z + hh);
+            fb = mk(0.0f, 0.0f, -1.0f);
+        } else {
+            v = mk(x.x, x.y, 0.0f);
+            fb = mk(0.0f, 0.0f, 1.0f);
+        }
+        *d = len(v) - r;
+        *n = unit_or(v, fb);
+        return 1;
+    }
+    if (s->type == NSPH_GEO_CYLINDER) { /* sdf_cylinder / _grad, kernels.py:332-446 */
+        const float r = s->scale[0], hh = s->scale[1];
+        const v3 v = mk(x.x, x.y, 0.0f);
+        const float vl = len(v);
+        const float dx = vl - r, dy = fabsf(x.z) - hh;
+        *d = fminf(fmaxf(dx, dy), 0.0f) + len2(fmaxf(dx, 0.0f), fmaxf(dy, 0.0f));
+        const v3 radial = vl > 1.0e-8f ? divs(v, vl) : mk(0.0f, 0.0f, 1.0f);
+        const v3 axial = mk(0.0f, 0.0f, sgn(x.z));
+        if (dx > 0.0f && dy > 0.0f)
+            *n = unit_or(add(mul(radial, dx), mul(axial, dy)), radial);
+        else
+            *n = dx > dy ? radial : axial;
+        return 1;
+    }
+    if (s->type == NSPH_GEO_CONE) { /* sdf_cone / _grad, kernels.py:515-565 */
+        const float r = s->scale[0], hh = s->scale[1];
+        *d = capped_cone_z(r, 0.0f, hh, x);
+        if (hh <= 0.0f) {
+            *n = mk(0.0f, 0.0f, sgn(x.z));
+            return 1;
+        }
+        const float rl = len(mk(x.x, x.y, 0.0f));
+        const float h2 = 2.0f * hh;
+        const float dx = rl - (r * (hh - x.z)) / h2, dy = fabsf(x.z) - hh;
+        if (dx > dy)
+            *n = rl > 0.0f ? normalize(add(divs(mk(x.x, x.y, 0.0f), rl), mk(0.0f, 0.0f, r / h2)))
+                           : mk(0.0f, 0.0f, 1.0f);
+        else
+            *n = mk(0.0f, 0.0f, sgn(x.z));
+        return 1;
+    }
+    if (s->type == NSPH_GEO_ELLIPSOID) { /* sdf_ellipsoid / _grad, kernels.py:449-512 */
+        const float e = 1.0e-8f;
+        const v3 r = mk(fmaxf(fabsf(s->scale[0]), e), fmaxf(fabsf(s->scale[1]), e), fmaxf(fabsf(s->scale[2]), e));
+        const v3 ir = mk(1.0f / r.x, 1.0f / r.y, 1.0f / r.z);
+        const v3 ir2 = mk(ir.x * ir.x, ir.y * ir.y, ir.z * ir.z);
+        const v3 q0 = mk(x.x * ir.x, x.y * ir.y, x.z * ir.z);
+        const v3 q1 = mk(x.x * ir2.x, x.y * ir2.y, x.z * ir2.z);
+        const float k0 = len(q0), k1 = len(q1);
+        *d = k1 > e ? (k0 * (k0 - 1.0f)) / k1 : -fminf(fminf(r.x, r.y), r.z);
+        *n = k1 < e ? mk(0.0f, 0.0f, 1.0f) : unit_or(mul(q1, k0 / k1), mk(0.0f, 0.0f, 1.0f));
+        return 1;
+    }
     if (s->type == NSPH_GEO_SPHERE) {
         const float l = len(x);
         *d = l - s->scale[0];

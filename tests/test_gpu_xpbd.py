@@ -4,7 +4,9 @@ steps on the GPU, through the Newton-shaped API -> the C ABI.
 Bars:
   - Model.collide (nsph_soft_contacts_create): contact count, particles,
     shapes, points and normals bit-exact against the oracle, in (particle,
-    shape) order, over several blocks of particles;
+    shape) order, over several blocks of particles, for every shape type
+    (ground and finite planes, sphere, box, capsule, cylinder, cone,
+    ellipsoid);
   - the contact kernels (forces, XPBD deltas, restitution) and
     apply_particle_deltas bit-exact against the oracle on those contacts;
   - SolverXPBD.step (iterations, particle-particle and particle-shape
@@ -43,6 +45,14 @@ def _scene(n=3000, seed=3, up_axis="Z", restitution=0.5):
     b.add_shape_sphere(-1, xform=((0.3, 0.2, 0.4), (0.0, 0.0, 0.0, 1.0)), radius=0.3, cfg=cfg)
     b.add_shape_box(-1, xform=((-0.5, -0.4, 0.3), (0.0, 0.0, 0.38268343, 0.92387953)), hx=0.3, hy=0.2, hz=0.25)
     b.add_shape_plane(plane=(1.0, 0.0, 0.0, 0.9), width=1.0, length=3.0)  # finite, facing +x at x = -0.9
+    # the round shapes, each tilted off its local +Z axis
+    b.add_shape_capsule(-1, xform=((0.55, -0.5, 0.45), (0.25881905, 0.0, 0.0, 0.96592583)), radius=0.15,
+                        half_height=0.2, cfg=cfg)
+    b.add_shape_cylinder(-1, xform=((-0.4, 0.55, 0.4), (0.0, 0.38268343, 0.0, 0.92387953)), radius=0.2,
+                         half_height=0.15)
+    b.add_shape_cone(-1, xform=((0.65, 0.6, 0.3), (0.0, 0.0, 0.0, 1.0)), radius=0.25, half_height=0.2, cfg=cfg)
+    b.add_shape_ellipsoid(-1, xform=((0.0, -0.15, 0.65), (0.18301270, 0.18301270, 0.0, 0.96592583)), rx=0.3,
+                          ry=0.15, rz=0.1)
     m = b.finalize(DEV)
     m.soft_contact_restitution = restitution
     m.particle_mu = 0.4
@@ -78,6 +88,7 @@ def test_collide_matches_oracle(oracle_mod):
                                           world=md["world"], margin=0.01)
     got = _contacts_host(c)
     assert got["count"][0] == ref["count"][0] > 1000
+    assert set(got["shape"][:got["n"]].tolist()) == set(range(len(md["shapes"]))), "every shape makes contacts"
     k = ref["n"]
     for key in ("particle", "shape", "body_pos", "body_vel", "normal"):
         np.testing.assert_array_equal(got[key][:k], ref[key][:k], err_msg=key)

@@ -6,8 +6,13 @@ Pins oracle/shapes.c (the restatement the GPU kernels are checked against):
     newton/_src/geometry/kernels.py:1001-1140): sphere, box (outside and
     inside), infinite and finite plane, a plane rotated onto +Y, the margin,
     the COLLIDE_PARTICLES flag and the world filter;
+  - known answers of the capsule, cylinder, cone and ellipsoid SDFs
+    (sdf_capsule / sdf_cylinder / sdf_cone / sdf_ellipsoid and their
+    gradients, newton/_src/geometry/kernels.py:132-565);
   - the signed distances and contact points of random particles against an
-    fp64 numpy restatement of the SDFs;
+    fp64 numpy restatement of the SDFs (capsule, cylinder and cone from
+    their exact distances: to a segment, to a rectangle and to a triangle in
+    the (radius, z) half plane);
   - known answers of the contact laws (eval_particle_body_contact,
     solve_particle_shape_contacts, apply_particle_shape_restitution) and of
     apply_particle_deltas (newton/_src/solvers/xpbd/kernels.py:777-808);
@@ -21,7 +26,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-PLANE, SPHERE, BOX = 1, 3, 7
+PLANE, SPHERE, CAPSULE, ELLIPSOID, CYLINDER, BOX, CONE = 1, 3, 4, 5, 6, 7, 9
 COLLIDE = 1 << 2
 
 
@@ -119,6 +124,137 @@ def _sdf64(s, p):
         d = q[2]
         n = np.array([0.0, 0.0, 1.0])
     return d, np.asarray(s["pos"]) + q - n * d, n
+
+
+def test_round_shape_known_answers(oracle_mod):
+    """Capsule, cylinder, cone and ellipsoid contacts at points whose
+    distance, contact point and normal are known in closed form."""
+    O = oracle_mod
+    shapes = [dict(type=CAPSULE, pos=(0, 0, 0), scale=(0.5, 1.0, 0)),
+              dict(type=CYLINDER, pos=(5, 0, 0), scale=(0.5, 1.0, 0)),
+              dict(type=CONE, pos=(10, 0, 0), scale=(0.5, 0.5, 0)),
+              dict(type=ELLIPSOID, pos=(15, 0, 0), scale=(1.0, 0.5, 0.5))]
+    s5 = 1.0 / np.sqrt(5.0)
+    x = np.array([[0.7, 0, 0.2],      # capsule side: d 0.2
+                  [0, 0, 1.6],        # capsule top cap: d 0.1
+                  [0, 0, -1.55],      # capsule bottom cap: d 0.05
+                  [0, 0, 0.3],        # on the capsule axis: the fallback normal +z, d -0.5
+                  [5.6, 0, 0],        # cylinder side: d 0.1
+                  [5, 0, 1.05],       # cylinder top: d 0.05
+                  [5.6, 0, 1.1],      # cylinder rim: d 0.1 sqrt 2 along (1, 0, 1) / sqrt 2
+                  [5.2, 0, 0.9],      # inside the cylinder, nearest the top: d -0.1
+                  [10, 0, 0.6],       # above the cone's apex: d 0.1
+                  [10, 0, -0.55],     # below the cone's base: d 0.05
+                  [10 + 0.25 + 0.1 * 2 * s5, 0, 0.1 * s5],  # off the cone's side by 0.1 along (2, 0, 1) / sqrt 5
+                  [17, 0, 0],         # ellipsoid: 1 beyond the x semi-axis
+                  [15, 0.7, 0]],      # ellipsoid: 0.2 beyond the y semi-axis
+                 np.float32)
+    r = np.full(len(x), 0.1, np.float32)
+    c = O.soft_contacts_create(shapes, x, r, np.ones(len(x), np.int32), margin=0.85)
+    got = list(zip(c["particle"][:c["n"]].tolist(), c["shape"][:c["n"]].tolist()))
+    assert got == [(0, 0), (1, 0), (2, 0), (3, 0), (4, 1), (5, 1), (6, 1), (7, 1), (8, 2), (9, 2), (10, 2),
+                   (12, 3)]  # particle 11 is 1 from the ellipsoid, beyond margin + radius = 0.95
+    bp, nn = c["body_pos"][:c["n"]], c["normal"][:c["n"]]
+    want_bp = [[0.5, 0, 0.2], [0, 0, 1.5], [0, 0, -1.5], [0, 0, 0.8], [5.5, 0, 0], [5, 0, 1], [5.5, 0, 1.0],
+               [5.2, 0, 1.0], [10, 0, 0.5], [10, 0, -0.5], [10.25, 0, 0], [15, 0.5, 0]]
+    want_n = [[1, 0, 0], [0, 0, 1], [0, 0, -1], [0, 0, 1], [1, 0, 0], [0, 0, 1], [np.sqrt(0.5), 0, np.sqrt(0.5)],
+              [0, 0, 1], [0, 0, 1], [0, 0, -1], [2 * s5, 0, s5], [0, 1, 0]]
+    np.testing.assert_allclose(bp, want_bp, atol=2e-6)
+    np.testing.assert_allclose(nn, want_n, atol=2e-6)
+    c3 = O.soft_contacts_create(shapes[3:], x[11:12], r[11:12], np.ones(1, np.int32), margin=0.95)
+    assert c3["n"] == 1
+    np.testing.assert_allclose(c3["body_pos"][0], [16, 0, 0], atol=2e-6)
+
+
+def _tri_dist2d(p, a, b):
+    """Distance from 2-D point p to the segment a-b."""
+    ab, ap = b - a, p - a
+    t = np.clip(np.dot(ap, ab) / np.dot(ab, ab), 0.0, 1.0)
+    return np.linalg.norm(ap - t * ab)
+
+
+def _round_sdf64(s, q):
+    """fp64 signed distance and outward normal of an axis-aligned capsule,
+    cylinder, cone or ellipsoid at local point q. Capsule, cylinder and cone
+    from their exact distances; the cone's normal and the ellipsoid (whose
+    SDF is the reference's approximation) restate the reference's formulas."""
+    r, hh = float(s["scale"][0]), float(s["scale"][1])
+    rho = np.hypot(q[0], q[1])
+    radial = np.array([q[0] / rho, q[1] / rho, 0.0]) if rho > 1e-8 else np.array([0.0, 0.0, 1.0])
+    axial = np.array([0.0, 0.0, 1.0 if q[2] >= 0 else -1.0])
+    if s["type"] == CAPSULE:
+        v = q - np.array([0.0, 0.0, np.clip(q[2], -hh, hh)])
+        ln = np.linalg.norm(v)
+        return ln - r, v / ln
+    if s["type"] == CYLINDER:
+        dx, dy = rho - r, abs(q[2]) - hh
+        d = min(max(dx, dy), 0.0) + np.hypot(max(dx, 0.0), max(dy, 0.0))
+        if dx > 0 and dy > 0:
+            g = radial * dx + axial * dy
+            return d, g / np.linalg.norm(g)
+        return d, radial if dx > dy else axial
+    if s["type"] == CONE:
+        p2 = np.array([rho, q[2]])
+        base = (np.array([0.0, -hh]), np.array([r, -hh]))
+        side = (np.array([r, -hh]), np.array([0.0, hh]))
+        dist = min(_tri_dist2d(p2, *base), _tri_dist2d(p2, *side))
+        inside = -hh <= q[2] <= hh and rho <= r * (hh - q[2]) / (2 * hh)
+        d = -dist if inside else dist
+        dx, dy = rho - r * (hh - q[2]) / (2 * hh), abs(q[2]) - hh
+        if dx > dy:
+            g = radial + np.array([0.0, 0.0, r / (2 * hh)])
+            return d, g / np.linalg.norm(g)
+        return d, axial
+    rr = np.abs(np.asarray(s["scale"], np.float64))
+    q0, q1 = q / rr, q / rr**2
+    k0, k1 = np.linalg.norm(q0), np.linalg.norm(q1)
+    g = q1 * (k0 / k1)
+    return k0 * (k0 - 1.0) / k1, g / np.linalg.norm(g)
+
+
+def test_round_shapes_against_fp64(oracle_mod):
+    rng = np.random.default_rng(7)
+    shapes = [dict(type=CAPSULE, pos=(0.1, 0.2, -0.1), scale=(0.3, 0.5, 0)),
+              dict(type=CYLINDER, pos=(-0.8, 0.4, 0.2), scale=(0.35, 0.25, 0)),
+              dict(type=CONE, pos=(0.7, -0.6, 0.1), scale=(0.4, 0.45, 0)),
+              dict(type=ELLIPSOID, pos=(-0.5, -0.7, -0.4), scale=(0.5, 0.3, 0.2))]
+    x = (rng.random((6000, 3)) * 3 - 1.5).astype(np.float32)
+    r = (rng.random(6000) * 0.05 + 0.01).astype(np.float32)
+    margin = 0.05
+    c = oracle_mod.soft_contacts_create(shapes, x, r, np.ones(len(x), np.int32), margin=margin)
+    want, near = set(), set()
+    for i in range(len(x)):
+        for k, s in enumerate(shapes):
+            d, _ = _round_sdf64(s, x[i].astype(np.float64) - np.asarray(s["pos"], np.float64))
+            if d < margin + r[i] - 1e-5:
+                want.add((i, k))
+            elif d < margin + r[i] + 1e-5:
+                near.add((i, k))  # within rounding of the threshold: either way
+    got = set(zip(c["particle"][:c["n"]].tolist(), c["shape"][:c["n"]].tolist()))
+    assert want <= got <= want | near
+    assert all(any(k == t for _, k in want) for t in range(4)), "every shape makes contacts"
+    for t in range(c["n"]):
+        i, k = int(c["particle"][t]), int(c["shape"][t])
+        pos = np.asarray(shapes[k]["pos"], np.float64)
+        q = x[i].astype(np.float64) - pos
+        d, n = _round_sdf64(shapes[k], q)
+        np.testing.assert_allclose(c["normal"][t], n, atol=5e-6, err_msg=f"shape {k}")
+        np.testing.assert_allclose(c["body_pos"][t], pos + q - n * d, atol=5e-6, err_msg=f"shape {k}")
+
+
+def test_site_shapes_make_no_contacts(oracle_mod):
+    import newton_sph_dev_b200 as nsph
+
+    b = nsph.ModelBuilder()
+    b.add_particle((0.0, 0.0, 0.05), (0.0, 0.0, 0.0), 1.0, radius=0.1)
+    b.add_shape_capsule(-1, radius=0.2, half_height=0.1, as_site=True)
+    b.add_shape_cone(-1, radius=0.2, half_height=0.1)
+    m = b.finalize("cpu")
+    md = _model_dict(m)
+    assert [s["type"] for s in md["shapes"]] == [CAPSULE, CONE]
+    assert [s["scale"] for s in md["shapes"]] == [(0.2, 0.1, 0.0), (0.2, 0.1, 0.0)]
+    c = oracle_mod.soft_contacts_create(md["shapes"], m.particle_q.numpy(), md["radius"], md["flags"], margin=0.01)
+    assert c["n"] == 1 and c["shape"][0] == 1
 
 
 def test_soft_contacts_against_fp64(oracle_mod):
