@@ -9,14 +9,17 @@ Drop-in for the particle part of NVIDIA Newton's API:
   pressure + XSPH forces, integration),
 - ``solvers.SolverXPBD`` / ``solvers.SolverSemiImplicit`` (their particle
   paths: particle-particle contacts on the grid, particle contacts with
-  static planes, spheres and boxes through ``Model.collide``),
-- ``sensors.SensorRaycast`` (the depth camera's particle raycast on the grid).
+  static planes, spheres, boxes, capsules, cylinders, cones and ellipsoids
+  through ``Model.collide``),
+- ``sensors.SensorRaycast`` (the depth camera's particle raycast on the grid),
+- ``recording`` (state dumps to resume from, trajectory recording, JSONL
+  metrics).
 
 All compute runs in libnsph.so (hand-written CUDA for sm_100a, C ABI in
 include/nsph.h); there is no CPU fallback.
 """
 
-from . import sensors, solvers
+from . import recording, sensors, solvers
 from .geometry import GeoType, ParticleFlags, ShapeFlags
 from .hashgrid import HashGrid
 from .sim import Contacts, Control, Model, ModelBuilder, State
@@ -24,4 +27,4 @@ from .sim import Contacts, Control, Model, ModelBuilder, State
 __version__ = "0.1.0"
 
 __all__ = ["Contacts", "Control", "GeoType", "HashGrid", "Model", "ModelBuilder", "ParticleFlags", "ShapeFlags", "State",
-           "sensors", "solvers"]
+           "recording", "sensors", "solvers"]

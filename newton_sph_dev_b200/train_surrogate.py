@@ -28,6 +28,23 @@ from .solvers import SolverSPH
 from .solvers.sph_surrogate import (SurrogateModel, SurrogateSPH, _lattice_model, generate_training_data, train)
 
 
+def save_training_data(path, features: torch.Tensor, targets: torch.Tensor, info: dict) -> None:
+    """Features (N, 16), targets (N, 3) and the generator's settings as one .npz."""
+    np.savez(path, features=features.detach().cpu().numpy(), targets=targets.detach().cpu().numpy(),
+             info=np.array(json.dumps(info)))
+
+
+def load_training_data(path, device="cuda:0"):
+    """(features, targets, info) of a file written by save_training_data."""
+    with np.load(path, allow_pickle=False) as d:
+        feats = torch.from_numpy(d["features"]).to(device)
+        targs = torch.from_numpy(d["targets"]).to(device)
+        info = json.loads(str(d["info"]))
+    if feats.ndim != 2 or targs.ndim != 2 or feats.shape[0] != targs.shape[0]:
+        raise ValueError(f"{path}: features {tuple(feats.shape)} and targets {tuple(targs.shape)} do not pair up")
+    return feats, targs, info
+
+
 def evaluate(model: SurrogateModel, shape=(32, 32, 32), spacing=0.01, dt=1e-4, substeps=4, macro_steps=50,
              vel_std=0.25, seed=12345, device="cuda:0") -> dict:
     """Surrogate and uncorrected large steps against plain steps on one held-out scene."""
@@ -91,11 +108,20 @@ def main(argv=None):
                          "over more of the flow)")
     ap.add_argument("--eval-steps", type=int, default=50, help="surrogate steps of the held-out rollout")
     ap.add_argument("--device", default="cuda:0")
+    ap.add_argument("--save-data", default=None, help="write the generated features and targets to this .npz")
+    ap.add_argument("--load-data", default=None, help="train on the features and targets of this .npz instead of "
+                                                       "generating them")
     args = ap.parse_args(argv)
     t0 = time.time()
-    feats, targs, info = generate_training_data(trajectories=args.trajectories, samples_per_trajectory=args.samples,
-                                                keep_fraction=args.keep, seed=args.seed, device=args.device,
-                                                substeps=args.substeps, stride=args.stride)
+    if args.load_data:
+        feats, targs, info = load_training_data(args.load_data, args.device)
+    else:
+        feats, targs, info = generate_training_data(trajectories=args.trajectories,
+                                                    samples_per_trajectory=args.samples, keep_fraction=args.keep,
+                                                    seed=args.seed, device=args.device, substeps=args.substeps,
+                                                    stride=args.stride)
+    if args.save_data:
+        save_training_data(args.save_data, feats, targs, info)
     t_data = time.time() - t0
     model = SurrogateModel(args.device, seed=args.seed)
     t0 = time.time()
