@@ -147,7 +147,11 @@ __device__ __forceinline__ void density_finish(int k, float m, float rho, const 
 // those of the fp32 oracle.
 constexpr int kNbrSlots = 64;
 constexpr int kNbrGroups = kNbrSlots / 4;
+// entries every sorted-position array that neighbor_list reads holds past
+// its last particle (the candidate groups' reads past a run's end)
+constexpr int kXsPad = 4;
 
+template <bool kPaddedGroups>
 __device__ __forceinline__ int neighbor_list(const GridDev& g, const float4* __restrict__ xs,
                                              const nsph_sph_params& p, float4 xi, int4* __restrict__ nbr, int n,
                                              int k)
@@ -166,24 +170,45 @@ __device__ __forceinline__ int neighbor_list(const GridDev& g, const float4* __r
     // of a run; the hits are appended after the chunk, so the append code runs
     // once per neighbour (a warp iterates over its lanes' largest hit count of
     // the chunk) instead of at every candidate where any lane has a hit.
+    // Candidates go in groups of four (four loads issued together). With
+    // kPaddedGroups there is no scalar tail loop: a run's last group reads
+    // up to three entries past the run, whose bits are then cleared. Those
+    // reads stay inside the array: every xs array the density passes read
+    // holds at least kXsPad entries past its last particle. (Padded groups
+    // took the 1M tank's density pass from 0.330 to 0.315 ms but the batched
+    // worlds' from 5.18 to 5.39 ms, so the worlds pass keeps the tail loop.)
     for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
         for (int c0 = lo; c0 < hi; c0 += 32) {
             const int m = min(32, hi - c0);
             unsigned bits = 0u;
-            int j = 0;
-            for (; j + 4 <= m; j += 4) {
-                float4 xj[4];
+            if constexpr (kPaddedGroups) {
+                for (int j = 0; j < m; j += 4) {
+                    float4 xj[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) xj[u] = __ldg(xs + c0 + j + u);
+                    for (int u = 0; u < 4; ++u) xj[u] = __ldg(xs + c0 + j + u);
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    float dx, dy, dz;
-                    bits |= (unsigned)(dist2(xi, xj[u], dx, dy, dz) < p.h2) << (j + u);
+                    for (int u = 0; u < 4; ++u) {
+                        float dx, dy, dz;
+                        bits |= (unsigned)(dist2(xi, xj[u], dx, dy, dz) < p.h2) << (j + u);
+                    }
                 }
-            }
-            for (; j < m; ++j) {
-                float dx, dy, dz;
-                bits |= (unsigned)(dist2(xi, __ldg(xs + c0 + j), dx, dy, dz) < p.h2) << j;
+                if (m < 32) bits &= (1u << m) - 1u;
+            } else {
+                int j = 0;
+                for (; j + 4 <= m; j += 4) {
+                    float4 xj[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) xj[u] = __ldg(xs + c0 + j + u);
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        float dx, dy, dz;
+                        bits |= (unsigned)(dist2(xi, xj[u], dx, dy, dz) < p.h2) << (j + u);
+                    }
+                }
+                for (; j < m; ++j) {
+                    float dx, dy, dz;
+                    bits |= (unsigned)(dist2(xi, __ldg(xs + c0 + j), dx, dy, dz) < p.h2) << j;
+                }
             }
             while (bits) {
                 append(c0 + __ffs(bits) - 1);
@@ -406,7 +431,7 @@ __global__ void __launch_bounds__(kSphThreads, 5) k_density_list(GridDev g, cons
             ncnt[k] = 0;
             continue;
         }
-        const int cnt = neighbor_list(g, xs, p, xi, nbr, n, k);
+        const int cnt = neighbor_list<true>(g, xs, p, xi, nbr, n, k);
         ncnt[k] = cnt;
         const float rho = density_from_list<Fast>(g, xs, p, xi, nbr, cnt, n, k);
         density_finish<Fast>(k, xi.w, rho, p, aux, rp, status);
@@ -527,7 +552,7 @@ __global__ void __launch_bounds__(kSphThreads, 4) k_density_worlds(const WorldCe
         const int w = attr >> kAttrGravShift;
         const nsph_sph_params p = wp[w];  // a copy: its fields stay in registers across the candidate loop
         const GridDev g = world_grid(wc[w], ranges, ids, n);
-        const int cnt = neighbor_list(g, xs, p, xi, nbr, n, k);
+        const int cnt = neighbor_list<false>(g, xs, p, xi, nbr, n, k);
         ncnt[k] = cnt;
         const float rho = density_from_list<false>(g, xs, p, xi, nbr, cnt, n, k);
         density_finish(k, xi.w, rho, p, aux, rp, status);
@@ -1517,7 +1542,8 @@ static int sph_create_common(nsph_sph* s, int device, int capacity)
     if (st == NSPH_OK) {
         DeviceGuard guard(device);
         const size_t c = (size_t)(capacity > 0 ? capacity : 1);
-        cudaError_t e = cudaMalloc(&s->xs, sizeof(float4) * c);
+        cudaError_t e = cudaMalloc(&s->xs, sizeof(float4) * (c + kXsPad));
+        if (e == cudaSuccess) e = cudaMemset(s->xs + c, 0, sizeof(float4) * kXsPad);
         if (e == cudaSuccess) e = cudaMalloc(&s->vs, sizeof(float4) * c);
         if (e == cudaSuccess) e = cudaMalloc(&s->aux, sizeof(float2) * c);
         if (e == cudaSuccess) e = cudaMalloc(&s->rp, sizeof(float2) * c);
