@@ -712,6 +712,12 @@ def run_gpu(args):
     eager_ms = max_over_ranks(pipelined_e2e(model, lambda a, b: solver.step(a, b, None, None, dt), hx, hv,
                                             e2e_steps, device), device)
     e2e_eager = n_job * e2e_steps / (eager_ms * 1e-3)
+    # the same uploads and downloads with no step between them: the host
+    # link's bound on (a)
+    barrier(device)
+    torch.cuda.synchronize()
+    copy_ms = max_over_ranks(pipelined_e2e(model, lambda a, b: None, hx, hv, e2e_steps, device), device)
+    e2e_copy_bound = n_job * e2e_steps / (copy_ms * 1e-3)
     # (b) serial host round trip: upload, step, download, and the next step
     # starts from the downloaded state
     serial_ms = 0.0
@@ -847,6 +853,9 @@ def run_gpu(args):
                            "state (the timed run's last state), uploads and downloads overlapping other steps' "
                            "compute on separate streams (double-buffered device states)",
                     "eager": {"value": e2e_eager, "how": "the same with eager SolverSPH.step calls"},
+                    "copy_bound": {"value": e2e_copy_bound,
+                                   "how": "the same uploads and downloads with no step between them (the host "
+                                          "link's bound on the pipelined figure)"},
                     "serial_round_trip": {"value": e2e_serial, "how": "upload, eager step, download, next step "
                                                                       "from the downloaded state, no overlap"}},
             "gpu_launches": launches_per_step * args.steps,
