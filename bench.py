@@ -1313,13 +1313,18 @@ def run_surrogate(args):
     # from the relaxed state with the fallback rule reset
     e2e_steps = min(args.steps, 50)
     hx, hv = start_q.cpu().pin_memory(), start_qd.cpu().pin_memory()
-    stepper = SurrogateSPH(solver, net, substeps=sub, threshold=sw["threshold"], window=sw["window"], graphs=True)
+    # a solver as a user makes it: the same launch shape, no phase-timing events
+    user_solver = SolverSPH(model, cfg)
+    user_solver.set_launch(*solver.launch)
+    stepper = SurrogateSPH(user_solver, net, substeps=sub, threshold=sw["threshold"], window=sw["window"],
+                           graphs=True)
     stepper.monitor = FallbackMonitor(sw["threshold"])
     e2e_ms = pipelined_e2e(model, lambda a, b: stepper.step(a, b, dt), hx, hv, e2e_steps, device)
     e2e_ms = max_over_ranks(e2e_ms, device)
     e2e_value = world * n * sub * e2e_steps / (e2e_ms * 1e-3)
     e2e_fallbacks = stepper.fallback_calls
     stepper._graphs.clear()
+    del stepper, user_solver
 
     peak, peak_kind = load_peak()
     tpeak, tpeak_kind = load_tensor_peak()
