@@ -482,14 +482,17 @@ def graph_replayed(step):
     return run
 
 
-def pipelined_e2e(model, step, hx, hv, steps: int, device, outputs=None, nbuf: int = 2) -> float:
+def pipelined_e2e(model, step, hx, hv, steps: int, device, outputs=None, nbuf: int = 2, copies: bool = True) -> float:
     """Milliseconds for `steps` end-to-end steps through the public API:
     upload (x, v) from the pinned host tensors hx, hv, step(state_in,
     state_out), download outputs(state_out) (default: x, v) into pinned host
     tensors. Three streams (upload, compute, download) and `nbuf` device
     state pairs let the uploads of the next steps and the downloads of the
     previous ones run while a step computes; events order every reuse of a
-    buffer. Timed with CUDA events from a common start to the last download."""
+    buffer. Timed with CUDA events from a common start to the last download.
+    With copies=False the uploads and downloads are left out (the inputs are
+    uploaded once, before the timing): the compute-only bound of the same
+    schedule."""
     import torch
 
     if outputs is None:
@@ -514,8 +517,9 @@ def pipelined_e2e(model, step, hx, hv, steps: int, device, outputs=None, nbuf: i
         with torch.cuda.stream(s_in):
             if k >= nbuf:
                 s_in.wait_event(done[b])  # step k - nbuf no longer reads ins[b]
-            ins[b].particle_q.copy_(hx, non_blocking=True)
-            ins[b].particle_qd.copy_(hv, non_blocking=True)
+            if copies or k < nbuf:
+                ins[b].particle_q.copy_(hx, non_blocking=True)
+                ins[b].particle_qd.copy_(hv, non_blocking=True)
             up[b].record(s_in)
         with torch.cuda.stream(s_c):
             s_c.wait_event(up[b])
@@ -525,8 +529,9 @@ def pipelined_e2e(model, step, hx, hv, steps: int, device, outputs=None, nbuf: i
             done[b].record(s_c)
         with torch.cuda.stream(s_out):
             s_out.wait_event(done[b])
-            for h, t in zip(host_out[b], outputs(outs[b])):
-                h.copy_(t, non_blocking=True)
+            if copies:
+                for h, t in zip(host_out[b], outputs(outs[b])):
+                    h.copy_(t, non_blocking=True)
             down[b].record(s_out)
     end.record(s_out)
     end.synchronize()
@@ -707,10 +712,16 @@ def run_gpu(args):
     # first use of each buffer pair, in the untimed warm-up round, captures)
     gstep = graph_replayed(lambda a, b: user_solver.step(a, b, None, None, dt))
     e2e_ms = pipelined_e2e(model, gstep, hx, hv, e2e_steps, device)
-    gstep.graphs.clear()
     barrier(device)
     e2e_ms_max = max_over_ranks(e2e_ms, device)
     e2e_value = n_job * e2e_steps / (e2e_ms_max * 1e-3)
+    # the same schedule and graphs with no uploads or downloads: the compute's
+    # bound on (a) (no L2 flush between these steps, unlike the timed run)
+    barrier(device)
+    torch.cuda.synchronize()
+    step_ms = max_over_ranks(pipelined_e2e(model, gstep, hx, hv, e2e_steps, device, copies=False), device)
+    e2e_step_bound = n_job * e2e_steps / (step_ms * 1e-3)
+    gstep.graphs.clear()
     # the same with eager SolverSPH.step calls
     barrier(device)
     torch.cuda.synchronize()
@@ -863,6 +874,10 @@ def run_gpu(args):
                     "copy_bound": {"value": e2e_copy_bound,
                                    "how": "the same uploads and downloads with no step between them (the host "
                                           "link's bound on the pipelined figure)"},
+                    "step_bound": {"value": e2e_step_bound,
+                                   "how": "the same graph-replayed steps with no uploads or downloads (the "
+                                          "compute's bound on the pipelined figure; unlike the timed run, no L2 "
+                                          "flush between steps and no phase-timing events)"},
                     "serial_round_trip": {"value": e2e_serial, "how": "upload, eager step, download, next step "
                                                                       "from the downloaded state, no overlap"}},
             "gpu_launches": launches_per_step * args.steps,

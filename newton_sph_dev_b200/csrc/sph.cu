@@ -151,6 +151,19 @@ constexpr int kNbrGroups = kNbrSlots / 4;
 // its last particle (the candidate groups' reads past a run's end)
 constexpr int kXsPad = 4;
 
+// One candidate's hit bit pushed into `acc` from the right: the sign bit of
+// fl(r2 - h2), by one funnel shift. fl(r2 - h2) is negative exactly when
+// r2 < h2: an IEEE subtraction of two unequal values is never zero and its
+// rounding keeps the sign, and r2 == h2 gives +0. A NaN difference (from a
+// non-finite position) is the GPU's canonical NaN, whose sign bit is clear,
+// as r2 < h2 is false for it. So the bits are those of the comparison, at
+// one FADD and one shift per candidate instead of a compare, a select, a
+// variable shift and an OR.
+__device__ __forceinline__ unsigned push_hit(unsigned acc, float r2, float h2)
+{
+    return __funnelshift_l(__float_as_uint(__fsub_rn(r2, h2)), acc, 1);
+}
+
 template <bool kPaddedGroups>
 __device__ __forceinline__ int neighbor_list(const GridDev& g, const float4* __restrict__ xs,
                                              const nsph_sph_params& p, float4 xi, int4* __restrict__ nbr, int n,
@@ -180,8 +193,10 @@ __device__ __forceinline__ int neighbor_list(const GridDev& g, const float4* __r
     for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
         for (int c0 = lo; c0 < hi; c0 += 32) {
             const int m = min(32, hi - c0);
-            unsigned bits = 0u;
+            unsigned bits;
             if constexpr (kPaddedGroups) {
+                unsigned acc = 0u;  // candidate t of the chunk at bit mp - 1 - t
+#pragma unroll 1
                 for (int j = 0; j < m; j += 4) {
                     float4 xj[4];
 #pragma unroll
@@ -189,11 +204,16 @@ __device__ __forceinline__ int neighbor_list(const GridDev& g, const float4* __r
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         float dx, dy, dz;
-                        bits |= (unsigned)(dist2(xi, xj[u], dx, dy, dz) < p.h2) << (j + u);
+                        acc = push_hit(acc, dist2(xi, xj[u], dx, dy, dz), p.h2);
                     }
                 }
+                // reversed, candidate t sits at bit t; the group's reads past
+                // the run (bits m .. mp - 1) are cleared
+                const int mp = (m + 3) & ~3;
+                bits = __brev(acc) >> (32 - mp);
                 if (m < 32) bits &= (1u << m) - 1u;
             } else {
+                bits = 0u;
                 int j = 0;
                 for (; j + 4 <= m; j += 4) {
                     float4 xj[4];
