@@ -277,6 +277,39 @@ struct NbrReader {
     }
 };
 
+// Element u (0..3, a constant after unrolling) of a list group.
+__device__ __forceinline__ int group_item(const int4& gr, int u)
+{
+    return u == 0 ? gr.x : (u == 1 ? gr.y : (u == 2 ? gr.z : gr.w));
+}
+
+// Walk of a particle's list by whole groups: visit(j) for its neighbours in
+// order. The group after the current one is loaded when the current one
+// starts, as NbrReader does; the four items of a group are unrolled, so each
+// index is a fixed register (no per-item select) and the visits' loads can
+// issue together. kReadOnly as for NbrReader.
+template <bool kReadOnly, class F>
+__device__ __forceinline__ void for_each_listed(const int4* __restrict__ nbr, int n, int k, int cnt, F&& visit)
+{
+    in_bounds(cnt >= 0 && cnt <= kNbrSlots);
+    const int4* a = nbr + k;
+    auto load = [&](int gi) { return kReadOnly ? __ldg(a + (size_t)gi * n) : a[(size_t)gi * n]; };
+    int4 cur = cnt > 0 ? load(0) : make_int4(0, 0, 0, 0);
+    int4 nxt = cnt > 4 ? load(1) : make_int4(0, 0, 0, 0);
+    for (int t = 0; t < cnt; t += 4) {
+        const int4 gr = cur;
+        cur = nxt;
+        if (t + 8 < cnt) nxt = load((t >> 2) + 2);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            if (t + u < cnt) {
+                const int j = group_item(gr, u);
+                visit(in_bounds(j >= 0 && j < n) ? j : 0);
+            }
+        }
+    }
+}
+
 // rho of particle k from its list (read back by the thread that wrote it,
 // with plain loads), or by re-testing its candidates when the list overflowed
 template <bool Fast>
@@ -287,12 +320,11 @@ __device__ __forceinline__ float density_from_list(const GridDev& g, const float
     float rho = 0.f;
     auto w = [&](float r2) { return Fast ? wterm_fast(r2, p) : wterm(r2, p); };
     if (cnt <= kNbrSlots) {
-        NbrReader<false> rd(nbr, n, k, cnt);
-        for (int t = 0; t < cnt; ++t) {
-            const float4 xj = __ldg(xs + rd.get(t));
+        for_each_listed<false>(nbr, n, k, cnt, [&](int j) {
+            const float4 xj = __ldg(xs + j);
             float dx, dy, dz;
             rho = __fmaf_rn(xj.w, w(dist2(xi, xj, dx, dy, dz)), rho);
-        }
+        });
     } else {
         for_each_candidate(g, xi.x, xi.y, xi.z, p.h, [&](int j) {
             const float4 xj = __ldg(xs + j);
@@ -471,10 +503,8 @@ __device__ __forceinline__ void force_from_list(const GridDev& g, const float4* 
         bool have = false;
         float4 pxj = make_float4(0.f, 0.f, 0.f, 0.f), pvj = pxj;
         float2 paj = make_float2(0.f, 0.f);
-        NbrReader<true> rd(nbr, n, k, cnt);
-        for (int t = 0; t < cnt; ++t) {
-            const int j = rd.get(t);
-            if (j == k) continue;
+        for_each_listed<true>(nbr, n, k, cnt, [&](int j) {
+            if (j == k) return;
             const float4 nxj = __ldg(xs + j);
             const float4 nvj = __ldg(vs + j);
             const float2 naj = __ldg(aux + j);
@@ -488,7 +518,7 @@ __device__ __forceinline__ void force_from_list(const GridDev& g, const float4* 
             pvj = nvj;
             paj = naj;
             have = true;
-        }
+        });
         if (have) {
             if (Fast)
                 force_term_fast(pxj, pvj, paj, xi, vi, pr2_i, p, acc);
