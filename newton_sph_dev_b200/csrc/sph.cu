@@ -243,40 +243,6 @@ __device__ __forceinline__ int neighbor_list(const GridDev& g, const float4* __r
     return cnt;
 }
 
-// Sequential reader of a particle's list: get(t) for t = 0, 1, ... in order.
-// The group after the current one is loaded when the current one starts.
-// kReadOnly: the list was written by an earlier kernel (read-only path);
-// otherwise it is read back by the thread that wrote it (plain loads).
-template <bool kReadOnly>
-struct NbrReader {
-    const int4* base;
-    size_t stride;
-    int cnt;
-    int4 cur, nxt;
-    __device__ __forceinline__ int4 load(int g) const
-    {
-        const int4* a = base + (size_t)g * stride;
-        return kReadOnly ? __ldg(a) : *a;
-    }
-    __device__ __forceinline__ NbrReader(const int4* nbr, int n, int k, int count)
-        : base(nbr + k), stride((size_t)n), cnt(count)
-    {
-        in_bounds(count >= 0 && count <= kNbrSlots);
-        cur = count > 0 ? load(0) : make_int4(0, 0, 0, 0);
-        nxt = count > 4 ? load(1) : make_int4(0, 0, 0, 0);
-    }
-    __device__ __forceinline__ int get(int t)
-    {
-        const int u = t & 3;
-        if (u == 0 && t > 0) {
-            cur = nxt;
-            if (t + 4 < cnt) nxt = load((t >> 2) + 1);
-        }
-        const int j = u == 0 ? cur.x : (u == 1 ? cur.y : (u == 2 ? cur.z : cur.w));
-        return in_bounds(j >= 0 && (size_t)j < stride) ? j : 0;
-    }
-};
-
 // Element u (0..3, a constant after unrolling) of a list group.
 __device__ __forceinline__ int group_item(const int4& gr, int u)
 {
@@ -285,10 +251,15 @@ __device__ __forceinline__ int group_item(const int4& gr, int u)
 
 // Walk of a particle's list by whole groups: visit(j) for its neighbours in
 // order. The group after the current one is loaded when the current one
-// starts, as NbrReader does; the four items of a group are unrolled, so each
-// index is a fixed register (no per-item select) and the visits' loads can
-// issue together. kReadOnly as for NbrReader.
-template <bool kReadOnly, class F>
+// starts; the four items of a group are unrolled, so each index is a fixed
+// register (no per-item select, as a reader returning one item at a time
+// needs) and the visits' loads can issue together. kReadOnly: the list was
+// written by an earlier kernel (read-only path); otherwise it is read back by
+// the thread that wrote it (plain loads). kUnrolled = false keeps a rolled
+// loop over a group's items (one item per iteration, selected at run time):
+// the batched worlds' force pass spills more when unrolled (2.16 -> 2.38 ms
+// on worlds_4096).
+template <bool kReadOnly, bool kUnrolled = true, class F>
 __device__ __forceinline__ void for_each_listed(const int4* __restrict__ nbr, int n, int k, int cnt, F&& visit)
 {
     in_bounds(cnt >= 0 && cnt <= kNbrSlots);
@@ -300,12 +271,18 @@ __device__ __forceinline__ void for_each_listed(const int4* __restrict__ nbr, in
         const int4 gr = cur;
         cur = nxt;
         if (t + 8 < cnt) nxt = load((t >> 2) + 2);
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
+        auto item = [&](int u) {
             if (t + u < cnt) {
                 const int j = group_item(gr, u);
                 visit(in_bounds(j >= 0 && j < n) ? j : 0);
             }
+        };
+        if constexpr (kUnrolled) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) item(u);
+        } else {
+#pragma unroll 1
+            for (int u = 0; u < 4; ++u) item(u);
         }
     }
 }
@@ -493,7 +470,7 @@ __global__ void __launch_bounds__(kSphThreads, 5) k_density_list(GridDev g, cons
 // pressure and XSPH sums of particle k over its list, in order (loads of
 // neighbour t+1 issued before the terms of neighbour t), or by re-testing
 // its candidates when the list overflowed
-template <bool Fast>
+template <bool Fast, bool kUnrolledWalk = true>
 __device__ __forceinline__ void force_from_list(const GridDev& g, const float4* __restrict__ xs,
                                                 const float4* __restrict__ vs, const float2* __restrict__ aux,
                                                 const int4* __restrict__ nbr, int cnt, int n, int k, float4 xi,
@@ -503,7 +480,7 @@ __device__ __forceinline__ void force_from_list(const GridDev& g, const float4* 
         bool have = false;
         float4 pxj = make_float4(0.f, 0.f, 0.f, 0.f), pvj = pxj;
         float2 paj = make_float2(0.f, 0.f);
-        for_each_listed<true>(nbr, n, k, cnt, [&](int j) {
+        for_each_listed<true, kUnrolledWalk>(nbr, n, k, cnt, [&](int j) {
             if (j == k) return;
             const float4 nxj = __ldg(xs + j);
             const float4 nvj = __ldg(vs + j);
@@ -629,7 +606,7 @@ __global__ void __launch_bounds__(kSphThreads, 4) k_force_worlds(const WorldCell
         const nsph_sph_params& p = wp[w];
         const GridDev g = world_grid(wc[w], ranges, ids, n);
         ForceAcc acc{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        if (attr & kAttrActive) force_from_list<false>(g, xs, vs, aux, nbr, ncnt[k], n, k, xi, vi, aux[k].y, p, acc);
+        if (attr & kAttrActive) force_from_list<false, false>(g, xs, vs, aux, nbr, ncnt[k], n, k, xi, vi, aux[k].y, p, acc);
         integrate_out((size_t)ids[k], xi, vi, attr, rp[k], acc, p, dt, o);
     }
 }
@@ -730,11 +707,9 @@ __device__ __forceinline__ void for_each_neighbor(const GridDev& g, const float4
                                                   const nsph_sph_params& p, V&& visit)
 {
     if (cnt <= kNbrSlots) {
-        NbrReader<true> rd(nbr, n, k, cnt);
-        for (int t = 0; t < cnt; ++t) {
-            const int j = rd.get(t);
+        for_each_listed<true>(nbr, n, k, cnt, [&](int j) {
             if (j != k) visit(j);
-        }
+        });
     } else {
         for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
             for (int j = lo; j < hi; ++j) {
@@ -1055,10 +1030,8 @@ __device__ __forceinline__ void force_features_from_list(const GridDev& g, const
         bool have = false;
         float4 pxj = make_float4(0.f, 0.f, 0.f, 0.f), pvj = pxj;
         float2 paj = make_float2(0.f, 0.f);
-        NbrReader<true> rd(nbr, n, k, cnt);
-        for (int t = 0; t < cnt; ++t) {
-            const int j = rd.get(t);
-            if (j == k) continue;
+        for_each_listed<true>(nbr, n, k, cnt, [&](int j) {
+            if (j == k) return;
             const float4 nxj = __ldg(xs + j);
             const float4 nvj = __ldg(vs + j);
             const float2 naj = __ldg(aux + j);
@@ -1067,7 +1040,7 @@ __device__ __forceinline__ void force_features_from_list(const GridDev& g, const
             pvj = nvj;
             paj = naj;
             have = true;
-        }
+        });
         if (have) force_feature_term(pxj, pvj, paj, xi, vi, pr2_i, p, acc, fa);
     } else {
         for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
