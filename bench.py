@@ -482,14 +482,18 @@ def graph_replayed(step):
     return run
 
 
-def pipelined_e2e(model, step, hx, hv, steps: int, device, outputs=None, nbuf: int = 2, copies: bool = True) -> float:
+def pipelined_e2e(model, step, hx, hv, steps: int, device, outputs=None, nbuf: int = 3, copies: bool = True) -> float:
     """Milliseconds for `steps` end-to-end steps through the public API:
     upload (x, v) from the pinned host tensors hx, hv, step(state_in,
     state_out), download outputs(state_out) (default: x, v) into pinned host
     tensors. Three streams (upload, compute, download) and `nbuf` device
     state pairs let the uploads of the next steps and the downloads of the
     previous ones run while a step computes; events order every reuse of a
-    buffer. Timed with CUDA events from a common start to the last download.
+    buffer. Three pairs: with two, a step k waits for the download of step
+    k - 2, and when a step and a copy take about as long (about 0.52 ms each
+    on tank_1m) the graph-replayed pipeline fell to 1.70-1.82e9 against
+    1.96e9 with three or four pairs (same box, both bounds at 2.0e9).
+    Timed with CUDA events from a common start to the last download.
     With copies=False the uploads and downloads are left out (the inputs are
     uploaded once, before the timing): the compute-only bound of the same
     schedule."""
@@ -868,7 +872,7 @@ def run_gpu(args):
                     "how": "each step uploads x, v from pinned host memory, runs SolverSPH.step (captured with "
                            "torch.cuda.graph, replayed) and downloads x, v; independent steps from the same host "
                            "state (the timed run's last state), uploads and downloads overlapping other steps' "
-                           "compute on separate streams (double-buffered device states); a second SolverSPH on the "
+                           "compute on separate streams (three device state pairs); a second SolverSPH on the "
                            "same model with the timed run's launch shape and no phase-timing events",
                     "eager": {"value": e2e_eager, "how": "the same with eager SolverSPH.step calls"},
                     "copy_bound": {"value": e2e_copy_bound,
