@@ -190,6 +190,8 @@ __device__ __forceinline__ int neighbor_list(const GridDev& g, const float4* __r
     // holds at least kXsPad entries past its last particle. (Padded groups
     // took the 1M tank's density pass from 0.330 to 0.315 ms but the batched
     // worlds' from 5.18 to 5.39 ms, so the worlds pass keeps the tail loop.)
+    // The padded path takes each hit bit from push_hit (0.318 -> 0.303 ms on
+    // the 1M tank); the worlds pass keeps the comparison, which spilled less.
     for_each_run(g, xi.x, xi.y, xi.z, p.h, [&](int lo, int hi) {
         for (int c0 = lo; c0 < hi; c0 += 32) {
             const int m = min(32, hi - c0);
